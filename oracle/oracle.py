@@ -1,0 +1,165 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Loaded by the test-suite, the smoke check and the CPU-baseline leg of the
+benchmark to check or time the CUDA operator; nothing in the product imports
+it.  Vectors are numpy float64 arrays of shape (C, N) in the lexicographic
+SoA layout described in sint_oracle.cpp.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libsint_oracle.so")
+
+_c_int, _c_double, _c_void = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+
+
+class Mesh(ctypes.Structure):
+    _fields_ = [("dim", _c_int), ("n", _c_int * 3), ("h", _c_double * 3)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("n_grains", _c_int), ("A", _c_double), ("B", _c_double),
+                ("kappa_c", _c_double), ("kappa_p", _c_double),
+                ("Mvol", _c_double), ("Mvap", _c_double), ("Msurf", _c_double),
+                ("Mgb", _c_double), ("L", _c_double), ("tensorial", _c_int)]
+
+
+class Time(ctypes.Structure):
+    _fields_ = [("w0", _c_double), ("w_alg", _c_double), ("order", _c_int),
+                ("w_hist", _c_double * 4)]
+
+
+_lib = None
+
+
+def build():
+    """Compile the oracle library with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        L.oracle_free_energy.argtypes = [_c_double, _c_double, P(_c_double), _c_int, P(_c_double)]
+        L.oracle_power_sum.argtypes = [P(_c_double), _c_int, _c_int]
+        L.oracle_power_sum.restype = _c_double
+        L.oracle_residual.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(P(_c_double)),
+                                      _c_int, P(_c_double), _c_int]
+        L.oracle_jvp.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double),
+                                 P(_c_double), _c_int]
+        L.oracle_ac_diagonal.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double), _c_int]
+        L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double), _c_int]
+        _lib = L
+    return _lib
+
+
+def _dptr(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(_c_double))
+
+
+def make_mesh(dim, cells, h=(1.0, 1.0, 1.0)):
+    m = Mesh()
+    m.dim = dim
+    for d in range(3):
+        m.n[d] = int(cells[d]) if d < dim else 0
+        m.h[d] = float(h[d]) if d < dim else 1.0
+    return m
+
+
+def make_params(n_grains, A=16.0, B=1.0, kappa_c=1.0, kappa_p=0.5, Mvol=1e-2, Mvap=1e-10,
+                Msurf=4.0, Mgb=0.4, L=1.0, tensorial=True):
+    return Params(n_grains, A, B, kappa_c, kappa_p, Mvol, Mvap, Msurf, Mgb, L, int(bool(tensorial)))
+
+
+def make_time(w0, w_alg=1.0, w_hist=()):
+    t = Time()
+    t.w0, t.w_alg, t.order = float(w0), float(w_alg), len(w_hist)
+    for i, w in enumerate(w_hist):
+        t.w_hist[i] = float(w)
+    return t
+
+
+def n_nodes(mesh):
+    n = 1
+    for d in range(mesh.dim):
+        n *= mesh.n[d] + 1
+    return n
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"oracle {what} failed with status {rc}")
+
+
+def free_energy(A, B, state, G):
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    out = np.zeros(2 + 3 * G + G * G + 1)
+    _check(lib().oracle_free_energy(A, B, _dptr(st), G, _dptr(out)), "free_energy")
+    k = 0
+    res = {"f": out[0], "df_dc": out[1]}
+    k = 2
+    res["df_detai"] = out[k:k + G].copy(); k += G
+    res["d2f_dc2"] = out[k]; k += 1
+    res["d2f_dcdetai"] = out[k:k + G].copy(); k += G
+    res["d2f_detai2"] = out[k:k + G].copy(); k += G
+    res["d2f_detaidetaj"] = out[k:k + G * G].reshape(G, G).copy()
+    return res
+
+
+def power_sum(x, p):
+    xs = np.ascontiguousarray(x, dtype=np.float64)
+    return lib().oracle_power_sum(_dptr(xs), len(xs), p)
+
+
+def residual(mesh, params, time, u, hist=(), with_td=2, threads=0):
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(C, N)
+    hs = [np.ascontiguousarray(h, dtype=np.float64).reshape(C, N) for h in hist]
+    arr = (ctypes.POINTER(_c_double) * max(1, len(hs)))(*[_dptr(h) for h in hs])
+    dst = np.zeros((C, N))
+    _check(lib().oracle_residual(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(u),
+                                 arr, with_td, _dptr(dst), threads or os.cpu_count()), "residual")
+    return dst
+
+
+def jvp(mesh, params, time, lin, src, threads=0):
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
+    src = np.ascontiguousarray(src, dtype=np.float64).reshape(C, N)
+    dst = np.zeros((C, N))
+    _check(lib().oracle_jvp(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin), _dptr(src),
+                            _dptr(dst), threads or os.cpu_count()), "jvp")
+    return dst
+
+
+def ac_diagonal(mesh, params, time, lin, threads=0):
+    C, N, G = params.n_grains + 2, n_nodes(mesh), params.n_grains
+    lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
+    d = np.zeros((G, N))
+    _check(lib().oracle_ac_diagonal(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
+                                    _dptr(d), threads or os.cpu_count()), "ac_diagonal")
+    return d
+
+
+def ch_blocks(mesh, params, time, lin, threads=0):
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
+    b = np.zeros((4, N))
+    _check(lib().oracle_ch_blocks(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
+                                  _dptr(b), threads or os.cpu_count()), "ch_blocks")
+    return b
+
+
+def inverse_diagonal(d):
+    """operator_base.h:386-388: 1/d where |d| > 1e-10, else 1."""
+    d = np.asarray(d, dtype=np.float64)
+    return np.where(np.abs(d) > 1.0e-10, 1.0 / np.where(d == 0, 1.0, d), 1.0)

@@ -1,0 +1,127 @@
+"""Extract hpsint's golden test vectors for the sintering operator into JSON.
+
+Run once in a checkout that has the reference sources (default location
+/root/reference, or pass the path as the first argument); the JSON fixtures
+it writes next to this script are committed, so nothing at test time reads
+the reference tree.
+
+Sources (paths inside the hpsint project):
+  tests/residual_generic_{scalar,tensorial}_no_rbm.mpirun=1.output
+      residual blocks of the 2x1-cell debug state, 4 significant digits
+  tests/include/pf-applications/tests/sintering_model.h:53-239
+      the model those residuals come from (parameters are re-typed below
+      from lines 64-72 and 78-98 and cited, not parsed)
+  applications/sintering/include/pf-applications/sintering/initial_values_debug.h:39-65
+      nodal state of the 2D debug case
+  tests/free_energy_sintering.{cc,output}
+      known-answer values of the Wang free energy and its derivatives
+  tests/power_sum.{cc,output}
+      power sums
+  tests/tangent_generic_{scalar,tensorial}.cc + .mpirun=1.output
+      tolerances of the analytic-vs-finite-difference tangent check
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def parse_residual(path):
+    blocks = []
+    lines = open(path).read().splitlines()
+    for i, line in enumerate(lines):
+        if line.startswith("Vector data:"):
+            blocks.append([float(x) for x in lines[i + 1].split()])
+    return blocks
+
+
+def parse_free_energy(path):
+    out = {}
+    for line in open(path).read().splitlines():
+        if not line.strip():
+            break  # first section only; the other four repeat it
+        m = re.match(r"^(\w+) = (\S+)$", line)
+        if m:
+            out[m.group(1)] = float(m.group(2))
+    return out
+
+
+def parse_power_sum(path):
+    txt = open(path).read().splitlines()
+    res = {"generalized": {}, "optimized": {}}
+    section = None
+    for line in txt:
+        if line.startswith("Generalized"):
+            section = "generalized"
+        elif line.startswith("Optimized"):
+            section = "optimized"
+        elif line.startswith("std::array"):
+            res[section]["input"] = [float(x) for x in line.split("=")[1].split()]
+            res[section].setdefault("sums", {})
+        m = re.match(r"^p=(\d+): (\S+)$", line)
+        if m and "sums" in res[section]:
+            res[section]["sums"].setdefault(m.group(1), float(m.group(2)))
+    return res
+
+
+def main(ref):
+    t = os.path.join(ref, "tests")
+    golden = {
+        "source": "hpsint tests (see make_golden.py for file list)",
+        # sintering_model.h:64-72 and :78-98
+        "model": {
+            "dim": 2,
+            "cells": [2, 1],
+            "h": [1.0, 1.0],
+            "A": 1.0, "B": 1.0, "kappa_c": 0.1, "kappa_p": 0.1,
+            "Mvol": 1e-1, "Mvap": 1e-8, "Msurf": 1e1, "Mgb": 1e0, "L": 1e1,
+            "bdf1_dt": 1e-5,
+            "note": "old solution == current solution, so the BDF1 time term cancels",
+        },
+        # initial_values_debug.h:39-65: (x, y) -> (c, mu, eta1, eta2)
+        "debug_state": {
+            "0,0": [1.0, 0.1, 1.0, 0.0],
+            "1,0": [0.8, 0.2, 0.4, 0.4],
+            "2,0": [1.0, 0.3, 0.0, 1.0],
+            "0,1": [1.0, 0.4, 1.0, 0.0],
+            "1,1": [0.8, 0.5, 0.4, 0.4],
+            "2,1": [1.0, 0.6, 0.0, 1.0],
+        },
+        # deal.II enumerates the DoFs of subdivided_hyper_rectangle cell by
+        # cell: (0,0) (1,0) (0,1) (1,1) of cell 0, then (2,0) (2,1) of cell 1
+        "dealii_dof_points": [[0, 0], [1, 0], [0, 1], [1, 1], [2, 0], [2, 1]],
+        "residual_scalar": parse_residual(
+            os.path.join(t, "residual_generic_scalar_no_rbm.mpirun=1.output")),
+        "residual_tensorial": parse_residual(
+            os.path.join(t, "residual_generic_tensorial_no_rbm.mpirun=1.output")),
+        "residual_digits": 4,
+        # free_energy_sintering.cc: FreeEnergy(A=2, B=3), c=0.95, mu=0, etas
+        "free_energy_kat": {
+            "A": 2.0, "B": 3.0, "c": 0.95, "mu": 0.0,
+            "etas": [0.3, 0.15, 0.47, 0.0],
+            "values": parse_free_energy(os.path.join(t, "free_energy_sintering.output")),
+            "digits": 6,
+        },
+        "power_sum": parse_power_sum(os.path.join(t, "power_sum.output")),
+        # tangent_generic_scalar.cc / tangent_generic_tensorial.cc defaults,
+        # and tangent_tester.h:38-106 (l1 norm of the difference, FD eps 1e-7
+        # from lac/evaluation.h:30-87)
+        "tangent": {
+            "fd_epsilon": 1e-7,
+            "scalar": {"tol_abs": 1e-3, "tol_rel": 1e-6},
+            "tensorial": {"tol_abs": 1e0, "tol_rel": 1e-5},
+            "outputs": {
+                "scalar": open(os.path.join(t, "tangent_generic_scalar.mpirun=1.output")).read().splitlines()[0],
+                "tensorial": open(os.path.join(t, "tangent_generic_tensorial.mpirun=1.output")).read().splitlines()[0],
+            },
+        },
+    }
+    with open(os.path.join(HERE, "hpsint_goldens.json"), "w") as f:
+        json.dump(golden, f, indent=1)
+    print("wrote", os.path.join(HERE, "hpsint_goldens.json"))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
