@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 sintering operator.
+
+Workload (one GPU): the 3D operator bench -- Q1 hexes, 128^3 unit cells, 8
+seeded spheres with radii U[12, 18] overlapping by 2 cells, greedy colouring
+to 4 order parameters (6 components, 12.88 M DoFs), tanh profiles of width 2
+plus U(-1e-3, 1e-3) noise, tensorial mobility.  A step is one FP64
+Jacobian-vector product J(u) v over the whole mesh (inputs already resident
+in HBM); the metric is DoFs processed per second (GDoF/s).  The FP32
+Jacobian-vector product and the FP64 residual are timed the same way and
+reported under "kernels".
+
+`e2e` times the same step through the public C ABI with host buffers: the
+direction v is copied from pinned host memory, J v is computed and copied
+back, every step.
+
+`--impl reference`: hpsint itself cannot be built here (deal.II, p4est and
+Trilinos are absent), so the reference arm times the CPU restatement of its
+operator (oracle/) on the host cores instead.
+
+Multi-GPU (`--gpus N` under torchrun): the operator path is run as N
+independent replicas, one per GPU (no collective on the data path); value is
+the sum over ranks, timed as the maximum over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Jacobian-vec GDoF/s & s/step: FP32-inner+learned vs FP64 plain, Newton tol 1e-8"
+UNIT = "GDoF/s"
+WORKLOAD = "3d-operator-bench-128^3-8spheres-G4"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=128, help="cells per direction")
+    ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def make_state(n):
+    from hpsint_b200 import packings as P
+    centers, radii, colours = P.operator_bench_packing(n=n)
+    G = int(colours.max()) + 1
+    u = P.initial_state(3, (n, n, n), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), centers, radii, colours, width=2.0,
+                        noise=1e-3, seed=1)
+    rng = np.random.default_rng(2)
+    v = rng.uniform(-1.0, 1.0, u.shape)
+    return u, v, G
+
+
+def model_params(G, tensorial):
+    # EnergyAbstractData / MobilityAbstractData defaults (sintering/parameters.h:113-134)
+    return dict(n_grains=G, A=16.0, B=1.0, kappa_c=1.0, kappa_p=0.5, Mvol=1e-2, Mvap=1e-10, Msurf=4.0, Mgb=0.4,
+                L=1.0, tensorial=tensorial)
+
+
+DT = 1e-3  # BDF1, dt0 of the solver configurations
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in open(self.file.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(u, v, G, tensorial, budget_s, n):
+    """Time the CPU restatement of the operator (oracle) on a bounded sample of
+    the same workload: a slab of z-layers, repeated until `budget_s` elapses."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    nz = max(2, min(n, 16))
+    N_slab = (n + 1) * (n + 1) * (nz + 1)
+    us = np.ascontiguousarray(u[:, :N_slab])
+    vs = np.ascontiguousarray(v[:, :N_slab])
+    mesh = O.make_mesh(3, [n, n, nz])
+    prm = O.make_params(**{k: val for k, val in model_params(G, tensorial).items()})
+    T = O.make_time(1.0 / DT, 1.0, [-1.0 / DT])
+    O.jvp(mesh, prm, T, us, vs, threads)  # warm-up
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.jvp(mesh, prm, T, us, vs, threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or reps >= 1000:
+            break
+    dofs = (G + 2) * N_slab * reps
+    return {"value": dofs / el / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"FP64 Jacobian-vector product, CPU restatement (OpenMP, {threads} threads), "
+                      f"{n}x{n}x{nz}-cell z-slab of the same state, {reps} reps in {el:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    u, v, G = make_state(args.n)
+    from oracle import oracle as O
+    O.build()
+    tensorial = not args.scalar
+    # each step is a bounded sample (a z-slab) of the workload on all host cores
+    per_step = max(1.0, args.cpu_seconds / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_baseline(u, v, G, tensorial, 0.0, args.n)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(u, v, G, tensorial, per_step, args.n))
+    value = float(np.mean([x["value"] for x in vals]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "mobility": "scalar" if args.scalar else "tensorial", "n_cells": args.n,
+                   "note": "hpsint needs deal.II/p4est/Trilinos (absent): CPU restatement of its operator"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[0]["cores"], "kind": "port",
+                         "sample": vals[0]["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import hpsint_b200 as hb
+    from hpsint_b200 import _lib as L
+
+    tensorial = not args.scalar
+    u, v, G = make_state(args.n)
+    n = args.n
+    op = hb.SinteringOperatorGeneric(hb.Mesh(3, (n, n, n)), hb.Params(**model_params(G, tensorial)))
+    op.set_time_weights(1.0 / DT, [-1.0 / DT], 1.0)
+    ud, vd = op.to_device(u), op.to_device(v)
+    op.fill_quadrature_point_values(ud)
+    dst = op.initialize_dof_vector()
+    dofs = op.C * op.N
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def time_loop(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(steps):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps
+
+    # --- headline: FP64 Jacobian-vector product --------------------------------
+    sampler = ClockSampler(local_rank)
+    for _ in range(args.warmup):
+        op.vmult(dst, vd)
+    barrier()
+    launches0 = hb.kernel_launch_count()
+    sampler.start()
+    time.sleep(0.3)
+    ms_jvp64 = time_loop(lambda: op.vmult(dst, vd), args.steps, 0)
+    clocks = sampler.stop()
+    launches = hb.kernel_launch_count() - launches0
+
+    # --- the other kernels of the path ----------------------------------------
+    v32, dst32 = vd.float(), op.initialize_dof_vector(torch.float32)
+    ms_jvp32 = time_loop(lambda: op.vmult(dst32, v32), args.steps, args.warmup)
+    hist = [ud.clone()]
+    res = op.initialize_dof_vector()
+    ms_res = time_loop(lambda: op.evaluate_nonlinear_residual(res, ud, 2, hist), args.steps, args.warmup)
+    pc = hb.BlockPreconditioner2(op)
+    ms_pcsetup = time_loop(pc.do_update, max(1, args.steps // 4), 1)
+    z32 = op.initialize_dof_vector(torch.float32)
+    ms_pc32 = time_loop(lambda: pc.vmult(z32, v32), args.steps, args.warmup)
+
+    # --- end to end through the C ABI with host buffers ------------------------
+    import ctypes
+    h_src = torch.empty((op.C, op.ld), dtype=torch.float64, pin_memory=True)
+    h_src.copy_(vd.cpu())
+    h_dst = torch.empty((op.C, op.ld), dtype=torch.float64, pin_memory=True)
+    d_src = op.initialize_dof_vector()
+    lib = L.lib()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    nbytes = op.C * op.ld * 8
+
+    def e2e_step():
+        d_src.copy_(h_src, non_blocking=True)
+        L.check(lib.sint_jvp_f64(op._h, ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(d_src.data_ptr()), sp),
+                "sint_jvp_f64")
+        h_dst.copy_(dst, non_blocking=True)
+
+    ms_e2e = time_loop(e2e_step, args.steps, args.warmup)
+    torch.cuda.synchronize()
+    assert np.isfinite(h_dst[:, :op.N].numpy()).all()
+
+    # --- roofline of the dominant kernel (algorithmic bytes) ------------------
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    alg_bytes = 24 * dofs  # src + dst + linearisation point, FP64
+    achieved = alg_bytes / (ms_jvp64 * 1e-3) / 1e9
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    gdofs = lambda ms: dofs / (ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "jvp_traffic.json")
+    if os.path.exists(tf):
+        try:
+            t = json.load(open(tf))
+            traffic = t.get("bytes_per_launch_scaled_to_workload")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC,
+        "value": gdofs(ms_jvp64) * world,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_jvp64,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_cells": [n, n, n], "n_grains": G, "n_components": op.C,
+                   "dofs": dofs, "mobility": "tensorial" if tensorial else "scalar", "step": "FP64 J(u) v",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (lin + src + dst = %.0f MB)" % (3 * dofs * 8 / 1e6)},
+        "kernels": {
+            "jvp_f64": {"ms": ms_jvp64, "gdofs": gdofs(ms_jvp64)},
+            "jvp_f32": {"ms": ms_jvp32, "gdofs": gdofs(ms_jvp32)},
+            "residual_f64_bdf1": {"ms": ms_res, "gdofs": gdofs(ms_res)},
+            "precond_setup_f64": {"ms": ms_pcsetup},
+            "precond_apply_f32": {"ms": ms_pc32, "gbs": (4 * 2 * dofs + 4 * (G + 4) * op.N) / (ms_pc32 * 1e-3) / 1e9},
+        },
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": traffic,
+                     "note": f"FP64 J v: algorithmic bytes 24*C*N = {alg_bytes/1e6:.1f} MB per launch; "
+                             f"peak {peak_src}; kernel is FP64-ALU bound (on-the-fly linearisation)"},
+        "e2e": {"value": gdofs(ms_e2e) * world, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(u, v, G, tensorial, args.cpu_seconds, n)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,397 @@
+// Shared device-side building blocks of the sintering cell kernels.
+//
+// Mesh: uniform Cartesian Q1 cells, nodes numbered lexicographically
+// (x fastest).  A thread block owns a brick ("tile") of cells; one thread
+// per (cell, quadrature point), so the 2^dim threads of a cell sit in
+// consecutive lanes and exchange data with warp shuffles.
+//
+// Data flow of a cell kernel
+//   1. the tile's node box (TX+1)(TY+1)(TZ+1) of every input component is
+//      staged in shared memory with coalesced loads;
+//   2. each thread evaluates values and gradients at its quadrature point by
+//      sum factorisation over the cell's 2^dim nodal values (1D Q1 matrices
+//      at the two Gauss points are 2x2);
+//   3. the point-wise physics (free energy, mobility) runs in registers;
+//   4. integration (test functions) is a sum-factorised butterfly across the
+//      2^dim lanes of a cell: afterwards lane l holds the cell's contribution
+//      to its local node l;
+//   5. the contributions are summed per node inside the tile in a fixed order
+//      (no atomics); nodes whose every adjacent cell lies in the tile are
+//      written to the output, nodes on a tile face go to a per-tile partial
+//      buffer that a second kernel (combine) sums in a fixed order.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sint
+{
+  constexpr int MAX_GRAINS = 12;
+
+  template <int DIM>
+  struct Tile;
+
+  template <>
+  struct Tile<3>
+  {
+    static constexpr int TX = 4, TY = 4, TZ = 2;
+    static constexpr int NQ      = 8;
+    static constexpr int CELLS   = TX * TY * TZ;
+    static constexpr int BX      = TX + 1, BY = TY + 1, BZ = TZ + 1;
+    static constexpr int BOX     = BX * BY * BZ;
+    static constexpr int THREADS = CELLS * NQ;
+  };
+
+  template <>
+  struct Tile<2>
+  {
+    static constexpr int TX = 8, TY = 8, TZ = 1;
+    static constexpr int NQ      = 4;
+    static constexpr int CELLS   = TX * TY;
+    static constexpr int BX      = TX + 1, BY = TY + 1, BZ = 1;
+    static constexpr int BOX     = BX * BY;
+    static constexpr int THREADS = CELLS * NQ;
+  };
+
+  // Mesh description passed by value to every kernel.
+  struct Grid
+  {
+    int       dim;
+    int       n[3];  // cells per direction (1 for unused directions)
+    int       nn[3]; // nodes per direction (1 for unused directions)
+    int       nt[3]; // tiles per direction (1 for unused directions)
+    long long N;     // number of nodes
+    long long ld;    // block stride of a DoF vector
+    long long n_tiles;
+    double    h[3];
+  };
+
+  // Point-wise model parameters (FP64 on the host, cast per kernel).
+  struct Phys
+  {
+    double A, B, kappa_c, kappa_p;
+    double Mvol, Mvap, Msurf, Mgb, L;
+    double w0, w_alg;
+    double w_hist[4];
+    int    order;
+  };
+
+  template <typename R>
+  struct PhysR
+  {
+    R A, B, kc, kp, Mvol, Mvap, Msurf, Mgb, L, w0, walg;
+    __host__ __device__ PhysR() {}
+    __host__ __device__ explicit PhysR(const Phys &p)
+      : A(R(p.A)), B(R(p.B)), kc(R(p.kappa_c)), kp(R(p.kappa_p)), Mvol(R(p.Mvol)), Mvap(R(p.Mvap)),
+        Msurf(R(p.Msurf)), Mgb(R(p.Mgb)), L(R(p.L)), w0(R(p.w0)), walg(R(p.w_alg))
+    {}
+  };
+
+  // Tile coordinates of this block.
+  struct TileCoord
+  {
+    int       t[3];   // tile index per direction
+    int       o[3];   // first cell of the tile per direction
+    long long linear; // blockIdx.x
+  };
+
+  template <int DIM>
+  __device__ __forceinline__ TileCoord tile_coord(const Grid &g)
+  {
+    using T = Tile<DIM>;
+    TileCoord tc;
+    tc.linear    = blockIdx.x;
+    long long r  = tc.linear;
+    tc.t[0]      = int(r % g.nt[0]);
+    r /= g.nt[0];
+    tc.t[1] = int(r % g.nt[1]);
+    r /= g.nt[1];
+    tc.t[2] = int(r);
+    tc.o[0] = tc.t[0] * T::TX;
+    tc.o[1] = tc.t[1] * T::TY;
+    tc.o[2] = tc.t[2] * T::TZ;
+    return tc;
+  }
+
+  __device__ __forceinline__ long long node_index(const Grid &g, int i, int j, int k)
+  {
+    return (long long)i + (long long)g.nn[0] * ((long long)j + (long long)g.nn[1] * k);
+  }
+
+  // Stage the node box of `ncomp` components of `src` (block stride g.ld) in
+  // shared memory, layout s[comp * BOX + box_node]; nodes outside the mesh
+  // read as zero.
+  template <int DIM, typename R, typename S>
+  __device__ __forceinline__ void load_box(R *s, const S *__restrict__ src, int ncomp, const Grid &g,
+                                           const TileCoord &tc)
+  {
+    using T = Tile<DIM>;
+    for (int idx = threadIdx.x; idx < ncomp * T::BOX; idx += T::THREADS)
+      {
+        const int comp = idx / T::BOX;
+        const int b    = idx - comp * T::BOX;
+        const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
+        const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
+        R v = R(0);
+        if (gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2])
+          v = R(src[comp * g.ld + node_index(g, gi, gj, gk)]);
+        s[idx] = v;
+      }
+  }
+
+  // Per-thread quadrature constants.  Lane bits of (threadIdx.x % NQ) are the
+  // quadrature point coordinates (qx, qy, qz); after the integration butterfly
+  // they are the local node coordinates (lx, ly, lz).
+  template <int DIM, typename R>
+  struct QP
+  {
+    R wA[DIM], wB[DIM]; // interpolation weights of the two nodes at this point
+    R ih[DIM];          // 1 / h
+    R sgn_ih[DIM];      // (+-1) / h: derivative sign of this lane's node
+    R g1, g0;           // Q1 shape values at the Gauss points: phi_l(x_q) = (l == q) ? g1 : g0
+    R JxW;
+    int q;
+
+    __device__ __forceinline__ explicit QP(const Grid &g)
+    {
+      q                 = threadIdx.x & ((1 << DIM) - 1);
+      const double s3   = 0.5 / 1.7320508075688772935274463415058723669428; // 1 / (2 sqrt 3)
+      const double gg0  = 0.5 - s3, gg1 = 0.5 + s3;
+      g1                = R(gg1);
+      g0                = R(gg0);
+      double jxw        = 1.0;
+      for (int d = 0; d < DIM; ++d)
+        {
+          const int b = (q >> d) & 1;
+          // node 0 of the 1D element has phi_0(x_q) = 1 - x_q, node 1 has x_q
+          wA[d]     = R(b ? gg0 : gg1);
+          wB[d]     = R(b ? gg1 : gg0);
+          ih[d]     = R(1.0 / g.h[d]);
+          sgn_ih[d] = R((b ? 1.0 : -1.0) / g.h[d]);
+          jxw *= 0.5 * g.h[d];
+        }
+      JxW = R(jxw);
+    }
+  };
+
+  // Box offset of local node (0,0,0) of cell `cell` of the tile.
+  template <int DIM>
+  __device__ __forceinline__ int cell_box_base(int cell)
+  {
+    using T      = Tile<DIM>;
+    const int cx = cell % T::TX, cy = (cell / T::TX) % T::TY, cz = cell / (T::TX * T::TY);
+    return cx + T::BX * (cy + T::BY * cz);
+  }
+
+  template <int DIM>
+  __device__ __forceinline__ bool cell_in_mesh(int cell, const TileCoord &tc, const Grid &g)
+  {
+    using T      = Tile<DIM>;
+    const int cx = cell % T::TX, cy = (cell / T::TX) % T::TY, cz = cell / (T::TX * T::TY);
+    return tc.o[0] + cx < g.n[0] && tc.o[1] + cy < g.n[1] && (DIM == 2 || tc.o[2] + cz < g.n[2]);
+  }
+
+  // Value and gradient of one component at this thread's quadrature point,
+  // by sum factorisation over the cell's nodal values in the staged box.
+  template <int DIM, typename R>
+  __device__ __forceinline__ void eval_vg(const R *s, int b0, const QP<DIM, R> &w, R &val, R (&grad)[DIM])
+  {
+    using T = Tile<DIM>;
+    if constexpr (DIM == 3)
+      {
+        constexpr int SY = T::BX, SZ = T::BX * T::BY;
+        R vx[2][2], dx[2][2];
+#pragma unroll
+        for (int lz = 0; lz < 2; ++lz)
+#pragma unroll
+          for (int ly = 0; ly < 2; ++ly)
+            {
+              const R u0 = s[b0 + ly * SY + lz * SZ], u1 = s[b0 + 1 + ly * SY + lz * SZ];
+              vx[lz][ly] = w.wA[0] * u0 + w.wB[0] * u1;
+              dx[lz][ly] = (u1 - u0) * w.ih[0];
+            }
+        R vxy[2], dxy[2], dyy[2];
+#pragma unroll
+        for (int lz = 0; lz < 2; ++lz)
+          {
+            vxy[lz] = w.wA[1] * vx[lz][0] + w.wB[1] * vx[lz][1];
+            dxy[lz] = w.wA[1] * dx[lz][0] + w.wB[1] * dx[lz][1];
+            dyy[lz] = (vx[lz][1] - vx[lz][0]) * w.ih[1];
+          }
+        val     = w.wA[2] * vxy[0] + w.wB[2] * vxy[1];
+        grad[0] = w.wA[2] * dxy[0] + w.wB[2] * dxy[1];
+        grad[1] = w.wA[2] * dyy[0] + w.wB[2] * dyy[1];
+        grad[2] = (vxy[1] - vxy[0]) * w.ih[2];
+      }
+    else
+      {
+        constexpr int SY = T::BX;
+        R vx[2], dx[2];
+#pragma unroll
+        for (int ly = 0; ly < 2; ++ly)
+          {
+            const R u0 = s[b0 + ly * SY], u1 = s[b0 + 1 + ly * SY];
+            vx[ly]     = w.wA[0] * u0 + w.wB[0] * u1;
+            dx[ly]     = (u1 - u0) * w.ih[0];
+          }
+        val     = w.wA[1] * vx[0] + w.wB[1] * vx[1];
+        grad[0] = w.wA[1] * dx[0] + w.wB[1] * dx[1];
+        grad[1] = (vx[1] - vx[0]) * w.ih[1];
+      }
+  }
+
+  // Value only.
+  template <int DIM, typename R>
+  __device__ __forceinline__ R eval_v(const R *s, int b0, const QP<DIM, R> &w)
+  {
+    using T = Tile<DIM>;
+    if constexpr (DIM == 3)
+      {
+        constexpr int SY = T::BX, SZ = T::BX * T::BY;
+        R vxy[2];
+#pragma unroll
+        for (int lz = 0; lz < 2; ++lz)
+          {
+            const R a = w.wA[0] * s[b0 + lz * SZ] + w.wB[0] * s[b0 + 1 + lz * SZ];
+            const R b = w.wA[0] * s[b0 + SY + lz * SZ] + w.wB[0] * s[b0 + 1 + SY + lz * SZ];
+            vxy[lz]   = w.wA[1] * a + w.wB[1] * b;
+          }
+        return w.wA[2] * vxy[0] + w.wB[2] * vxy[1];
+      }
+    else
+      {
+        constexpr int SY = T::BX;
+        const R a = w.wA[0] * s[b0] + w.wB[0] * s[b0 + 1];
+        const R b = w.wA[0] * s[b0 + SY] + w.wB[0] * s[b0 + 1 + SY];
+        return w.wA[1] * a + w.wB[1] * b;
+      }
+  }
+
+  // Integration butterfly.  Input: this lane's point value v and gradient g
+  // of a residual row at its quadrature point.  Output: the cell integral
+  //   sum_q JxW (v_q phi_l(x_q) + g_q . grad phi_l(x_q))
+  // for the local node l given by this lane's bits.  Sum factorised: one
+  // stage per direction, each exchanging with the lane that differs in that bit.
+  template <int DIM, typename R>
+  __device__ __forceinline__ R integrate_butterfly(R v, const R (&g)[DIM], const QP<DIM, R> &w)
+  {
+    constexpr unsigned FULL = 0xffffffffu;
+    if constexpr (DIM == 3)
+      {
+        // stage x
+        const R vp = __shfl_xor_sync(FULL, v, 1), gxp = __shfl_xor_sync(FULL, g[0], 1);
+        const R gyp = __shfl_xor_sync(FULL, g[1], 1), gzp = __shfl_xor_sync(FULL, g[2], 1);
+        const R t   = w.g1 * v + w.g0 * vp + w.sgn_ih[0] * (g[0] + gxp);
+        const R gy  = w.g1 * g[1] + w.g0 * gyp;
+        const R gz  = w.g1 * g[2] + w.g0 * gzp;
+        // stage y
+        const R tp = __shfl_xor_sync(FULL, t, 2), gyp2 = __shfl_xor_sync(FULL, gy, 2),
+                gzp2 = __shfl_xor_sync(FULL, gz, 2);
+        const R t2  = w.g1 * t + w.g0 * tp + w.sgn_ih[1] * (gy + gyp2);
+        const R gz2 = w.g1 * gz + w.g0 * gzp2;
+        // stage z
+        const R t2p = __shfl_xor_sync(FULL, t2, 4), gz2p = __shfl_xor_sync(FULL, gz2, 4);
+        const R r   = w.g1 * t2 + w.g0 * t2p + w.sgn_ih[2] * (gz2 + gz2p);
+        return r * w.JxW;
+      }
+    else
+      {
+        const R vp = __shfl_xor_sync(FULL, v, 1), gxp = __shfl_xor_sync(FULL, g[0], 1);
+        const R gyp = __shfl_xor_sync(FULL, g[1], 1);
+        const R t   = w.g1 * v + w.g0 * vp + w.sgn_ih[0] * (g[0] + gxp);
+        const R gy  = w.g1 * g[1] + w.g0 * gyp;
+        const R tp = __shfl_xor_sync(FULL, t, 2), gyp2 = __shfl_xor_sync(FULL, gy, 2);
+        const R r  = w.g1 * t + w.g0 * tp + w.sgn_ih[1] * (gy + gyp2);
+        return r * w.JxW;
+      }
+  }
+
+  // Step 5 of the data flow: sum the per-cell node contributions
+  // s_con[comp * THREADS + cell * NQ + l] of the tile per box node, write
+  // nodes owned by the tile to dst and the others to the tile's slot of the
+  // partial buffer (layout [tile][comp][BOX]).
+  template <int DIM, typename R>
+  __device__ __forceinline__ void sum_and_store(const R *s_con, int ncomp, const Grid &g, const TileCoord &tc,
+                                                R *__restrict__ dst, R *__restrict__ partial)
+  {
+    using T = Tile<DIM>;
+    for (int idx = threadIdx.x; idx < ncomp * T::BOX; idx += T::THREADS)
+      {
+        const int comp = idx / T::BOX;
+        const int b    = idx - comp * T::BOX;
+        const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
+        const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
+        if (gi >= g.nn[0] || gj >= g.nn[1] || gk >= g.nn[2])
+          continue;
+        R sum = R(0);
+#pragma unroll
+        for (int l = 0; l < T::NQ; ++l)
+          {
+            const int cx = bx - (l & 1), cy = by - ((l >> 1) & 1), cz = (DIM == 3) ? bz - ((l >> 2) & 1) : 0;
+            if (cx >= 0 && cx < T::TX && cy >= 0 && cy < T::TY && cz >= 0 && cz < T::TZ)
+              sum += s_con[comp * T::THREADS + (cx + T::TX * (cy + T::TY * cz)) * T::NQ + l];
+          }
+        bool owned = (bx > 0 || gi == 0) && (bx < T::TX || gi == g.n[0]) && (by > 0 || gj == 0) &&
+                     (by < T::TY || gj == g.n[1]);
+        if (DIM == 3)
+          owned = owned && (bz > 0 || gk == 0) && (bz < T::TZ || gk == g.n[2]);
+        if (owned)
+          dst[comp * g.ld + node_index(g, gi, gj, gk)] = sum;
+        else
+          partial[(tc.linear * ncomp + comp) * (long long)T::BOX + b] = sum;
+      }
+  }
+
+  // Second pass of the scatter: nodes on an interior tile face sum the
+  // partials of the 2, 4 or 8 tiles that share them, in a fixed order.
+  template <int DIM, typename R>
+  __global__ void __launch_bounds__(256) combine_kernel(const Grid g, int ncomp, const R *__restrict__ partial,
+                                                        R *__restrict__ dst)
+  {
+    using T             = Tile<DIM>;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= g.N)
+      return;
+    int c[3];
+    c[0]             = int(idx % g.nn[0]);
+    c[1]             = int((idx / g.nn[0]) % g.nn[1]);
+    c[2]             = int(idx / ((long long)g.nn[0] * g.nn[1]));
+    const int TT[3]  = {T::TX, T::TY, T::TZ};
+    int       nt[3]  = {1, 1, 1}; // number of candidate tiles per direction
+    int       t0[3]  = {0, 0, 0}; // first candidate tile
+    int       lo[3]  = {0, 0, 0}; // local box coordinate in the first candidate
+    bool      shared = false;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      {
+        if (c[d] % TT[d] == 0 && c[d] > 0 && c[d] < g.n[d])
+          {
+            shared = true;
+            nt[d]  = 2;
+            t0[d]  = c[d] / TT[d] - 1;
+            lo[d]  = TT[d];
+          }
+        else
+          {
+            t0[d] = min(c[d] / TT[d], g.nt[d] - 1);
+            lo[d] = c[d] - t0[d] * TT[d];
+          }
+      }
+    if (!shared)
+      return;
+    for (int comp = 0; comp < ncomp; ++comp)
+      {
+        R sum = R(0);
+        for (int a = 0; a < nt[2]; ++a)
+          for (int bb = 0; bb < nt[1]; ++bb)
+            for (int cc = 0; cc < nt[0]; ++cc)
+              {
+                const int       ti = t0[0] + cc, tj = t0[1] + bb, tk = t0[2] + a;
+                const int       bx = lo[0] - cc * TT[0], by = lo[1] - bb * TT[1], bz = lo[2] - a * TT[2];
+                const long long tile = ti + (long long)g.nt[0] * (tj + (long long)g.nt[1] * tk);
+                sum += partial[(tile * ncomp + comp) * (long long)T::BOX + bx + T::BX * (by + T::BY * bz)];
+              }
+        dst[comp * g.ld + idx] = sum;
+      }
+  }
+} // namespace sint

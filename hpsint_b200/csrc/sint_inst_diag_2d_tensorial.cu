@@ -1,0 +1,8 @@
+// Instantiates the preconditioner-diagonal kernels for dim = 2, tensorial mobility, G = 1..12.
+#include "sint_launch_impl.cuh"
+
+namespace sint
+{
+  template cudaError_t launch_diag<2, true>(int, const Grid &, const Phys &, const double *, double *, double *,
+                                            cudaStream_t);
+} // namespace sint

@@ -1,0 +1,10 @@
+// Instantiates the Jacobian-vector product kernels for dim = 2, scalar mobility, G = 1..12, FP64 and FP32.
+#include "sint_launch_impl.cuh"
+
+namespace sint
+{
+  template cudaError_t launch_jvp<2, false, double>(int, const Grid &, const Phys &, const double *, const double *,
+                                                   double *, double *, cudaStream_t);
+  template cudaError_t launch_jvp<2, false, float>(int, const Grid &, const Phys &, const float *, const float *,
+                                                  float *, float *, cudaStream_t);
+} // namespace sint

@@ -1,0 +1,10 @@
+// Instantiates the Jacobian-vector product kernels for dim = 2, tensorial mobility, G = 1..12, FP64 and FP32.
+#include "sint_launch_impl.cuh"
+
+namespace sint
+{
+  template cudaError_t launch_jvp<2, true, double>(int, const Grid &, const Phys &, const double *, const double *,
+                                                   double *, double *, cudaStream_t);
+  template cudaError_t launch_jvp<2, true, float>(int, const Grid &, const Phys &, const float *, const float *,
+                                                  float *, float *, cudaStream_t);
+} // namespace sint

@@ -1,0 +1,8 @@
+// Instantiates the nonlinear-residual kernels for dim = 3, tensorial mobility, G = 1..12, with_time_derivative 0..2.
+#include "sint_launch_impl.cuh"
+
+namespace sint
+{
+  template cudaError_t launch_residual<3, true>(int, int, const Grid &, const Phys &, const double *,
+                                                const double *const *, double *, double *, cudaStream_t);
+} // namespace sint

@@ -1,0 +1,75 @@
+// Internal state of a sintering-operator context (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/hpsint_b200.h"
+#include "sint_common.cuh"
+
+namespace sint
+{
+  void set_error(const std::string &msg);
+  int  cuda_fail(cudaError_t e, const char *what);
+
+  // Deterministic reductions: NB_RED fixed block partials, then one block.
+  constexpr int NB_RED       = 592; // 4 x 148 SMs
+  constexpr int MAX_MULTIDOT = 64;
+
+  struct Workspace; // Newton/GMRES vectors, sint_newton.cu
+
+  struct Ctx
+  {
+    sint_mesh   mesh;
+    sint_params params;
+    Grid        grid;
+    Phys        phys;
+    int         G = 0, C = 0;
+    long long   N = 0, ld = 0;
+
+    double *lin64 = nullptr; // linearisation point, C blocks
+    float  *lin32 = nullptr; // FP32 shadow
+    bool    has_lin = false;
+
+    double *partial       = nullptr; // tile-face partial sums of the cell kernels
+    size_t  partial_bytes = 0;
+
+    double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
+    double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
+    float  *pc_inv32 = nullptr;
+    bool    has_pc   = false;
+
+    double *red = nullptr; // reduction partials: MAX_MULTIDOT x NB_RED doubles
+
+    // DampedNewtonSolver state that outlives one solve (solvers_nonlinear.h:390-391)
+    unsigned history_newton_iterations      = 0;
+    unsigned history_linear_iterations_last = 0;
+
+    Workspace *ws = nullptr;
+  };
+
+  // Reductions (sint_blas.cu); `out` is a device pointer.
+  int dot_f64(Ctx *c, long long n, const double *x, const double *y, double *out, cudaStream_t s);
+  int dot_f32(Ctx *c, long long n, const float *x, const float *y, double *out, cudaStream_t s);
+  // out[i] = <w, V + i * stride> for i < m (FP64 accumulation)
+  template <typename R>
+  int multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, cudaStream_t s);
+  // w -= sum_i coef[i] * (V + i * stride), coef on the device
+  template <typename R>
+  int multiaxpy(long long n, R *w, const R *V, long long stride, int m, const double *coef, cudaStream_t s);
+  // y = a * x + b * y  (a, b on the host)
+  template <typename R>
+  int axpby(long long n, double a, const R *x, double b, R *y, cudaStream_t s);
+  // y = sum_i y_i-combination: y = x + sum_i coef[i] * V_i (coef on the device), FP32/FP64 V
+  template <typename R>
+  int lincomb(long long n, R *y, const R *V, long long stride, int m, const double *coef, cudaStream_t s);
+  template <typename S, typename D>
+  int convert(long long n, const S *x, D *y, cudaStream_t s);
+
+  int free_workspace(Ctx *c);
+} // namespace sint
+
+struct sint_ctx : public sint::Ctx
+{};

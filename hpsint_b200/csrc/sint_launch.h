@@ -1,0 +1,35 @@
+// Host-side launchers of the cell kernels.  The runtime number of grains is
+// mapped onto a compile-time template argument here, the way hpsint's
+// EXPAND_OPERATIONS maps n_grains onto n_comp
+// (applications/sintering/include/pf-applications/sintering/instantiation.h:97-141).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sint_common.cuh"
+
+namespace sint
+{
+  // Dynamic shared memory of each kernel (bytes).
+  size_t smem_jvp(int dim, int G, size_t real_bytes);
+  size_t smem_residual(int dim, int G, int wtd);
+  size_t smem_diag(int dim, int G);
+
+  template <int DIM, bool TENS, typename R>
+  cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
+                         cudaStream_t s);
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
+                              const double *const *hist, double *dst, double *partial, cudaStream_t s);
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
+                          cudaStream_t s);
+
+  template <int DIM, typename R>
+  cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, cudaStream_t s);
+
+  // Counts kernel launches issued by this library.
+  void count_launches(int n);
+} // namespace sint

@@ -1,0 +1,123 @@
+// Definitions of the launchers declared in sint_launch.h; included by the
+// sint_inst_*.cu translation units, each of which instantiates one
+// (dimension, mobility) combination for all grain counts.
+#pragma once
+
+#include "sint_kernels.cuh"
+#include "sint_launch.h"
+
+namespace sint
+{
+  template <typename Kernel>
+  inline cudaError_t prepare_smem(Kernel k, size_t bytes)
+  {
+    if (bytes > 48 * 1024)
+      return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    return cudaSuccess;
+  }
+
+  template <int DIM, int G, bool TENS, typename R>
+  cudaError_t launch_jvp_g(const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
+                           cudaStream_t s)
+  {
+    const size_t smem = smem_jvp(DIM, G, sizeof(R));
+    auto         k    = jvp_kernel<DIM, G, TENS, R>;
+    cudaError_t  e    = prepare_smem(k, smem);
+    if (e != cudaSuccess)
+      return e;
+    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial);
+    count_launches(1);
+    return cudaGetLastError();
+  }
+
+  template <int DIM, int G, bool TENS, int WTD>
+  cudaError_t launch_residual_g(const Grid &g, const Phys &p, const double *src, const double *const *hist,
+                                double *dst, double *partial, cudaStream_t s)
+  {
+    const size_t  smem = smem_residual(DIM, G, WTD);
+    auto          k    = residual_kernel<DIM, G, TENS, WTD>;
+    cudaError_t   e    = prepare_smem(k, smem);
+    if (e != cudaSuccess)
+      return e;
+    const double *h0 = WTD == 2 ? hist[0] : nullptr;
+    const double *h1 = (WTD == 2 && p.order > 1) ? hist[1] : nullptr;
+    const double *h2 = (WTD == 2 && p.order > 2) ? hist[2] : nullptr;
+    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial);
+    count_launches(1);
+    return cudaGetLastError();
+  }
+
+  template <int DIM, int G, bool TENS>
+  cudaError_t launch_diag_g(const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
+                            cudaStream_t s)
+  {
+    const size_t smem = smem_diag(DIM, G);
+    auto         k    = diag_kernel<DIM, G, TENS>;
+    cudaError_t  e    = prepare_smem(k, smem);
+    if (e != cudaSuccess)
+      return e;
+    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, dst, partial);
+    count_launches(1);
+    return cudaGetLastError();
+  }
+
+#define SINT_G_SWITCH(CALL)                                                                                       \
+  switch (G)                                                                                                      \
+    {                                                                                                             \
+      case 1: return CALL(1);                                                                                     \
+      case 2: return CALL(2);                                                                                     \
+      case 3: return CALL(3);                                                                                     \
+      case 4: return CALL(4);                                                                                     \
+      case 5: return CALL(5);                                                                                     \
+      case 6: return CALL(6);                                                                                     \
+      case 7: return CALL(7);                                                                                     \
+      case 8: return CALL(8);                                                                                     \
+      case 9: return CALL(9);                                                                                     \
+      case 10: return CALL(10);                                                                                   \
+      case 11: return CALL(11);                                                                                   \
+      case 12: return CALL(12);                                                                                   \
+      default: return cudaErrorInvalidValue;                                                                      \
+    }
+
+  template <int DIM, bool TENS, typename R>
+  cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
+                         cudaStream_t s)
+  {
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R>(g, p, lin, src, dst, partial, s)
+    SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+  }
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
+                              const double *const *hist, double *dst, double *partial, cudaStream_t s)
+  {
+    if (wtd == 0)
+      {
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 0>(g, p, src, hist, dst, partial, s)
+        SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+      }
+    else if (wtd == 1)
+      {
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 1>(g, p, src, hist, dst, partial, s)
+        SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+      }
+    else
+      {
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 2>(g, p, src, hist, dst, partial, s)
+        SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+      }
+  }
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
+                          cudaStream_t s)
+  {
+#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS>(g, p, lin, dst, partial, s)
+    SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+  }
+} // namespace sint

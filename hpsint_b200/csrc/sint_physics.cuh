@@ -1,0 +1,303 @@
+// Point-wise physics of the sintering operator at one quadrature point.
+//
+// Restates, for Real = double or float and a compile-time number of grains G:
+//   sintering/free_energy.h:111-168, :233-252     (Wang bulk energy)
+//   sintering/mobility.h:439-534                  (MobilityScalar)
+//   sintering/mobility.h:668-916, :960            (MobilityTensorial)
+//   include/pf-applications/base/tensor.h:137-186 (unit_vector, filters, projector)
+// Vectors are plain arrays of length DIM.  The grain-boundary pair loops keep
+// hpsint's lower-triangular (i > j) order; algebraically equal terms that only
+// depend on the linearisation point are grouped to save operations.
+#pragma once
+
+#include "sint_common.cuh"
+
+namespace sint
+{
+  template <int D, typename R>
+  __device__ __forceinline__ R dotv(const R (&a)[D], const R (&b)[D])
+  {
+    R s = a[0] * b[0];
+#pragma unroll
+    for (int d = 1; d < D; ++d)
+      s += a[d] * b[d];
+    return s;
+  }
+
+  template <typename R>
+  __device__ __forceinline__ R clamp01(R x)
+  {
+    x = x < R(0) ? R(0) : x;
+    return x > R(1) ? R(1) : x;
+  }
+
+  // tensor.h:137-154; also returns |v|.
+  template <int D, typename R>
+  __device__ __forceinline__ void unit_vector(const R (&v)[D], R (&n)[D], R &nrm)
+  {
+    nrm          = sqrt(dotv<D>(v, v));
+    const R tol  = R(1e-10);
+    const R fn   = nrm < tol ? R(1) : nrm;
+    const bool f = nrm > tol;
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      n[d] = f ? v[d] / fn : R(0);
+  }
+
+  // tensor.h:156-174
+  template <int D, typename R>
+  __device__ __forceinline__ R unit_vector_filter_2(const R (&v)[D])
+  {
+    const R n2  = dotv<D>(v, v);
+    const R tol = R(1e-20);
+    return n2 > tol ? R(1) / n2 : R(0);
+  }
+
+  template <typename R>
+  __device__ __forceinline__ R phi_clamped(R c)
+  {
+    return clamp01(c * c * c * (R(10) - R(15) * c + R(6) * c * c));
+  }
+
+  // ---------------------------------------------------------------------
+  // Residual flux of the c row: M(c, eta, grad c, grad eta) grad mu
+  // scalar: mobility.h:439-472, tensorial: mobility.h:756-804
+  template <int DIM, int G, bool TENS, typename R>
+  __device__ __forceinline__ void apply_M(const PhysR<R> &p, R c, const R (&eta)[G], const R (&gc)[DIM],
+                                          const R (*geta)[DIM], const R (&gmu)[DIM], R (&out)[DIM])
+  {
+    const R phi = phi_clamped(c);
+    if constexpr (!TENS)
+      {
+        R etaij = R(0);
+#pragma unroll
+        for (int i = 0; i < G; ++i)
+#pragma unroll
+          for (int j = 0; j < i; ++j)
+            etaij += eta[i] * eta[j];
+        const R M = p.Mvol * phi + p.Mvap * (R(1) - phi) + p.Msurf * R(4) * c * c * (R(1) - c) * (R(1) - c) +
+                    (R(2) * p.Mgb) * etaij;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          out[d] = M * gmu[d];
+      }
+    else
+      {
+        const R fvv   = p.Mvol * phi + p.Mvap * (R(1) - phi);
+        const R fsurf = p.Msurf * R(4) * (c * c) * ((R(1) - c) * (R(1) - c));
+        R       nc[DIM], nrm;
+        unit_vector<DIM>(gc, nc, nrm);
+        const R a  = fvv + fsurf * R(1.001);
+        const R b  = fsurf * dotv<DIM>(nc, gmu);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          out[d] = a * gmu[d] - nc[d] * b;
+        if constexpr (G > 1)
+          {
+            // sum_{i>j} eta_i eta_j (grad mu - f_ij d_ij (d_ij . grad mu))
+            R s1 = R(0), acc[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+              acc[d] = R(0);
+#pragma unroll
+            for (int i = 0; i < G; ++i)
+#pragma unroll
+              for (int j = 0; j < i; ++j)
+                {
+                  R dd[DIM];
+#pragma unroll
+                  for (int d = 0; d < DIM; ++d)
+                    dd[d] = geta[i][d] - geta[j][d];
+                  const R f  = unit_vector_filter_2<DIM>(dd);
+                  const R pe = eta[i] * eta[j];
+                  s1 += pe;
+                  const R t = pe * f * dotv<DIM>(dd, gmu);
+#pragma unroll
+                  for (int d = 0; d < DIM; ++d)
+                    acc[d] -= t * dd[d];
+                }
+            const R m2 = R(2) * p.Mgb;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+              out[d] += m2 * (s1 * gmu[d] + acc[d]);
+          }
+      }
+  }
+
+  // ---------------------------------------------------------------------
+  // Jacobian flux of the c row: d/du [M grad mu] applied to (dc, grad dc,
+  // grad dmu, deta).  scalar: mobility.h:476-534, tensorial: mobility.h:808-916
+  template <int DIM, int G, bool TENS, typename R>
+  __device__ __forceinline__ void apply_M_derivative(const PhysR<R> &p, R c, const R (&gc)[DIM],
+                                                     const R (&gmu)[DIM], const R (&eta)[G], const R (*geta)[DIM],
+                                                     R dc, const R (&gdc)[DIM], const R (&gdmu)[DIM],
+                                                     const R (&deta)[G], R (&out)[DIM])
+  {
+    const R phi = phi_clamped(c);
+    const R omc = R(1) - c;
+    if constexpr (!TENS)
+      {
+        R eta_sum = R(0), eta_ij = R(0);
+#pragma unroll
+        for (int i = 0; i < G; ++i)
+          {
+            eta_sum += eta[i];
+#pragma unroll
+            for (int j = 0; j < i; ++j)
+              eta_ij += eta[i] * eta[j];
+          }
+        const R M = p.Mvol * phi + p.Mvap * (R(1) - phi) + p.Msurf * R(4) * c * c * omc * omc + (R(2) * p.Mgb) * eta_ij;
+        const R dphidc = R(30) * c * c * omc * omc;
+        const R dMdc   = p.Mvol * dphidc - p.Mvap * dphidc + p.Msurf * R(8) * c * (R(1) - R(3) * c + R(2) * c * c);
+        R       factor = R(0);
+#pragma unroll
+        for (int i = 0; i < G; ++i)
+          factor += (eta_sum - eta[i]) * deta[i];
+        const R k = dMdc * dc + (R(2) * p.Mgb) * factor;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          out[d] = M * gdmu[d] + k * gmu[d];
+      }
+    else
+      {
+        R nc[DIM], nrm;
+        unit_vector<DIM>(gc, nc, nrm);
+        const R c2 = R(4) * c * c * omc * omc; // 4 c^2 (1-c)^2
+        // 1) M
+        const R fvv   = p.Mvol * phi + p.Mvap * (R(1) - phi);
+        const R fsurf = p.Msurf * c2;
+        const R nc_gdmu = dotv<DIM>(nc, gdmu);
+        const R nc_gmu  = dotv<DIM>(nc, gmu);
+        // 2) dM/dc (hpsint uses dphidc = 30 * 4 c^2 (1-c)^2 here, mobility.h:852-854)
+        const R fvv2  = (p.Mvol - p.Mvap) * (R(30) * c2);
+        R       dfs   = p.Msurf * R(8) * c * omc * (R(1) - R(2) * c);
+        dfs           = fsurf < R(1e-6) ? R(0) : dfs;
+        // 3) dM/dgrad c
+        const R fs3   = fsurf < R(1e-6) ? R(0) : fsurf;
+        const R nrm3  = nrm < R(1e-4) ? R(1) : nrm;
+        const R nc_gdc = dotv<DIM>(nc, gdc);
+        R       temp[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          temp[d] = gdc[d] - nc[d] * nc_gdc;
+        const R gmu_temp = dotv<DIM>(gmu, temp);
+        const R k3       = -fs3 / nrm3;
+        const R a2       = (fvv2 + dfs * R(1.001)) * dc;
+        const R b2       = dfs * nc_gmu * dc;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          out[d] = (fvv + fsurf) * gdmu[d] - nc[d] * (fsurf * nc_gdmu) + a2 * gmu[d] - nc[d] * b2 +
+                   k3 * (nc_gmu * temp[d] + nc[d] * gmu_temp);
+        if constexpr (G > 1)
+          {
+            // 4) sum_{i>j} [ eta_i eta_j P_ij grad dmu + (eta_j deta_i + eta_i deta_j) P_ij grad mu ]
+            //    with P_ij = I - f_ij d_ij d_ij^T, d_ij = grad eta_i - grad eta_j
+            R s1 = R(0), s2 = R(0), acc[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+              acc[d] = R(0);
+#pragma unroll
+            for (int i = 0; i < G; ++i)
+#pragma unroll
+              for (int j = 0; j < i; ++j)
+                {
+                  R dd[DIM];
+#pragma unroll
+                  for (int d = 0; d < DIM; ++d)
+                    dd[d] = geta[i][d] - geta[j][d];
+                  const R f  = unit_vector_filter_2<DIM>(dd);
+                  const R p1 = eta[i] * eta[j];
+                  const R p2 = eta[j] * deta[i] + eta[i] * deta[j];
+                  s1 += p1;
+                  s2 += p2;
+                  const R t = f * (p1 * dotv<DIM>(dd, gdmu) + p2 * dotv<DIM>(dd, gmu));
+#pragma unroll
+                  for (int d = 0; d < DIM; ++d)
+                    acc[d] -= t * dd[d];
+                }
+            const R m2 = R(2) * p.Mgb;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+              out[d] += m2 * (s1 * gdmu[d] + s2 * gmu[d] + acc[d]);
+          }
+      }
+  }
+
+  // ---------------------------------------------------------------------
+  // dM/dc applied to grad mu (a vector): scalar mobility.h:378-394,
+  // tensorial mobility.h:668-696.  Used by the Cahn-Hilliard block tangent.
+  template <int DIM, bool TENS, typename R>
+  __device__ __forceinline__ void dM_dc_times(const PhysR<R> &p, R c, const R (&gc)[DIM], const R (&v)[DIM],
+                                              R (&out)[DIM])
+  {
+    const R omc = R(1) - c;
+    if constexpr (!TENS)
+      {
+        const R dphidc = R(30) * c * c * omc * omc;
+        const R dMdc   = p.Mvol * dphidc - p.Mvap * dphidc + p.Msurf * R(8) * c * (R(1) - R(3) * c + R(2) * c * c);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          out[d] = dMdc * v[d];
+      }
+    else
+      {
+        const R c2     = R(4) * c * c * omc * omc;
+        const R dphidc = R(30) * c2;
+        const R fsurf  = p.Msurf * c2;
+        R       dfs    = p.Msurf * R(8) * c * omc * (R(1) - R(2) * c);
+        dfs            = fsurf < R(1e-6) ? R(0) : dfs;
+        R nc[DIM], nrm;
+        unit_vector<DIM>(gc, nc, nrm);
+        const R ncv = dotv<DIM>(nc, v);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          out[d] = (p.Mvol - p.Mvap) * dphidc * v[d] + dfs * (R(1.001) * v[d] - nc[d] * ncv);
+      }
+  }
+
+  // dM/d(grad c) as a DIM x DIM matrix K (row-major): tensorial
+  // mobility.h:700-721, zero for scalar mobility (mobility.h:399-409).
+  template <int DIM, bool TENS, typename R>
+  __device__ __forceinline__ void dM_dgrad_c(const PhysR<R> &p, R c, const R (&gc)[DIM], const R (&gmu)[DIM],
+                                             R (&K)[DIM][DIM])
+  {
+    if constexpr (!TENS)
+      {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b)
+            K[a][b] = R(0);
+      }
+    else
+      {
+        R fsurf = p.Msurf * R(4) * (c * c) * ((R(1) - c) * (R(1) - c));
+        R nc[DIM], nrm;
+        unit_vector<DIM>(gc, nc, nrm);
+        fsurf         = fsurf < R(1e-6) ? R(0) : fsurf;
+        const R nrm3  = nrm < R(1e-4) ? R(1) : nrm;
+        const R ncmu  = dotv<DIM>(nc, gmu);
+        // T = -fsurf (ncmu I + nc mu^T),  M = (I - nc nc^T) / nrm,  K = T M
+        R Tm[DIM][DIM], Mm[DIM][DIM];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b)
+            {
+              Tm[a][b] = -fsurf * ((a == b ? ncmu : R(0)) + nc[a] * gmu[b]);
+              Mm[a][b] = ((a == b ? R(1) : R(0)) - nc[a] * nc[b]) * (R(1) / nrm3);
+            }
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+#pragma unroll
+          for (int b = 0; b < DIM; ++b)
+            {
+              R s = R(0);
+#pragma unroll
+              for (int e = 0; e < DIM; ++e)
+                s += Tm[a][e] * Mm[e][b];
+              K[a][b] = s;
+            }
+      }
+  }
+} // namespace sint

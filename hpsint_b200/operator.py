@@ -1,0 +1,294 @@
+"""Host-side mirror of hpsint's sintering operator interface over the C ABI.
+
+Class and method names follow the reference so that driver code reads the same:
+  SinteringOperatorGeneric   applications/sintering/include/pf-applications/sintering/
+                             operator_sintering_generic.h:323-1085
+  BlockPreconditioner2       sintering/preconditioners.h:978-1343
+  DampedNewtonSolver         include/pf-applications/lac/solvers_nonlinear.h:236-394
+  bdf_weights                include/pf-applications/time_integration/time_schemes.h:64-153
+
+Block vectors are torch CUDA tensors of shape (C, block_stride): torch only
+provides device memory and the current stream; all arithmetic runs in the
+library's CUDA kernels.
+"""
+import ctypes
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib as L
+
+
+@dataclass
+class Mesh:
+    """Uniform Cartesian mesh: n_cells cells of size h per direction."""
+    dim: int
+    n_cells: tuple
+    h: tuple = (1.0, 1.0, 1.0)
+    origin: tuple = (0.0, 0.0, 0.0)
+
+    def to_c(self):
+        m = L.SintMesh()
+        m.dim = self.dim
+        for d in range(3):
+            m.n_cells[d] = int(self.n_cells[d]) if d < self.dim else 1
+            m.h[d] = float(self.h[d]) if d < self.dim else 1.0
+            m.origin[d] = float(self.origin[d]) if d < self.dim else 0.0
+        return m
+
+    @property
+    def n_nodes(self):
+        n = 1
+        for d in range(self.dim):
+            n *= int(self.n_cells[d]) + 1
+        return n
+
+    @property
+    def node_shape(self):
+        """(nz, ny, nx) node counts, the numpy shape of one block in C order."""
+        s = [int(self.n_cells[d]) + 1 for d in range(self.dim)]
+        return tuple(reversed(s))
+
+
+@dataclass
+class Params:
+    """Model parameters; defaults are hpsint's EnergyAbstractData/MobilityAbstractData
+    (sintering/parameters.h:113-134)."""
+    n_grains: int
+    A: float = 16.0
+    B: float = 1.0
+    kappa_c: float = 1.0
+    kappa_p: float = 0.5
+    Mvol: float = 1e-2
+    Mvap: float = 1e-10
+    Msurf: float = 4.0
+    Mgb: float = 0.4
+    L: float = 1.0
+    tensorial: bool = True
+
+    def to_c(self):
+        return L.SintParams(self.n_grains, self.A, self.B, self.kappa_c, self.kappa_p, self.Mvol, self.Mvap,
+                            self.Msurf, self.Mgb, self.L, int(bool(self.tensorial)))
+
+
+def bdf_weights(order, dt):
+    """BDF{1,2,3}Scheme::compute_weights (time_schemes.h:64-153) with the
+    effective-order fallback; dt = [dt_n, dt_{n-1}, ...].  Returns w[0..order]."""
+    dt = list(dt)
+    eff = sum(1 for v in dt[:order] if v > 0)
+    w = [0.0] * (len(dt) + 1)
+    if eff >= 3 and order >= 3:
+        w[1] = -(dt[0] + dt[1]) * (dt[0] + dt[1] + dt[2]) / (dt[0] * dt[1] * (dt[1] + dt[2]))
+        w[2] = dt[0] * (dt[0] + dt[1] + dt[2]) / (dt[1] * dt[2] * (dt[0] + dt[1]))
+        w[3] = -dt[0] * (dt[0] + dt[1]) / (dt[2] * (dt[1] + dt[2]) * (dt[0] + dt[1] + dt[2]))
+        w[0] = -(w[1] + w[2] + w[3])
+    elif eff >= 2 and order >= 2:
+        w[0] = (2 * dt[0] + dt[1]) / (dt[0] * (dt[0] + dt[1]))
+        w[1] = -(dt[0] + dt[1]) / (dt[0] * dt[1])
+        w[2] = dt[0] / (dt[1] * (dt[0] + dt[1]))
+    else:
+        w[0] = 1.0 / dt[0]
+        w[1] = -1.0 / dt[0]
+    return w
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class SinteringOperatorGeneric:
+    """Matrix-free sintering operator on the GPU (one CUDA context per instance)."""
+
+    op_components_offset = 2
+
+    def __init__(self, mesh: Mesh, params: Params):
+        if not torch.cuda.is_available():
+            raise RuntimeError("SinteringOperatorGeneric needs a CUDA device")
+        self.mesh, self.params = mesh, params
+        lib = L.lib()
+        handle = ctypes.c_void_p()
+        L.check(lib.sint_create(ctypes.byref(mesh.to_c()), ctypes.byref(params.to_c()), ctypes.byref(handle)),
+                "sint_create")
+        self._h = handle
+        n, c, ld = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int64()
+        L.check(lib.sint_dof_layout(self._h, ctypes.byref(n), ctypes.byref(c), ctypes.byref(ld)), "sint_dof_layout")
+        self.N, self.C, self.ld = n.value, c.value, ld.value
+        self.order = 0
+
+    @classmethod
+    def create(cls, mesh, params):
+        return cls(mesh, params)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                L.lib().sint_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # --- reference interface ------------------------------------------------
+    def n_components(self):
+        return self.C
+
+    def n_grains(self):
+        return self.C - 2
+
+    def equation_type(self, component):
+        """operator_sintering_generic.h:634-639: mu is stationary."""
+        return "Stationary" if component == 1 else "TimeDependent"
+
+    def initialize_dof_vector(self, dtype=torch.float64):
+        return torch.zeros((self.C, self.ld), dtype=dtype, device="cuda")
+
+    def set_time_weights(self, w0, w_hist=(), w_alg=1.0):
+        arr = (ctypes.c_double * max(1, len(w_hist)))(*w_hist)
+        L.check(L.lib().sint_set_time_weights(self._h, float(w0), arr, len(w_hist), float(w_alg)),
+                "sint_set_time_weights")
+        self.order = len(w_hist)
+
+    def set_mobility(self, Mvol, Mvap, Msurf, Mgb, L_):
+        L.check(L.lib().sint_set_mobility(self._h, Mvol, Mvap, Msurf, Mgb, L_), "sint_set_mobility")
+
+    def fill_quadrature_point_values(self, src):
+        """Linearisation point (operator_sintering_data.h:300-409)."""
+        self._check_vec(src, torch.float64)
+        L.check(L.lib().sint_set_linearization_point(self._h, _ptr(src), _stream()), "sint_set_linearization_point")
+
+    set_linearization_point = fill_quadrature_point_values
+
+    def evaluate_nonlinear_residual(self, dst, src, with_time_derivative=2, history=()):
+        self._check_vec(dst, torch.float64)
+        self._check_vec(src, torch.float64)
+        hist = list(history)
+        for h in hist:
+            self._check_vec(h, torch.float64)
+        arr = (ctypes.c_void_p * max(1, len(hist)))(*[h.data_ptr() for h in hist])
+        L.check(L.lib().sint_residual_f64(self._h, _ptr(dst), _ptr(src), arr, int(with_time_derivative), _stream()),
+                "sint_residual_f64")
+
+    def vmult(self, dst, src):
+        if src.dtype == torch.float32:
+            self._check_vec(dst, torch.float32)
+            self._check_vec(src, torch.float32)
+            L.check(L.lib().sint_jvp_f32(self._h, _ptr(dst), _ptr(src), _stream()), "sint_jvp_f32")
+        else:
+            self._check_vec(dst, torch.float64)
+            self._check_vec(src, torch.float64)
+            L.check(L.lib().sint_jvp_f64(self._h, _ptr(dst), _ptr(src), _stream()), "sint_jvp_f64")
+
+    def do_update(self):
+        pass
+
+    def clear(self):
+        pass
+
+    # --- helpers --------------------------------------------------------------
+    def _check_vec(self, t, dtype):
+        if not (t.is_cuda and t.dtype == dtype and t.is_contiguous() and t.numel() == self.C * self.ld):
+            raise ValueError(f"expected a contiguous CUDA {dtype} block vector of shape ({self.C}, {self.ld})")
+
+    def to_device(self, arr_cn, dtype=torch.float64):
+        """(C, N) array-like -> (C, ld) device block vector (padding zero)."""
+        v = self.initialize_dof_vector(dtype)
+        v[:, :self.N] = torch.as_tensor(arr_cn, dtype=dtype).reshape(self.C, self.N).to("cuda")
+        return v
+
+    def to_host(self, v):
+        return v[:, :self.N].double().cpu().numpy()
+
+
+class BlockPreconditioner2:
+    """z = P^-1 r with CH 2x2 node-block Jacobi and AC point Jacobi (FP64 and FP32)."""
+
+    def __init__(self, op: SinteringOperatorGeneric):
+        self.op = op
+
+    def do_update(self):
+        L.check(L.lib().sint_precond_setup(self.op._h, _stream()), "sint_precond_setup")
+
+    def vmult(self, dst, src):
+        op = self.op
+        if src.dtype == torch.float32:
+            L.check(L.lib().sint_precond_apply_f32(op._h, _ptr(dst), _ptr(src), _stream()), "sint_precond_apply_f32")
+        else:
+            L.check(L.lib().sint_precond_apply_f64(op._h, _ptr(dst), _ptr(src), _stream()), "sint_precond_apply_f64")
+
+    def inverse_diagonal(self):
+        G = self.op.n_grains()
+        out = torch.zeros((G, self.op.ld), dtype=torch.float64, device="cuda")
+        L.check(L.lib().sint_ac_inverse_diagonal_f64(self.op._h, _ptr(out), _stream()), "sint_ac_inverse_diagonal_f64")
+        return out
+
+    def ch_blocks(self):
+        out = torch.zeros((4, self.op.ld), dtype=torch.float64, device="cuda")
+        L.check(L.lib().sint_ch_blocks_f64(self.op._h, _ptr(out), _stream()), "sint_ch_blocks_f64")
+        return out
+
+    def clear(self):
+        pass
+
+
+@dataclass
+class NonLinearData:
+    """lac/solvers_nonlinear_parameters.h:40-60 (+ GMRES restart and inner precision)."""
+    nl_max_iter: int = 10
+    nl_abs_tol: float = 1e-20
+    nl_rel_tol: float = 1e-5
+    l_max_iter: int = 1000
+    l_abs_tol: float = 1e-10
+    l_rel_tol: float = 1e-2
+    gmres_restart: int = 30
+    threshold_newton_iter: int = 100
+    threshold_linear_iter: int = 20
+    use_damping: bool = True
+    reuse_preconditioner: bool = True
+    inner_precision: int = 64
+
+    def to_c(self):
+        return L.SintNewtonParams(self.nl_max_iter, self.nl_abs_tol, self.nl_rel_tol, self.l_max_iter,
+                                  self.l_abs_tol, self.l_rel_tol, self.gmres_restart, self.threshold_newton_iter,
+                                  self.threshold_linear_iter, int(self.use_damping), int(self.reuse_preconditioner),
+                                  self.inner_precision)
+
+
+@dataclass
+class NewtonStatistics:
+    newton_iterations: int = 0
+    linear_iterations: int = 0
+    residual_evaluations: int = 0
+    jacobian_setups: int = 0
+    preconditioner_setups: int = 0
+    initial_residual: float = 0.0
+    final_residual: float = 0.0
+    status: int = 0
+
+
+class DampedNewtonSolver:
+    """Device damped Newton-GMRES for R(u) = 0 (time weights set on the operator)."""
+
+    def __init__(self, op: SinteringOperatorGeneric, data: NonLinearData = None):
+        self.op = op
+        self.data = data or NonLinearData()
+
+    def solve(self, u, history, raise_on_failure=True):
+        op = self.op
+        op._check_vec(u, torch.float64)
+        arr = (ctypes.c_void_p * max(1, len(history)))(*[h.data_ptr() for h in history])
+        st = L.SintNewtonStats()
+        prm = self.data.to_c()
+        rc = L.lib().sint_newton_solve(op._h, _ptr(u), arr, ctypes.byref(prm), ctypes.byref(st), _stream())
+        stats = NewtonStatistics(st.newton_iterations, st.linear_iterations, st.residual_evaluations,
+                                 st.jacobian_setups, st.preconditioner_setups, st.initial_residual,
+                                 st.final_residual, rc)
+        if rc != L.SINT_OK and raise_on_failure:
+            L.check(rc, "sint_newton_solve")
+        return stats
+
+    def clear(self):
+        L.check(L.lib().sint_newton_clear(self.op._h), "sint_newton_clear")

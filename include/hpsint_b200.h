@@ -1,0 +1,239 @@
+/*
+ * hpsint_b200: B200-native matrix-free sintering operator (C ABI).
+ *
+ * The operator is hpsint's coupled Cahn-Hilliard / Allen-Cahn system in
+ * (c, mu, eta_1 .. eta_G) on uniform Cartesian Q1 meshes (2D quads, 3D hexes),
+ * QGauss(2) quadrature, Wang bulk free energy, scalar or tensorial
+ * volume/vapour/surface/grain-boundary mobility.
+ *
+ * Conventions shared by every entry point
+ *   - All vector pointers are DEVICE pointers owned by the caller.
+ *   - A block vector ("DoF vector") holds C = G + 2 blocks; block b starts at
+ *     element b * block_stride and holds the N nodal values of component b
+ *     (c, mu, eta_1, .., eta_G) in lexicographic node order: x fastest, then y,
+ *     then z.  sint_dof_layout() reports N, C and block_stride; entries
+ *     between N and block_stride are never read and are written as zero by the
+ *     BLAS-1 routines only.  Device pointers must be 16-byte aligned.
+ *   - Every call is asynchronous on `stream` (a cudaStream_t; NULL = legacy
+ *     default stream) unless it says otherwise.
+ *   - Every call returns a sint_status; no C++ exception crosses the ABI.
+ *   - A context is not re-entrant: calls on one context must not overlap
+ *     (the reference operator is single-threaded per MPI rank as well).
+ */
+#ifndef HPSINT_B200_H
+#define HPSINT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SINT_MAX_GRAINS 12
+#define SINT_ABI_VERSION 1
+
+typedef struct CUstream_st *sint_stream_t; /* identical to cudaStream_t */
+typedef struct sint_ctx     sint_ctx;
+
+typedef enum
+{
+  SINT_OK                 = 0,
+  SINT_ERR_ARG            = 1, /* null pointer, bad size or misaligned pointer */
+  SINT_ERR_GRAINS         = 2, /* n_grains outside [1, SINT_MAX_GRAINS];
+                                  instantiation.h:61-68 ExcInvalidNumberOfComponents */
+  SINT_ERR_CUDA           = 3, /* a CUDA runtime call failed; see sint_last_error() */
+  SINT_ERR_NOT_READY      = 4, /* e.g. vmult before a linearisation point was set */
+  SINT_ERR_NO_CONVERGENCE = 5, /* linear solver did not converge:
+                                  deal.II SolverControl::NoConvergence */
+  SINT_ERR_NEWTON         = 6, /* damped Newton failed: solvers_nonlinear.h:183-206
+                                  ExcNewtonDidNotConverge ("Newton" or "damping") */
+  SINT_ERR_NONFINITE      = 7, /* NaN/Inf in a residual norm */
+  SINT_ERR_DT_MIN         = 8  /* time step fell below the minimum (driver.h:2189-2191) */
+} sint_status;
+
+/* Uniform Cartesian mesh: n_cells[d] cells of size h[d] in direction d
+ * (entries d >= dim are ignored).  Replaces the reference's
+ * create_mesh_from_divisions / subdivided_hyper_rectangle
+ * (include/pf-applications/grid/grid_tools.h:698-719) with no constraints. */
+typedef struct
+{
+  int    dim;
+  int    n_cells[3];
+  double h[3];
+  double origin[3];
+} sint_mesh;
+
+/* Model parameters.  A, B: FreeEnergy(A, B) (sintering/free_energy.h:187-190);
+ * kappa_c, kappa_p: SinteringOperatorData (operator_sintering_data.h:51-62);
+ * Mvol..L: ProviderAbstract (mobility.h:45-76); tensorial selects
+ * MobilityTensorial instead of MobilityScalar (operator_sintering_data.h:38-49). */
+typedef struct
+{
+  int    n_grains;
+  double A, B;
+  double kappa_c, kappa_p;
+  double Mvol, Mvap, Msurf, Mgb, L;
+  int    tensorial;
+} sint_params;
+
+/* ---------------------------------------------------------------------- */
+/* Operator: SinteringOperatorGeneric                                      */
+/* (applications/sintering/include/pf-applications/sintering/              */
+/*  operator_sintering_generic.h:323-1085)                                 */
+
+/* SinteringOperatorGeneric::create (operator_sintering_generic.h:369-391),
+ * with the MatrixFree set-up for the uniform mesh. */
+int sint_create(const sint_mesh *mesh, const sint_params *params, sint_ctx **ctx);
+
+/* Releases every device buffer owned by the context (synchronises first). */
+int sint_destroy(sint_ctx *ctx);
+
+/* OperatorBase::initialize_dof_vector (sintering/operator_base.h:143-149):
+ * reports the block-vector layout the operator expects. */
+int sint_dof_layout(const sint_ctx *ctx, int64_t *n_nodes, int *n_components, int64_t *block_stride);
+
+/* TimeIntegratorData weights (time_integration/time_integrator_data.h:150-163):
+ * w0 = primary weight, w_hist[0..order-1] = weights[1..order] applied to the old
+ * solutions, w_alg = algebraic weight of the mu row (1 for implicit schemes).
+ * order <= 3 (BDF1..BDF3, time_schemes.h:64-153). */
+int sint_set_time_weights(sint_ctx *ctx, double w0, const double *w_hist, int order, double w_alg);
+
+/* Mobility::update (sintering/mobility.h:224-234): new mobility coefficients,
+ * e.g. from ProviderRealistic at the new time. */
+int sint_set_mobility(sint_ctx *ctx, double Mvol, double Mvap, double Msurf, double Mgb, double L);
+
+/* SinteringOperatorData::fill_quadrature_point_values
+ * (sintering/operator_sintering_data.h:300-409).  Instead of caching values
+ * and gradients at quadrature points, the context copies the nodal state u
+ * (C blocks) and an FP32 shadow of it; both are re-evaluated on the fly. */
+int sint_set_linearization_point(sint_ctx *ctx, const double *u, sint_stream_t stream);
+
+/* SinteringOperatorGeneric::evaluate_nonlinear_residual<with_time_derivative>
+ * (operator_sintering_generic.h:393-448): dst = R(src).  with_time_derivative:
+ * 0 drops the time terms, 1 keeps w0*u only, 2 adds the BDF history
+ * sum_i w_hist[i] * hist[i].  hist is a HOST array of `order` device pointers
+ * to old solutions (SolutionHistory::get_old_solutions); ignored unless
+ * with_time_derivative == 2.  dst is overwritten. */
+int sint_residual_f64(sint_ctx *ctx, double *dst, const double *src, const double *const *hist,
+                      int with_time_derivative, sint_stream_t stream);
+
+/* OperatorBase::vmult -> SinteringOperatorGeneric::vmult_internal
+ * (operator_base.h:294-353, operator_sintering_generic.h:539-606):
+ * dst = J(u_lin) src in FP64.  dst is overwritten. */
+int sint_jvp_f64(sint_ctx *ctx, double *dst, const double *src, sint_stream_t stream);
+
+/* Same product in FP32 with FP32 accumulation, linearised at the FP32 shadow. */
+int sint_jvp_f32(sint_ctx *ctx, float *dst, const float *src, sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* Preconditioner: BlockPreconditioner2 (sintering/preconditioners.h:978-1343) */
+
+/* BlockPreconditioner2::do_update (preconditioners.h:1260-1283) at the current
+ * linearisation point.  Block 0 (c, mu): the inverse of each node's 2x2
+ * diagonal block of the OperatorCahnHilliard tangent (preconditioners.h:85-169),
+ * a point-block Jacobi in the spirit of InverseComponentBlockDiagonalMatrix
+ * (lac/preconditioners.h:217-315) in place of the reference's ILU.
+ * Block 1 (eta): InverseDiagonalMatrix of OperatorAllenCahn
+ * (preconditioners.h:342-414, lac/preconditioners.h:159-213,
+ * operator_base.h:364-389).  Kept in FP64 and FP32. */
+int sint_precond_setup(sint_ctx *ctx, sint_stream_t stream);
+
+/* BlockPreconditioner2::vmult (preconditioners.h:1222-1258): z = P^-1 r. */
+int sint_precond_apply_f64(sint_ctx *ctx, double *z, const double *r, sint_stream_t stream);
+int sint_precond_apply_f32(sint_ctx *ctx, float *z, const float *r, sint_stream_t stream);
+
+/* OperatorBase::compute_inverse_diagonal of OperatorAllenCahn
+ * (operator_base.h:364-389): G blocks of block_stride, 1/d where |d| > 1e-10,
+ * else 1.  Requires sint_precond_setup first. */
+int sint_ac_inverse_diagonal_f64(sint_ctx *ctx, double *inv_diag, sint_stream_t stream);
+
+/* The assembled (not inverted) 2x2 node blocks of the Cahn-Hilliard tangent,
+ * 4 blocks of block_stride: J_cc, J_c,mu, J_mu,c, J_mu,mu (row = tested
+ * equation, column = unknown).  Requires sint_precond_setup first. */
+int sint_ch_blocks_f64(sint_ctx *ctx, double *blocks, sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* BLAS-1 on block vectors: DynamicBlockVector                              */
+/* (include/pf-applications/lac/dynamic_block_vector.h:346-516).            */
+/* n = number of elements (C * block_stride for a whole block vector).      */
+/* Reductions accumulate in FP64 and write one double to a DEVICE pointer;  */
+/* they use the context's reduction workspace (fixed block partials summed  */
+/* in a fixed order, so results are bitwise reproducible).                  */
+
+int sint_vec_axpy_f64(int64_t n, double a, const double *x, double *y, sint_stream_t stream); /* y += a x  (add) */
+int sint_vec_sadd_f64(int64_t n, double s, double a, const double *x, double *y,
+                      sint_stream_t stream);                                           /* y = s y + a x (sadd) */
+int sint_vec_scale_f64(int64_t n, double a, double *x, sint_stream_t stream);          /* x *= a */
+int sint_vec_dot_f64(sint_ctx *ctx, int64_t n, const double *x, const double *y, double *result,
+                     sint_stream_t stream);                                                    /* operator* */
+int sint_vec_norm2_f64(sint_ctx *ctx, int64_t n, const double *x, double *result, sint_stream_t stream); /* l2_norm */
+int sint_vec_axpy_f32(int64_t n, float a, const float *x, float *y, sint_stream_t stream);
+int sint_vec_dot_f32(sint_ctx *ctx, int64_t n, const float *x, const float *y, double *result, sint_stream_t stream);
+int sint_vec_norm2_f32(sint_ctx *ctx, int64_t n, const float *x, double *result, sint_stream_t stream);
+int sint_vec_f64_to_f32(int64_t n, const double *x, float *y, sint_stream_t stream);   /* FP32 shadow */
+int sint_vec_f32_to_f64(int64_t n, const float *x, double *y, sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* Nonlinear solve: DampedNewtonSolver (lac/solvers_nonlinear.h:236-394)     */
+/* with GMRES (lac/solvers_linear.h:57-117, deal.II SolverGMRES, classical  */
+/* Gram-Schmidt) and BlockPreconditioner2, all on the device.              */
+
+typedef struct
+{
+  /* NonLinearData (lac/solvers_nonlinear_parameters.h:40-60) */
+  int    nl_max_iter;          /* 10 */
+  double nl_abs_tol;           /* 1e-20 */
+  double nl_rel_tol;           /* 1e-5 */
+  int    l_max_iter;           /* 1000 */
+  double l_abs_tol;            /* 1e-10 */
+  double l_rel_tol;            /* 1e-2 */
+  int    gmres_restart;        /* 30 (deal.II max_n_tmp_vectors) */
+  int    threshold_newton_iter;/* 100: rebuild preconditioner every this many Newton its */
+  int    threshold_linear_iter;/* 20: ... or when the last solve took more linear its */
+  int    use_damping;          /* 1 */
+  int    reuse_preconditioner; /* 1 */
+  int    inner_precision;      /* 64: FP64 GMRES/Jacobian/preconditioner,
+                                  32: FP32 Arnoldi vectors, Jacobian and
+                                  preconditioner with FP64 dots and norms */
+} sint_newton_params;
+
+typedef struct
+{
+  int    newton_iterations;
+  int    linear_iterations;
+  int    residual_evaluations;
+  int    jacobian_setups;
+  int    preconditioner_setups;
+  double initial_residual;
+  double final_residual;
+} sint_newton_stats;
+
+/* Fills the reference defaults listed above. */
+void sint_newton_default_params(sint_newton_params *p);
+
+/* DampedNewtonSolver::clear (solvers_nonlinear.h:359-364): forgets the Newton
+ * and linear iteration history that decides when the preconditioner is rebuilt
+ * (the driver calls it after a failed step, driver.h:2193-2195). */
+int sint_newton_clear(sint_ctx *ctx);
+
+/* DampedNewtonSolver::solve (solvers_nonlinear.h:247-357) for R(u) = 0 with the
+ * time weights already set: u (device, C blocks) is the initial guess on entry
+ * and the solution on SINT_OK.  hist: HOST array of `order` device pointers
+ * (residual history term, with_time_derivative = 2).  On SINT_ERR_NEWTON or
+ * SINT_ERR_NO_CONVERGENCE u holds the last iterate.  Synchronises `stream`. */
+int sint_newton_solve(sint_ctx *ctx, double *u, const double *const *hist, const sint_newton_params *params,
+                      sint_newton_stats *stats, sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+
+/* Text of the last error recorded on this thread (never NULL). */
+const char *sint_last_error(void);
+
+/* Number of CUDA kernels this library has launched in this process. */
+int64_t sint_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPSINT_B200_H */
