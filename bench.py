@@ -275,6 +275,13 @@ def main():
     torch.cuda.synchronize()
     assert np.isfinite(h_dst[:, :op.N].numpy()).all()
 
+    # --- measured FMA throughput: denominator of the ALU roofline ---------------
+    fma = {}
+    for prec in (64, 32):
+        t = ctypes.c_double()
+        L.check(lib.sint_device_fma_peak(prec, ctypes.byref(t), sp), "sint_device_fma_peak")
+        fma[prec] = t.value
+
     # --- roofline of the dominant kernel (algorithmic bytes) ------------------
     peaks = {}
     try:
@@ -293,14 +300,18 @@ def main():
         return
 
     gdofs = lambda ms: dofs / (ms * 1e-3) / 1e9
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "jvp_traffic.json")
+    # per-launch DRAM traffic and executed FP64 operations of the FP64 J v kernel
+    # from one ncu capture of this workload (profiles/jvp_f64_counters.json)
+    traffic, flops = None, None
+    tf = os.path.join(ROOT, "profiles", "jvp_f64_counters.json")
     if os.path.exists(tf):
         try:
             t = json.load(open(tf))
-            traffic = t.get("bytes_per_launch_scaled_to_workload")
+            if t.get("workload") == WORKLOAD and t.get("mobility") == ("tensorial" if tensorial else "scalar"):
+                traffic = t.get("dram_bytes_per_launch")
+                flops = t.get("fp64_flops_per_launch")
         except Exception:
-            traffic = None
+            traffic, flops = None, None
     line = {
         "metric": METRIC,
         "value": gdofs(ms_jvp64) * world,
@@ -329,6 +340,11 @@ def main():
                      "frac": achieved / hbm_peak, "traffic": traffic,
                      "note": f"FP64 J v: algorithmic bytes 24*C*N = {alg_bytes/1e6:.1f} MB per launch; "
                              f"peak {peak_src}; kernel is FP64-ALU bound (on-the-fly linearisation)"},
+        "roofline_alu": {"bound": "fp64", "peak_fp64_tflops": fma[64], "peak_fp32_tflops": fma[32],
+                         "peak_note": "measured FMA-chain throughput on this GPU (sint_device_fma_peak)",
+                         "achieved_fp64_tflops": (flops / (ms_jvp64 * 1e-3) / 1e12) if flops else None,
+                         "frac": (flops / (ms_jvp64 * 1e-3) / 1e12 / fma[64]) if flops else None,
+                         "flops_source": "executed FP64 add/mul/fma (fma = 2) of one ncu capture" if flops else None},
         "e2e": {"value": gdofs(ms_e2e) * world, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes},
         "gpu_launches": int(launches),

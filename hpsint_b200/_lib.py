@@ -77,6 +77,7 @@ SIGNATURES = {
     "sint_newton_clear": (_c_int, [_c_void]),
     "sint_newton_solve": (_c_int, [_c_void, _c_void, P(_c_void), P(SintNewtonParams), P(SintNewtonStats),
                                    _c_void]),
+    "sint_device_fma_peak": (_c_int, [_c_int, P(_c_double), _c_void]),
     "sint_last_error": (ctypes.c_char_p, []),
     "sint_kernel_launch_count": (_c_int64, []),
 }

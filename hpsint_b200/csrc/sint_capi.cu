@@ -274,6 +274,23 @@ int sint_create(const sint_mesh *mesh, const sint_params *params, sint_ctx **out
     }
   g.N       = N;
   g.n_tiles = nt;
+  // exact Q1 element Laplacian of the uniform cell: K_lm = kx[l xor m], built
+  // from the 1D stiffness (1/h)[[1,-1],[-1,1]] and mass (h/6)[[2,1],[1,2]]
+  for (int x = 0; x < 8; ++x)
+    {
+      double k = 0.0;
+      if (x < (1 << mesh->dim))
+        for (int d = 0; d < mesh->dim; ++d)
+          {
+            double t = (((x >> d) & 1) ? -1.0 : 1.0) / g.h[d];
+            for (int e = 0; e < mesh->dim; ++e)
+              if (e != d)
+                t *= ((x >> e) & 1) ? g.h[e] / 6.0 : g.h[e] / 3.0;
+            k += t;
+          }
+      g.kxd[x] = k;
+      g.kxf[x] = float(k);
+    }
   g.ld      = (N + 31) / 32 * 32;
   c->N      = N;
   c->ld     = g.ld;

@@ -64,7 +64,24 @@ namespace sint
     long long ld;    // block stride of a DoF vector
     long long n_tiles;
     double    h[3];
+    // Exact element Laplacian of the uniform cell, K_lm = kx[l xor m]
+    // (kx[x] = int grad phi_l . grad phi_(l xor x)), in both precisions.
+    double kxd[8];
+    float  kxf[8];
   };
+
+  template <typename R>
+  __device__ __forceinline__ R kx(const Grid &g, int x);
+  template <>
+  __device__ __forceinline__ double kx<double>(const Grid &g, int x)
+  {
+    return g.kxd[x];
+  }
+  template <>
+  __device__ __forceinline__ float kx<float>(const Grid &g, int x)
+  {
+    return g.kxf[x];
+  }
 
   // Point-wise model parameters (FP64 on the host, cast per kernel).
   struct Phys
@@ -151,6 +168,8 @@ namespace sint
     R g1, g0;           // Q1 shape values at the Gauss points: phi_l(x_q) = (l == q) ? g1 : g0
     R JxW;
     int q;
+    // box offsets of the nodes l xor x of this lane's node l (stiffness stencil)
+    int koff[1 << DIM];
 
     __device__ __forceinline__ explicit QP(const Grid &g)
     {
@@ -171,6 +190,17 @@ namespace sint
           jxw *= 0.5 * g.h[d];
         }
       JxW = R(jxw);
+      using T = Tile<DIM>;
+      const int stride[3] = {1, T::BX, T::BX * T::BY};
+#pragma unroll
+      for (int x = 0; x < (1 << DIM); ++x)
+        {
+          int off = 0;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d)
+            off += (((q >> d) & 1) ^ ((x >> d) & 1)) * stride[d]; // bit d of node l xor x
+          koff[x] = off;
+        }
     }
   };
 
@@ -304,6 +334,30 @@ namespace sint
         const R r  = w.g1 * t + w.g0 * tp + w.sgn_ih[1] * (gy + gyp2);
         return r * w.JxW;
       }
+  }
+
+  // Value-only integration butterfly: sum_q JxW v_q phi_l(x_q).
+  template <int DIM, typename R>
+  __device__ __forceinline__ R integrate_value_butterfly(R v, const QP<DIM, R> &w)
+  {
+    constexpr unsigned FULL = 0xffffffffu;
+    R t = w.g1 * v + w.g0 * __shfl_xor_sync(FULL, v, 1);
+    t   = w.g1 * t + w.g0 * __shfl_xor_sync(FULL, t, 2);
+    if constexpr (DIM == 3)
+      t = w.g1 * t + w.g0 * __shfl_xor_sync(FULL, t, 4);
+    return t * w.JxW;
+  }
+
+  // (K u)_l for this lane's node l: the cell integral of grad phi_l . grad u_h,
+  // exact on the uniform cell (the 2-point Gauss rule integrates it exactly).
+  template <int DIM, typename R>
+  __device__ __forceinline__ R stiffness_apply(const R *s, int b0, const QP<DIM, R> &w, const Grid &g)
+  {
+    R acc = kx<R>(g, 0) * s[b0 + w.koff[0]];
+#pragma unroll
+    for (int x = 1; x < (1 << DIM); ++x)
+      acc += kx<R>(g, x) * s[b0 + w.koff[x]];
+    return acc;
   }
 
   // Step 5 of the data flow: sum the per-cell node contributions

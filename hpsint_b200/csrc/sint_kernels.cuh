@@ -7,13 +7,10 @@
 
 namespace sint
 {
-  // Integrate one residual row at this thread's point and park the cell's
-  // node contribution in shared memory (masked for cells outside the mesh).
+  // Park a lane's node contribution in shared memory (zero for cells outside the mesh).
   template <int DIM, typename R>
-  __device__ __forceinline__ void integrate_store(R *s_con, int comp, R v, const R (&g)[DIM], const QP<DIM, R> &w,
-                                                  bool valid)
+  __device__ __forceinline__ void store_contrib(R *s_con, int comp, R r, bool valid)
   {
-    const R r = integrate_butterfly<DIM>(v, g, w);
     s_con[comp * Tile<DIM>::THREADS + threadIdx.x] = valid ? r : R(0);
   }
 
@@ -22,6 +19,11 @@ namespace sint
   // SinteringOperatorGenericQuad::operator() (operator_sintering_generic.h:101-190)
   // inside do_vmult_range (:539-577).  The linearisation point is evaluated
   // from the nodal state instead of a quadrature-point cache.
+  //
+  // Only the c row has a point-dependent gradient flux (the mobility term); the
+  // mu and eta rows have constant-coefficient gradient terms (-kappa_c grad dc,
+  // L kappa_p grad deta), which are applied with the exact element stiffness
+  // stencil to the nodal values, so those rows only integrate point values.
   template <int DIM, int G, bool TENS, typename R>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS)
     jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
@@ -47,7 +49,10 @@ namespace sint
 
     // linearisation point at this quadrature point
     R c, gc[DIM], mu_unused, gmu[DIM];
-    eval_vg<DIM>(s_lin, b0, w, c, gc);
+    if constexpr (TENS)
+      eval_vg<DIM>(s_lin, b0, w, c, gc);
+    else
+      c = eval_v<DIM>(s_lin, b0, w);
     eval_vg<DIM>(s_lin + T::BOX, b0, w, mu_unused, gmu);
     R eta[G];
     R geta[TENS ? G : 1][DIM];
@@ -61,7 +66,10 @@ namespace sint
       }
     // direction
     R dc, gdc[DIM], dmu, gdmu[DIM];
-    eval_vg<DIM>(s_src, b0, w, dc, gdc);
+    if constexpr (TENS)
+      eval_vg<DIM>(s_src, b0, w, dc, gdc);
+    else
+      dc = eval_v<DIM>(s_src, b0, w);
     eval_vg<DIM>(s_src + T::BOX, b0, w, dmu, gdmu);
     R deta[G];
 #pragma unroll
@@ -81,21 +89,18 @@ namespace sint
     {
       R gres[DIM];
       apply_M_derivative<DIM, G, TENS>(p, c, gc, gmu, eta, geta, dc, gdc, gdmu, deta, gres);
-      integrate_store<DIM>(s_con, 0, dc * p.w0, gres, w, valid);
+      store_contrib<DIM>(s_con, 0, integrate_butterfly<DIM>(dc * p.w0, gres, w), valid);
     }
-    // 2) mu row (generic.h:138-146)
+    // 2) mu row (generic.h:138-146): value part + (-kappa_c) K dc
     {
       R v = p.walg * dmu - fcc * dc;
 #pragma unroll
       for (int i = 0; i < G; ++i)
         v -= B12 * eta[i] * (eta[i] - R(1)) * deta[i];
-      R gres[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        gres[d] = -p.kc * gdc[d];
-      integrate_store<DIM>(s_con, 1, v, gres, w, valid);
+      const R r = integrate_value_butterfly<DIM>(v, w) - p.kc * stiffness_apply<DIM>(s_src, b0, w, g);
+      store_contrib<DIM>(s_con, 1, r, valid);
     }
-    // 3) eta rows (generic.h:150-163, free_energy.h:233-252)
+    // 3) eta rows (generic.h:150-163, free_energy.h:233-252): value part + L kappa_p K deta_i
     {
       R S = R(0);
 #pragma unroll
@@ -106,18 +111,15 @@ namespace sint
 #pragma unroll
       for (int i = 0; i < G; ++i)
         {
-          const R e     = eta[i];
-          const R fce   = B12 * e * (e - R(1));
-          const R fee   = p.B * (R(12) - R(12) * c + R(2) * e * (R(12) * c - R(24)) + R(24) * (e * e) + R(12) * s2);
-          R       v     = deta[i] * p.w0 + p.L * (fce * dc + fee * deta[i]);
+          const R e   = eta[i];
+          const R fce = B12 * e * (e - R(1));
+          const R fee = p.B * (R(12) - R(12) * c + R(2) * e * (R(12) * c - R(24)) + R(24) * (e * e) + R(12) * s2);
+          R       v   = deta[i] * p.w0 + p.L * (fce * dc + fee * deta[i]);
           if constexpr (G > 1)
             v += cL24B * e * (S - e * deta[i]);
-          R vtmp, gd[DIM];
-          eval_vg<DIM>(s_src + (2 + i) * T::BOX, b0, w, vtmp, gd);
-#pragma unroll
-          for (int d = 0; d < DIM; ++d)
-            gd[d] *= Lkp;
-          integrate_store<DIM>(s_con, 2 + i, v, gd, w, valid);
+          const R r = integrate_value_butterfly<DIM>(v, w) +
+                      Lkp * stiffness_apply<DIM>(s_src + (2 + i) * T::BOX, b0, w, g);
+          store_contrib<DIM>(s_con, 2 + i, r, valid);
         }
     }
     __syncthreads();
@@ -127,7 +129,8 @@ namespace sint
   // -------------------------------------------------------------------------
   // Nonlinear residual: dst = R(src), SinteringOperatorGenericResidualQuad
   // (operator_sintering_generic.h:254-308) with the history of
-  // do_evalute_history (:927-975) for WTD == 2.
+  // do_evalute_history (:927-975) for WTD == 2.  As in the Jacobian, the mu and
+  // eta rows' constant-coefficient gradient terms use the stiffness stencil.
   template <int DIM, int G, bool TENS, int WTD>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS)
     residual_kernel(const Grid g, const Phys ph, const double *__restrict__ src, const double *__restrict__ h0,
@@ -153,7 +156,7 @@ namespace sint
             const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
             const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
             R         v  = R(0);
-            if (gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2])
+            if (comp != 1 && gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2])
               {
                 const long long off = comp * g.ld + node_index(g, gi, gj, gk);
                 v                   = h0[off] * ph.w_hist[0];
@@ -174,13 +177,21 @@ namespace sint
     const bool       valid = cell_in_mesh<DIM>(cell, tc, g);
 
     R c, gc[DIM], mu, gmu[DIM];
-    eval_vg<DIM>(s_u, b0, w, c, gc);
+    if constexpr (TENS)
+      eval_vg<DIM>(s_u, b0, w, c, gc);
+    else
+      c = eval_v<DIM>(s_u, b0, w);
     eval_vg<DIM>(s_u + T::BOX, b0, w, mu, gmu);
     R eta[G];
-    R geta[G][DIM];
+    R geta[TENS ? G : 1][DIM];
 #pragma unroll
     for (int i = 0; i < G; ++i)
-      eval_vg<DIM>(s_u + (2 + i) * T::BOX, b0, w, eta[i], geta[i]);
+      {
+        if constexpr (TENS)
+          eval_vg<DIM>(s_u + (2 + i) * T::BOX, b0, w, eta[i], geta[i]);
+        else
+          eta[i] = eval_v<DIM>(s_u + (2 + i) * T::BOX, b0, w);
+      }
 
     R s2 = R(0), s3 = R(0);
 #pragma unroll
@@ -200,19 +211,16 @@ namespace sint
         v += eval_v<DIM>(s_h, b0, w);
       R gres[DIM];
       apply_M<DIM, G, TENS>(p, c, eta, gc, geta, gmu, gres);
-      integrate_store<DIM>(s_con, 0, v, gres, w, valid);
+      store_contrib<DIM>(s_con, 0, integrate_butterfly<DIM>(v, gres, w), valid);
     }
-    // 2) mu row (generic.h:288-289, free_energy.h:124-134)
+    // 2) mu row (generic.h:288-289, free_energy.h:124-134): value part - kappa_c K c
     {
       const R df_dc = p.A * (c * c) * (R(2) * c - R(2)) + R(2) * p.A * c * (omc * omc) +
                       p.B * (R(2) * c - R(6) * s2 + R(4) * s3);
-      R gres[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        gres[d] = -p.kc * gc[d];
-      integrate_store<DIM>(s_con, 1, p.walg * mu - df_dc, gres, w, valid);
+      const R r = integrate_value_butterfly<DIM>(p.walg * mu - df_dc, w) - p.kc * stiffness_apply<DIM>(s_u, b0, w, g);
+      store_contrib<DIM>(s_con, 1, r, valid);
     }
-    // 3) eta rows (generic.h:293-304, free_energy.h:136-141)
+    // 3) eta rows (generic.h:293-304, free_energy.h:136-141): value part + L kappa_p K eta_i
     {
       const R Lkp = p.L * p.kp;
 #pragma unroll
@@ -224,11 +232,9 @@ namespace sint
             v += e * p.w0;
           if constexpr (WTD == 2)
             v += eval_v<DIM>(s_h + (2 + i) * T::BOX, b0, w);
-          R gres[DIM];
-#pragma unroll
-          for (int d = 0; d < DIM; ++d)
-            gres[d] = Lkp * geta[i][d];
-          integrate_store<DIM>(s_con, 2 + i, v, gres, w, valid);
+          const R r = integrate_value_butterfly<DIM>(v, w) +
+                      Lkp * stiffness_apply<DIM>(s_u + (2 + i) * T::BOX, b0, w, g);
+          store_contrib<DIM>(s_con, 2 + i, r, valid);
         }
     }
     __syncthreads();

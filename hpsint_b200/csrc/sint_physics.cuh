@@ -24,6 +24,71 @@ namespace sint
     return s;
   }
 
+  // Reciprocal and inverse square root of a positive number by Newton-Raphson
+  // refinement of a single-precision hardware seed (rcp.approx / rsqrt.approx,
+  // relative error ~2^-23):
+  //   reciprocal:          y <- y + y (1 - x y)
+  //   inverse square root: y <- y + (y / 2) (1 - x y^2)
+  // Each step squares the relative error: one step for float, two for double
+  // reach the rounding level.  Arguments outside [1e-30, 1e30] (never met by
+  // the squared gradient norms this is used for) take the IEEE operation.
+  __device__ __forceinline__ float rcp_seed(float x)
+  {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+  }
+  __device__ __forceinline__ float rsqrt_seed(float x)
+  {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+  }
+
+  template <typename R>
+  __device__ __forceinline__ R rcp_pos(R x);
+  template <>
+  __device__ __forceinline__ double rcp_pos<double>(double x)
+  {
+    if (!(x > 1e-30 && x < 1e30))
+      return 1.0 / x;
+    double y = double(rcp_seed(float(x)));
+    double e = fma(-x, y, 1.0);
+    y        = fma(y, e, y);
+    e        = fma(-x, y, 1.0);
+    return fma(y, e, y);
+  }
+  template <>
+  __device__ __forceinline__ float rcp_pos<float>(float x)
+  {
+    if (!(x > 1e-30f && x < 1e30f))
+      return 1.0f / x;
+    float y = rcp_seed(x);
+    return fmaf(y, fmaf(-x, y, 1.0f), y);
+  }
+
+  template <typename R>
+  __device__ __forceinline__ R rsqrt_pos(R x);
+  template <>
+  __device__ __forceinline__ double rsqrt_pos<double>(double x)
+  {
+    if (!(x > 1e-30 && x < 1e30))
+      return 1.0 / sqrt(x);
+    double y = double(rsqrt_seed(float(x)));
+    double r = fma(-x * y, y, 1.0);
+    y        = fma(0.5 * y, r, y);
+    r        = fma(-x * y, y, 1.0);
+    return fma(0.5 * y, r, y);
+  }
+  template <>
+  __device__ __forceinline__ float rsqrt_pos<float>(float x)
+  {
+    if (!(x > 1e-30f && x < 1e30f))
+      return 1.0f / sqrtf(x);
+    float y = rsqrt_seed(x);
+    return fmaf(0.5f * y, fmaf(-x * y, y, 1.0f), y);
+  }
+
   template <typename R>
   __device__ __forceinline__ R clamp01(R x)
   {
@@ -31,26 +96,26 @@ namespace sint
     return x > R(1) ? R(1) : x;
   }
 
-  // tensor.h:137-154; also returns |v|.
+  // tensor.h:137-154 unit_vector(v, 1e-10): v / |v| if |v| > 1e-10, else 0.
+  // Also returns n2 = |v|^2 and rs = 1 / |v| (0 below the threshold), which
+  // the dM/dgrad c term reuses.
   template <int D, typename R>
-  __device__ __forceinline__ void unit_vector(const R (&v)[D], R (&n)[D], R &nrm)
+  __device__ __forceinline__ void unit_vector(const R (&v)[D], R (&n)[D], R &n2, R &rs)
   {
-    nrm          = sqrt(dotv<D>(v, v));
-    const R tol  = R(1e-10);
-    const R fn   = nrm < tol ? R(1) : nrm;
-    const bool f = nrm > tol;
+    n2 = dotv<D>(v, v);
+    // |v| > 1e-10  <=>  |v|^2 > 1e-20
+    rs = n2 > R(1e-20) ? rsqrt_pos<R>(n2) : R(0);
 #pragma unroll
     for (int d = 0; d < D; ++d)
-      n[d] = f ? v[d] / fn : R(0);
+      n[d] = v[d] * rs;
   }
 
-  // tensor.h:156-174
+  // tensor.h:156-174 unit_vector_filter_2(v, 1e-20): 1 / |v|^2 or 0
   template <int D, typename R>
   __device__ __forceinline__ R unit_vector_filter_2(const R (&v)[D])
   {
-    const R n2  = dotv<D>(v, v);
-    const R tol = R(1e-20);
-    return n2 > tol ? R(1) / n2 : R(0);
+    const R n2 = dotv<D>(v, v);
+    return n2 > R(1e-20) ? rcp_pos<R>(n2) : R(0);
   }
 
   template <typename R>
@@ -85,8 +150,8 @@ namespace sint
       {
         const R fvv   = p.Mvol * phi + p.Mvap * (R(1) - phi);
         const R fsurf = p.Msurf * R(4) * (c * c) * ((R(1) - c) * (R(1) - c));
-        R       nc[DIM], nrm;
-        unit_vector<DIM>(gc, nc, nrm);
+        R       nc[DIM], n2, rs;
+        unit_vector<DIM>(gc, nc, n2, rs);
         const R a  = fvv + fsurf * R(1.001);
         const R b  = fsurf * dotv<DIM>(nc, gmu);
 #pragma unroll
@@ -160,8 +225,8 @@ namespace sint
       }
     else
       {
-        R nc[DIM], nrm;
-        unit_vector<DIM>(gc, nc, nrm);
+        R nc[DIM], n2, rs;
+        unit_vector<DIM>(gc, nc, n2, rs);
         const R c2 = R(4) * c * c * omc * omc; // 4 c^2 (1-c)^2
         // 1) M
         const R fvv   = p.Mvol * phi + p.Mvap * (R(1) - phi);
@@ -172,16 +237,16 @@ namespace sint
         const R fvv2  = (p.Mvol - p.Mvap) * (R(30) * c2);
         R       dfs   = p.Msurf * R(8) * c * omc * (R(1) - R(2) * c);
         dfs           = fsurf < R(1e-6) ? R(0) : dfs;
-        // 3) dM/dgrad c
+        // 3) dM/dgrad c; |grad c| < 1e-4 (|grad c|^2 < 1e-8) counts as 1
         const R fs3   = fsurf < R(1e-6) ? R(0) : fsurf;
-        const R nrm3  = nrm < R(1e-4) ? R(1) : nrm;
+        const R inrm3 = n2 < R(1e-8) ? R(1) : rs;
         const R nc_gdc = dotv<DIM>(nc, gdc);
         R       temp[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d)
           temp[d] = gdc[d] - nc[d] * nc_gdc;
         const R gmu_temp = dotv<DIM>(gmu, temp);
-        const R k3       = -fs3 / nrm3;
+        const R k3       = -fs3 * inrm3;
         const R a2       = (fvv2 + dfs * R(1.001)) * dc;
         const R b2       = dfs * nc_gmu * dc;
 #pragma unroll
@@ -246,8 +311,8 @@ namespace sint
         const R fsurf  = p.Msurf * c2;
         R       dfs    = p.Msurf * R(8) * c * omc * (R(1) - R(2) * c);
         dfs            = fsurf < R(1e-6) ? R(0) : dfs;
-        R nc[DIM], nrm;
-        unit_vector<DIM>(gc, nc, nrm);
+        R nc[DIM], n2, rs;
+        unit_vector<DIM>(gc, nc, n2, rs);
         const R ncv = dotv<DIM>(nc, v);
 #pragma unroll
         for (int d = 0; d < DIM; ++d)
@@ -272,10 +337,10 @@ namespace sint
     else
       {
         R fsurf = p.Msurf * R(4) * (c * c) * ((R(1) - c) * (R(1) - c));
-        R nc[DIM], nrm;
-        unit_vector<DIM>(gc, nc, nrm);
+        R nc[DIM], n2, rs;
+        unit_vector<DIM>(gc, nc, n2, rs);
         fsurf         = fsurf < R(1e-6) ? R(0) : fsurf;
-        const R nrm3  = nrm < R(1e-4) ? R(1) : nrm;
+        const R inrm3 = n2 < R(1e-8) ? R(1) : rs;
         const R ncmu  = dotv<DIM>(nc, gmu);
         // T = -fsurf (ncmu I + nc mu^T),  M = (I - nc nc^T) / nrm,  K = T M
         R Tm[DIM][DIM], Mm[DIM][DIM];
@@ -285,7 +350,7 @@ namespace sint
           for (int b = 0; b < DIM; ++b)
             {
               Tm[a][b] = -fsurf * ((a == b ? ncmu : R(0)) + nc[a] * gmu[b]);
-              Mm[a][b] = ((a == b ? R(1) : R(0)) - nc[a] * nc[b]) * (R(1) / nrm3);
+              Mm[a][b] = ((a == b ? R(1) : R(0)) - nc[a] * nc[b]) * inrm3;
             }
 #pragma unroll
         for (int a = 0; a < DIM; ++a)

@@ -226,6 +226,10 @@ int sint_newton_solve(sint_ctx *ctx, double *u, const double *const *hist, const
 
 /* ---------------------------------------------------------------------- */
 
+/* Measured FMA throughput of the current device in TFLOP/s (precision 64 or
+ * 32): the denominator of the cell kernels' ALU roofline.  Synchronous. */
+int sint_device_fma_peak(int precision, double *tflops, sint_stream_t stream);
+
 /* Text of the last error recorded on this thread (never NULL). */
 const char *sint_last_error(void);
 
