@@ -28,28 +28,24 @@ namespace sint
   size_t smem_jvp(int dim, int G, size_t rb)
   {
     const int C = G + 2;
-    return dim == 3 ? (2 * C * Tile<3>::BOX + C * Tile<3>::THREADS) * rb
-                    : (2 * C * Tile<2>::BOX + C * Tile<2>::THREADS) * rb;
+    return dim == 3 ? (2 * C * Tile<3>::BOX + C * Tile<3>::CS) * rb : (2 * C * Tile<2>::BOX + C * Tile<2>::CS) * rb;
   }
 
   size_t smem_residual(int dim, int G, int wtd)
   {
     const int C  = G + 2;
     const int nv = wtd == 2 ? 2 * C : C;
-    return dim == 3 ? (nv * Tile<3>::BOX + C * Tile<3>::THREADS) * sizeof(double)
-                    : (nv * Tile<2>::BOX + C * Tile<2>::THREADS) * sizeof(double);
+    return dim == 3 ? (nv * Tile<3>::BOX + C * Tile<3>::CS) * sizeof(double)
+                    : (nv * Tile<2>::BOX + C * Tile<2>::CS) * sizeof(double);
   }
 
   size_t smem_diag(int dim, int G)
   {
     const int C = G + 2;
+    // NCOEF = 2 dim^2 + dim + 1 + G coefficients per point, NOUT = G + 4 outputs
     if (dim == 3)
-      return (C * Tile<3>::BOX + (DiagLayout<3, 1, true>::NCOEF - 1 + G + DiagLayout<3, 1, true>::NOUT - 1 + G) *
-                                   Tile<3>::THREADS) *
-             sizeof(double);
-    return (C * Tile<2>::BOX +
-            (DiagLayout<2, 1, true>::NCOEF - 1 + G + DiagLayout<2, 1, true>::NOUT - 1 + G) * Tile<2>::THREADS) *
-           sizeof(double);
+      return (C * Tile<3>::BOX + (22 + G) * Tile<3>::THREADS + (G + 4) * Tile<3>::CS) * sizeof(double);
+    return (C * Tile<2>::BOX + (11 + G) * Tile<2>::THREADS + (G + 4) * Tile<2>::CS) * sizeof(double);
   }
 
   template <int DIM, typename R>

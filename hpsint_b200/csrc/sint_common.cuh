@@ -40,6 +40,12 @@ namespace sint
     static constexpr int BX      = TX + 1, BY = TY + 1, BZ = TZ + 1;
     static constexpr int BOX     = BX * BY * BZ;
     static constexpr int THREADS = CELLS * NQ;
+    // node contributions are parked as [comp][l][cell] with row pitch CP: the
+    // +2 makes both the write (lane = cell * 8 + l) and the per-node read
+    // (consecutive cells) free of shared-memory bank conflicts
+    static constexpr int CP = CELLS + 2;
+    static constexpr int CS = NQ * CP; // per component
+    static constexpr int NG = THREADS / BOX; // node-major phases: threads per box node
   };
 
   template <>
@@ -51,6 +57,9 @@ namespace sint
     static constexpr int BX      = TX + 1, BY = TY + 1, BZ = 1;
     static constexpr int BOX     = BX * BY;
     static constexpr int THREADS = CELLS * NQ;
+    static constexpr int CP      = CELLS + 4;
+    static constexpr int CS      = NQ * CP;
+    static constexpr int NG      = THREADS / BOX;
   };
 
   // Mesh description passed by value to every kernel.
@@ -135,25 +144,48 @@ namespace sint
     return (long long)i + (long long)g.nn[0] * ((long long)j + (long long)g.nn[1] * k);
   }
 
+  // Node-major view of the tile's node box for the load and store phases:
+  // thread t serves box node t % BOX and every NG-th component starting at
+  // t / BOX (threads with t / BOX >= NG idle), so the index arithmetic is done
+  // once per node.
+  template <int DIM>
+  struct BoxNode
+  {
+    int       b;      // box node index
+    int       grp;    // first component served
+    int       bx, by, bz;
+    bool      active; // thread serves a node
+    bool      inside; // node exists in the mesh
+    long long gidx;   // global node index (valid if inside)
+
+    __device__ __forceinline__ BoxNode(const Grid &g, const TileCoord &tc)
+    {
+      using T = Tile<DIM>;
+      b       = threadIdx.x % T::BOX;
+      grp     = threadIdx.x / T::BOX;
+      active  = grp < T::NG;
+      bx      = b % T::BX;
+      by      = (b / T::BX) % T::BY;
+      bz      = b / (T::BX * T::BY);
+      const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
+      inside       = gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2];
+      gidx         = inside ? node_index(g, gi, gj, gk) : 0;
+    }
+  };
+
   // Stage the node box of `ncomp` components of `src` (block stride g.ld) in
   // shared memory, layout s[comp * BOX + box_node]; nodes outside the mesh
   // read as zero.
   template <int DIM, typename R, typename S>
   __device__ __forceinline__ void load_box(R *s, const S *__restrict__ src, int ncomp, const Grid &g,
-                                           const TileCoord &tc)
+                                           const BoxNode<DIM> &bn)
   {
     using T = Tile<DIM>;
-    for (int idx = threadIdx.x; idx < ncomp * T::BOX; idx += T::THREADS)
-      {
-        const int comp = idx / T::BOX;
-        const int b    = idx - comp * T::BOX;
-        const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
-        const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
-        R v = R(0);
-        if (gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2])
-          v = R(src[comp * g.ld + node_index(g, gi, gj, gk)]);
-        s[idx] = v;
-      }
+    if (!bn.active)
+      return;
+    const S *p = src + bn.gidx;
+    for (int comp = bn.grp; comp < ncomp; comp += T::NG)
+      s[comp * T::BOX + bn.b] = bn.inside ? R(p[comp * g.ld]) : R(0);
   }
 
   // Per-thread quadrature constants.  Lane bits of (threadIdx.x % NQ) are the
@@ -361,38 +393,42 @@ namespace sint
   }
 
   // Step 5 of the data flow: sum the per-cell node contributions
-  // s_con[comp * THREADS + cell * NQ + l] of the tile per box node, write
-  // nodes owned by the tile to dst and the others to the tile's slot of the
-  // partial buffer (layout [tile][comp][BOX]).
+  // s_con[comp * CS + l * CP + cell] of the tile per box node (fixed order),
+  // write nodes owned by the tile to dst and the others to the tile's slot of
+  // the partial buffer (layout [tile][comp][BOX]).
   template <int DIM, typename R>
   __device__ __forceinline__ void sum_and_store(const R *s_con, int ncomp, const Grid &g, const TileCoord &tc,
-                                                R *__restrict__ dst, R *__restrict__ partial)
+                                                const BoxNode<DIM> &bn, R *__restrict__ dst, R *__restrict__ partial)
   {
     using T = Tile<DIM>;
-    for (int idx = threadIdx.x; idx < ncomp * T::BOX; idx += T::THREADS)
+    if (!bn.active || !bn.inside)
+      return;
+    // contributing (local node l, cell) pairs of this box node
+    int  src_off[T::NQ];
+    bool ok[T::NQ];
+#pragma unroll
+    for (int l = 0; l < T::NQ; ++l)
       {
-        const int comp = idx / T::BOX;
-        const int b    = idx - comp * T::BOX;
-        const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
-        const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
-        if (gi >= g.nn[0] || gj >= g.nn[1] || gk >= g.nn[2])
-          continue;
-        R sum = R(0);
+        const int cx = bn.bx - (l & 1), cy = bn.by - ((l >> 1) & 1), cz = (DIM == 3) ? bn.bz - ((l >> 2) & 1) : 0;
+        ok[l]      = cx >= 0 && cx < T::TX && cy >= 0 && cy < T::TY && cz >= 0 && cz < T::TZ;
+        src_off[l] = l * T::CP + (ok[l] ? cx + T::TX * (cy + T::TY * cz) : 0);
+      }
+    const int gi = tc.o[0] + bn.bx, gj = tc.o[1] + bn.by, gk = (DIM == 3) ? tc.o[2] + bn.bz : 0;
+    bool owned   = (bn.bx > 0 || gi == 0) && (bn.bx < T::TX || gi == g.n[0]) && (bn.by > 0 || gj == 0) &&
+                 (bn.by < T::TY || gj == g.n[1]);
+    if (DIM == 3)
+      owned = owned && (bn.bz > 0 || gk == 0) && (bn.bz < T::TZ || gk == g.n[2]);
+    R *out              = owned ? dst + bn.gidx : partial + tc.linear * ncomp * (long long)T::BOX + bn.b;
+    const long long ost = owned ? g.ld : (long long)T::BOX;
+    for (int comp = bn.grp; comp < ncomp; comp += T::NG)
+      {
+        const R *sc  = s_con + comp * T::CS;
+        R        sum = R(0);
 #pragma unroll
         for (int l = 0; l < T::NQ; ++l)
-          {
-            const int cx = bx - (l & 1), cy = by - ((l >> 1) & 1), cz = (DIM == 3) ? bz - ((l >> 2) & 1) : 0;
-            if (cx >= 0 && cx < T::TX && cy >= 0 && cy < T::TY && cz >= 0 && cz < T::TZ)
-              sum += s_con[comp * T::THREADS + (cx + T::TX * (cy + T::TY * cz)) * T::NQ + l];
-          }
-        bool owned = (bx > 0 || gi == 0) && (bx < T::TX || gi == g.n[0]) && (by > 0 || gj == 0) &&
-                     (by < T::TY || gj == g.n[1]);
-        if (DIM == 3)
-          owned = owned && (bz > 0 || gk == 0) && (bz < T::TZ || gk == g.n[2]);
-        if (owned)
-          dst[comp * g.ld + node_index(g, gi, gj, gk)] = sum;
-        else
-          partial[(tc.linear * ncomp + comp) * (long long)T::BOX + b] = sum;
+          if (ok[l])
+            sum += sc[src_off[l]];
+        out[comp * ost] = sum;
       }
   }
 

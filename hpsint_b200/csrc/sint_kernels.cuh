@@ -11,7 +11,8 @@ namespace sint
   template <int DIM, typename R>
   __device__ __forceinline__ void store_contrib(R *s_con, int comp, R r, bool valid)
   {
-    s_con[comp * Tile<DIM>::THREADS + threadIdx.x] = valid ? r : R(0);
+    using T = Tile<DIM>;
+    s_con[comp * T::CS + (threadIdx.x & (T::NQ - 1)) * T::CP + threadIdx.x / T::NQ] = valid ? r : R(0);
   }
 
   // -------------------------------------------------------------------------
@@ -36,9 +37,10 @@ namespace sint
     R *s_src = s_lin + C * T::BOX;
     R *s_con = s_src + C * T::BOX;
 
-    const TileCoord tc = tile_coord<DIM>(g);
-    load_box<DIM>(s_lin, lin, C, g, tc);
-    load_box<DIM>(s_src, src, C, g, tc);
+    const TileCoord    tc = tile_coord<DIM>(g);
+    const BoxNode<DIM> bn(g, tc);
+    load_box<DIM>(s_lin, lin, C, g, bn);
+    load_box<DIM>(s_src, src, C, g, bn);
     __syncthreads();
 
     const PhysR<R>   p(ph);
@@ -123,7 +125,7 @@ namespace sint
         }
     }
     __syncthreads();
-    sum_and_store<DIM>(s_con, C, g, tc, dst, partial);
+    sum_and_store<DIM>(s_con, C, g, tc, bn, dst, partial);
   }
 
   // -------------------------------------------------------------------------
@@ -145,28 +147,27 @@ namespace sint
     R *s_h   = s_u + C * T::BOX;
     R *s_con = s_h + (WTD == 2 ? C : 0) * T::BOX;
 
-    const TileCoord tc = tile_coord<DIM>(g);
-    load_box<DIM>(s_u, src, C, g, tc);
+    const TileCoord    tc = tile_coord<DIM>(g);
+    const BoxNode<DIM> bn(g, tc);
+    load_box<DIM>(s_u, src, C, g, bn);
     if constexpr (WTD == 2)
       {
-        // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966)
-        for (int idx = threadIdx.x; idx < C * T::BOX; idx += T::THREADS)
-          {
-            const int comp = idx / T::BOX, b = idx - comp * T::BOX;
-            const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
-            const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
-            R         v  = R(0);
-            if (comp != 1 && gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2])
-              {
-                const long long off = comp * g.ld + node_index(g, gi, gj, gk);
-                v                   = h0[off] * ph.w_hist[0];
-                if (ph.order > 1)
-                  v += h1[off] * ph.w_hist[1];
-                if (ph.order > 2)
-                  v += h2[off] * ph.w_hist[2];
-              }
-            s_h[idx] = v;
-          }
+        // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966); mu has no history
+        if (bn.active)
+          for (int comp = bn.grp; comp < C; comp += T::NG)
+            {
+              R v = R(0);
+              if (comp != 1 && bn.inside)
+                {
+                  const long long off = comp * g.ld + bn.gidx;
+                  v                   = h0[off] * ph.w_hist[0];
+                  if (ph.order > 1)
+                    v += h1[off] * ph.w_hist[1];
+                  if (ph.order > 2)
+                    v += h2[off] * ph.w_hist[2];
+                }
+              s_h[comp * T::BOX + bn.b] = v;
+            }
       }
     __syncthreads();
 
@@ -238,7 +239,7 @@ namespace sint
         }
     }
     __syncthreads();
-    sum_and_store<DIM>(s_con, C, g, tc, dst, partial);
+    sum_and_store<DIM>(s_con, C, g, tc, bn, dst, partial);
   }
 
   // -------------------------------------------------------------------------
@@ -269,10 +270,11 @@ namespace sint
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *s_lin  = reinterpret_cast<R *>(smem_raw);
     R *s_coef = s_lin + C * T::BOX;
-    R *s_con  = s_coef + LY::NCOEF * T::THREADS;
+    R *s_con  = s_coef + LY::NCOEF * T::THREADS; // NOUT * CS
 
-    const TileCoord tc = tile_coord<DIM>(g);
-    load_box<DIM>(s_lin, lin, C, g, tc);
+    const TileCoord    tc = tile_coord<DIM>(g);
+    const BoxNode<DIM> bn(g, tc);
+    load_box<DIM>(s_lin, lin, C, g, bn);
     __syncthreads();
 
     const PhysR<R>   p(ph);
@@ -389,9 +391,9 @@ namespace sint
         }
 #pragma unroll
       for (int k = 0; k < LY::NOUT; ++k)
-        s_con[k * T::THREADS + threadIdx.x] = valid ? acc[k] : R(0);
+        store_contrib<DIM>(s_con, k, acc[k], valid);
     }
     __syncthreads();
-    sum_and_store<DIM>(s_con, LY::NOUT, g, tc, dst, partial);
+    sum_and_store<DIM>(s_con, LY::NOUT, g, tc, bn, dst, partial);
   }
 } // namespace sint

@@ -30,8 +30,10 @@ namespace sint
   //   reciprocal:          y <- y + y (1 - x y)
   //   inverse square root: y <- y + (y / 2) (1 - x y^2)
   // Each step squares the relative error: one step for float, two for double
-  // reach the rounding level.  Arguments outside [1e-30, 1e30] (never met by
-  // the squared gradient norms this is used for) take the IEEE operation.
+  // reach the rounding level.  The seed is taken at the argument clamped to
+  // [1e-30, 1e30]; the squared gradient norms this is used for lie in
+  // (1e-20, 1e30) (callers filter the lower end), where the result is exact to
+  // rounding.
   __device__ __forceinline__ float rcp_seed(float x)
   {
     float y;
@@ -50,9 +52,7 @@ namespace sint
   template <>
   __device__ __forceinline__ double rcp_pos<double>(double x)
   {
-    if (!(x > 1e-30 && x < 1e30))
-      return 1.0 / x;
-    double y = double(rcp_seed(float(x)));
+    double y = double(rcp_seed(float(fmin(fmax(x, 1e-30), 1e30))));
     double e = fma(-x, y, 1.0);
     y        = fma(y, e, y);
     e        = fma(-x, y, 1.0);
@@ -61,9 +61,7 @@ namespace sint
   template <>
   __device__ __forceinline__ float rcp_pos<float>(float x)
   {
-    if (!(x > 1e-30f && x < 1e30f))
-      return 1.0f / x;
-    float y = rcp_seed(x);
+    float y = rcp_seed(fminf(fmaxf(x, 1e-30f), 1e30f));
     return fmaf(y, fmaf(-x, y, 1.0f), y);
   }
 
@@ -72,9 +70,7 @@ namespace sint
   template <>
   __device__ __forceinline__ double rsqrt_pos<double>(double x)
   {
-    if (!(x > 1e-30 && x < 1e30))
-      return 1.0 / sqrt(x);
-    double y = double(rsqrt_seed(float(x)));
+    double y = double(rsqrt_seed(float(fmin(fmax(x, 1e-30), 1e30))));
     double r = fma(-x * y, y, 1.0);
     y        = fma(0.5 * y, r, y);
     r        = fma(-x * y, y, 1.0);
@@ -83,9 +79,7 @@ namespace sint
   template <>
   __device__ __forceinline__ float rsqrt_pos<float>(float x)
   {
-    if (!(x > 1e-30f && x < 1e30f))
-      return 1.0f / sqrtf(x);
-    float y = rsqrt_seed(x);
+    float y = rsqrt_seed(fminf(fmaxf(x, 1e-30f), 1e30f));
     return fmaf(0.5f * y, fmaf(-x * y, y, 1.0f), y);
   }
 
