@@ -28,7 +28,8 @@ namespace sint
   size_t smem_jvp(int dim, int G, size_t rb)
   {
     const int C = G + 2;
-    return dim == 3 ? (2 * C * Tile<3>::BOX + C * Tile<3>::CS) * rb : (2 * C * Tile<2>::BOX + C * Tile<2>::CS) * rb;
+    // double-buffered node boxes (linearisation point + direction) + contributions
+    return dim == 3 ? (4 * C * Tile<3>::BOX + C * Tile<3>::CS) * rb : (4 * C * Tile<2>::BOX + C * Tile<2>::CS) * rb;
   }
 
   size_t smem_residual(int dim, int G, int wtd)

@@ -188,6 +188,59 @@ namespace sint
       s[comp * T::BOX + bn.b] = bn.inside ? R(p[comp * g.ld]) : R(0);
   }
 
+  // Asynchronous global->shared copies (cp.async, sm_80+): the node box of the
+  // next tile is fetched while the current one is computed.  Nodes outside
+  // the mesh are zero-filled (source size 0; the source address then only has
+  // to be a valid pointer, the vector base is used).
+  __device__ __forceinline__ void cp_async_elem(double *s, const double *gptr, bool valid)
+  {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gptr), "r"(valid ? 8 : 0));
+  }
+  __device__ __forceinline__ void cp_async_elem(float *s, const float *gptr, bool valid)
+  {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gptr), "r"(valid ? 4 : 0));
+  }
+  __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+  template <int N>
+  __device__ __forceinline__ void cp_async_wait()
+  {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+  }
+
+  // Issue the asynchronous load of `ncomp` components of `src` into the box
+  // buffer s (layout s[comp * BOX + box_node]).
+  template <int DIM, typename R>
+  __device__ __forceinline__ void load_box_async(R *s, const R *__restrict__ src, int ncomp, const Grid &g,
+                                                 const BoxNode<DIM> &bn)
+  {
+    using T = Tile<DIM>;
+    if (!bn.active)
+      return;
+    const R *p = bn.inside ? src + bn.gidx : src;
+    for (int comp = bn.grp; comp < ncomp; comp += T::NG)
+      cp_async_elem(s + comp * T::BOX + bn.b, bn.inside ? p + comp * g.ld : src, bn.inside);
+  }
+
+  template <int DIM>
+  __device__ __forceinline__ TileCoord tile_coord_of(const Grid &g, long long tile)
+  {
+    using T = Tile<DIM>;
+    TileCoord tc;
+    tc.linear   = tile;
+    long long r = tile;
+    tc.t[0]     = int(r % g.nt[0]);
+    r /= g.nt[0];
+    tc.t[1] = int(r % g.nt[1]);
+    r /= g.nt[1];
+    tc.t[2] = int(r);
+    tc.o[0] = tc.t[0] * T::TX;
+    tc.o[1] = tc.t[1] * T::TY;
+    tc.o[2] = tc.t[2] * T::TZ;
+    return tc;
+  }
+
   // Per-thread quadrature constants.  Lane bits of (threadIdx.x % NQ) are the
   // quadrature point coordinates (qx, qy, qz); after the integration butterfly
   // they are the local node coordinates (lx, ly, lz).

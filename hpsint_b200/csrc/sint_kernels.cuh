@@ -25,25 +25,15 @@ namespace sint
   // mu and eta rows have constant-coefficient gradient terms (-kappa_c grad dc,
   // L kappa_p grad deta), which are applied with the exact element stiffness
   // stencil to the nodal values, so those rows only integrate point values.
+  //
+  // Persistent and software pipelined: block b handles tiles b, b + grid, ...;
+  // the node boxes of the next tile are copied (cp.async) into the second half
+  // of a double buffer while the current tile is computed.
   template <int DIM, int G, bool TENS, typename R>
-  __global__ void __launch_bounds__(Tile<DIM>::THREADS)
-    jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
-               R *__restrict__ dst, R *__restrict__ partial)
+  __device__ __forceinline__ void jvp_tile(const Grid &g, const PhysR<R> &p, const R *s_lin, const R *s_src,
+                                           R *s_con, const TileCoord &tc)
   {
-    using T          = Tile<DIM>;
-    constexpr int C  = G + 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *s_lin = reinterpret_cast<R *>(smem_raw);
-    R *s_src = s_lin + C * T::BOX;
-    R *s_con = s_src + C * T::BOX;
-
-    const TileCoord    tc = tile_coord<DIM>(g);
-    const BoxNode<DIM> bn(g, tc);
-    load_box<DIM>(s_lin, lin, C, g, bn);
-    load_box<DIM>(s_src, src, C, g, bn);
-    __syncthreads();
-
-    const PhysR<R>   p(ph);
+    using T           = Tile<DIM>;
     const QP<DIM, R> w(g);
     const int        cell  = threadIdx.x / T::NQ;
     const int        b0    = cell_box_base<DIM>(cell);
@@ -124,8 +114,52 @@ namespace sint
           store_contrib<DIM>(s_con, 2 + i, r, valid);
         }
     }
-    __syncthreads();
-    sum_and_store<DIM>(s_con, C, g, tc, bn, dst, partial);
+  }
+
+  // Two resident blocks per SM (<= 128 registers) unless the FP64 grain state
+  // of large G would spill; those run one block with up to 255 registers.
+  template <int DIM, int G, bool TENS, typename R>
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, (sizeof(R) == 8 && G > 5) ? 1 : 2)
+    jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
+               R *__restrict__ dst, R *__restrict__ partial)
+  {
+    using T          = Tile<DIM>;
+    constexpr int C  = G + 2;
+    constexpr int VB = 2 * C * T::BOX; // one buffer: linearisation point + direction
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *s_buf = reinterpret_cast<R *>(smem_raw); // 2 x VB
+    R *s_con = s_buf + 2 * VB;
+
+    const PhysR<R> p(ph);
+    long long      tile = blockIdx.x;
+    if (tile < g.n_tiles)
+      {
+        const BoxNode<DIM> bn(g, tile_coord_of<DIM>(g, tile));
+        load_box_async<DIM>(s_buf, lin, C, g, bn);
+        load_box_async<DIM>(s_buf + C * T::BOX, src, C, g, bn);
+      }
+    cp_async_commit();
+    for (int it = 0; tile < g.n_tiles; ++it, tile += gridDim.x)
+      {
+        const long long next = tile + gridDim.x;
+        R              *nb   = s_buf + ((it + 1) & 1) * VB;
+        if (next < g.n_tiles)
+          {
+            const BoxNode<DIM> bnn(g, tile_coord_of<DIM>(g, next));
+            load_box_async<DIM>(nb, lin, C, g, bnn);
+            load_box_async<DIM>(nb + C * T::BOX, src, C, g, bnn);
+          }
+        cp_async_commit();
+        cp_async_wait<1>(); // this tile's group has landed (only the prefetch may be pending)
+        __syncthreads();
+        const TileCoord tc = tile_coord_of<DIM>(g, tile);
+        const R        *cb = s_buf + (it & 1) * VB;
+        jvp_tile<DIM, G, TENS, R>(g, p, cb, cb + C * T::BOX, s_con, tc);
+        __syncthreads();
+        sum_and_store<DIM>(s_con, C, g, tc, BoxNode<DIM>(g, tc), dst, partial);
+        __syncthreads(); // s_con and this buffer are reused by the next iterations
+      }
+    cp_async_wait<0>();
   }
 
   // -------------------------------------------------------------------------

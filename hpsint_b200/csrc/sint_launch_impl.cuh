@@ -22,10 +22,22 @@ namespace sint
   {
     const size_t smem = smem_jvp(DIM, G, sizeof(R));
     auto         k    = jvp_kernel<DIM, G, TENS, R>;
-    cudaError_t  e    = prepare_smem(k, smem);
-    if (e != cudaSuccess)
-      return e;
-    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial);
+    // persistent grid: as many blocks as are resident at once
+    static int   grid_cap = 0;
+    cudaError_t  e        = cudaSuccess;
+    if (grid_cap == 0)
+      {
+        if ((e = prepare_smem(k, smem)) != cudaSuccess)
+          return e;
+        int dev = 0, sms = 0, per_sm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+            (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Tile<DIM>::THREADS, smem)) != cudaSuccess)
+          return e;
+        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
+      }
+    const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial);
     count_launches(1);
     return cudaGetLastError();
   }
