@@ -58,6 +58,8 @@ SIGNATURES = {
     "sint_residual_f64": (_c_int, [_c_void, _c_void, _c_void, P(_c_void), _c_int, _c_void]),
     "sint_jvp_f64": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_jvp_f32": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
+    "sint_jvp_f64_noalloc": (_c_int, [P(SintMesh), P(SintParams), _c_double, _c_double, _c_void, _c_void, _c_void,
+                                      _c_void]),
     "sint_precond_setup": (_c_int, [_c_void, _c_void]),
     "sint_precond_apply_f64": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_precond_apply_f32": (_c_int, [_c_void, _c_void, _c_void, _c_void]),

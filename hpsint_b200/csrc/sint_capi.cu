@@ -64,7 +64,7 @@ namespace sint
 
   // --- dispatch over (dim, mobility) ---------------------------------------
   template <typename R>
-  static cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s)
+  cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s)
   {
     R *part = reinterpret_cast<R *>(c->partial);
     const bool t = c->params.tensorial != 0;
@@ -80,6 +80,9 @@ namespace sint
     return c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, s)
                             : launch_combine<2, R>(c->C, c->grid, part, dst, s);
   }
+
+  template cudaError_t dispatch_jvp<double>(const Ctx *, const double *, const double *, double *, cudaStream_t);
+  template cudaError_t dispatch_jvp<float>(const Ctx *, const float *, const float *, float *, cudaStream_t);
 
   static cudaError_t dispatch_residual(const Ctx *c, int wtd, const double *src, const double *const *hist,
                                        double *dst, cudaStream_t s)
@@ -184,6 +187,98 @@ namespace sint
 
 using namespace sint;
 
+namespace sint
+{
+  // Validates mesh and parameters and fills the operator description (mesh,
+  // grid, point-wise parameters, layout) of `c`; allocates nothing.
+  int describe_operator(const sint_mesh *mesh, const sint_params *params, Ctx *c)
+  {
+    if (mesh->dim != 2 && mesh->dim != 3)
+      {
+        set_error("sint_create: dim must be 2 or 3");
+        return SINT_ERR_ARG;
+      }
+    if (params->n_grains < 1 || params->n_grains > SINT_MAX_GRAINS)
+      {
+        set_error("This operation is precompiled for the number of grains in range [1, " +
+                  std::to_string(SINT_MAX_GRAINS) + "] but you provided n_grains = " +
+                  std::to_string(params->n_grains));
+        return SINT_ERR_GRAINS;
+      }
+    for (int d = 0; d < mesh->dim; ++d)
+      if (mesh->n_cells[d] < 1 || !(mesh->h[d] > 0.0) || !std::isfinite(mesh->h[d]))
+        {
+          set_error("sint_create: every n_cells[d] must be >= 1 and h[d] > 0");
+          return SINT_ERR_ARG;
+        }
+
+    c->mesh     = *mesh;
+    c->params   = *params;
+    c->G        = params->n_grains;
+    c->C        = params->n_grains + 2;
+    Grid &g     = c->grid;
+    g.dim       = mesh->dim;
+    const int TT[3] = {mesh->dim == 3 ? Tile<3>::TX : Tile<2>::TX, mesh->dim == 3 ? Tile<3>::TY : Tile<2>::TY,
+                       mesh->dim == 3 ? Tile<3>::TZ : 1};
+    long long N = 1, nt = 1;
+    for (int d = 0; d < 3; ++d)
+      {
+        if (d < mesh->dim)
+          {
+            g.n[d]  = mesh->n_cells[d];
+            g.nn[d] = mesh->n_cells[d] + 1;
+            g.nt[d] = (mesh->n_cells[d] + TT[d] - 1) / TT[d];
+            g.h[d]  = mesh->h[d];
+          }
+        else
+          {
+            g.n[d] = g.nn[d] = g.nt[d] = 1;
+            g.h[d]                     = 1.0;
+          }
+        N *= g.nn[d];
+        nt *= g.nt[d];
+      }
+    g.N       = N;
+    g.n_tiles = nt;
+    // exact Q1 element Laplacian of the uniform cell: K_lm = kx[l xor m], built
+    // from the 1D stiffness (1/h)[[1,-1],[-1,1]] and mass (h/6)[[2,1],[1,2]]
+    for (int x = 0; x < 8; ++x)
+      {
+        double k = 0.0;
+        if (x < (1 << mesh->dim))
+          for (int d = 0; d < mesh->dim; ++d)
+            {
+              double t = (((x >> d) & 1) ? -1.0 : 1.0) / g.h[d];
+              for (int e = 0; e < mesh->dim; ++e)
+                if (e != d)
+                  t *= ((x >> e) & 1) ? g.h[e] / 6.0 : g.h[e] / 3.0;
+              k += t;
+            }
+        g.kxd[x] = k;
+        g.kxf[x] = float(k);
+      }
+    g.ld      = (N + 31) / 32 * 32;
+    c->N      = N;
+    c->ld     = g.ld;
+
+    Phys &p = c->phys;
+    std::memset(&p, 0, sizeof(p));
+    p.A       = params->A;
+    p.B       = params->B;
+    p.kappa_c = params->kappa_c;
+    p.kappa_p = params->kappa_p;
+    p.Mvol    = params->Mvol;
+    p.Mvap    = params->Mvap;
+    p.Msurf   = params->Msurf;
+    p.Mgb     = params->Mgb;
+    p.L       = params->L;
+    p.w0      = 0.0;
+    p.w_alg   = 1.0;
+    p.order   = 0;
+    return SINT_OK;
+  }
+} // namespace sint
+
 static int check_ctx(const sint_ctx *ctx)
 {
   if (!ctx)
@@ -223,90 +318,14 @@ int sint_create(const sint_mesh *mesh, const sint_params *params, sint_ctx **out
       return SINT_ERR_ARG;
     }
   *out = nullptr;
-  if (mesh->dim != 2 && mesh->dim != 3)
-    {
-      set_error("sint_create: dim must be 2 or 3");
-      return SINT_ERR_ARG;
-    }
-  if (params->n_grains < 1 || params->n_grains > SINT_MAX_GRAINS)
-    {
-      set_error("This operation is precompiled for the number of grains in range [1, " +
-                std::to_string(SINT_MAX_GRAINS) + "] but you provided n_grains = " +
-                std::to_string(params->n_grains));
-      return SINT_ERR_GRAINS;
-    }
-  for (int d = 0; d < mesh->dim; ++d)
-    if (mesh->n_cells[d] < 1 || !(mesh->h[d] > 0.0) || !std::isfinite(mesh->h[d]))
-      {
-        set_error("sint_create: every n_cells[d] must be >= 1 and h[d] > 0");
-        return SINT_ERR_ARG;
-      }
-
   sint_ctx *c = new sint_ctx();
-  c->mesh     = *mesh;
-  c->params   = *params;
-  c->G        = params->n_grains;
-  c->C        = params->n_grains + 2;
-  Grid &g     = c->grid;
-  g.dim       = mesh->dim;
-  const int TT[3] = {mesh->dim == 3 ? Tile<3>::TX : Tile<2>::TX, mesh->dim == 3 ? Tile<3>::TY : Tile<2>::TY,
-                     mesh->dim == 3 ? Tile<3>::TZ : 1};
-  long long N = 1, nt = 1;
-  for (int d = 0; d < 3; ++d)
+  if (int rc = describe_operator(mesh, params, c))
     {
-      if (d < mesh->dim)
-        {
-          g.n[d]  = mesh->n_cells[d];
-          g.nn[d] = mesh->n_cells[d] + 1;
-          g.nt[d] = (mesh->n_cells[d] + TT[d] - 1) / TT[d];
-          g.h[d]  = mesh->h[d];
-        }
-      else
-        {
-          g.n[d] = g.nn[d] = g.nt[d] = 1;
-          g.h[d]                     = 1.0;
-        }
-      N *= g.nn[d];
-      nt *= g.nt[d];
+      delete c;
+      return rc;
     }
-  g.N       = N;
-  g.n_tiles = nt;
-  // exact Q1 element Laplacian of the uniform cell: K_lm = kx[l xor m], built
-  // from the 1D stiffness (1/h)[[1,-1],[-1,1]] and mass (h/6)[[2,1],[1,2]]
-  for (int x = 0; x < 8; ++x)
-    {
-      double k = 0.0;
-      if (x < (1 << mesh->dim))
-        for (int d = 0; d < mesh->dim; ++d)
-          {
-            double t = (((x >> d) & 1) ? -1.0 : 1.0) / g.h[d];
-            for (int e = 0; e < mesh->dim; ++e)
-              if (e != d)
-                t *= ((x >> e) & 1) ? g.h[e] / 6.0 : g.h[e] / 3.0;
-            k += t;
-          }
-      g.kxd[x] = k;
-      g.kxf[x] = float(k);
-    }
-  g.ld      = (N + 31) / 32 * 32;
-  c->N      = N;
-  c->ld     = g.ld;
-
-  Phys &p = c->phys;
-  std::memset(&p, 0, sizeof(p));
-  p.A       = params->A;
-  p.B       = params->B;
-  p.kappa_c = params->kappa_c;
-  p.kappa_p = params->kappa_p;
-  p.Mvol    = params->Mvol;
-  p.Mvap    = params->Mvap;
-  p.Msurf   = params->Msurf;
-  p.Mgb     = params->Mgb;
-  p.L       = params->L;
-  p.w0      = 0.0;
-  p.w_alg   = 1.0;
-  p.order   = 0;
-
+  const Grid &g  = c->grid;
+  const long long nt = g.n_tiles;
   const int box   = mesh->dim == 3 ? Tile<3>::BOX : Tile<2>::BOX;
   c->partial_bytes = size_t(nt) * size_t(c->G + 4) * size_t(box) * sizeof(double);
   cudaError_t e;

@@ -69,6 +69,12 @@ namespace sint
   int convert(long long n, const S *x, D *y, cudaStream_t s);
 
   int free_workspace(Ctx *c);
+
+  // Validates and fills the operator description of c (no allocation).
+  int describe_operator(const sint_mesh *mesh, const sint_params *params, Ctx *c);
+  // J v through the cell kernel + combine, with c->partial as scratch.
+  template <typename R>
+  cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s);
 } // namespace sint
 
 struct sint_ctx : public sint::Ctx

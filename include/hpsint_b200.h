@@ -125,6 +125,27 @@ int sint_jvp_f64(sint_ctx *ctx, double *dst, const double *src, sint_stream_t st
 /* Same product in FP32 with FP32 accumulation, linearised at the FP32 shadow. */
 int sint_jvp_f32(sint_ctx *ctx, float *dst, const float *src, sint_stream_t stream);
 
+/* Allocation-free FP64 Jacobian-vector product (no counterpart in the
+ * reference).  For callers that may not call cudaMalloc -- e.g. code running
+ * under another framework's memory pool, inside stream callbacks, or embedded
+ * solvers with a fixed memory budget: no context is needed and nothing is
+ * allocated.  The caller passes the mesh, the parameters, the time weights
+ * (w0, w_alg as in sint_set_time_weights), the linearisation point `lin` and
+ * the direction `src` (C blocks each, the layout sint_dof_layout reports) and
+ * owns `dst`; the result equals sint_jvp_f64 on a context with the same state.
+ * The product's only scratch, the partial sums on tile faces, lives in a
+ * fixed device array of SINT_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until exit; meshes needing more return SINT_ERR_ARG.  The
+ * need is 600 * (G + 2) bytes per 4 x 4 x 2 cells in 3D and 648 * (G + 2)
+ * bytes per 8 x 8 cells in 2D: with G = 4, up to 64 x 64 x 36 cells in 3D or
+ * 520 x 520 cells in 2D.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current, so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * (different streams, or different host threads) race and give wrong results. */
+#define SINT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int sint_jvp_f64_noalloc(const sint_mesh *mesh, const sint_params *params, double w0, double w_alg,
+                         const double *lin, const double *src, double *dst, sint_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* Preconditioner: BlockPreconditioner2 (sintering/preconditioners.h:978-1343) */
 
