@@ -1,0 +1,114 @@
+"""Implicit BDF time stepping around the device Newton solve.
+
+Mirrors the parts of hpsint's time loop that decide what the hot path is
+asked to do:
+  TimeIntegratorData / BDF weights  time_integration/time_integrator_data.h:98-163,
+                                    time_schemes.h:64-153
+  SolutionHistory                   time_integration/solution_history.h:136-205
+  predictor hook                    sintering/driver.h:2001-2058 (initial Newton iterate)
+  failure -> dt halving, restore    sintering/driver.h:2163-2202, :2489-2505
+  dt growth after "good" steps      sintering/driver.h:2239-2243, :2387-2409
+  defaults                          time_integration/time_integrator_parameters.h:32-36
+The solution stays on the device; a step is one sint_newton_solve call (or
+several after failures).
+"""
+import time
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib as L
+from .operator import DampedNewtonSolver, NonLinearData, SinteringOperatorGeneric, bdf_weights
+
+
+@dataclass
+class TimeIntegrationData:
+    scheme_order: int = 1          # BDF order
+    time_step_init: float = 1e-3
+    time_step_min: float = 1e-5
+    time_step_max: float = 1e2
+    growth_factor: float = 1.2
+    desirable_newton_iterations: int = 5
+    desirable_linear_iterations: int = 100
+
+
+@dataclass
+class StepRecord:
+    t: float
+    dt: float
+    newton_iterations: int
+    linear_iterations: int
+    residual_evaluations: int
+    failed_tries: int
+    wall_s: float
+
+
+class TimeIntegrator:
+    """Advance u_t = ... with BDF and adaptive dt on the GPU.
+
+    predictor(u_old_list, dt) -> device tensor or None: optional initial
+    Newton iterate (the learned predictor plugs in here); None means the
+    previous solution (hpsint's "None" predictor).
+    """
+
+    def __init__(self, op: SinteringOperatorGeneric, nl: NonLinearData = None, td: TimeIntegrationData = None,
+                 predictor=None):
+        self.op = op
+        self.nl = nl or NonLinearData()
+        self.td = td or TimeIntegrationData()
+        self.newton = DampedNewtonSolver(op, self.nl)
+        self.predictor = predictor
+        self.history = []     # old solutions, most recent first (device tensors)
+        self.dts = []         # accepted time steps, most recent first
+        self.t = 0.0
+        self.dt = self.td.time_step_init
+        self.records = []
+
+    def initialize(self, u0):
+        self.history = [u0.clone()]
+        self.dts = []
+        self.t = 0.0
+
+    def _weights(self, dt):
+        order = min(self.td.scheme_order, len(self.history))
+        w = bdf_weights(order, [dt] + self.dts[:order - 1])
+        return w[0], w[1:order + 1]
+
+    def step(self, u_out=None):
+        """One accepted time step; returns the new solution (device)."""
+        tries = 0
+        t0 = time.perf_counter()
+        while True:
+            w0, wh = self._weights(self.dt)
+            self.op.set_time_weights(w0, wh, 1.0)
+            guess = self.predictor(self.history, self.dt) if self.predictor else None
+            u = (guess if guess is not None else self.history[0]).clone()
+            st = self.newton.solve(u, self.history[:len(wh)], raise_on_failure=False)
+            if st.status == L.SINT_OK:
+                break
+            # process_failure: halve dt, restore the last good state, forget the
+            # Newton history that decides preconditioner rebuilds
+            tries += 1
+            self.dt *= 0.5
+            self.newton.clear()
+            if self.dt <= self.td.time_step_min:
+                raise L.SintError(8, "TimeIntegrator.step", "Minimum timestep size exceeded, solution failed!")
+        torch.cuda.synchronize()
+        self.t += self.dt
+        self.records.append(StepRecord(self.t, self.dt, st.newton_iterations, st.linear_iterations,
+                                       st.residual_evaluations, tries, time.perf_counter() - t0))
+        self.history.insert(0, u)
+        self.dts.insert(0, self.dt)
+        keep = max(1, self.td.scheme_order)
+        self.history = self.history[:keep]
+        self.dts = self.dts[:keep]
+        good = (st.newton_iterations < self.td.desirable_newton_iterations and
+                st.linear_iterations < self.td.desirable_linear_iterations)
+        if good and self.td.growth_factor > 1.0:
+            self.dt = min(self.dt * self.td.growth_factor, self.td.time_step_max)
+        return u
+
+    def run(self, n_steps):
+        for _ in range(n_steps):
+            self.step()
+        return self.history[0]
