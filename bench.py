@@ -50,6 +50,9 @@ def parse_args():
     ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--workload", choices=["operator", "solve2d"], default="operator",
+                    help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve")
+    ap.add_argument("--solve-steps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -178,10 +181,69 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def two_particle_solve(args):
+    """2D two-particle sintering: 256 x 128 Q1 cells on [-40, 40] x [-20, 20],
+    circles R = 10 at (+-10, 0), tanh width 2, G = 2, hpsint's default
+    constants, BDF1 with dt0 = 1e-3 and hpsint's dt control, Newton relative
+    tolerance 1e-8.  Runs the plain FP64 solve and the FP32-inner solve from
+    the same state and reports s/step, iteration counts, and the FP32-inner
+    run's error against the FP64 run."""
+    import torch
+
+    import hpsint_b200 as hb
+    from hpsint_b200 import packings as P
+    from hpsint_b200.time_integration import TimeIntegrationData, TimeIntegrator
+
+    nx, ny = 256, 128
+    h = (80.0 / nx, 40.0 / ny)
+    centers, radii, colours = P.two_particle_2d()
+    u0 = P.initial_state(2, (nx, ny), h, (-40.0, -20.0), centers, radii, colours, width=2.0)
+    wx = np.full(nx + 1, h[0]); wx[[0, -1]] *= 0.5
+    wy = np.full(ny + 1, h[1]); wy[[0, -1]] *= 0.5
+    mass = np.outer(wy, wx).ravel()  # lumped weights: int c_h = sum_n m_n c_n
+
+    runs = {}
+    for label, prec in (("fp64", 64), ("fp32_inner", 32)):
+        op = hb.SinteringOperatorGeneric(hb.Mesh(2, (nx, ny, 1), (h[0], h[1], 1.0)), hb.Params(2))
+        ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec),
+                            TimeIntegrationData(time_step_init=1e-3))
+        ti.initialize(op.to_device(u0))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ti.run(args.solve_steps)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        u = op.to_host(ti.history[0])
+        runs[label] = dict(u=u, wall=wall, t=ti.t, rec=ti.records)
+    ref, mp = runs["fp64"], runs["fp32_inner"]
+    n_common = min(len(ref["rec"]), len(mp["rec"]))
+    line = {"metric": METRIC, "workload": "2d-two-particle-256x128-G2", "steps": args.solve_steps,
+            "unit": "s/step", "higher_is_better": False, "dtype": "f64 Newton", "data": "synthetic"}
+    for label, r in runs.items():
+        recs = r["rec"]
+        line[label] = {"s_per_step": r["wall"] / len(recs), "sim_time": r["t"],
+                       "newton_iterations": sum(x.newton_iterations for x in recs),
+                       "linear_iterations": sum(x.linear_iterations for x in recs),
+                       "failed_tries": sum(x.failed_tries for x in recs), "final_dt": recs[-1].dt}
+    same_t = abs(ref["t"] - mp["t"]) <= 1e-12 * max(1.0, ref["t"])
+    line["fp32_inner_vs_fp64"] = {
+        "same_time_grid": same_t,
+        "max_abs_diff_c": float(np.abs(mp["u"][0] - ref["u"][0]).max()),
+        "max_abs_diff_eta": float(np.abs(mp["u"][2:] - ref["u"][2:]).max()),
+        "int_c_conservation_fp64": float(abs(mass @ ref["u"][0] - mass @ u0[0]) / abs(mass @ u0[0])),
+        "int_c_conservation_fp32_inner": float(abs(mass @ mp["u"][0] - mass @ u0[0]) / abs(mass @ u0[0])),
+        "speedup_s_per_step": (ref["wall"] / len(ref["rec"])) / (mp["wall"] / len(mp["rec"])),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "solve2d":
+        two_particle_solve(args)
         return
     import torch
 

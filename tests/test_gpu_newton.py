@@ -138,18 +138,34 @@ def test_non_finite_state_fails_cleanly():
 
 
 def test_time_integrator_halves_dt_on_failure_and_grows_after_good_steps():
+    """driver.h:2163-2202 / :2387-2409 semantics; the failure is injected on the
+    host: the predictor's first initial guess carries a NaN."""
     import hpsint_b200 as hb
     from hpsint_b200.time_integration import TimeIntegrationData, TimeIntegrator
     cells, G = (32, 16), 2
     u0 = two_particle_state(cells, R=5.0)
     op = hb.SinteringOperatorGeneric(hb.Mesh(2, cells + (1,)), hb.Params(G))
-    # a Newton budget of 2 iterations at rel 1e-8 forces failures at large dt
-    ti = TimeIntegrator(op, hb.NonLinearData(nl_max_iter=2, nl_rel_tol=1e-8),
-                        TimeIntegrationData(time_step_init=1.0, time_step_min=1e-6))
+    calls = []
+
+    def poisoned_once(history, dt):
+        calls.append(dt)
+        if len(calls) == 1:
+            g = history[0].clone()
+            g[0, 3] = float("nan")
+            return g
+        return None
+
+    dt0 = 1e-3
+    ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8), TimeIntegrationData(time_step_init=dt0),
+                        predictor=poisoned_once)
     ti.initialize(op.to_device(u0))
     ti.run(3)
-    assert ti.records[0].failed_tries >= 1
-    assert ti.records[0].dt < 1.0
+    r = ti.records
+    assert r[0].failed_tries == 1 and r[0].dt == pytest.approx(dt0 / 2)
+    assert calls[:2] == [dt0, dt0 / 2]
+    for a, b in zip(r[:-1], r[1:]):
+        good = a.newton_iterations < 5 and a.linear_iterations < 100
+        assert b.dt == pytest.approx(a.dt * (1.2 if good else 1.0))
     # conservation of int c (natural boundary conditions): the c rows of the
     # residual sum to int (c - c_old) / dt, so int c_h = sum_n m_n c_n with the
     # row sums m_n of the mass matrix (half weight per boundary direction)
