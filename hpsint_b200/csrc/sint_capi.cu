@@ -25,21 +25,6 @@ namespace sint
 
   void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
-  size_t smem_jvp(int dim, int G, size_t rb)
-  {
-    const int C = G + 2;
-    // double-buffered node boxes (linearisation point + direction) + contributions
-    return dim == 3 ? (4 * C * Tile<3>::BOX + C * Tile<3>::CS) * rb : (4 * C * Tile<2>::BOX + C * Tile<2>::CS) * rb;
-  }
-
-  size_t smem_residual(int dim, int G, int wtd)
-  {
-    const int C  = G + 2;
-    const int nv = wtd == 2 ? 2 * C : C;
-    return dim == 3 ? (nv * Tile<3>::BOX + C * Tile<3>::CS) * sizeof(double)
-                    : (nv * Tile<2>::BOX + C * Tile<2>::CS) * sizeof(double);
-  }
-
   size_t smem_diag(int dim, int G)
   {
     const int C = G + 2;

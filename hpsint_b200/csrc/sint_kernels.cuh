@@ -2,6 +2,7 @@
 // dimension, number of grains and mobility type in sint_inst_*.cu).
 #pragma once
 
+#include "sint_cellfact.cuh"
 #include "sint_common.cuh"
 #include "sint_physics.cuh"
 
@@ -16,57 +17,169 @@ namespace sint
   }
 
   // -------------------------------------------------------------------------
-  // Jacobian-vector product: dst = J(lin) src.
-  // SinteringOperatorGenericQuad::operator() (operator_sintering_generic.h:101-190)
-  // inside do_vmult_range (:539-577).  The linearisation point is evaluated
-  // from the nodal state instead of a quadrature-point cache.
+  // Three-phase cell kernels (Jacobian-vector product and residual).
   //
-  // Only the c row has a point-dependent gradient flux (the mobility term); the
-  // mu and eta rows have constant-coefficient gradient terms (-kappa_c grad dc,
-  // L kappa_p grad deta), which are applied with the exact element stiffness
-  // stencil to the nodal values, so those rows only integrate point values.
+  // Per tile: phase 1 evaluates every needed component at all points of a cell
+  // (one thread per (cell, component), per-cell sum factorisation) into the
+  // point-field buffer F[slot][cell]; phase 2 runs the point physics (one
+  // thread per (point, cell)) and writes the point results to P[res][q][cell];
+  // phase 3 integrates each residual row of a cell (one thread per (cell,
+  // row)) into the node contributions K[row][l][cell] (aliasing F); the node
+  // sum and the tile-face partials follow.  Warps always work on 32
+  // consecutive cells of one component/point/row, so the shared-memory
+  // accesses of the three phases are free of bank conflicts.
   //
-  // Persistent and software pipelined: block b handles tiles b, b + grid, ...;
-  // the node boxes of the next tile are copied (cp.async) into the second half
-  // of a double buffer while the current tile is computed.
-  template <int DIM, int G, bool TENS, typename R>
-  __device__ __forceinline__ void jvp_tile(const Grid &g, const PhysR<R> &p, const R *s_lin, const R *s_src,
-                                           R *s_con, const TileCoord &tc)
-  {
-    using T           = Tile<DIM>;
-    const QP<DIM, R> w(g);
-    const int        cell  = threadIdx.x / T::NQ;
-    const int        b0    = cell_box_base<DIM>(cell);
-    const bool       valid = cell_in_mesh<DIM>(cell, tc, g);
+  // Only the c row has a point-dependent gradient flux (mobility); the mu and
+  // eta rows' gradient terms (-kappa_c grad c, L kappa_p grad eta) have
+  // constant coefficients and are applied with the exact element stiffness to
+  // the nodal values, so those rows integrate point values only.
 
-    // linearisation point at this quadrature point
-    R c, gc[DIM], mu_unused, gmu[DIM];
+  // Components evaluated in phase 1, in slot order.  Jacobian product:
+  //   tensorial: [lin c, lin mu, lin eta_i] (value + gradient),
+  //              [src c, src mu] (value + gradient), [src eta_i] (value)
+  //   scalar:    [lin mu, src mu] (value + gradient),
+  //              [lin c, lin eta_i, src c, src eta_i] (value)
+  // Residual (u = the state, h = the weighted history):
+  //   tensorial: [c, mu, eta_i] (value + gradient), [h c, h eta_i] (value)
+  //   scalar:    [mu] (value + gradient), [c, eta_i] (value), [h c, h eta_i] (value)
+  template <int DIM, int G, bool TENS, bool JVP, bool HIST>
+  struct FieldMap
+  {
+    using SL = Slots<DIM>;
+    static constexpr int NVG    = JVP ? (TENS ? 4 + G : 2) : (TENS ? 2 + G : 1);
+    static constexpr int NV     = JVP ? (TENS ? G : 2 + 2 * G) : ((TENS ? 0 : 1 + G) + (HIST ? 1 + G : 0));
+    static constexpr int NITEMS = NVG + NV;
+    static constexpr int NSLOT  = NVG * SL::VG + NV * SL::V;
+
+    __host__ __device__ static constexpr int base(int item)
+    {
+      return item < NVG ? item * SL::VG : NVG * SL::VG + (item - NVG) * SL::V;
+    }
+    // item index of each quantity (residual: "lin" is the state itself)
+    static constexpr int lin_c  = TENS ? 0 : (JVP ? 2 : 1);
+    static constexpr int lin_mu = TENS ? 1 : 0;
+    __host__ __device__ static constexpr int lin_eta(int i) { return TENS ? 2 + i : (JVP ? 3 + i : 2 + i); }
+    static constexpr int src_c  = TENS ? 2 + G : 3 + G;
+    static constexpr int src_mu = TENS ? 3 + G : 1;
+    __host__ __device__ static constexpr int src_eta(int i) { return 4 + G + i; }
+    static constexpr int h_c = 2 + G;
+    __host__ __device__ static constexpr int h_eta(int i) { return 3 + G + i; }
+
+    // phase 1 item -> (buffer 0 = lin / state, 1 = src / history; component; value+gradient?)
+    __device__ static void source(int it, int &buf, int &comp)
+    {
+      if constexpr (JVP)
+        {
+          if constexpr (TENS)
+            {
+              if (it < 2 + G) { buf = 0; comp = it; }
+              else if (it < 4 + G) { buf = 1; comp = it - 2 - G; }
+              else { buf = 1; comp = 2 + (it - 4 - G); }
+            }
+          else
+            {
+              if (it == 0) { buf = 0; comp = 1; }
+              else if (it == 1) { buf = 1; comp = 1; }
+              else if (it == 2) { buf = 0; comp = 0; }
+              else if (it < 3 + G) { buf = 0; comp = 2 + (it - 3); }
+              else if (it == 3 + G) { buf = 1; comp = 0; }
+              else { buf = 1; comp = 2 + (it - 4 - G); }
+            }
+        }
+      else
+        {
+          if constexpr (TENS)
+            {
+              if (it < 2 + G) { buf = 0; comp = it; }
+              else if (it == 2 + G) { buf = 1; comp = 0; }
+              else { buf = 1; comp = 2 + (it - 3 - G); }
+            }
+          else
+            {
+              if (it == 0) { buf = 0; comp = 1; }
+              else if (it == 1) { buf = 0; comp = 0; }
+              else if (it < 2 + G) { buf = 0; comp = 2 + (it - 2); }
+              else if (it == 2 + G) { buf = 1; comp = 0; }
+              else { buf = 1; comp = 2 + (it - 3 - G); }
+            }
+        }
+    }
+  };
+
+  // Phase 1: evaluate all items of the tile.
+  template <int DIM, int G, bool TENS, bool JVP, bool HIST, typename R>
+  __device__ __forceinline__ void phase_evaluate(const R *box0, const R *box1, R *F, const CellConsts<DIM, R> &k)
+  {
+    using T            = Tile<DIM>;
+    using FM           = FieldMap<DIM, G, TENS, JVP, HIST>;
+    constexpr int NGRP = T::THREADS / T::CELLS;
+    const int     cell = threadIdx.x % T::CELLS;
+    const int     b0   = cell_box_base<DIM>(cell);
+    for (int it = threadIdx.x / T::CELLS; it < FM::NITEMS; it += NGRP)
+      {
+        int buf = 0, comp = 0;
+        FM::source(it, buf, comp);
+        R u[1 << DIM];
+        cell_nodes<DIM>((buf == 0 ? box0 : box1) + comp * T::BOX, b0, u);
+        if (it < FM::NVG)
+          cell_eval_vg<DIM>(u, k, F, FM::base(it), cell);
+        else
+          cell_eval_v<DIM>(u, k, F, FM::base(it), cell);
+      }
+  }
+
+  // point-field accessors for phase 2 (thread = (point q, cell))
+  template <int DIM, typename R>
+  __device__ __forceinline__ R fval(const R *F, int base, int q, int cell)
+  {
+    return F[(base + q) * Tile<DIM>::CELLS + cell];
+  }
+  template <int DIM, typename R>
+  __device__ __forceinline__ void fgrad(const R *F, int base, int q, int cell, R (&g)[DIM])
+  {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      g[d] = F[(base + Slots<DIM>::NQ + d * Slots<DIM>::NG1 + grad_slot<DIM>(d, q)) * Tile<DIM>::CELLS + cell];
+  }
+
+  // point results: P[(res * NQ + q) * CELLS + cell]; res 0 = c row value,
+  // 1..DIM = c row flux, DIM + 1 = mu row value, DIM + 2 + i = eta_i row value
+  template <int DIM, typename R>
+  __device__ __forceinline__ void pstore(R *P, int res, int q, int cell, R v)
+  {
+    P[(res * Slots<DIM>::NQ + q) * Tile<DIM>::CELLS + cell] = v;
+  }
+
+  // Phase 2 of the Jacobian product at point q of cell `cell`
+  // (SinteringOperatorGenericQuad::operator(), generic.h:101-190).
+  template <int DIM, int G, bool TENS, typename R>
+  __device__ __forceinline__ void jvp_point(const PhysR<R> &p, const R *F, R *P, int q, int cell)
+  {
+    using FM = FieldMap<DIM, G, TENS, true, false>;
+    R c, gc[DIM], gmu[DIM];
+    c = fval<DIM>(F, FM::base(FM::lin_c), q, cell);
     if constexpr (TENS)
-      eval_vg<DIM>(s_lin, b0, w, c, gc);
-    else
-      c = eval_v<DIM>(s_lin, b0, w);
-    eval_vg<DIM>(s_lin + T::BOX, b0, w, mu_unused, gmu);
+      fgrad<DIM>(F, FM::base(FM::lin_c), q, cell, gc);
+    fgrad<DIM>(F, FM::base(FM::lin_mu), q, cell, gmu);
     R eta[G];
     R geta[TENS ? G : 1][DIM];
 #pragma unroll
     for (int i = 0; i < G; ++i)
       {
+        eta[i] = fval<DIM>(F, FM::base(FM::lin_eta(i)), q, cell);
         if constexpr (TENS)
-          eval_vg<DIM>(s_lin + (2 + i) * T::BOX, b0, w, eta[i], geta[i]);
-        else
-          eta[i] = eval_v<DIM>(s_lin + (2 + i) * T::BOX, b0, w);
+          fgrad<DIM>(F, FM::base(FM::lin_eta(i)), q, cell, geta[i]);
       }
-    // direction
     R dc, gdc[DIM], dmu, gdmu[DIM];
+    dc = fval<DIM>(F, FM::base(FM::src_c), q, cell);
     if constexpr (TENS)
-      eval_vg<DIM>(s_src, b0, w, dc, gdc);
-    else
-      dc = eval_v<DIM>(s_src, b0, w);
-    eval_vg<DIM>(s_src + T::BOX, b0, w, dmu, gdmu);
+      fgrad<DIM>(F, FM::base(FM::src_c), q, cell, gdc);
+    dmu = fval<DIM>(F, FM::base(FM::src_mu), q, cell);
+    fgrad<DIM>(F, FM::base(FM::src_mu), q, cell, gdmu);
     R deta[G];
 #pragma unroll
     for (int i = 0; i < G; ++i)
-      deta[i] = eval_v<DIM>(s_src + (2 + i) * T::BOX, b0, w);
+      deta[i] = fval<DIM>(F, FM::base(FM::src_eta(i)), q, cell);
 
     // free energy second derivatives at the linearisation point (free_energy.h:143-161)
     R s2 = R(0);
@@ -81,25 +194,26 @@ namespace sint
     {
       R gres[DIM];
       apply_M_derivative<DIM, G, TENS>(p, c, gc, gmu, eta, geta, dc, gdc, gdmu, deta, gres);
-      store_contrib<DIM>(s_con, 0, integrate_butterfly<DIM>(dc * p.w0, gres, w), valid);
+      pstore<DIM>(P, 0, q, cell, dc * p.w0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        pstore<DIM>(P, 1 + d, q, cell, gres[d]);
     }
-    // 2) mu row (generic.h:138-146): value part + (-kappa_c) K dc
+    // 2) mu row value (generic.h:138-144)
     {
       R v = p.walg * dmu - fcc * dc;
 #pragma unroll
       for (int i = 0; i < G; ++i)
         v -= B12 * eta[i] * (eta[i] - R(1)) * deta[i];
-      const R r = integrate_value_butterfly<DIM>(v, w) - p.kc * stiffness_apply<DIM>(s_src, b0, w, g);
-      store_contrib<DIM>(s_con, 1, r, valid);
+      pstore<DIM>(P, DIM + 1, q, cell, v);
     }
-    // 3) eta rows (generic.h:150-163, free_energy.h:233-252): value part + L kappa_p K deta_i
+    // 3) eta row values (generic.h:150-163, free_energy.h:233-252)
     {
       R S = R(0);
 #pragma unroll
       for (int i = 0; i < G; ++i)
         S += eta[i] * deta[i];
       const R cL24B = p.L * R(24) * p.B;
-      const R Lkp   = p.L * p.kp;
 #pragma unroll
       for (int i = 0; i < G; ++i)
         {
@@ -109,13 +223,147 @@ namespace sint
           R       v   = deta[i] * p.w0 + p.L * (fce * dc + fee * deta[i]);
           if constexpr (G > 1)
             v += cL24B * e * (S - e * deta[i]);
-          const R r = integrate_value_butterfly<DIM>(v, w) +
-                      Lkp * stiffness_apply<DIM>(s_src + (2 + i) * T::BOX, b0, w, g);
-          store_contrib<DIM>(s_con, 2 + i, r, valid);
+          pstore<DIM>(P, DIM + 2 + i, q, cell, v);
         }
     }
   }
 
+  // Phase 2 of the residual at point q of cell `cell`
+  // (SinteringOperatorGenericResidualQuad::operator(), generic.h:254-308).
+  template <int DIM, int G, bool TENS, int WTD, typename R>
+  __device__ __forceinline__ void residual_point(const PhysR<R> &p, const R *F, R *P, int q, int cell)
+  {
+    using FM = FieldMap<DIM, G, TENS, false, WTD == 2>;
+    R c, gc[DIM], mu, gmu[DIM];
+    c = fval<DIM>(F, FM::base(FM::lin_c), q, cell);
+    if constexpr (TENS)
+      fgrad<DIM>(F, FM::base(FM::lin_c), q, cell, gc);
+    mu = fval<DIM>(F, FM::base(FM::lin_mu), q, cell);
+    fgrad<DIM>(F, FM::base(FM::lin_mu), q, cell, gmu);
+    R eta[G];
+    R geta[TENS ? G : 1][DIM];
+#pragma unroll
+    for (int i = 0; i < G; ++i)
+      {
+        eta[i] = fval<DIM>(F, FM::base(FM::lin_eta(i)), q, cell);
+        if constexpr (TENS)
+          fgrad<DIM>(F, FM::base(FM::lin_eta(i)), q, cell, geta[i]);
+      }
+    R s2 = R(0), s3 = R(0);
+#pragma unroll
+    for (int i = 0; i < G; ++i)
+      {
+        s2 += eta[i] * eta[i];
+        s3 += eta[i] * eta[i] * eta[i];
+      }
+    const R omc = R(1) - c;
+    // 1) c row (generic.h:275-285)
+    {
+      R v = R(0);
+      if constexpr (WTD >= 1)
+        v = c * p.w0;
+      if constexpr (WTD == 2)
+        v += fval<DIM>(F, FM::base(FM::h_c), q, cell);
+      R gres[DIM];
+      apply_M<DIM, G, TENS>(p, c, eta, gc, geta, gmu, gres);
+      pstore<DIM>(P, 0, q, cell, v);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        pstore<DIM>(P, 1 + d, q, cell, gres[d]);
+    }
+    // 2) mu row value (generic.h:288, free_energy.h:124-134)
+    {
+      const R df_dc = p.A * (c * c) * (R(2) * c - R(2)) + R(2) * p.A * c * (omc * omc) +
+                      p.B * (R(2) * c - R(6) * s2 + R(4) * s3);
+      pstore<DIM>(P, DIM + 1, q, cell, p.walg * mu - df_dc);
+    }
+    // 3) eta row values (generic.h:293-302, free_energy.h:136-141)
+#pragma unroll
+    for (int i = 0; i < G; ++i)
+      {
+        const R e = eta[i];
+        R       v = p.L * (e * (p.B * R(12)) * (e * (c - R(2)) + omc + s2));
+        if constexpr (WTD >= 1)
+          v += e * p.w0;
+        if constexpr (WTD == 2)
+          v += fval<DIM>(F, FM::base(FM::h_eta(i)), q, cell);
+        pstore<DIM>(P, DIM + 2 + i, q, cell, v);
+      }
+  }
+
+  // Phase 3: integrate every row of every cell into K[(row * NQ + l) * CP + cell];
+  // contributions of cells outside the mesh (partial tiles) are zero.  `stiff`
+  // holds the nodal values the constant-coefficient gradient terms act on
+  // (component 0 = c for the mu row, component 2 + i = eta_i for the eta rows).
+  template <int DIM, int G, typename R>
+  __device__ __forceinline__ void phase_integrate(const PhysR<R> &p, const Grid &g, const CellConsts<DIM, R> &k,
+                                                  const TileCoord &tc, const R *P, const R *stiff, R *K)
+  {
+    using T            = Tile<DIM>;
+    constexpr int NQ   = 1 << DIM;
+    constexpr int C    = G + 2;
+    constexpr int NGRP = T::THREADS / T::CELLS;
+    const int     cell = threadIdx.x % T::CELLS;
+    const int     b0   = cell_box_base<DIM>(cell);
+    const bool    in   = cell_in_mesh<DIM>(cell, tc, g);
+    for (int row = threadIdx.x / T::CELLS; row < C; row += NGRP)
+      {
+        R r[NQ];
+        if (row == 0)
+          {
+            R v[NQ], gg[DIM][NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+              {
+                v[q] = P[(0 * NQ + q) * T::CELLS + cell];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                  gg[d][q] = P[((1 + d) * NQ + q) * T::CELLS + cell];
+              }
+            cell_integrate_vg<DIM>(v, gg, k, r);
+          }
+        else
+          {
+            const int res = DIM + row; // mu row: DIM + 1, eta_i row (row = 2 + i): DIM + 2 + i
+            R         v[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+              v[q] = P[(res * NQ + q) * T::CELLS + cell];
+            cell_integrate_v<DIM>(v, k, r);
+            R u[NQ];
+            cell_nodes<DIM>(stiff + (row == 1 ? 0 : row) * T::BOX, b0, u);
+            cell_stiffness_add<DIM>(row == 1 ? -p.kc : p.L * p.kp, u, g, r);
+          }
+#pragma unroll
+        for (int l = 0; l < NQ; ++l)
+          K[(row * NQ + l) * T::CP + cell] = in ? r[l] : R(0);
+      }
+  }
+
+  template <int DIM, int G, bool TENS, bool JVP, bool HIST>
+  struct ThreePhaseSmem
+  {
+    using T                     = Tile<DIM>;
+    using FM                    = FieldMap<DIM, G, TENS, JVP, HIST>;
+    static constexpr int C      = G + 2;
+    static constexpr int NQ     = 1 << DIM;
+    static constexpr int BOXES  = 2 * C * T::BOX;                  // both inputs of one tile
+    static constexpr int F_SIZE = FM::NSLOT * T::CELLS;            // point fields (K aliases it)
+    static constexpr int P_SIZE = (DIM + 2 + G) * NQ * T::CELLS;   // point results
+    static constexpr int K_SIZE = C * NQ * T::CP;
+    static_assert(K_SIZE <= F_SIZE, "node contributions must fit in the point-field buffer");
+    // elements: the JVP double-buffers its boxes, the residual does not
+    static constexpr int TOTAL = (JVP ? 2 : 1) * BOXES + F_SIZE + P_SIZE;
+  };
+
+  // -------------------------------------------------------------------------
+  // Jacobian-vector product: dst = J(lin) src.
+  // SinteringOperatorGenericQuad::operator() (operator_sintering_generic.h:101-190)
+  // inside do_vmult_range (:539-577), with the linearisation point evaluated
+  // from the nodal state instead of a quadrature-point cache.  Persistent and
+  // software pipelined: block b handles tiles b, b + grid, ...; the node boxes
+  // of the next tile are copied (cp.async) into the second half of a double
+  // buffer while the current tile is computed.
   // Two resident blocks per SM (<= 128 registers) unless the FP64 grain state
   // of large G would spill; those run one block with up to 255 registers.
   template <int DIM, int G, bool TENS, typename R>
@@ -123,15 +371,18 @@ namespace sint
     jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
                R *__restrict__ dst, R *__restrict__ partial)
   {
-    using T          = Tile<DIM>;
-    constexpr int C  = G + 2;
-    constexpr int VB = 2 * C * T::BOX; // one buffer: linearisation point + direction
+    using T  = Tile<DIM>;
+    using SM = ThreePhaseSmem<DIM, G, TENS, true, false>;
+    constexpr int C = G + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *s_buf = reinterpret_cast<R *>(smem_raw); // 2 x VB
-    R *s_con = s_buf + 2 * VB;
+    R *s_buf = reinterpret_cast<R *>(smem_raw); // 2 x BOXES
+    R *F     = s_buf + 2 * SM::BOXES;
+    R *P     = F + SM::F_SIZE;
+    R *K     = F; // aliases the point fields, dead after phase 2
 
-    const PhysR<R> p(ph);
-    long long      tile = blockIdx.x;
+    const PhysR<R>           p(ph);
+    const CellConsts<DIM, R> k(g);
+    long long                tile = blockIdx.x;
     if (tile < g.n_tiles)
       {
         const BoxNode<DIM> bn(g, tile_coord_of<DIM>(g, tile));
@@ -142,7 +393,7 @@ namespace sint
     for (int it = 0; tile < g.n_tiles; ++it, tile += gridDim.x)
       {
         const long long next = tile + gridDim.x;
-        R              *nb   = s_buf + ((it + 1) & 1) * VB;
+        R              *nb   = s_buf + ((it + 1) & 1) * SM::BOXES;
         if (next < g.n_tiles)
           {
             const BoxNode<DIM> bnn(g, tile_coord_of<DIM>(g, next));
@@ -153,11 +404,15 @@ namespace sint
         cp_async_wait<1>(); // this tile's group has landed (only the prefetch may be pending)
         __syncthreads();
         const TileCoord tc = tile_coord_of<DIM>(g, tile);
-        const R        *cb = s_buf + (it & 1) * VB;
-        jvp_tile<DIM, G, TENS, R>(g, p, cb, cb + C * T::BOX, s_con, tc);
+        const R        *cb = s_buf + (it & 1) * SM::BOXES;
+        phase_evaluate<DIM, G, TENS, true, false, R>(cb, cb + C * T::BOX, F, k);
         __syncthreads();
-        sum_and_store<DIM>(s_con, C, g, tc, BoxNode<DIM>(g, tc), dst, partial);
-        __syncthreads(); // s_con and this buffer are reused by the next iterations
+        jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS);
+        __syncthreads();
+        phase_integrate<DIM, G, R>(p, g, k, tc, P, cb + C * T::BOX, K);
+        __syncthreads();
+        sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial);
+        __syncthreads(); // K and this buffer are reused by the next iterations
       }
     cp_async_wait<0>();
   }
@@ -165,115 +420,61 @@ namespace sint
   // -------------------------------------------------------------------------
   // Nonlinear residual: dst = R(src), SinteringOperatorGenericResidualQuad
   // (operator_sintering_generic.h:254-308) with the history of
-  // do_evalute_history (:927-975) for WTD == 2.  As in the Jacobian, the mu and
-  // eta rows' constant-coefficient gradient terms use the stiffness stencil.
+  // do_evalute_history (:927-975) for WTD == 2: the weighted sum of the old
+  // solutions is formed at the nodes while staging and evaluated at the points.
   template <int DIM, int G, bool TENS, int WTD>
-  __global__ void __launch_bounds__(Tile<DIM>::THREADS)
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, G > 5 ? 1 : 2)
     residual_kernel(const Grid g, const Phys ph, const double *__restrict__ src, const double *__restrict__ h0,
                     const double *__restrict__ h1, const double *__restrict__ h2, double *__restrict__ dst,
                     double *__restrict__ partial)
   {
-    using R          = double;
-    using T          = Tile<DIM>;
-    constexpr int C  = G + 2;
+    using R  = double;
+    using T  = Tile<DIM>;
+    using SM = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2>;
+    constexpr int C = G + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *s_u   = reinterpret_cast<R *>(smem_raw);
-    R *s_h   = s_u + C * T::BOX;
-    R *s_con = s_h + (WTD == 2 ? C : 0) * T::BOX;
+    R *s_u = reinterpret_cast<R *>(smem_raw);
+    R *s_h = s_u + C * T::BOX;
+    R *F   = s_u + SM::BOXES;
+    R *P   = F + SM::F_SIZE;
+    R *K   = F;
 
-    const TileCoord    tc = tile_coord<DIM>(g);
-    const BoxNode<DIM> bn(g, tc);
-    load_box<DIM>(s_u, src, C, g, bn);
-    if constexpr (WTD == 2)
+    const PhysR<R>           p(ph);
+    const CellConsts<DIM, R> k(g);
+    for (long long tile = blockIdx.x; tile < g.n_tiles; tile += gridDim.x)
       {
-        // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966); mu has no history
-        if (bn.active)
-          for (int comp = bn.grp; comp < C; comp += T::NG)
-            {
-              R v = R(0);
-              if (comp != 1 && bn.inside)
+        const TileCoord    tc = tile_coord_of<DIM>(g, tile);
+        const BoxNode<DIM> bn(g, tc);
+        load_box<DIM>(s_u, src, C, g, bn);
+        if constexpr (WTD == 2)
+          {
+            // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966); mu has no history
+            if (bn.active)
+              for (int comp = bn.grp; comp < C; comp += T::NG)
                 {
-                  const long long off = comp * g.ld + bn.gidx;
-                  v                   = h0[off] * ph.w_hist[0];
-                  if (ph.order > 1)
-                    v += h1[off] * ph.w_hist[1];
-                  if (ph.order > 2)
-                    v += h2[off] * ph.w_hist[2];
+                  R v = R(0);
+                  if (comp != 1 && bn.inside)
+                    {
+                      const long long off = comp * g.ld + bn.gidx;
+                      v                   = h0[off] * ph.w_hist[0];
+                      if (ph.order > 1)
+                        v += h1[off] * ph.w_hist[1];
+                      if (ph.order > 2)
+                        v += h2[off] * ph.w_hist[2];
+                    }
+                  s_h[comp * T::BOX + bn.b] = v;
                 }
-              s_h[comp * T::BOX + bn.b] = v;
-            }
+          }
+        __syncthreads();
+        phase_evaluate<DIM, G, TENS, false, WTD == 2, R>(s_u, s_h, F, k);
+        __syncthreads();
+        residual_point<DIM, G, TENS, WTD, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS);
+        __syncthreads();
+        phase_integrate<DIM, G, R>(p, g, k, tc, P, s_u, K);
+        __syncthreads();
+        sum_and_store<DIM>(K, C, g, tc, bn, dst, partial);
+        __syncthreads();
       }
-    __syncthreads();
-
-    const PhysR<R>   p(ph);
-    const QP<DIM, R> w(g);
-    const int        cell  = threadIdx.x / T::NQ;
-    const int        b0    = cell_box_base<DIM>(cell);
-    const bool       valid = cell_in_mesh<DIM>(cell, tc, g);
-
-    R c, gc[DIM], mu, gmu[DIM];
-    if constexpr (TENS)
-      eval_vg<DIM>(s_u, b0, w, c, gc);
-    else
-      c = eval_v<DIM>(s_u, b0, w);
-    eval_vg<DIM>(s_u + T::BOX, b0, w, mu, gmu);
-    R eta[G];
-    R geta[TENS ? G : 1][DIM];
-#pragma unroll
-    for (int i = 0; i < G; ++i)
-      {
-        if constexpr (TENS)
-          eval_vg<DIM>(s_u + (2 + i) * T::BOX, b0, w, eta[i], geta[i]);
-        else
-          eta[i] = eval_v<DIM>(s_u + (2 + i) * T::BOX, b0, w);
-      }
-
-    R s2 = R(0), s3 = R(0);
-#pragma unroll
-    for (int i = 0; i < G; ++i)
-      {
-        s2 += eta[i] * eta[i];
-        s3 += eta[i] * eta[i] * eta[i];
-      }
-    const R omc = R(1) - c;
-
-    // 1) c row (generic.h:275-285)
-    {
-      R v = R(0);
-      if constexpr (WTD >= 1)
-        v = c * p.w0;
-      if constexpr (WTD == 2)
-        v += eval_v<DIM>(s_h, b0, w);
-      R gres[DIM];
-      apply_M<DIM, G, TENS>(p, c, eta, gc, geta, gmu, gres);
-      store_contrib<DIM>(s_con, 0, integrate_butterfly<DIM>(v, gres, w), valid);
-    }
-    // 2) mu row (generic.h:288-289, free_energy.h:124-134): value part - kappa_c K c
-    {
-      const R df_dc = p.A * (c * c) * (R(2) * c - R(2)) + R(2) * p.A * c * (omc * omc) +
-                      p.B * (R(2) * c - R(6) * s2 + R(4) * s3);
-      const R r = integrate_value_butterfly<DIM>(p.walg * mu - df_dc, w) - p.kc * stiffness_apply<DIM>(s_u, b0, w, g);
-      store_contrib<DIM>(s_con, 1, r, valid);
-    }
-    // 3) eta rows (generic.h:293-304, free_energy.h:136-141): value part + L kappa_p K eta_i
-    {
-      const R Lkp = p.L * p.kp;
-#pragma unroll
-      for (int i = 0; i < G; ++i)
-        {
-          const R e = eta[i];
-          R       v = p.L * (e * (p.B * R(12)) * (e * (c - R(2)) + omc + s2));
-          if constexpr (WTD >= 1)
-            v += e * p.w0;
-          if constexpr (WTD == 2)
-            v += eval_v<DIM>(s_h + (2 + i) * T::BOX, b0, w);
-          const R r = integrate_value_butterfly<DIM>(v, w) +
-                      Lkp * stiffness_apply<DIM>(s_u + (2 + i) * T::BOX, b0, w, g);
-          store_contrib<DIM>(s_con, 2 + i, r, valid);
-        }
-    }
-    __syncthreads();
-    sum_and_store<DIM>(s_con, C, g, tc, bn, dst, partial);
   }
 
   // -------------------------------------------------------------------------

@@ -10,9 +10,7 @@
 
 namespace sint
 {
-  // Dynamic shared memory of each kernel (bytes).
-  size_t smem_jvp(int dim, int G, size_t real_bytes);
-  size_t smem_residual(int dim, int G, int wtd);
+  // Dynamic shared memory of the diagonal kernel (bytes).
   size_t smem_diag(int dim, int G);
 
   template <int DIM, bool TENS, typename R>

@@ -20,7 +20,7 @@ namespace sint
   cudaError_t launch_jvp_g(const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
                            cudaStream_t s)
   {
-    const size_t smem = smem_jvp(DIM, G, sizeof(R));
+    const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false>::TOTAL * sizeof(R);
     auto         k    = jvp_kernel<DIM, G, TENS, R>;
     // persistent grid: as many blocks as are resident at once
     static int   grid_cap = 0;
@@ -46,15 +46,26 @@ namespace sint
   cudaError_t launch_residual_g(const Grid &g, const Phys &p, const double *src, const double *const *hist,
                                 double *dst, double *partial, cudaStream_t s)
   {
-    const size_t  smem = smem_residual(DIM, G, WTD);
-    auto          k    = residual_kernel<DIM, G, TENS, WTD>;
-    cudaError_t   e    = prepare_smem(k, smem);
-    if (e != cudaSuccess)
-      return e;
-    const double *h0 = WTD == 2 ? hist[0] : nullptr;
-    const double *h1 = (WTD == 2 && p.order > 1) ? hist[1] : nullptr;
-    const double *h2 = (WTD == 2 && p.order > 2) ? hist[2] : nullptr;
-    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial);
+    const size_t  smem     = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2>::TOTAL * sizeof(double);
+    auto          k        = residual_kernel<DIM, G, TENS, WTD>;
+    static int    grid_cap = 0;
+    cudaError_t   e        = cudaSuccess;
+    if (grid_cap == 0)
+      {
+        if ((e = prepare_smem(k, smem)) != cudaSuccess)
+          return e;
+        int dev = 0, sms = 0, per_sm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+            (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Tile<DIM>::THREADS, smem)) != cudaSuccess)
+          return e;
+        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
+      }
+    const double *h0     = WTD == 2 ? hist[0] : nullptr;
+    const double *h1     = (WTD == 2 && p.order > 1) ? hist[1] : nullptr;
+    const double *h2     = (WTD == 2 && p.order > 2) ? hist[2] : nullptr;
+    const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial);
     count_launches(1);
     return cudaGetLastError();
   }
