@@ -225,6 +225,13 @@ namespace sint
       }
     g.N       = N;
     g.n_tiles = nt;
+    if (nt >= (1ll << 31) || N >= (1ll << 40))
+      {
+        set_error("mesh too large: at most 2^31 - 1 tiles");
+        return SINT_ERR_ARG;
+      }
+    for (int d = 0; d < 2; ++d)
+      make_divisor((unsigned)g.nt[d], g.mdiv[d], g.sdiv[d]);
     // exact Q1 element Laplacian of the uniform cell: K_lm = kx[l xor m], built
     // from the 1D stiffness (1/h)[[1,-1],[-1,1]] and mass (h/6)[[2,1],[1,2]]
     for (int x = 0; x < 8; ++x)

@@ -77,7 +77,28 @@ namespace sint
     // (kx[x] = int grad phi_l . grad phi_(l xor x)), in both precisions.
     double kxd[8];
     float  kxf[8];
+    // division by nt[0] and nt[1] as multiply-shift (exact for n < 2^31):
+    // n / nt[d] = (n * mdiv[d]) >> (32 + sdiv[d])
+    unsigned long long mdiv[2];
+    int                sdiv[2];
   };
+
+  // Granlund-Montgomery division by an invariant integer d >= 1: with
+  // s = ceil(log2 d) and m = ceil(2^(32+s) / d), floor(n / d) = (n m) >> (32+s)
+  // for every 0 <= n < 2^31 (m < 2^33, so n m < 2^64).
+  inline void make_divisor(unsigned d, unsigned long long &m, int &s)
+  {
+    s = 0;
+    while ((1ull << s) < d)
+      ++s;
+    const unsigned long long num = 1ull << (32 + s);
+    m                            = num / d + (num % d != 0 ? 1 : 0);
+  }
+
+  __device__ __forceinline__ unsigned fast_div(unsigned n, unsigned long long m, int s)
+  {
+    return (unsigned)(((unsigned long long)n * m) >> (32 + s));
+  }
 
   template <typename R>
   __device__ __forceinline__ R kx(const Grid &g, int x);
@@ -227,14 +248,14 @@ namespace sint
   __device__ __forceinline__ TileCoord tile_coord_of(const Grid &g, long long tile)
   {
     using T = Tile<DIM>;
-    TileCoord tc;
-    tc.linear   = tile;
-    long long r = tile;
-    tc.t[0]     = int(r % g.nt[0]);
-    r /= g.nt[0];
-    tc.t[1] = int(r % g.nt[1]);
-    r /= g.nt[1];
-    tc.t[2] = int(r);
+    TileCoord      tc;
+    tc.linear         = tile;
+    const unsigned n  = (unsigned)tile; // n_tiles < 2^31 (checked at set-up)
+    const unsigned q0 = fast_div(n, g.mdiv[0], g.sdiv[0]);
+    const unsigned q1 = fast_div(q0, g.mdiv[1], g.sdiv[1]);
+    tc.t[0]           = int(n - q0 * (unsigned)g.nt[0]);
+    tc.t[1]           = int(q0 - q1 * (unsigned)g.nt[1]);
+    tc.t[2]           = int(q1);
     tc.o[0] = tc.t[0] * T::TX;
     tc.o[1] = tc.t[1] * T::TY;
     tc.o[2] = tc.t[2] * T::TZ;

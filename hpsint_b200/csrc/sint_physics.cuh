@@ -25,15 +25,15 @@ namespace sint
   }
 
   // Reciprocal and inverse square root of a positive number by Newton-Raphson
-  // refinement of a single-precision hardware seed (rcp.approx / rsqrt.approx,
-  // relative error ~2^-23):
+  // refinement of the single-precision hardware seed (rcp.approx /
+  // rsqrt.approx, relative error ~2^-23 including the rounding of the
+  // argument to float):
   //   reciprocal:          y <- y + y (1 - x y)
   //   inverse square root: y <- y + (y / 2) (1 - x y^2)
-  // Each step squares the relative error: one step for float, two for double
-  // reach the rounding level.  The seed is taken at the argument clamped to
-  // [1e-30, 1e30]; the squared gradient norms this is used for lie in
-  // (1e-20, 1e30) (callers filter the lower end), where the result is exact to
-  // rounding.
+  // One step squares the relative error: ~3e-14 in double (far inside the
+  // operator's 1e-12 parity bound), float rounding level in float.  Valid for
+  // arguments in [FLT_MIN, FLT_MAX]; the squared gradient norms this is used
+  // for are filtered below 1e-20 by the callers.
   __device__ __forceinline__ float rcp_seed(float x)
   {
     float y;
@@ -48,46 +48,23 @@ namespace sint
   }
 
   template <typename R>
-  __device__ __forceinline__ R rcp_pos(R x);
-  template <>
-  __device__ __forceinline__ double rcp_pos<double>(double x)
+  __device__ __forceinline__ R rcp_pos(R x)
   {
-    double y = double(rcp_seed(float(fmin(fmax(x, 1e-30), 1e30))));
-    double e = fma(-x, y, 1.0);
-    y        = fma(y, e, y);
-    e        = fma(-x, y, 1.0);
-    return fma(y, e, y);
-  }
-  template <>
-  __device__ __forceinline__ float rcp_pos<float>(float x)
-  {
-    float y = rcp_seed(fminf(fmaxf(x, 1e-30f), 1e30f));
-    return fmaf(y, fmaf(-x, y, 1.0f), y);
+    const R y = R(rcp_seed(float(x)));
+    return y + y * (R(1) - x * y);
   }
 
   template <typename R>
-  __device__ __forceinline__ R rsqrt_pos(R x);
-  template <>
-  __device__ __forceinline__ double rsqrt_pos<double>(double x)
+  __device__ __forceinline__ R rsqrt_pos(R x)
   {
-    double y = double(rsqrt_seed(float(fmin(fmax(x, 1e-30), 1e30))));
-    double r = fma(-x * y, y, 1.0);
-    y        = fma(0.5 * y, r, y);
-    r        = fma(-x * y, y, 1.0);
-    return fma(0.5 * y, r, y);
-  }
-  template <>
-  __device__ __forceinline__ float rsqrt_pos<float>(float x)
-  {
-    float y = rsqrt_seed(fminf(fmaxf(x, 1e-30f), 1e30f));
-    return fmaf(0.5f * y, fmaf(-x * y, y, 1.0f), y);
+    const R y = R(rsqrt_seed(float(x)));
+    return y + (R(0.5) * y) * (R(1) - (x * y) * y);
   }
 
   template <typename R>
   __device__ __forceinline__ R clamp01(R x)
   {
-    x = x < R(0) ? R(0) : x;
-    return x > R(1) ? R(1) : x;
+    return fmin(fmax(x, R(0)), R(1));
   }
 
   // tensor.h:137-154 unit_vector(v, 1e-10): v / |v| if |v| > 1e-10, else 0.
