@@ -79,6 +79,26 @@ SIGNATURES = {
     "sint_newton_clear": (_c_int, [_c_void]),
     "sint_newton_solve": (_c_int, [_c_void, _c_void, P(_c_void), P(SintNewtonParams), P(SintNewtonStats),
                                    _c_void]),
+    "sint_nn_conv3x3_f32": (_c_int, [_c_void, _c_int, _c_int, _c_int, _c_int, _c_void, _c_void, _c_void, _c_int,
+                                     _c_int, _c_void]),
+    "sint_nn_conv3x3_flip_f32": (_c_int, [_c_void, _c_int, _c_int, _c_void, _c_void]),
+    "sint_nn_conv3x3_wgrad_workspace": (_c_int64, [_c_int, _c_int, _c_int, _c_int, _c_int]),
+    "sint_nn_conv3x3_wgrad_f32": (_c_int, [_c_void, _c_void, _c_int, _c_int, _c_int, _c_int, _c_int, _c_void, _c_void,
+                                           _c_int, _c_void, _c_void]),
+    "sint_nn_leaky_relu_f32": (_c_int, [_c_int64, ctypes.c_float, _c_void, _c_void, _c_void]),
+    "sint_nn_leaky_relu_bwd_f32": (_c_int, [_c_int64, ctypes.c_float, _c_void, _c_void, _c_void, _c_void]),
+    "sint_nn_grain_sum_f32": (_c_int, [_c_void, _c_int, _c_int, _c_int64, _c_void, _c_void]),
+    "sint_nn_grain_bcast_add_f32": (_c_int, [_c_void, _c_int, _c_int, _c_int64, _c_void, _c_void]),
+    "sint_nn_adam_f32": (_c_int, [_c_int64, _c_void, _c_void, _c_void, _c_void, ctypes.c_float, ctypes.c_float,
+                                  ctypes.c_float, ctypes.c_float, _c_int, _c_void]),
+    "sint_nn_mse_workspace": (_c_int64, []),
+    "sint_nn_mse_f32": (_c_int, [_c_int64, _c_void, _c_void, _c_void, _c_void, _c_void, _c_void, _c_void]),
+    "sint_nn_features_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                      _c_int, ctypes.c_float, _c_void, _c_void, _c_void, _c_int, _c_void]),
+    "sint_nn_targets_f64": (_c_int, [_c_void, _c_void, _c_void, _c_int64, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                     _c_int, _c_int, ctypes.c_float, _c_void, _c_void, _c_void, _c_int, _c_void]),
+    "sint_nn_apply_guess_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,
+                                         _c_void, _c_void, _c_void, _c_void]),
     "sint_device_fma_peak": (_c_int, [_c_int, P(_c_double), _c_void]),
     "sint_last_error": (ctypes.c_char_p, []),
     "sint_kernel_launch_count": (_c_int64, []),

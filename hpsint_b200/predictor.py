@@ -1,0 +1,246 @@
+"""Learned Newton initial guess: a grain-permutation-equivariant conv net.
+
+The net predicts, for each node, the deviation of the next increment from
+linear extrapolation,
+    u_{n+1} - u_n - r (u_n - u_{n-1}),   r = dt_n / dt_{n-1},
+from the last two states; the guess handed to Newton is
+    u_n + r (u_n - u_{n-1}) + prediction.
+It only replaces the initial iterate at the driver's predictor hook
+(sintering/driver.h:2001-2058); the unchanged damped Newton solve to the same
+tolerance decides the answer, so a bad prediction costs iterations, never
+accuracy.
+
+Equivariance: every order parameter eta_i is processed by the same weights
+("grain streams"); grains interact only through the sum over grains (sum
+pooling), and c, mu form a separate "shared stream".  Layer l maps
+    grain:  h_i <- act(A * h_i + B * (sum_j h_j) + C * s + a)
+    shared: s   <- act(D * s + E * (sum_j h_j) + d)
+with 3x3 convolutions A..E (the last layer has no activation and outputs one
+channel per grain and two shared channels: mu-free c and mu corrections).
+Forward, backward and Adam run in the library's CUDA kernels (FP32); torch
+only holds the device memory.
+"""
+import ctypes
+import math
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib as L
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _s():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def conv3x3(x, w, bias, out, accumulate=False):
+    """out (+)= conv(x, w) + bias; x [B][Cin][H][W], w [Cout][Cin][3][3]."""
+    B, Cin, H, W = x.shape
+    Cout = w.shape[0]
+    L.check(L.lib().sint_nn_conv3x3_f32(_p(x), B, Cin, H, W, _p(w), _p(bias), _p(out), Cout, int(accumulate), _s()),
+            "sint_nn_conv3x3_f32")
+
+
+def conv3x3_input_grad(dout, w, din, accumulate=False, wT=None):
+    """din (+)= d(conv(x, w))/dx applied to dout (convolution with the flipped kernel)."""
+    Cout, Cin = w.shape[0], w.shape[1]
+    if wT is None:
+        wT = torch.empty((Cin, Cout, 3, 3), dtype=torch.float32, device="cuda")
+    L.check(L.lib().sint_nn_conv3x3_flip_f32(_p(w), Cout, Cin, _p(wT), _s()), "sint_nn_conv3x3_flip_f32")
+    conv3x3(dout, wT, None, din, accumulate)
+
+
+class _Workspace:
+    """Grow-only scratch for the weight-gradient and loss reductions."""
+
+    def __init__(self):
+        self.buf = torch.empty(0, dtype=torch.float32, device="cuda")
+        self.dbuf = torch.empty(L.lib().sint_nn_mse_workspace(), dtype=torch.float64, device="cuda")
+
+    def get(self, n):
+        if self.buf.numel() < n:
+            self.buf = torch.empty(int(n * 1.25) + 1024, dtype=torch.float32, device="cuda")
+        return self.buf
+
+
+def conv3x3_weight_grad(x, dout, dw, db, ws, accumulate=True):
+    B, Cin, H, W = x.shape
+    Cout = dout.shape[1]
+    n = L.lib().sint_nn_conv3x3_wgrad_workspace(B, Cin, Cout, H, W)
+    work = ws.get(n)
+    L.check(L.lib().sint_nn_conv3x3_wgrad_f32(_p(x), _p(dout), B, Cin, Cout, H, W, _p(dw), _p(db), int(accumulate),
+                                              _p(work), _s()), "sint_nn_conv3x3_wgrad_f32")
+
+
+def leaky(x, y, slope):
+    L.check(L.lib().sint_nn_leaky_relu_f32(x.numel(), slope, _p(x), _p(y), _s()), "sint_nn_leaky_relu_f32")
+
+
+def leaky_bwd(pre, dy, dx, slope):
+    L.check(L.lib().sint_nn_leaky_relu_bwd_f32(pre.numel(), slope, _p(pre), _p(dy), _p(dx), _s()),
+            "sint_nn_leaky_relu_bwd_f32")
+
+
+def grain_sum(h, B, G, P):
+    chw = h[0].numel()
+    L.check(L.lib().sint_nn_grain_sum_f32(_p(h), B, G, chw, _p(P), _s()), "sint_nn_grain_sum_f32")
+
+
+def grain_bcast_add(Q, B, G, Z):
+    chw = Q[0].numel()
+    L.check(L.lib().sint_nn_grain_bcast_add_f32(_p(Q), B, G, chw, _p(Z), _s()), "sint_nn_grain_bcast_add_f32")
+
+
+@dataclass
+class NetConfig:
+    width: int = 32
+    layers: int = 4
+    grain_in: int = 2     # eta_i, extrapolated eta_i increment
+    shared_in: int = 4    # c, c increment, mu, mu increment
+    shared_out: int = 2   # corrections of c and mu (one grain channel per eta_i)
+    slope: float = 0.1    # leaky-ReLU slope
+    seed: int = 0
+
+
+class EquivariantNet:
+    """Parameters live in one flat FP32 device tensor (views per weight); so do
+    their gradients and the Adam moments."""
+
+    NAMES = ("A", "B", "C", "D", "E", "a", "d")
+
+    def __init__(self, cfg: NetConfig = None):
+        self.cfg = cfg = cfg or NetConfig()
+        self.dims = []
+        cg, cs = cfg.grain_in, cfg.shared_in
+        for l in range(cfg.layers):
+            last = l == cfg.layers - 1
+            go, so = (1, cfg.shared_out) if last else (cfg.width, cfg.width)
+            self.dims.append((cg, cs, go, so))
+            cg, cs = go, so
+        self.shapes = []
+        for (cg, cs, go, so) in self.dims:
+            self.shapes.append({"A": (go, cg, 3, 3), "B": (go, cg, 3, 3), "C": (go, cs, 3, 3), "D": (so, cs, 3, 3),
+                                "E": (so, cg, 3, 3), "a": (go,), "d": (so,)})
+        n = sum(math.prod(s) for sh in self.shapes for s in sh.values())
+        self.n_params = n
+        self.params = torch.zeros(n, dtype=torch.float32, device="cuda")
+        self.grads = torch.zeros_like(self.params)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.step_count = 0
+        self.w = self._views(self.params)
+        self.g = self._views(self.grads)
+        self.ws = _Workspace()
+        self._init(cfg.seed)
+
+    def _views(self, flat):
+        out, off = [], 0
+        for sh in self.shapes:
+            d = {}
+            for k in self.NAMES:
+                s = sh[k]
+                d[k] = flat[off:off + math.prod(s)].view(s)
+                off += math.prod(s)
+            out.append(d)
+        return out
+
+    def _init(self, seed):
+        """He-normal weights for the hidden layers, small output layer, zero biases."""
+        gen = torch.Generator().manual_seed(seed)
+        for l, (cg, cs, go, so) in enumerate(self.dims):
+            last = l == len(self.dims) - 1
+            for k in ("A", "B", "C"):
+                fan = 9 * (2 * cg + cs)
+                std = math.sqrt(2.0 / fan) * (0.1 if last else 1.0)
+                self.w[l][k].copy_(torch.randn(self.shapes[l][k], generator=gen) * std)
+            for k in ("D", "E"):
+                fan = 9 * (cs + cg)
+                std = math.sqrt(2.0 / fan) * (0.1 if last else 1.0)
+                self.w[l][k].copy_(torch.randn(self.shapes[l][k], generator=gen) * std)
+
+    # -- forward -------------------------------------------------------------
+    def forward(self, xg, xs, B, G, keep=False):
+        """xg [B*G][grain_in][H][W], xs [B][shared_in][H][W] -> (yg [B*G][1], ys [B][2])."""
+        H, W = xs.shape[2], xs.shape[3]
+        cache = []
+        hg, hs = xg, xs
+        for l, (cg, cs, go, so) in enumerate(self.dims):
+            w = self.w[l]
+            P = torch.empty((B, cg, H, W), dtype=torch.float32, device="cuda")
+            grain_sum(hg, B, G, P)
+            Zg = torch.empty((B * G, go, H, W), dtype=torch.float32, device="cuda")
+            conv3x3(hg, w["A"], w["a"], Zg)
+            Q = torch.empty((B, go, H, W), dtype=torch.float32, device="cuda")
+            conv3x3(P, w["B"], None, Q)
+            conv3x3(hs, w["C"], None, Q, accumulate=True)
+            grain_bcast_add(Q, B, G, Zg)
+            Zs = torch.empty((B, so, H, W), dtype=torch.float32, device="cuda")
+            conv3x3(hs, w["D"], w["d"], Zs)
+            conv3x3(P, w["E"], None, Zs, accumulate=True)
+            if keep:
+                cache.append((hg, hs, P, Zg, Zs))
+            if l < len(self.dims) - 1:
+                ng, ns = torch.empty_like(Zg), torch.empty_like(Zs)
+                leaky(Zg, ng, self.cfg.slope)
+                leaky(Zs, ns, self.cfg.slope)
+                hg, hs = ng, ns
+            else:
+                hg, hs = Zg, Zs
+        return hg, hs, cache
+
+    # -- backward ------------------------------------------------------------
+    def backward(self, cache, dyg, dys, B, G):
+        """Accumulate parameter gradients of a loss with output gradients (dyg, dys)."""
+        dZg, dZs = dyg, dys
+        for l in reversed(range(len(self.dims))):
+            hg, hs, P, Zg, Zs = cache[l]
+            if l < len(self.dims) - 1:
+                leaky_bwd(Zg, dZg, dZg, self.cfg.slope)
+                leaky_bwd(Zs, dZs, dZs, self.cfg.slope)
+            w, g = self.w[l], self.g[l]
+            cg, cs, go, so = self.dims[l]
+            H, W = hs.shape[2], hs.shape[3]
+            dQ = torch.empty((B, go, H, W), dtype=torch.float32, device="cuda")
+            grain_sum(dZg, B, G, dQ)
+            conv3x3_weight_grad(hg, dZg, g["A"], g["a"], self.ws)
+            conv3x3_weight_grad(P, dQ, g["B"], None, self.ws)
+            conv3x3_weight_grad(hs, dQ, g["C"], None, self.ws)
+            conv3x3_weight_grad(hs, dZs, g["D"], g["d"], self.ws)
+            conv3x3_weight_grad(P, dZs, g["E"], None, self.ws)
+            if l == 0:
+                break
+            dhg = torch.empty((B * G, cg, H, W), dtype=torch.float32, device="cuda")
+            conv3x3_input_grad(dZg, w["A"], dhg)
+            dP = torch.empty((B, cg, H, W), dtype=torch.float32, device="cuda")
+            conv3x3_input_grad(dQ, w["B"], dP)
+            conv3x3_input_grad(dZs, w["E"], dP, accumulate=True)
+            grain_bcast_add(dP, B, G, dhg)
+            dhs = torch.empty((B, cs, H, W), dtype=torch.float32, device="cuda")
+            conv3x3_input_grad(dQ, w["C"], dhs)
+            conv3x3_input_grad(dZs, w["D"], dhs, accumulate=True)
+            dZg, dZs = dhg, dhs
+
+    def zero_grad(self):
+        self.grads.zero_()
+
+    def adam_step(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.step_count += 1
+        L.check(L.lib().sint_nn_adam_f32(self.n_params, _p(self.params), _p(self.grads), _p(self.m), _p(self.v),
+                                         lr, beta1, beta2, eps, self.step_count, _s()), "sint_nn_adam_f32")
+
+    def mse(self, pred, target, weight, grad):
+        """loss (device double) and, into grad, its gradient (mean over elements)."""
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        L.check(L.lib().sint_nn_mse_f32(pred.numel(), _p(pred), _p(target), _p(weight), _p(grad), _p(loss),
+                                        _p(self.ws.dbuf), _s()), "sint_nn_mse_f32")
+        return loss
+
+    def state_dict(self):
+        return {"cfg": self.cfg.__dict__, "params": self.params.detach().cpu()}
+
+    def load_params(self, flat):
+        self.params.copy_(flat.to(self.params.device))

@@ -46,9 +46,11 @@ class StepRecord:
 class TimeIntegrator:
     """Advance u_t = ... with BDF and adaptive dt on the GPU.
 
-    predictor(u_old_list, dt) -> device tensor or None: optional initial
-    Newton iterate (the learned predictor plugs in here); None means the
-    previous solution (hpsint's "None" predictor).
+    predictor(history, dts, dt) -> device tensor or None: optional initial
+    Newton iterate for the step of size dt, given the last solutions
+    (history[0] = u_n, history[1] = u_{n-1} once it exists) and the accepted
+    steps (dts[0] = dt_{n-1} ...); the learned predictor plugs in here.  None
+    means the previous solution (hpsint's "None" predictor).
     """
 
     def __init__(self, op: SinteringOperatorGeneric, nl: NonLinearData = None, td: TimeIntegrationData = None,
@@ -81,7 +83,7 @@ class TimeIntegrator:
         while True:
             w0, wh = self._weights(self.dt)
             self.op.set_time_weights(w0, wh, 1.0)
-            guess = self.predictor(self.history, self.dt) if self.predictor else None
+            guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
             u = (guess if guess is not None else self.history[0]).clone()
             st = self.newton.solve(u, self.history[:len(wh)], raise_on_failure=False)
             if st.status == L.SINT_OK:
@@ -99,7 +101,7 @@ class TimeIntegrator:
                                        st.residual_evaluations, tries, time.perf_counter() - t0))
         self.history.insert(0, u)
         self.dts.insert(0, self.dt)
-        keep = max(1, self.td.scheme_order)
+        keep = max(2, self.td.scheme_order)  # predictors use the last two states
         self.history = self.history[:keep]
         self.dts = self.dts[:keep]
         good = (st.newton_iterations < self.td.desirable_newton_iterations and
@@ -108,7 +110,22 @@ class TimeIntegrator:
             self.dt = min(self.dt * self.td.growth_factor, self.td.time_step_max)
         return u
 
-    def run(self, n_steps):
-        for _ in range(n_steps):
-            self.step()
-        return self.history[0]
+    def run(self, n_steps, dt_schedule=None, keep_states=False):
+        """n_steps accepted steps.  dt_schedule: replay these step sizes instead
+        of the adaptive control (a failure then raises).  keep_states: return
+        every accepted solution (device tensors) as well."""
+        states = [self.history[0].clone()] if keep_states else None
+        for i in range(n_steps):
+            if dt_schedule is not None:
+                self.dt = dt_schedule[i]
+                min_dt = self.td.time_step_min
+                self.td.time_step_min = dt_schedule[i]  # no halving below the schedule: fail instead
+                try:
+                    self.step()
+                finally:
+                    self.td.time_step_min = min_dt
+            else:
+                self.step()
+            if keep_states:
+                states.append(self.history[0].clone())
+        return (self.history[0], states) if keep_states else self.history[0]

@@ -247,6 +247,62 @@ int sint_newton_solve(sint_ctx *ctx, double *u, const double *const *hist, const
 
 /* ---------------------------------------------------------------------- */
 
+/* ---------------------------------------------------------------------- */
+/* Learned Newton initial guess (no counterpart in the reference: it plugs  */
+/* in at the driver's predictor hook, sintering/driver.h:2001-2058).  FP32 */
+/* building blocks of a grain-permutation-equivariant convolutional net;    */
+/* tensors are NCHW float32 device arrays, grain streams of sample b are    */
+/* batch entries b * G + i.  All calls are asynchronous on `stream`.        */
+
+/* out[b][co] (+)= bias[co] + sum_ci w[co][ci] (*) in[b][ci]: 3x3, zero padding,
+ * stride 1.  bias may be NULL; accumulate != 0 adds to out. */
+int sint_nn_conv3x3_f32(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias,
+                        float *out, int Cout, int accumulate, sint_stream_t stream);
+/* wT[ci][co][8 - k] = w[co][ci][k]: the kernel whose convolution with the
+ * output gradient is the input gradient. */
+int sint_nn_conv3x3_flip_f32(const float *w, int Cout, int Cin, float *wT, sint_stream_t stream);
+/* floats of workspace sint_nn_conv3x3_wgrad_f32 needs for these sizes */
+int64_t sint_nn_conv3x3_wgrad_workspace(int B, int Cin, int Cout, int H, int W);
+/* dw[co][ci][k] (+)= sum_{b,pixels} dout[b][co] in[b][ci] shifted by tap k;
+ * db[co] (+)= sum dout[b][co] (db may be NULL).  Deterministic. */
+int sint_nn_conv3x3_wgrad_f32(const float *in, const float *dout, int B, int Cin, int Cout, int H, int W, float *dw,
+                              float *db, int accumulate, float *work, sint_stream_t stream);
+int sint_nn_leaky_relu_f32(int64_t n, float slope, const float *x, float *y, sint_stream_t stream);
+/* dx = dy * f'(pre); dx may alias dy */
+int sint_nn_leaky_relu_bwd_f32(int64_t n, float slope, const float *pre, const float *dy, float *dx,
+                               sint_stream_t stream);
+/* P[b] = sum_i h[b G + i] over tensors of chw elements per entry */
+int sint_nn_grain_sum_f32(const float *h, int B, int G, int64_t chw, float *P, sint_stream_t stream);
+/* Z[b G + i] += Q[b] */
+int sint_nn_grain_bcast_add_f32(const float *Q, int B, int G, int64_t chw, float *Z, sint_stream_t stream);
+/* Adam (Kingma & Ba 2015) with bias correction at step >= 1 */
+int sint_nn_adam_f32(int64_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1,
+                     float beta2, float eps, int step, sint_stream_t stream);
+/* doubles of workspace sint_nn_mse_f32 needs */
+int64_t sint_nn_mse_workspace(void);
+/* loss[0] = sum w (pred - target)^2 / n (weight may be NULL = 1); grad (may be
+ * NULL) = 2 w (pred - target) / n.  Deterministic. */
+int sint_nn_mse_f32(int64_t n, const float *pred, const float *target, const float *weight, float *grad,
+                    double *loss, double *work, sint_stream_t stream);
+/* Network inputs of the Hc x Wc node window at (x0, y0) of a 2D mesh with
+ * nx x ny nodes, written to batch entry b: shared channels
+ * (c, ratio (c_n - c_{n-1}), mu, ratio (mu_n - mu_{n-1})) scaled by scale[0..3],
+ * grain channels (eta_i, ratio (eta_i,n - eta_i,n-1)) scaled by scale[4..5];
+ * nodes outside the mesh read 0.  ratio = dt_n / dt_{n-1}. */
+int sint_nn_features_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int nx, int ny, int G, int x0,
+                         int y0, int Hc, int Wc, float ratio, const float *scale, float *grain_in, float *shared_in,
+                         int b, sint_stream_t stream);
+/* Training targets of the same window: (u_{n+1} - u_n - ratio (u_n - u_{n-1}))
+ * scaled by oscale[0] (c), oscale[1] (mu), oscale[2] (eta). */
+int sint_nn_targets_f64(const double *u_np1, const double *u_n, const double *u_nm1, int64_t block_stride, int nx,
+                        int ny, int G, int x0, int y0, int Hc, int Wc, float ratio, const float *oscale,
+                        float *grain_t, float *shared_t, int b, sint_stream_t stream);
+/* guess = u_n + ratio (u_n - u_{n-1}) + out / oscale over all n_nodes nodes
+ * (network outputs of one whole-mesh window). */
+int sint_nn_apply_guess_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int64_t n_nodes, int G,
+                            float ratio, const float *oscale, const float *grain_out, const float *shared_out,
+                            double *guess, sint_stream_t stream);
+
 /* Measured FMA throughput of the current device in TFLOP/s (precision 64 or
  * 32): the denominator of the cell kernels' ALU roofline.  Synchronous. */
 int sint_device_fma_peak(int precision, double *tflops, sint_stream_t stream);

@@ -147,7 +147,7 @@ def test_time_integrator_halves_dt_on_failure_and_grows_after_good_steps():
     op = hb.SinteringOperatorGeneric(hb.Mesh(2, cells + (1,)), hb.Params(G))
     calls = []
 
-    def poisoned_once(history, dt):
+    def poisoned_once(history, dts, dt):
         calls.append(dt)
         if len(calls) == 1:
             g = history[0].clone()

@@ -1,0 +1,91 @@
+"""CUDA kernels of the learned Newton guess against the NumPy reference
+(oracle/predictor_ref.py, itself checked against finite differences).
+FP32 kernels vs FP64 reference: relative tolerance 2e-5 of the tensor norm."""
+import numpy as np
+import pytest
+
+from oracle import predictor_ref as R
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def dev(x):
+    return torch.tensor(np.asarray(x, np.float32), device="cuda").contiguous()
+
+
+@pytest.mark.parametrize("N,Cin,Cout,H,W", [(2, 3, 5, 19, 23), (1, 32, 32, 33, 17), (3, 2, 1, 16, 16)])
+def test_conv3x3_forward_and_gradients(N, Cin, Cout, H, W):
+    from hpsint_b200 import predictor as P
+    rng = np.random.default_rng(N * 100 + Cin)
+    x, w, b = rng.normal(size=(N, Cin, H, W)), rng.normal(size=(Cout, Cin, 3, 3)), rng.normal(size=Cout)
+    dout = rng.normal(size=(N, Cout, H, W))
+    out = torch.empty((N, Cout, H, W), device="cuda")
+    P.conv3x3(dev(x), dev(w), dev(b), out)
+    assert rel(out.cpu().numpy(), R.conv3x3(x, w, b)) < 2e-5
+    din = torch.empty((N, Cin, H, W), device="cuda")
+    P.conv3x3_input_grad(dev(dout), dev(w), din)
+    assert rel(din.cpu().numpy(), R.conv3x3_input_grad(dout, w)) < 2e-5
+    dw, db = torch.zeros((Cout, Cin, 3, 3), device="cuda"), torch.zeros(Cout, device="cuda")
+    P.conv3x3_weight_grad(dev(x), dev(dout), dw, db, P._Workspace(), accumulate=False)
+    rw, rb = R.conv3x3_weight_grad(x, dout)
+    assert rel(dw.cpu().numpy(), rw) < 2e-5 and rel(db.cpu().numpy(), rb) < 2e-5
+
+
+def to_ref(net):
+    return [{k: v.detach().double().cpu().numpy() for k, v in layer.items()} for layer in net.w]
+
+
+def test_network_forward_backward_match_reference():
+    from hpsint_b200 import predictor as P
+    net = P.EquivariantNet(P.NetConfig(width=6, layers=3, seed=3))
+    B, G, H, W = 2, 3, 18, 20
+    rng = np.random.default_rng(5)
+    xg, xs = rng.normal(size=(B * G, 2, H, W)), rng.normal(size=(B, 4, H, W))
+    tg, ts = rng.normal(size=(B * G, 1, H, W)), rng.normal(size=(B, 2, H, W))
+    yg, ys, cache = net.forward(dev(xg), dev(xs), B, G, keep=True)
+    params = to_ref(net)
+    ryg, rys, rcache = R.forward(params, xg, xs, B, G, net.cfg.slope)
+    assert rel(yg.cpu().numpy(), ryg) < 2e-5 and rel(ys.cpu().numpy(), rys) < 2e-5
+    net.zero_grad()
+    net.backward(cache, dev(ryg - tg), dev(rys - ts), B, G)
+    rgrads = R.backward(params, rcache, ryg - tg, rys - ts, B, G, net.cfg.slope)
+    for l, layer in enumerate(net.g):
+        for k, g in layer.items():
+            assert rel(g.cpu().numpy(), rgrads[l][k]) < 1e-4, (l, k)
+
+
+def test_network_is_grain_permutation_equivariant():
+    from hpsint_b200 import predictor as P
+    net = P.EquivariantNet(P.NetConfig(width=8, layers=3, seed=1))
+    B, G, H, W = 1, 4, 16, 16
+    rng = np.random.default_rng(2)
+    xg, xs = rng.normal(size=(B * G, 2, H, W)), rng.normal(size=(B, 4, H, W))
+    perm = [3, 1, 0, 2]
+    yg, ys, _ = net.forward(dev(xg), dev(xs), B, G)
+    yg2, ys2, _ = net.forward(dev(xg[perm]), dev(xs), B, G)
+    assert torch.allclose(yg2, yg[perm], atol=1e-5) and torch.allclose(ys2, ys, atol=1e-5)
+
+
+def test_adam_and_mse_match_reference():
+    from hpsint_b200 import predictor as P
+    net = P.EquivariantNet(P.NetConfig(width=4, layers=2))
+    rng = np.random.default_rng(7)
+    p0 = net.params.cpu().numpy().astype(np.float64)
+    g = rng.normal(size=net.n_params)
+    net.grads.copy_(dev(g))
+    net.adam_step(lr=1e-2)
+    net.adam_step(lr=1e-2)
+    rp, rm, rv = R.adam(p0, g, np.zeros_like(p0), np.zeros_like(p0), 1e-2, 0.9, 0.999, 1e-8, 1)
+    rp, rm, rv = R.adam(rp, g, rm, rv, 1e-2, 0.9, 0.999, 1e-8, 2)
+    assert rel(net.params.cpu().numpy(), rp) < 1e-6
+    pred, tgt, wt = rng.normal(size=1000), rng.normal(size=1000), rng.uniform(0, 1, 1000)
+    grad = torch.empty(1000, device="cuda")
+    loss = net.mse(dev(pred), dev(tgt), dev(wt), grad).item()
+    assert abs(loss - np.sum(wt * (pred - tgt) ** 2) / 1000) < 1e-5 * loss
+    assert rel(grad.cpu().numpy(), 2 * wt * (pred - tgt) / 1000) < 1e-6
