@@ -50,8 +50,17 @@ def parse_args():
     ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["operator", "solve2d"], default="operator",
-                    help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve")
+    ap.add_argument("--workload", choices=["operator", "solve2d", "learned2d"], default="operator",
+                    help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
+                         "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
+    ap.add_argument("--train-seeds", type=int, default=10)
+    ap.add_argument("--train-steps", type=int, default=200, help="FP64 steps per training trajectory")
+    ap.add_argument("--train-iters", type=int, default=4000)
+    ap.add_argument("--eval-seeds", type=int, default=2)
+    ap.add_argument("--eval-steps", type=int, default=100)
+    ap.add_argument("--cells", type=int, default=512)
+    ap.add_argument("--circles", type=int, default=100)
+    ap.add_argument("--save-net", default=None, help="write the trained parameters (.pt) here")
     ap.add_argument("--solve-steps", type=int, default=100)
     return ap.parse_args()
 
@@ -237,6 +246,59 @@ def two_particle_solve(args):
     print(json.dumps(line), flush=True)
 
 
+def learned_guess_solve(args):
+    """2D many-grain packings (cells^2 Q1 cells, circles with radii U[6, 12],
+    <= 8 order parameters, scalar mobility, BDF1, dt0 = 1e-3, Newton
+    relative tolerance 1e-8): FP64 training trajectories on train seeds,
+    Adam training of the equivariant net on the device, then on held-out
+    seeds the plain FP64 solve (previous-solution guess, hpsint's dt control)
+    against FP64 + linear guess, FP64 + learned guess, FP32-inner plain and
+    FP32-inner + learned guess on the plain run's time grid.  Every arm stops
+    at the same absolute Newton tolerance (1e-8 relative to the residual of the
+    old solution), so the final fields must agree."""
+    import torch
+
+    from hpsint_b200 import learned_guess as LG
+    from hpsint_b200.predictor import NetConfig
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    train = list(range(args.train_seeds))
+    held = list(range(1000, 1000 + args.eval_seeds))
+    net, norm, trainer, info = LG.train_learned_guess(
+        train, n=args.cells, n_circles=args.circles, n_steps=args.train_steps, net_cfg=NetConfig(),
+        train_cfg=LG.TrainConfig(iterations=args.train_iters), verbose=False)
+    if args.save_net:
+        torch.save({"state": net.state_dict(), "base": norm.base}, args.save_net)
+    evals = []
+    for seed in held:
+        case = LG.make_case(seed, n=args.cells, n_circles=args.circles)
+        res = LG.compare_arms(case, args.eval_steps, net, norm)
+        evals.append({"seed": seed, "G": case.G, "dofs": case.op.C * case.op.N, "arms": res})
+        del case
+        torch.cuda.empty_cache()
+
+    def total(arm, key):
+        return sum(e["arms"][arm][key] for e in evals if arm in e["arms"] and key in e["arms"][arm])
+
+    steps = args.eval_steps * len(evals)
+    plain_s = total("fp64_plain", "wall_s") / steps
+    best_s = total("fp32_inner_learned", "wall_s") / steps
+    line = {"metric": METRIC, "workload": f"2d-{args.cells}x{args.cells}-{args.circles}-circles-learned-guess",
+            "value": best_s, "unit": "s/step", "higher_is_better": False, "n_gpus": 1,
+            "dtype": "f64 Newton, f32 GMRES + f32 net", "data": "synthetic seeded packings",
+            "fp64_plain_s_per_step": plain_s, "speedup_vs_fp64_plain": plain_s / best_s if best_s > 0 else None,
+            "arms_s_per_step": {a: total(a, "wall_s") / steps for a in LG.ARMS},
+            "arms_newton_iterations": {a: total(a, "newton_iterations") for a in LG.ARMS},
+            "arms_linear_iterations": {a: total(a, "linear_iterations") for a in LG.ARMS},
+            "max_abs_diff_vs_fp64_plain": {a: max((max(e["arms"][a]["max_abs_diff_c"], e["arms"][a]["max_abs_diff_eta"])
+                                                   for e in evals if "max_abs_diff_c" in e["arms"].get(a, {})),
+                                                  default=None) for a in LG.ARMS},
+            "training": {k: v for k, v in info.items() if k != "loss_history"},
+            "loss_first_last": [info["loss_history"][0][1], info["loss_history"][-1][1]],
+            "eval": evals}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -244,6 +306,9 @@ def main():
         return
     if args.workload == "solve2d":
         two_particle_solve(args)
+        return
+    if args.workload == "learned2d":
+        learned_guess_solve(args)
         return
     import torch
 

@@ -97,6 +97,8 @@ SIGNATURES = {
                                       _c_int, ctypes.c_float, _c_void, _c_void, _c_void, _c_int, _c_void]),
     "sint_nn_targets_f64": (_c_int, [_c_void, _c_void, _c_void, _c_int64, _c_int, _c_int, _c_int, _c_int, _c_int,
                                      _c_int, _c_int, ctypes.c_float, _c_void, _c_void, _c_void, _c_int, _c_void]),
+    "sint_nn_increment_scales_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,
+                                              _c_void, _c_void, _c_void, _c_void]),
     "sint_nn_apply_guess_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,
                                          _c_void, _c_void, _c_void, _c_void]),
     "sint_device_fma_peak": (_c_int, [_c_int, P(_c_double), _c_void]),
@@ -128,6 +130,11 @@ def lib():
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def last_error():
+    """Text of the last error the library recorded on this thread."""
+    return lib().sint_last_error().decode(errors="replace")
 
 
 def check(status, where):

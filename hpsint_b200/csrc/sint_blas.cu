@@ -37,10 +37,75 @@ namespace sint
     return r;
   }
 
-  // partial[j * NB_RED + blockIdx.x] = sum over this block's slice of w . V_j
-  template <typename R, int M>
+  // --- 16-byte packs ---------------------------------------------------------
+  // The Krylov kernels move 16 bytes per load (2 doubles or 4 floats) when
+  // every pointer is 16-byte aligned and n, stride are multiples of the pack;
+  // otherwise one element per load (E = 1).  Block vectors of a context
+  // always qualify: ld is a multiple of 32.
+  template <typename R, int E>
+  struct Pack
+  {
+    R v[E];
+  };
+
+  template <typename R, int E>
+  __device__ __forceinline__ Pack<R, E> ld_pack(const R *__restrict__ p, long long c)
+  {
+    Pack<R, E> x;
+    if constexpr (E * sizeof(R) == 16 && sizeof(R) == 8)
+      {
+        const double2 t = reinterpret_cast<const double2 *>(p)[c];
+        x.v[0] = t.x, x.v[1] = t.y;
+      }
+    else if constexpr (E * sizeof(R) == 16 && sizeof(R) == 4)
+      {
+        const float4 t = reinterpret_cast<const float4 *>(p)[c];
+        x.v[0] = t.x, x.v[1] = t.y, x.v[2] = t.z, x.v[3] = t.w;
+      }
+    else
+      {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          x.v[e] = p[c * E + e];
+      }
+    return x;
+  }
+
+  template <typename R, int E>
+  __device__ __forceinline__ void st_pack(R *__restrict__ p, long long c, const Pack<R, E> &x)
+  {
+    if constexpr (E * sizeof(R) == 16 && sizeof(R) == 8)
+      reinterpret_cast<double2 *>(p)[c] = make_double2(x.v[0], x.v[1]);
+    else if constexpr (E * sizeof(R) == 16 && sizeof(R) == 4)
+      reinterpret_cast<float4 *>(p)[c] = make_float4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    else
+      {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          p[c * E + e] = x.v[e];
+      }
+  }
+
+  template <typename R>
+  constexpr int pack_of()
+  {
+    return 16 / int(sizeof(R));
+  }
+
+  inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+  template <typename R>
+  inline bool can_pack(long long n, long long stride, const void *a, const void *b)
+  {
+    constexpr int E = pack_of<R>();
+    return n % E == 0 && stride % E == 0 && aligned16(a) && aligned16(b);
+  }
+
+  // partial[j * NB_RED + blockIdx.x] = sum over this block's chunks of w . V_j
+  // (FP64 products and sums; m <= M).
+  template <typename R, int M, int E>
   __global__ void __launch_bounds__(RED_THREADS)
-    multidot_kernel(long long n, const R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
+    multidot_kernel(long long nc, const R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
                     double *__restrict__ partial)
   {
     __shared__ double s_w[RED_THREADS / 32];
@@ -48,13 +113,18 @@ namespace sint
 #pragma unroll
     for (int j = 0; j < M; ++j)
       acc[j] = 0.0;
-    for (long long i = (long long)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (long long)NB_RED * RED_THREADS)
+    for (long long c = (long long)blockIdx.x * RED_THREADS + threadIdx.x; c < nc; c += (long long)NB_RED * RED_THREADS)
       {
-        const double wi = double(w[i]);
+        const Pack<R, E> wi = ld_pack<R, E>(w, c);
 #pragma unroll
         for (int j = 0; j < M; ++j)
           if (j < m)
-            acc[j] += wi * double(V[j * stride + i]);
+            {
+              const Pack<R, E> vj = ld_pack<R, E>(V + j * stride, c);
+#pragma unroll
+              for (int e = 0; e < E; ++e)
+                acc[j] += double(wi.v[e]) * double(vj.v[e]);
+            }
       }
 #pragma unroll
     for (int j = 0; j < M; ++j)
@@ -78,6 +148,8 @@ namespace sint
       out[blockIdx.x] = v;
   }
 
+  constexpr int MD = 16; // vectors per multidot / multiaxpy pass (accumulators in registers)
+
   template <typename R>
   static int launch_multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out,
                              cudaStream_t s)
@@ -87,12 +159,16 @@ namespace sint
         set_error("multidot: m out of range");
         return SINT_ERR_ARG;
       }
-    for (int j0 = 0; j0 < m; j0 += 8)
+    constexpr int E    = pack_of<R>();
+    const bool    pack = can_pack<R>(n, stride, w, V);
+    for (int j0 = 0; j0 < m; j0 += MD)
       {
-        const int mm = m - j0 < 8 ? m - j0 : 8;
-        // one pass per 8 vectors keeps the accumulators in registers
-        multidot_kernel<R, 8><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm,
-                                                             c->red + (size_t)j0 * NB_RED);
+        const int mm = m - j0 < MD ? m - j0 : MD;
+        double   *pp = c->red + (size_t)j0 * NB_RED;
+        if (pack)
+          multidot_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride / E * E, mm, pp);
+        else
+          multidot_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, pp);
         count_launches(1);
       }
     finish_kernel<<<m, RED_THREADS, 0, s>>>(c->red, out);
@@ -120,68 +196,130 @@ namespace sint
     return launch_multidot<float>(c, n, x, y, 0, 1, out, s);
   }
 
-  // w -= sum_j coef[j] V_j
-  template <typename R, int M>
-  __global__ void __launch_bounds__(256) multiaxpy_kernel(long long n, R *__restrict__ w, const R *__restrict__ V,
-                                                          long long stride, int m, const double *__restrict__ coef)
+  // w -= sum_j coef[j] V_j (j < m <= M); with `partial`, also the block
+  // partials of |w|^2 after the update (FP64), for the norm that follows.
+  template <typename R, int M, int E>
+  __global__ void __launch_bounds__(RED_THREADS)
+    multiaxpy_kernel(long long nc, R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
+                     const double *__restrict__ coef, double *__restrict__ partial)
   {
-    __shared__ R s_c[M];
+    __shared__ R      s_c[M];
+    __shared__ double s_w[RED_THREADS / 32];
     if (threadIdx.x < M)
       s_c[threadIdx.x] = threadIdx.x < m ? R(coef[threadIdx.x]) : R(0);
     __syncthreads();
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    double nrm = 0.0;
+    for (long long c = (long long)blockIdx.x * RED_THREADS + threadIdx.x; c < nc; c += (long long)gridDim.x * RED_THREADS)
       {
-        R acc = w[i];
+        Pack<R, E> acc = ld_pack<R, E>(w, c);
 #pragma unroll
         for (int j = 0; j < M; ++j)
           if (j < m)
-            acc -= s_c[j] * V[j * stride + i];
-        w[i] = acc;
+            {
+              const Pack<R, E> vj = ld_pack<R, E>(V + j * stride, c);
+#pragma unroll
+              for (int e = 0; e < E; ++e)
+                acc.v[e] -= s_c[j] * vj.v[e];
+            }
+        st_pack<R, E>(w, c, acc);
+        if (partial)
+          {
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+              nrm += double(acc.v[e]) * double(acc.v[e]);
+          }
+      }
+    if (partial)
+      {
+        const double t = block_sum(nrm, s_w);
+        if (threadIdx.x == 0)
+          partial[blockIdx.x] = t;
       }
   }
 
   template <typename R>
-  int multiaxpy(long long n, R *w, const R *V, long long stride, int m, const double *coef, cudaStream_t s)
+  static int launch_multiaxpy(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
+                              double *norm2_out, cudaStream_t s)
   {
-    for (int j0 = 0; j0 < m; j0 += 8)
+    constexpr int E    = pack_of<R>();
+    const bool    pack = can_pack<R>(n, stride, w, V);
+    for (int j0 = 0; j0 < m; j0 += MD)
       {
-        const int mm = m - j0 < 8 ? m - j0 : 8;
-        multiaxpy_kernel<R, 8><<<1184, 256, 0, s>>>(n, w, V + j0 * stride, stride, mm, coef + j0);
+        const int mm   = m - j0 < MD ? m - j0 : MD;
+        double   *part = (norm2_out && j0 + MD >= m) ? c->red : nullptr; // norm in the last pass
+        if (pack)
+          multiaxpy_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, coef + j0,
+                                                                    part);
+        else
+          multiaxpy_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, coef + j0,
+                                                                    part);
+        count_launches(1);
+      }
+    if (norm2_out)
+      {
+        finish_kernel<<<1, RED_THREADS, 0, s>>>(c->red, norm2_out);
         count_launches(1);
       }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SINT_OK : cuda_fail(e, "multiaxpy");
   }
+
+  template <typename R>
+  int multiaxpy(long long n, R *w, const R *V, long long stride, int m, const double *coef, cudaStream_t s)
+  {
+    return launch_multiaxpy<R>(nullptr, n, w, V, stride, m, coef, nullptr, s);
+  }
   template int multiaxpy<double>(long long, double *, const double *, long long, int, const double *, cudaStream_t);
   template int multiaxpy<float>(long long, float *, const float *, long long, int, const double *, cudaStream_t);
 
+  template <typename R>
+  int multiaxpy_norm2(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
+                      double *norm2_out, cudaStream_t s)
+  {
+    return launch_multiaxpy<R>(c, n, w, V, stride, m, coef, norm2_out, s);
+  }
+  template int multiaxpy_norm2<double>(Ctx *, long long, double *, const double *, long long, int, const double *,
+                                       double *, cudaStream_t);
+  template int multiaxpy_norm2<float>(Ctx *, long long, float *, const float *, long long, int, const double *,
+                                      double *, cudaStream_t);
+
   // y += sum_j coef[j] V_j
-  template <typename R, int M>
-  __global__ void __launch_bounds__(256) lincomb_kernel(long long n, R *__restrict__ y, const R *__restrict__ V,
+  template <typename R, int M, int E>
+  __global__ void __launch_bounds__(256) lincomb_kernel(long long nc, R *__restrict__ y, const R *__restrict__ V,
                                                         long long stride, int m, const double *__restrict__ coef)
   {
     __shared__ R s_c[M];
     if (threadIdx.x < M)
       s_c[threadIdx.x] = threadIdx.x < m ? R(coef[threadIdx.x]) : R(0);
     __syncthreads();
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x)
       {
-        R acc = y[i];
+        Pack<R, E> acc = ld_pack<R, E>(y, c);
 #pragma unroll
         for (int j = 0; j < M; ++j)
           if (j < m)
-            acc += s_c[j] * V[j * stride + i];
-        y[i] = acc;
+            {
+              const Pack<R, E> vj = ld_pack<R, E>(V + j * stride, c);
+#pragma unroll
+              for (int e = 0; e < E; ++e)
+                acc.v[e] += s_c[j] * vj.v[e];
+            }
+        st_pack<R, E>(y, c, acc);
       }
   }
 
   template <typename R>
   int lincomb(long long n, R *y, const R *V, long long stride, int m, const double *coef, cudaStream_t s)
   {
-    for (int j0 = 0; j0 < m; j0 += 8)
+    constexpr int E    = pack_of<R>();
+    const bool    pack = can_pack<R>(n, stride, y, V);
+    for (int j0 = 0; j0 < m; j0 += MD)
       {
-        const int mm = m - j0 < 8 ? m - j0 : 8;
-        lincomb_kernel<R, 8><<<1184, 256, 0, s>>>(n, y, V + j0 * stride, stride, mm, coef + j0);
+        const int mm = m - j0 < MD ? m - j0 : MD;
+        if (pack)
+          lincomb_kernel<R, MD, E><<<1184, 256, 0, s>>>(n / E, y, V + j0 * stride, stride, mm, coef + j0);
+        else
+          lincomb_kernel<R, MD, 1><<<1184, 256, 0, s>>>(n, y, V + j0 * stride, stride, mm, coef + j0);
         count_launches(1);
       }
     const cudaError_t e = cudaGetLastError();
@@ -190,23 +328,56 @@ namespace sint
   template int lincomb<double>(long long, double *, const double *, long long, int, const double *, cudaStream_t);
   template int lincomb<float>(long long, float *, const float *, long long, int, const double *, cudaStream_t);
 
-  template <typename R>
-  __global__ void axpby_kernel(long long n, R a, const R *__restrict__ x, R b, R *__restrict__ y)
+  // y = b y + a x; a term whose factor is 0 is dropped, so NaN in an unused
+  // operand does not spread.  With d_div: a = 1 / d_div[0] read on the device.
+  template <typename R, int E>
+  __global__ void axpby_kernel(long long nc, R a, const R *__restrict__ x, R b, R *__restrict__ y,
+                               const double *__restrict__ d_div)
   {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-      y[i] = (b == R(0) ? R(0) : b * y[i]) + (a == R(0) ? R(0) : a * x[i]);
+    if (d_div)
+      a = R(1.0 / d_div[0]);
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x)
+      {
+        Pack<R, E> xv{}, yv{}, out;
+        if (a != R(0))
+          xv = ld_pack<R, E>(x, c);
+        if (b != R(0))
+          yv = ld_pack<R, E>(y, c);
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          out.v[e] = (b == R(0) ? R(0) : b * yv.v[e]) + (a == R(0) ? R(0) : a * xv.v[e]);
+        st_pack<R, E>(y, c, out);
+      }
+  }
+
+  template <typename R>
+  static int launch_axpby(long long n, double a, const R *x, double b, R *y, const double *d_div, cudaStream_t s)
+  {
+    constexpr int E = pack_of<R>();
+    if (can_pack<R>(n, 0, x, y))
+      axpby_kernel<R, E><<<1184, 256, 0, s>>>(n / E, R(a), x, R(b), y, d_div);
+    else
+      axpby_kernel<R, 1><<<1184, 256, 0, s>>>(n, R(a), x, R(b), y, d_div);
+    count_launches(1);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SINT_OK : cuda_fail(e, "axpby");
   }
 
   template <typename R>
   int axpby(long long n, double a, const R *x, double b, R *y, cudaStream_t s)
   {
-    axpby_kernel<R><<<1184, 256, 0, s>>>(n, R(a), x, R(b), y);
-    count_launches(1);
-    const cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? SINT_OK : cuda_fail(e, "axpby");
+    return launch_axpby<R>(n, a, x, b, y, nullptr, s);
   }
   template int axpby<double>(long long, double, const double *, double, double *, cudaStream_t);
   template int axpby<float>(long long, double, const float *, double, float *, cudaStream_t);
+
+  template <typename R>
+  int scale_by_device(long long n, const R *x, const double *d_div, R *y, cudaStream_t s)
+  {
+    return launch_axpby<R>(n, 1.0, x, 0.0, y, d_div, s);
+  }
+  template int scale_by_device<double>(long long, const double *, const double *, double *, cudaStream_t);
+  template int scale_by_device<float>(long long, const float *, const double *, float *, cudaStream_t);
 
   template <typename S, typename D>
   __global__ void convert_kernel(long long n, const S *__restrict__ x, D *__restrict__ y)

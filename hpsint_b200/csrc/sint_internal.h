@@ -59,6 +59,13 @@ namespace sint
   // w -= sum_i coef[i] * (V + i * stride), coef on the device
   template <typename R>
   int multiaxpy(long long n, R *w, const R *V, long long stride, int m, const double *coef, cudaStream_t s);
+  // w -= sum_i coef[i] * V_i and norm2_out[0] = |w|^2 after the update (device scalar)
+  template <typename R>
+  int multiaxpy_norm2(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
+                      double *norm2_out, cudaStream_t s);
+  // y = x / d_div[0] (divisor on the device)
+  template <typename R>
+  int scale_by_device(long long n, const R *x, const double *d_div, R *y, cudaStream_t s);
   // y = a * x + b * y  (a, b on the host)
   template <typename R>
   int axpby(long long n, double a, const R *x, double b, R *y, cudaStream_t s);

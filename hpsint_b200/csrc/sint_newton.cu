@@ -199,8 +199,7 @@ namespace sint
             // classical Gram-Schmidt: h = V^T w, w -= V h
             double *hcol = &H[j * (m + 1)];
             if ((rc = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s)) ||
-                (rc = multiaxpy<R>(n, w, V, n, j + 1, ws->d_s, s)) ||
-                (rc = multidot<R>(c, n, w, w, 0, 1, ws->d_s + MAX_MULTIDOT, s)))
+                (rc = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s)))
               return rc;
             {
               cudaError_t e = cudaMemcpyAsync(ws->h_s, ws->d_s, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s);
@@ -223,8 +222,7 @@ namespace sint
               {
                 // second Gram-Schmidt pass (norm dropped by more than 30%)
                 if ((rc = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s)) ||
-                    (rc = multiaxpy<R>(n, w, V, n, j + 1, ws->d_s, s)) ||
-                    (rc = multidot<R>(c, n, w, w, 0, 1, ws->d_s + MAX_MULTIDOT, s)))
+                    (rc = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s)))
                   return rc;
                 cudaError_t e =
                   cudaMemcpyAsync(ws->h_s, ws->d_s, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s);

@@ -345,6 +345,51 @@ namespace sint
         }
   }
 
+  // Largest extrapolated increment |ratio (u_n - u_{n-1})| of c, mu and the
+  // order parameters over all nodes.  Non-negative floats order like their
+  // bit patterns, so an unsigned atomicMax gives the same result in any order.
+  __global__ void increment_max_kernel(const double *__restrict__ u_n, const double *__restrict__ u_nm1, long long ld,
+                                       long long N, int G, float ratio, unsigned *__restrict__ work)
+  {
+    float m[3] = {0.f, 0.f, 0.f};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+      for (int k = 0; k < 2 + G; ++k)
+        {
+          const long long o = k * ld + i;
+          const float     d = fabsf(float((u_n[o] - u_nm1[o]) * double(ratio)));
+          const int       g = k < 2 ? k : 2;
+          m[g]              = fmaxf(m[g], d);
+        }
+#pragma unroll
+    for (int g = 0; g < 3; ++g)
+      {
+        float v = m[g];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+          v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0)
+          atomicMax(work + g, __float_as_uint(v));
+      }
+  }
+
+  // scale = (base_c, 1/m_c, base_mu, 1/m_mu, base_eta, 1/m_eta),
+  // oscale = (k_c/m_c, k_mu/m_mu, k_eta/m_eta); base = (base_c, base_mu,
+  // base_eta, k_c, k_mu, k_eta).  A zero increment keeps scale 1.
+  __global__ void increment_scales_kernel(const unsigned *__restrict__ work, const float *__restrict__ base,
+                                          float *__restrict__ scale, float *__restrict__ oscale)
+  {
+    if (threadIdx.x != 0)
+      return;
+    for (int g = 0; g < 3; ++g)
+      {
+        const float m   = __uint_as_float(work[g]);
+        const float inv = m > 1e-30f ? 1.f / m : 1.f;
+        scale[2 * g]     = base[g];
+        scale[2 * g + 1] = inv;
+        oscale[g]        = base[3 + g] * inv;
+      }
+  }
+
   static int launch_err(const char *what)
   {
     count_launches(1);
@@ -516,6 +561,25 @@ int sint_nn_apply_guess_f64(const double *u_n, const double *u_nm1, int64_t bloc
   apply_guess_kernel<<<1184, 256, 0, s>>>(u_n, u_nm1, block_stride, n_nodes, G, ratio, oscale, grain_out, shared_out,
                                           guess);
   return launch_err("sint_nn_apply_guess_f64");
+}
+
+int sint_nn_increment_scales_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int64_t n_nodes, int G,
+                                 float ratio, const float *base, unsigned *work, float *scale, float *oscale,
+                                 sint_stream_t s)
+{
+  if (!u_n || !u_nm1 || !base || !work || !scale || !oscale || G < 1 || n_nodes < 1)
+    {
+      set_error("sint_nn_increment_scales_f64: bad argument");
+      return SINT_ERR_ARG;
+    }
+  const cudaError_t e = cudaMemsetAsync(work, 0, 3 * sizeof(unsigned), s);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "sint_nn_increment_scales_f64: memset");
+  increment_max_kernel<<<592, 256, 0, s>>>(u_n, u_nm1, block_stride, n_nodes, G, ratio, work);
+  if (int rc = launch_err("sint_nn_increment_scales_f64"))
+    return rc;
+  increment_scales_kernel<<<1, 32, 0, s>>>(work, base, scale, oscale);
+  return launch_err("sint_nn_increment_scales_f64: scales");
 }
 
 } // extern "C"

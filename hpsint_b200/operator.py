@@ -188,6 +188,13 @@ class SinteringOperatorGeneric:
     def clear(self):
         pass
 
+    def norm(self, v):
+        """l2 norm of a whole FP64 block vector (deterministic device reduction); synchronises."""
+        self._check_vec(v, torch.float64)
+        out = torch.empty(1, dtype=torch.float64, device="cuda")
+        L.check(L.lib().sint_vec_norm2_f64(self._h, v.numel(), _ptr(v), _ptr(out), _stream()), "sint_vec_norm2_f64")
+        return float(out.item())
+
     # --- helpers --------------------------------------------------------------
     def _check_vec(self, t, dtype):
         if not (t.is_cuda and t.dtype == dtype and t.is_contiguous() and t.numel() == self.C * self.ld):
@@ -276,12 +283,13 @@ class DampedNewtonSolver:
         self.op = op
         self.data = data or NonLinearData()
 
-    def solve(self, u, history, raise_on_failure=True):
+    def solve(self, u, history, raise_on_failure=True, data: NonLinearData = None):
+        """data overrides the solver's NonLinearData for this solve only."""
         op = self.op
         op._check_vec(u, torch.float64)
         arr = (ctypes.c_void_p * max(1, len(history)))(*[h.data_ptr() for h in history])
         st = L.SintNewtonStats()
-        prm = self.data.to_c()
+        prm = (data or self.data).to_c()
         rc = L.lib().sint_newton_solve(op._h, _ptr(u), arr, ctypes.byref(prm), ctypes.byref(st), _stream())
         stats = NewtonStatistics(st.newton_iterations, st.linear_iterations, st.residual_evaluations,
                                  st.jacobian_setups, st.preconditioner_setups, st.initial_residual,

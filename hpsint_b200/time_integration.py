@@ -13,7 +13,7 @@ The solution stays on the device; a step is one sint_newton_solve call (or
 several after failures).
 """
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 
 import torch
 
@@ -41,6 +41,8 @@ class StepRecord:
     residual_evaluations: int
     failed_tries: int
     wall_s: float
+    initial_residual: float = 0.0
+    final_residual: float = 0.0
 
 
 class TimeIntegrator:
@@ -51,30 +53,61 @@ class TimeIntegrator:
     (history[0] = u_n, history[1] = u_{n-1} once it exists) and the accepted
     steps (dts[0] = dt_{n-1} ...); the learned predictor plugs in here.  None
     means the previous solution (hpsint's "None" predictor).
+
+    tolerance_base decides what Newton's relative tolerance is relative to:
+      "initial_guess"  the residual at the initial iterate, as hpsint's
+                       NewtonSolverSolverControl (solvers_nonlinear.h:92-117);
+      "old_solution"   the residual at u_n under the new step's weights, i.e.
+                       the initial residual of the unpredicted solve.  Every
+                       predictor is then held to the same absolute stop
+                       nl_rel_tol * |R(u_n)|, so a better guess can only save
+                       iterations, never loosen the answer.  Without a
+                       predictor the two rules coincide.
     """
 
     def __init__(self, op: SinteringOperatorGeneric, nl: NonLinearData = None, td: TimeIntegrationData = None,
-                 predictor=None):
+                 predictor=None, tolerance_base="initial_guess"):
+        if tolerance_base not in ("initial_guess", "old_solution"):
+            raise ValueError(f"tolerance_base must be 'initial_guess' or 'old_solution', not {tolerance_base!r}")
         self.op = op
         self.nl = nl or NonLinearData()
         self.td = td or TimeIntegrationData()
         self.newton = DampedNewtonSolver(op, self.nl)
         self.predictor = predictor
+        self.tolerance_base = tolerance_base
+        self._r = None
         self.history = []     # old solutions, most recent first (device tensors)
         self.dts = []         # accepted time steps, most recent first
         self.t = 0.0
         self.dt = self.td.time_step_init
         self.records = []
+        self.failures = []    # (t, dt, status, message, newton its, linear its, |r0|, |r|) of failed attempts
 
     def initialize(self, u0):
+        """Start a run from u0: forgets earlier steps and the Newton history
+        that decides preconditioner rebuilds."""
         self.history = [u0.clone()]
         self.dts = []
         self.t = 0.0
+        self.dt = self.td.time_step_init
+        self.records = []
+        self.newton.clear()
 
     def _weights(self, dt):
         order = min(self.td.scheme_order, len(self.history))
         w = bdf_weights(order, [dt] + self.dts[:order - 1])
         return w[0], w[1:order + 1]
+
+    def _stop_rule(self, wh):
+        """NonLinearData for a predicted solve under tolerance_base."""
+        if self.tolerance_base == "initial_guess":
+            return None
+        if self._r is None:
+            self._r = self.op.initialize_dof_vector()
+        hist = self.history[:len(wh)]
+        self.op.evaluate_nonlinear_residual(self._r, self.history[0], 2, hist)
+        ref = self.op.norm(self._r)
+        return replace(self.nl, nl_abs_tol=max(self.nl.nl_abs_tol, self.nl.nl_rel_tol * ref), nl_rel_tol=0.0)
 
     def step(self, u_out=None):
         """One accepted time step; returns the new solution (device)."""
@@ -84,21 +117,28 @@ class TimeIntegrator:
             w0, wh = self._weights(self.dt)
             self.op.set_time_weights(w0, wh, 1.0)
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
+            data = self._stop_rule(wh) if guess is not None else None
             u = (guess if guess is not None else self.history[0]).clone()
-            st = self.newton.solve(u, self.history[:len(wh)], raise_on_failure=False)
+            st = self.newton.solve(u, self.history[:len(wh)], raise_on_failure=False, data=data)
             if st.status == L.SINT_OK:
                 break
             # process_failure: halve dt, restore the last good state, forget the
             # Newton history that decides preconditioner rebuilds
             tries += 1
+            self.failures.append((self.t, self.dt, st.status, L.last_error(), st.newton_iterations,
+                                  st.linear_iterations, st.initial_residual, st.final_residual))
             self.dt *= 0.5
             self.newton.clear()
             if self.dt <= self.td.time_step_min:
-                raise L.SintError(8, "TimeIntegrator.step", "Minimum timestep size exceeded, solution failed!")
+                last = self.failures[-1]
+                raise L.SintError(8, "TimeIntegrator.step",
+                                  f"Minimum timestep size exceeded, solution failed! (t = {self.t:.6g}, last "
+                                  f"Newton status {last[2]}: {last[3]})")
         torch.cuda.synchronize()
         self.t += self.dt
         self.records.append(StepRecord(self.t, self.dt, st.newton_iterations, st.linear_iterations,
-                                       st.residual_evaluations, tries, time.perf_counter() - t0))
+                                       st.residual_evaluations, tries, time.perf_counter() - t0,
+                                       st.initial_residual, st.final_residual))
         self.history.insert(0, u)
         self.dts.insert(0, self.dt)
         keep = max(2, self.td.scheme_order)  # predictors use the last two states

@@ -303,6 +303,15 @@ int sint_nn_apply_guess_f64(const double *u_n, const double *u_nm1, int64_t bloc
                             float ratio, const float *oscale, const float *grain_out, const float *shared_out,
                             double *guess, sint_stream_t stream);
 
+/* Per-state scales of the network inputs and outputs: with m_c, m_mu, m_eta
+ * the largest |ratio (u_n - u_{n-1})| of c, mu and any eta_i over the mesh,
+ * scale = (base[0], 1/m_c, base[1], 1/m_mu, base[2], 1/m_eta) and
+ * oscale = (base[3]/m_c, base[4]/m_mu, base[5]/m_eta) (device arrays; a zero
+ * increment gives 1/m = 1).  work: 3 device unsigned ints of scratch. */
+int sint_nn_increment_scales_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int64_t n_nodes, int G,
+                                 float ratio, const float *base, unsigned *work, float *scale, float *oscale,
+                                 sint_stream_t stream);
+
 /* Measured FMA throughput of the current device in TFLOP/s (precision 64 or
  * 32): the denominator of the cell kernels' ALU roofline.  Synchronous. */
 int sint_device_fma_peak(int precision, double *tflops, sint_stream_t stream);
