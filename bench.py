@@ -50,9 +50,10 @@ def parse_args():
     ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["operator", "solve2d", "learned2d"], default="operator",
+    ap.add_argument("--workload", choices=["operator", "solve2d", "solve3d", "learned2d"], default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
+    ap.add_argument("--n3", type=int, default=192, help="cells per direction of the 3D solve workload")
     ap.add_argument("--train-seeds", type=int, default=10)
     ap.add_argument("--train-steps", type=int, default=200, help="FP64 steps per training trajectory")
     ap.add_argument("--train-iters", type=int, default=4000)
@@ -246,6 +247,76 @@ def two_particle_solve(args):
     print(json.dumps(line), flush=True)
 
 
+def mixed_precision_solve_3d(args):
+    """3D mixed-precision solve: 192^3 Q1 cells at unit spacing, 51 spheres
+    with lognormal radii (median 10, sigma 0.2) in a random sequential packing
+    with 2-cell overlaps, coloured to <= 10 order parameters, width-2 tanh
+    profiles, tensorial mobility with hpsint's default constants, BDF1 with
+    dt0 = 1e-4 and hpsint's dt control, Newton relative tolerance 1e-8.  The
+    FP64-inner solve fixes the time grid; the FP32-inner solve (FP32 GMRES(30)
+    vectors, Jacobian and block-Jacobi inside FP64 Newton) replays it.  Reports
+    s/step of both and the FP32-inner run's errors against the FP64-inner run."""
+    import torch
+
+    import hpsint_b200 as hb
+    from hpsint_b200 import packings as P
+    from hpsint_b200.time_integration import TimeIntegrationData, TimeIntegrator
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = args.n3
+    centers, radii, colours = P.lognormal_packing_3d(n=n)
+    G = int(colours.max()) + 1
+    u0 = P.initial_state(3, (n, n, n), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), centers, radii, colours, width=2.0)
+    w = np.ones(n + 1)
+    w[[0, -1]] = 0.5
+    op = hb.SinteringOperatorGeneric(hb.Mesh(3, (n, n, n)), hb.Params(**model_params(G, not args.scalar)))
+    u0d = op.to_device(u0)
+    c0 = float(np.einsum("k,j,i,kji->", w, w, w, u0[0].reshape(n + 1, n + 1, n + 1)))
+    del u0
+    runs, schedule = {}, None
+    for label, prec in (("fp64_inner", 64), ("fp32_inner", 32)):
+        ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec),
+                            TimeIntegrationData(time_step_init=1e-4))
+        ti.initialize(u0d)
+        ti.run(2, dt_schedule=[1e-4, 1e-4])  # warm-up: workspaces, first launches (discarded)
+        ti.initialize(u0d)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ti.run(args.solve_steps, dt_schedule=schedule)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        if schedule is None:
+            schedule = [r.dt for r in ti.records]
+        u = op.to_host(ti.history[0])
+        c_int = float(np.einsum("k,j,i,kji->", w, w, w, u[0].reshape(n + 1, n + 1, n + 1)))
+        recs = ti.records
+        runs[label] = dict(u=u, wall=wall, recs=recs, c_int=c_int)
+        del ti
+    ref, mp = runs["fp64_inner"], runs["fp32_inner"]
+    line = {"metric": METRIC, "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-G{G}",
+            "unit": "s/step", "higher_is_better": False, "dofs": op.C * op.N, "grains": G,
+            "steps": args.solve_steps, "dtype": "f64 Newton", "data": "synthetic seeded packing",
+            "mobility": "scalar" if args.scalar else "tensorial"}
+    for label, r in runs.items():
+        recs = r["recs"]
+        line[label] = {"s_per_step": r["wall"] / len(recs), "sim_time": float(sum(x.dt for x in recs)),
+                       "s_per_accepted_attempt": sum(x.accepted_wall_s for x in recs) / len(recs),
+                       "newton_iterations": sum(x.newton_iterations for x in recs),
+                       "linear_iterations": sum(x.linear_iterations for x in recs),
+                       "failed_tries": sum(x.failed_tries for x in recs),
+                       "max_final_residual": max(x.final_residual for x in recs),
+                       "int_c_rel_change": abs(r["c_int"] - c0) / abs(c0)}
+    line["fp32_inner_vs_fp64_inner"] = {
+        "max_abs_diff_c": float(np.abs(mp["u"][0] - ref["u"][0]).max()),
+        "max_abs_diff_eta": float(np.abs(mp["u"][2:] - ref["u"][2:]).max()),
+        "speedup_s_per_step": (ref["wall"] / len(ref["recs"])) / (mp["wall"] / len(mp["recs"])),
+        # failed FP64 attempts (dt halvings) fix the grid the FP32 run replays; without their time:
+        "speedup_accepted_attempts": sum(x.accepted_wall_s for x in ref["recs"]) /
+                                     sum(x.accepted_wall_s for x in mp["recs"]),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def learned_guess_solve(args):
     """2D many-grain packings (cells^2 Q1 cells, circles with radii U[6, 12],
     <= 8 order parameters, scalar mobility, BDF1, dt0 = 1e-3, Newton
@@ -306,6 +377,9 @@ def main():
         return
     if args.workload == "solve2d":
         two_particle_solve(args)
+        return
+    if args.workload == "solve3d":
+        mixed_precision_solve_3d(args)
         return
     if args.workload == "learned2d":
         learned_guess_solve(args)

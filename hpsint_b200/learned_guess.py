@@ -351,8 +351,8 @@ class LearnedPredictor:
     """Whole-mesh inference: features of (u_{n-1}, u_n, r) -> net -> guess
     u_n + r (u_n - u_{n-1}) + output / oscale.  FP32 network, FP64 guess."""
 
-    def __init__(self, op: SinteringOperatorGeneric, net: EquivariantNet, norm: Normaliser):
-        self.op, self.net = op, net
+    def __init__(self, op: SinteringOperatorGeneric, net: EquivariantNet, norm: Normaliser, tensor_cores=True):
+        self.op, self.net, self.tensor_cores = op, net, tensor_cores
         self.base, self.inc = norm.device(), IncrementScales()
         self.scale = torch.ones(6, dtype=torch.float32, device="cuda")
         self.oscale = torch.ones(3, dtype=torch.float32, device="cuda")
@@ -375,7 +375,7 @@ class LearnedPredictor:
         L.check(lib.sint_nn_features_f64(_p(history[0]), _p(history[1]), op.ld, self.nx, self.ny, G, 0, 0, self.ny,
                                          self.nx, r, _p(self.scale), _p(self.xg), _p(self.xs), 0, _s()),
                 "sint_nn_features_f64")
-        yg, ys, _ = self.net.forward(self.xg, self.xs, 1, G)
+        yg, ys, _ = self.net.forward(self.xg, self.xs, 1, G, tensor_cores=self.tensor_cores)
         L.check(lib.sint_nn_apply_guess_f64(_p(history[0]), _p(history[1]), op.ld, op.N, G, r, _p(self.oscale),
                                             _p(yg), _p(ys), _p(self.guess), _s()), "sint_nn_apply_guess_f64")
         self.calls += 1

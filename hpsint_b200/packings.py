@@ -107,3 +107,24 @@ def two_particle_2d():
     centers = np.array([[-10.0, 0.0], [10.0, 0.0]])
     radii = np.array([10.0, 10.0])
     return centers, radii, np.array([0, 1])
+
+
+def colour_with_budget(centers, radii, max_grains, buffers=(32.0, 28.0, 24.0, 20.0, 16.0, 12.0, 8.0, 4.0)):
+    """Greedy colouring with the largest buffer (cells between surfaces) whose
+    colouring needs at most max_grains order parameters."""
+    for buffer in buffers:
+        colours = greedy_colouring(centers, radii, buffer)
+        if colours.max() + 1 <= max_grains:
+            return colours
+    raise RuntimeError(f"no colouring with <= {max_grains} order parameters")
+
+
+def lognormal_packing_3d(n=192, n_spheres=51, median=10.0, sigma=0.2, overlap=2.0, max_grains=10, seed=0):
+    """3D solve workload: n^3 unit cells, spheres with lognormal radii
+    (median, sigma of log r) in a random sequential packing where every new
+    sphere touches an earlier one with a 2-cell overlap, coloured to at most
+    max_grains order parameters; returns (centers, radii, colours)."""
+    rng = np.random.default_rng(seed)
+    centers, radii = place_spheres(3, [0, 0, 0], [n, n, n], n_spheres,
+                                   lambda r: float(np.exp(r.normal(np.log(median), sigma))), overlap, rng)
+    return centers, radii, colour_with_budget(centers, radii, max_grains)

@@ -45,6 +45,15 @@ def conv3x3(x, w, bias, out, accumulate=False):
             "sint_nn_conv3x3_f32")
 
 
+def conv3x3_tc(x, w, bias, out, status, accumulate=False):
+    """conv3x3 on the tensor cores (TF32 products, FP32 accumulation); Cout <= 32, Cin <= 32.
+    status: device int32 tensor, set to 1 by the kernel if a tensor-core wait timed out."""
+    B, Cin, H, W = x.shape
+    Cout = w.shape[0]
+    L.check(L.lib().sint_nn_conv3x3_tc_f32(_p(x), B, Cin, H, W, _p(w), _p(bias), _p(out), Cout, int(accumulate),
+                                           _p(status), _s()), "sint_nn_conv3x3_tc_f32")
+
+
 def conv3x3_input_grad(dout, w, din, accumulate=False, wT=None):
     """din (+)= d(conv(x, w))/dx applied to dout (convolution with the flipped kernel)."""
     Cout, Cin = w.shape[0], w.shape[1]
@@ -135,6 +144,7 @@ class EquivariantNet:
         self.w = self._views(self.params)
         self.g = self._views(self.grads)
         self.ws = _Workspace()
+        self.tc_status = torch.zeros(1, dtype=torch.int32, device="cuda")
         self._init(cfg.seed)
 
     def _views(self, flat):
@@ -163,24 +173,33 @@ class EquivariantNet:
                 self.w[l][k].copy_(torch.randn(self.shapes[l][k], generator=gen) * std)
 
     # -- forward -------------------------------------------------------------
-    def forward(self, xg, xs, B, G, keep=False):
-        """xg [B*G][grain_in][H][W], xs [B][shared_in][H][W] -> (yg [B*G][1], ys [B][2])."""
+    def forward(self, xg, xs, B, G, keep=False, tensor_cores=False):
+        """xg [B*G][grain_in][H][W], xs [B][shared_in][H][W] -> (yg [B*G][1], ys [B][2]).
+        tensor_cores: run the convolutions on the tensor cores (TF32 products,
+        FP32 accumulation; inference) instead of the FP32 kernel."""
         H, W = xs.shape[2], xs.shape[3]
         cache = []
         hg, hs = xg, xs
+
+        def conv(x, wt, bias, out, accumulate=False):
+            if tensor_cores and wt.shape[0] <= 32 and wt.shape[1] <= 32:
+                conv3x3_tc(x, wt, bias, out, self.tc_status, accumulate)
+            else:
+                conv3x3(x, wt, bias, out, accumulate)
+
         for l, (cg, cs, go, so) in enumerate(self.dims):
             w = self.w[l]
             P = torch.empty((B, cg, H, W), dtype=torch.float32, device="cuda")
             grain_sum(hg, B, G, P)
             Zg = torch.empty((B * G, go, H, W), dtype=torch.float32, device="cuda")
-            conv3x3(hg, w["A"], w["a"], Zg)
+            conv(hg, w["A"], w["a"], Zg)
             Q = torch.empty((B, go, H, W), dtype=torch.float32, device="cuda")
-            conv3x3(P, w["B"], None, Q)
-            conv3x3(hs, w["C"], None, Q, accumulate=True)
+            conv(P, w["B"], None, Q)
+            conv(hs, w["C"], None, Q, accumulate=True)
             grain_bcast_add(Q, B, G, Zg)
             Zs = torch.empty((B, so, H, W), dtype=torch.float32, device="cuda")
-            conv3x3(hs, w["D"], w["d"], Zs)
-            conv3x3(P, w["E"], None, Zs, accumulate=True)
+            conv(hs, w["D"], w["d"], Zs)
+            conv(P, w["E"], None, Zs, accumulate=True)
             if keep:
                 cache.append((hg, hs, P, Zg, Zs))
             if l < len(self.dims) - 1:
@@ -223,6 +242,13 @@ class EquivariantNet:
             conv3x3_input_grad(dQ, w["C"], dhs)
             conv3x3_input_grad(dZs, w["D"], dhs, accumulate=True)
             dZg, dZs = dhg, dhs
+
+    def check_tensor_cores(self):
+        """Raise if a tensor-core convolution reported a timed-out wait (synchronises)."""
+        if int(self.tc_status.item()) != 0:
+            self.tc_status.zero_()
+            raise L.SintError(3, "EquivariantNet",
+                              "tensor-core convolution timed out waiting for its MMAs")
 
     def zero_grad(self):
         self.grads.zero_()

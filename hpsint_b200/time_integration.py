@@ -43,6 +43,7 @@ class StepRecord:
     wall_s: float
     initial_residual: float = 0.0
     final_residual: float = 0.0
+    accepted_wall_s: float = 0.0   # the successful attempt alone (wall_s includes failed tries)
 
 
 class TimeIntegrator:
@@ -114,6 +115,7 @@ class TimeIntegrator:
         tries = 0
         t0 = time.perf_counter()
         while True:
+            t_try = time.perf_counter()
             w0, wh = self._weights(self.dt)
             self.op.set_time_weights(w0, wh, 1.0)
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
@@ -136,9 +138,10 @@ class TimeIntegrator:
                                   f"Newton status {last[2]}: {last[3]})")
         torch.cuda.synchronize()
         self.t += self.dt
+        t1 = time.perf_counter()
         self.records.append(StepRecord(self.t, self.dt, st.newton_iterations, st.linear_iterations,
-                                       st.residual_evaluations, tries, time.perf_counter() - t0,
-                                       st.initial_residual, st.final_residual))
+                                       st.residual_evaluations, tries, t1 - t0, st.initial_residual,
+                                       st.final_residual, t1 - t_try))
         self.history.insert(0, u)
         self.dts.insert(0, self.dt)
         keep = max(2, self.td.scheme_order)  # predictors use the last two states

@@ -258,6 +258,13 @@ int sint_newton_solve(sint_ctx *ctx, double *u, const double *const *hist, const
  * stride 1.  bias may be NULL; accumulate != 0 adds to out. */
 int sint_nn_conv3x3_f32(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias,
                         float *out, int Cout, int accumulate, sint_stream_t stream);
+/* The same convolution on the tensor cores (tcgen05.mma kind::tf32, FP32
+ * accumulation in TMEM) for 1 <= Cin <= 32 and 1 <= Cout <= 32: products of TF32
+ * operands (FP32 values with the low 13 mantissa bits ignored).  status: a
+ * device int the caller zeroes; set to 1 if a wait for the tensor core timed
+ * out (the output is then incomplete). */
+int sint_nn_conv3x3_tc_f32(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias,
+                           float *out, int Cout, int accumulate, int *status, sint_stream_t stream);
 /* wT[ci][co][8 - k] = w[co][ci][k]: the kernel whose convolution with the
  * output gradient is the input gradient. */
 int sint_nn_conv3x3_flip_f32(const float *w, int Cout, int Cin, float *wT, sint_stream_t stream);

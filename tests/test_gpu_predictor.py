@@ -89,3 +89,37 @@ def test_adam_and_mse_match_reference():
     loss = net.mse(dev(pred), dev(tgt), dev(wt), grad).item()
     assert abs(loss - np.sum(wt * (pred - tgt) ** 2) / 1000) < 1e-5 * loss
     assert rel(grad.cpu().numpy(), 2 * wt * (pred - tgt) / 1000) < 1e-6
+
+
+@pytest.mark.parametrize("N,Cin,Cout,H,W", [(2, 32, 32, 33, 47), (1, 2, 32, 129, 129), (3, 4, 32, 16, 16),
+                                            (1, 32, 32, 7, 300), (2, 32, 1, 40, 33), (1, 32, 2, 17, 65),
+                                            (1, 5, 17, 21, 9)])
+def test_tensor_core_conv_matches_fp32(N, Cin, Cout, H, W):
+    """tcgen05 kind::tf32 convolution vs the FP32 kernel: TF32 operands keep
+    10 mantissa bits, so the relative error of the output is ~1e-3 at most."""
+    from hpsint_b200 import predictor as P
+    rng = np.random.default_rng(Cin * 7 + H)
+    x, w, b = rng.normal(size=(N, Cin, H, W)), rng.normal(size=(Cout, Cin, 3, 3)), rng.normal(size=Cout)
+    ref = torch.empty((N, Cout, H, W), device="cuda")
+    P.conv3x3(dev(x), dev(w), dev(b), ref)
+    out = torch.full((N, Cout, H, W), 7.0, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    P.conv3x3_tc(dev(x), dev(w), dev(b), out, status)
+    assert int(status.item()) == 0
+    assert rel(out.cpu().numpy(), ref.cpu().numpy()) < 3e-3
+    # accumulate mode adds onto the existing output
+    P.conv3x3_tc(dev(x), dev(w), None, out, status, accumulate=True)
+    P.conv3x3(dev(x), dev(w), None, ref, accumulate=True)
+    assert rel(out.cpu().numpy(), ref.cpu().numpy()) < 3e-3
+
+
+def test_network_inference_on_tensor_cores():
+    from hpsint_b200 import predictor as P
+    net = P.EquivariantNet(P.NetConfig(width=32, layers=4, seed=2))
+    B, G, H, W = 1, 5, 40, 37
+    rng = np.random.default_rng(9)
+    xg, xs = dev(rng.normal(size=(B * G, 2, H, W))), dev(rng.normal(size=(B, 4, H, W)))
+    yg, ys, _ = net.forward(xg, xs, B, G)
+    yg2, ys2, _ = net.forward(xg, xs, B, G, tensor_cores=True)
+    net.check_tensor_cores()
+    assert rel(yg2.cpu().numpy(), yg.cpu().numpy()) < 1e-2 and rel(ys2.cpu().numpy(), ys.cpu().numpy()) < 1e-2
