@@ -353,7 +353,7 @@ def learned_guess_solve(args):
 
     steps = args.eval_steps * len(evals)
     plain_s = total("fp64_plain", "wall_s") / steps
-    best_s = total("fp32_inner_learned", "wall_s") / steps
+    best_s = total("fp32_inner_learned_safeguarded", "wall_s") / steps
     line = {"metric": METRIC, "workload": f"2d-{args.cells}x{args.cells}-{args.circles}-circles-learned-guess",
             "value": best_s, "unit": "s/step", "higher_is_better": False, "n_gpus": 1,
             "dtype": "f64 Newton, f32 GMRES + f32 net", "data": "synthetic seeded packings",
@@ -361,11 +361,14 @@ def learned_guess_solve(args):
             "arms_s_per_step": {a: total(a, "wall_s") / steps for a in LG.ARMS},
             "arms_newton_iterations": {a: total(a, "newton_iterations") for a in LG.ARMS},
             "arms_linear_iterations": {a: total(a, "linear_iterations") for a in LG.ARMS},
+            "guess_residual_ratio_gmean": {a: [e["arms"][a].get("guess_residual_ratio_gmean") for e in evals
+                                               if a in e["arms"]] for a in LG.ARMS},
             "max_abs_diff_vs_fp64_plain": {a: max((max(e["arms"][a]["max_abs_diff_c"], e["arms"][a]["max_abs_diff_eta"])
                                                    for e in evals if "max_abs_diff_c" in e["arms"].get(a, {})),
                                                   default=None) for a in LG.ARMS},
             "training": {k: v for k, v in info.items() if k != "loss_history"},
-            "loss_first_last": [info["loss_history"][0][1], info["loss_history"][-1][1]],
+            # (iteration, training loss, loss of the zero correction = linear extrapolation) at start and end
+            "loss_first_last": [info["loss_history"][0], info["loss_history"][-1]],
             "eval": evals}
     print(json.dumps(line), flush=True)
 

@@ -75,6 +75,7 @@ SIGNATURES = {
     "sint_vec_norm2_f32": (_c_int, [_c_void, _c_int64, _c_void, _c_void, _c_void]),
     "sint_vec_f64_to_f32": (_c_int, [_c_int64, _c_void, _c_void, _c_void]),
     "sint_vec_f32_to_f64": (_c_int, [_c_int64, _c_void, _c_void, _c_void]),
+    "sint_vec_select_f64": (_c_int, [_c_int64, _c_void, _c_void, _c_void, _c_void, _c_void, _c_void]),
     "sint_newton_default_params": (None, [P(SintNewtonParams)]),
     "sint_newton_clear": (_c_int, [_c_void]),
     "sint_newton_solve": (_c_int, [_c_void, _c_void, P(_c_void), P(SintNewtonParams), P(SintNewtonStats),
@@ -99,8 +100,8 @@ SIGNATURES = {
                                      _c_int, _c_int, ctypes.c_float, _c_void, _c_void, _c_void, _c_int, _c_void]),
     "sint_nn_conv3x3_tc_f32": (_c_int, [_c_void, _c_int, _c_int, _c_int, _c_int, _c_void, _c_void, _c_void, _c_int,
                                         _c_int, _c_void, _c_void]),
-    "sint_nn_increment_scales_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,
-                                              _c_void, _c_void, _c_void, _c_void]),
+    "sint_nn_increment_scales_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float,
+                                              ctypes.c_float, _c_void, _c_void, _c_void, _c_void, _c_void]),
     "sint_nn_apply_guess_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,
                                          _c_void, _c_void, _c_void, _c_void]),
     "sint_device_fma_peak": (_c_int, [_c_int, P(_c_double), _c_void]),

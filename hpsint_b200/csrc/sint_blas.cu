@@ -106,8 +106,10 @@ namespace sint
   template <typename R, int M, int E>
   __global__ void __launch_bounds__(RED_THREADS)
     multidot_kernel(long long nc, const R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
-                    double *__restrict__ partial)
+                    double *__restrict__ partial, const int *__restrict__ cond)
   {
+    if (cond && *cond == 0)
+      return;
     __shared__ double s_w[RED_THREADS / 32];
     double            acc[M];
 #pragma unroll
@@ -137,8 +139,11 @@ namespace sint
   }
 
   // out[j] = sum_b partial[j * NB_RED + b] (one block per j, fixed order)
-  __global__ void __launch_bounds__(RED_THREADS) finish_kernel(const double *__restrict__ partial, double *__restrict__ out)
+  __global__ void __launch_bounds__(RED_THREADS)
+    finish_kernel(const double *__restrict__ partial, double *__restrict__ out, const int *__restrict__ cond)
   {
+    if (cond && *cond == 0)
+      return;
     __shared__ double s_w[RED_THREADS / 32];
     double            v = 0.0;
     for (int b = threadIdx.x; b < NB_RED; b += RED_THREADS)
@@ -152,7 +157,7 @@ namespace sint
 
   template <typename R>
   static int launch_multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out,
-                             cudaStream_t s)
+                             cudaStream_t s, const int *cond = nullptr)
   {
     if (m < 1 || m > MAX_MULTIDOT)
       {
@@ -166,12 +171,12 @@ namespace sint
         const int mm = m - j0 < MD ? m - j0 : MD;
         double   *pp = c->red + (size_t)j0 * NB_RED;
         if (pack)
-          multidot_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride / E * E, mm, pp);
+          multidot_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, pp, cond);
         else
-          multidot_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, pp);
+          multidot_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, pp, cond);
         count_launches(1);
       }
-    finish_kernel<<<m, RED_THREADS, 0, s>>>(c->red, out);
+    finish_kernel<<<m, RED_THREADS, 0, s>>>(c->red, out, cond);
     count_launches(1);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SINT_OK : cuda_fail(e, "multidot");
@@ -187,6 +192,17 @@ namespace sint
   template int multidot<float>(Ctx *, long long, const float *, const float *, long long, int, double *,
                                cudaStream_t);
 
+  template <typename R>
+  int multidot_if(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, const int *cond,
+                  cudaStream_t s)
+  {
+    return launch_multidot<R>(c, n, w, V, stride, m, out, s, cond);
+  }
+  template int multidot_if<double>(Ctx *, long long, const double *, const double *, long long, int, double *,
+                                   const int *, cudaStream_t);
+  template int multidot_if<float>(Ctx *, long long, const float *, const float *, long long, int, double *,
+                                  const int *, cudaStream_t);
+
   int dot_f64(Ctx *c, long long n, const double *x, const double *y, double *out, cudaStream_t s)
   {
     return launch_multidot<double>(c, n, x, y, 0, 1, out, s);
@@ -201,8 +217,10 @@ namespace sint
   template <typename R, int M, int E>
   __global__ void __launch_bounds__(RED_THREADS)
     multiaxpy_kernel(long long nc, R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
-                     const double *__restrict__ coef, double *__restrict__ partial)
+                     const double *__restrict__ coef, double *__restrict__ partial, const int *__restrict__ cond)
   {
+    if (cond && *cond == 0)
+      return;
     __shared__ R      s_c[M];
     __shared__ double s_w[RED_THREADS / 32];
     if (threadIdx.x < M)
@@ -239,7 +257,7 @@ namespace sint
 
   template <typename R>
   static int launch_multiaxpy(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
-                              double *norm2_out, cudaStream_t s)
+                              double *norm2_out, cudaStream_t s, const int *cond = nullptr)
   {
     constexpr int E    = pack_of<R>();
     const bool    pack = can_pack<R>(n, stride, w, V);
@@ -249,15 +267,15 @@ namespace sint
         double   *part = (norm2_out && j0 + MD >= m) ? c->red : nullptr; // norm in the last pass
         if (pack)
           multiaxpy_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, coef + j0,
-                                                                    part);
+                                                                    part, cond);
         else
           multiaxpy_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, coef + j0,
-                                                                    part);
+                                                                    part, cond);
         count_launches(1);
       }
     if (norm2_out)
       {
-        finish_kernel<<<1, RED_THREADS, 0, s>>>(c->red, norm2_out);
+        finish_kernel<<<1, RED_THREADS, 0, s>>>(c->red, norm2_out, cond);
         count_launches(1);
       }
     const cudaError_t e = cudaGetLastError();
@@ -282,6 +300,17 @@ namespace sint
                                        double *, cudaStream_t);
   template int multiaxpy_norm2<float>(Ctx *, long long, float *, const float *, long long, int, const double *,
                                       double *, cudaStream_t);
+
+  template <typename R>
+  int multiaxpy_norm2_if(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
+                         double *norm2_out, const int *cond, cudaStream_t s)
+  {
+    return launch_multiaxpy<R>(c, n, w, V, stride, m, coef, norm2_out, s, cond);
+  }
+  template int multiaxpy_norm2_if<double>(Ctx *, long long, double *, const double *, long long, int, const double *,
+                                          double *, const int *, cudaStream_t);
+  template int multiaxpy_norm2_if<float>(Ctx *, long long, float *, const float *, long long, int, const double *,
+                                         double *, const int *, cudaStream_t);
 
   // y += sum_j coef[j] V_j
   template <typename R, int M, int E>
@@ -398,6 +427,16 @@ namespace sint
   template int convert<float, double>(long long, const float *, double *, cudaStream_t);
 
   __global__ void sqrt_kernel(double *x) { x[0] = sqrt(x[0]); }
+
+  __global__ void select_kernel(long long n, const double *__restrict__ a, const double *__restrict__ b,
+                                const double *__restrict__ na, const double *__restrict__ nb, double *out)
+  {
+    const double *src = *na <= *nb ? a : b;
+    if (src == out)
+      return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      out[i] = src[i];
+  }
 } // namespace sint
 
 using namespace sint;
@@ -505,6 +544,24 @@ int sint_vec_f64_to_f32(int64_t n, const double *x, float *y, sint_stream_t s)
   if (int e = check_ptrs(x, y, n))
     return e;
   return n ? convert<double, float>(n, x, y, s) : SINT_OK;
+}
+
+int sint_vec_select_f64(int64_t n, const double *a, const double *b, const double *norm_a, const double *norm_b,
+                        double *out, sint_stream_t s)
+{
+  if (int e = check_ptrs(a, b, n))
+    return e;
+  if (!norm_a || !norm_b || !out)
+    {
+      set_error("sint_vec_select_f64: null pointer");
+      return SINT_ERR_ARG;
+    }
+  if (n == 0)
+    return SINT_OK;
+  select_kernel<<<1184, 256, 0, s>>>(n, a, b, norm_a, norm_b, out);
+  count_launches(1);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SINT_OK : cuda_fail(e, "sint_vec_select_f64");
 }
 
 int sint_vec_f32_to_f64(int64_t n, const float *x, double *y, sint_stream_t s)

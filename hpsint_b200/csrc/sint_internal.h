@@ -63,6 +63,13 @@ namespace sint
   template <typename R>
   int multiaxpy_norm2(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
                       double *norm2_out, cudaStream_t s);
+  // the same two, skipped on the device when *cond == 0 (launched unconditionally, decided on the GPU)
+  template <typename R>
+  int multidot_if(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, const int *cond,
+                  cudaStream_t s);
+  template <typename R>
+  int multiaxpy_norm2_if(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
+                         double *norm2_out, const int *cond, cudaStream_t s);
   // y = x / d_div[0] (divisor on the device)
   template <typename R>
   int scale_by_device(long long n, const R *x, const double *d_div, R *y, cudaStream_t s);

@@ -32,6 +32,13 @@ namespace sint
     double   *d_s = nullptr; // device scalars: [0, MAX_MULTIDOT) dots, [MAX_MULTIDOT] norm
     double   *h_s = nullptr; // pinned host mirror
     double   *d_y = nullptr; // device copy of the GMRES coefficients
+    // device-resident Arnoldi state: Hessenberg matrix (column j at j * (restart + 1)),
+    // Givens rotations, rotated right-hand side g, scalars {|w|, tol}, the DGKS flag
+    double  *d_H = nullptr, *d_cs = nullptr, *d_sn = nullptr, *d_g = nullptr, *d_sc = nullptr;
+    int     *d_flag = nullptr;
+    double2 *d_out = nullptr, *h_out = nullptr; // per iteration {|g_{j+1}|, status}
+    double  *h_H   = nullptr;                   // pinned host copy of H and g at the end of a cycle
+    cudaEvent_t ev[MAX_MULTIDOT] = {};
   };
 
   int free_workspace(Ctx *c)
@@ -50,6 +57,18 @@ namespace sint
     cudaFree(w->d_s);
     cudaFree(w->d_y);
     cudaFreeHost(w->h_s);
+    cudaFree(w->d_H);
+    cudaFree(w->d_cs);
+    cudaFree(w->d_sn);
+    cudaFree(w->d_g);
+    cudaFree(w->d_sc);
+    cudaFree(w->d_flag);
+    cudaFree(w->d_out);
+    cudaFreeHost(w->h_out);
+    cudaFreeHost(w->h_H);
+    for (cudaEvent_t &e : w->ev)
+      if (e)
+        cudaEventDestroy(e);
     delete w;
     c->ws = nullptr;
     return SINT_OK;
@@ -75,12 +94,28 @@ namespace sint
         (e = cudaMalloc(&w->b, nr)) != cudaSuccess || (e = cudaMalloc(&w->x, nr)) != cudaSuccess ||
         (e = cudaMalloc(&w->d_s, sizeof(double) * (MAX_MULTIDOT + 2))) != cudaSuccess ||
         (e = cudaMalloc(&w->d_y, sizeof(double) * (MAX_MULTIDOT + 2))) != cudaSuccess ||
-        (e = cudaMallocHost(&w->h_s, sizeof(double) * (MAX_MULTIDOT + 2))) != cudaSuccess)
+        (e = cudaMallocHost(&w->h_s, sizeof(double) * (MAX_MULTIDOT + 2))) != cudaSuccess ||
+        (e = cudaMalloc(&w->d_H, sizeof(double) * (restart + 1) * (restart + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&w->d_cs, sizeof(double) * (restart + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&w->d_sn, sizeof(double) * (restart + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&w->d_g, sizeof(double) * (restart + 2))) != cudaSuccess ||
+        (e = cudaMalloc(&w->d_sc, sizeof(double) * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&w->d_flag, sizeof(int) * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&w->d_out, sizeof(double2) * (restart + 1))) != cudaSuccess ||
+        (e = cudaMallocHost(&w->h_out, sizeof(double2) * (restart + 1))) != cudaSuccess ||
+        (e = cudaMallocHost(&w->h_H, sizeof(double) * ((restart + 1) * (restart + 1) + restart + 2))) != cudaSuccess)
       {
         const int rc = cuda_fail(e, "newton workspace allocation");
         free_workspace(c);
         return rc;
       }
+    for (int j = 0; j <= restart; ++j)
+      if ((e = cudaEventCreateWithFlags(&w->ev[j], cudaEventDisableTiming)) != cudaSuccess)
+        {
+          const int rc = cuda_fail(e, "newton workspace events");
+          free_workspace(c);
+          return rc;
+        }
     // padding entries take part in dot products: keep every vector zeroed
     if ((e = cudaMemset(w->r, 0, n64)) != cudaSuccess || (e = cudaMemset(w->du, 0, n64)) != cudaSuccess ||
         (e = cudaMemset(w->tmp, 0, n64)) != cudaSuccess || (e = cudaMemset(w->V, 0, nr * (restart + 1))) != cudaSuccess ||
@@ -128,21 +163,127 @@ namespace sint
     return sint_precond_apply_f32(static_cast<sint_ctx *>(c), z, r, s);
   }
 
+  // --- device-resident Arnoldi bookkeeping ------------------------------------
+  // One thread does the O(restart) scalar work of an Arnoldi step on the GPU,
+  // so the host never waits for a Hessenberg column: it only reads the
+  // residual estimate of iteration j while iteration j + 1 already runs.
+
+  // start of a cycle: g = (beta, 0, ...), sc[1] = tol (first cycle) and status
+  __global__ void gmres_cycle_init_kernel(int m, double beta, double *g)
+  {
+    for (int i = threadIdx.x; i <= m; i += blockDim.x)
+      g[i] = i == 0 ? beta : 0.0;
+  }
+
+  // after the first Gram-Schmidt pass: Hessenberg column j = h and the DGKS
+  // decision (second pass when the norm dropped by more than 30 %)
+  __global__ void arnoldi_check_kernel(int j, int ldh, const double *__restrict__ d_s, double *__restrict__ H,
+                                       int *__restrict__ reorth)
+  {
+    if (threadIdx.x != 0)
+      return;
+    double *hcol = H + (long long)j * ldh;
+    double  hh   = 0.0;
+    for (int i = 0; i <= j; ++i)
+      {
+        hcol[i] = d_s[i];
+        hh += d_s[i] * d_s[i];
+      }
+    const double nw2 = d_s[MAX_MULTIDOT];
+    *reorth          = nw2 < 0.49 * (hh + nw2) ? 1 : 0;
+  }
+
+  // after the (optional) second pass: |w|, Givens rotations, residual estimate.
+  // out[j] = {|g_{j+1}|, status}: 0 continue, 1 converged, 2 breakdown, 3 non-finite
+  __global__ void arnoldi_finish_kernel(int j, int ldh, const double *__restrict__ d_s, double *__restrict__ H,
+                                        double *__restrict__ cs, double *__restrict__ sn, double *__restrict__ g,
+                                        const int *__restrict__ reorth, double *__restrict__ sc,
+                                        double2 *__restrict__ out)
+  {
+    if (threadIdx.x != 0)
+      return;
+    double *hcol = H + (long long)j * ldh;
+    if (*reorth)
+      for (int i = 0; i <= j; ++i)
+        hcol[i] += d_s[i];
+    const double nw = sqrt(fmax(d_s[MAX_MULTIDOT], 0.0));
+    hcol[j + 1]     = nw;
+    for (int i = 0; i < j; ++i)
+      {
+        const double a = hcol[i], b = hcol[i + 1];
+        hcol[i]         = cs[i] * a + sn[i] * b;
+        hcol[i + 1]     = -sn[i] * a + cs[i] * b;
+      }
+    const double a = hcol[j], b = hcol[j + 1];
+    const double rr = hypot(a, b);
+    cs[j]           = rr == 0.0 ? 1.0 : a / rr;
+    sn[j]           = rr == 0.0 ? 0.0 : b / rr;
+    hcol[j]         = rr;
+    hcol[j + 1]     = 0.0;
+    g[j + 1]        = -sn[j] * g[j];
+    g[j]            = cs[j] * g[j];
+    const double res = fabs(g[j + 1]);
+    double       status;
+    if (!isfinite(res) || !isfinite(nw))
+      status = 3.0;
+    else if (res <= sc[1])
+      status = 1.0;
+    else if (nw == 0.0)
+      status = 2.0;
+    else
+      status = 0.0;
+    sc[0]  = nw;
+    out[j] = make_double2(res, status);
+  }
+
   // Restarted, left-preconditioned GMRES for J x = b with x0 = 0; classical
   // Gram-Schmidt with a second pass when the first one loses more than 30%
   // of the norm.  Returns SINT_OK / SINT_ERR_NO_CONVERGENCE; *its = iterations.
+  //
+  // Each Arnoldi iteration is a fixed sequence of kernels (J v, P^-1, fused
+  // multi-dot, fused multi-axpy + norm, check, conditional second pass,
+  // finish, normalisation of the next basis vector) plus a 16-byte copy of
+  // its residual estimate; the host enqueues iteration j + 1 before it waits
+  // for iteration j's estimate, unless the residual history predicts that j
+  // converges.  An iteration enqueued past convergence only writes basis
+  // vector j + 2 and Hessenberg column j + 1, which the solution update
+  // (columns 0..j) never reads.
   template <typename R>
   static int gmres(Ctx *c, const sint_newton_params &prm, cudaStream_t s, int *its_out)
   {
     Workspace      *ws = c->ws;
     const long long n  = ws->nvec;
-    const int       m  = ws->restart;
+    const int       m  = ws->restart, ldh = m + 1;
     R              *V = static_cast<R *>(ws->V), *w = static_cast<R *>(ws->w), *t = static_cast<R *>(ws->t);
     R              *b = static_cast<R *>(ws->b), *x = static_cast<R *>(ws->x);
-    std::vector<double> H((m + 1) * m, 0.0), cs(m, 0.0), sn(m, 0.0), gv(m + 1, 0.0), y(m, 0.0);
+    std::vector<double> y(m, 0.0);
     int    its = 0, rc;
     double tol = 0.0;
     bool   first = true;
+
+    auto enqueue = [&](int j) -> int {
+      R  *vj = V + (long long)j * n;
+      int r;
+      if ((r = jvp<R>(c, t, vj, s)) || (r = prec<R>(c, w, t, s)) ||
+          (r = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s)) ||
+          (r = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s)))
+        return r;
+      arnoldi_check_kernel<<<1, 32, 0, s>>>(j, ldh, ws->d_s, ws->d_H, ws->d_flag);
+      count_launches(1);
+      if ((r = multidot_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_flag, s)) ||
+          (r = multiaxpy_norm2_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, ws->d_flag, s)))
+        return r;
+      arnoldi_finish_kernel<<<1, 32, 0, s>>>(j, ldh, ws->d_s, ws->d_H, ws->d_cs, ws->d_sn, ws->d_g, ws->d_flag,
+                                             ws->d_sc, ws->d_out);
+      count_launches(1);
+      if ((r = scale_by_device<R>(n, w, ws->d_sc, V + (long long)(j + 1) * n, s)))
+        return r;
+      cudaError_t e = cudaMemcpyAsync(ws->h_out + j, ws->d_out + j, sizeof(double2), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess)
+        e = cudaEventRecord(ws->ev[j], s);
+      return e == cudaSuccess ? SINT_OK : cuda_fail(e, "GMRES: enqueue");
+    };
+
     if ((rc = axpby<R>(n, 0.0, b, 0.0, x, s)))
       return rc;
     for (;;)
@@ -172,6 +313,10 @@ namespace sint
             // deal.II ReductionControl: tolerance = max(abs_tol, rel_tol * |r0|)
             tol   = std::max(prm.l_abs_tol, prm.l_rel_tol * beta);
             first = false;
+            const double sc[2] = {0.0, tol};
+            cudaError_t  e     = cudaMemcpyAsync(ws->d_sc, sc, sizeof(sc), cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess)
+              return cuda_fail(e, "GMRES: tolerance");
           }
         if (beta <= tol)
           {
@@ -186,94 +331,65 @@ namespace sint
           }
         if ((rc = axpby<R>(n, 1.0 / beta, w, 0.0, V, s)))
           return rc;
-        std::fill(gv.begin(), gv.end(), 0.0);
-        gv[0]     = beta;
-        int    k  = 0; // number of basis vectors beyond V_0 built in this cycle
-        double res = beta;
-        for (int j = 0; j < m; ++j)
+        gmres_cycle_init_kernel<<<1, 64, 0, s>>>(m, beta, ws->d_g);
+        count_launches(1);
+
+        int    k = 0, status = 0;
+        double res = beta, res_prev = beta, res_prev2 = 0.0;
+        bool   queued = false; // iteration j + 1 already enqueued
+        if ((rc = enqueue(0)))
+          return rc;
+        for (int j = 0;; ++j)
           {
+            queued = false;
+            if (j + 1 < m && its + 1 < prm.l_max_iter)
+              {
+                // predicted estimate of iteration j from the last two (geometric decay)
+                const double pred = res_prev2 > 0.0 ? res_prev * (res_prev / res_prev2) : 0.5 * res_prev;
+                if (pred > tol)
+                  {
+                    if ((rc = enqueue(j + 1)))
+                      return rc;
+                    queued = true;
+                  }
+              }
+            cudaError_t e = cudaEventSynchronize(ws->ev[j]);
+            if (e != cudaSuccess)
+              return cuda_fail(e, "GMRES: wait for iteration");
             ++its;
-            R *vj = V + (long long)j * n;
-            if ((rc = jvp<R>(c, t, vj, s)) || (rc = prec<R>(c, w, t, s)))
-              return rc;
-            // classical Gram-Schmidt: h = V^T w, w -= V h
-            double *hcol = &H[j * (m + 1)];
-            if ((rc = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s)) ||
-                (rc = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s)))
-              return rc;
-            {
-              cudaError_t e = cudaMemcpyAsync(ws->h_s, ws->d_s, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s);
-              if (e == cudaSuccess)
-                e = cudaMemcpyAsync(ws->h_s + MAX_MULTIDOT, ws->d_s + MAX_MULTIDOT, sizeof(double),
-                                    cudaMemcpyDeviceToHost, s);
-              if (e == cudaSuccess)
-                e = cudaStreamSynchronize(s);
-              if (e != cudaSuccess)
-                return cuda_fail(e, "GMRES: fetch Hessenberg column");
-            }
-            double hh = 0.0;
-            for (int i = 0; i <= j; ++i)
-              {
-                hcol[i] = ws->h_s[i];
-                hh += hcol[i] * hcol[i];
-              }
-            double nw2 = ws->h_s[MAX_MULTIDOT];
-            if (nw2 < 0.49 * (hh + nw2))
-              {
-                // second Gram-Schmidt pass (norm dropped by more than 30%)
-                if ((rc = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s)) ||
-                    (rc = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s)))
-                  return rc;
-                cudaError_t e =
-                  cudaMemcpyAsync(ws->h_s, ws->d_s, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s);
-                if (e == cudaSuccess)
-                  e = cudaMemcpyAsync(ws->h_s + MAX_MULTIDOT, ws->d_s + MAX_MULTIDOT, sizeof(double),
-                                      cudaMemcpyDeviceToHost, s);
-                if (e == cudaSuccess)
-                  e = cudaStreamSynchronize(s);
-                if (e != cudaSuccess)
-                  return cuda_fail(e, "GMRES: fetch second pass");
-                for (int i = 0; i <= j; ++i)
-                  hcol[i] += ws->h_s[i];
-                nw2 = ws->h_s[MAX_MULTIDOT];
-              }
-            const double nw = std::sqrt(std::max(nw2, 0.0));
-            hcol[j + 1]     = nw;
-            // apply the previous Givens rotations, then a new one
-            for (int i = 0; i < j; ++i)
-              {
-                const double a = hcol[i], bb = hcol[i + 1];
-                hcol[i]         = cs[i] * a + sn[i] * bb;
-                hcol[i + 1]     = -sn[i] * a + cs[i] * bb;
-              }
-            const double a = hcol[j], bb = hcol[j + 1];
-            const double rr = std::hypot(a, bb);
-            cs[j]           = rr == 0.0 ? 1.0 : a / rr;
-            sn[j]           = rr == 0.0 ? 0.0 : bb / rr;
-            hcol[j]         = rr;
-            hcol[j + 1]     = 0.0;
-            gv[j + 1]       = -sn[j] * gv[j];
-            gv[j]           = cs[j] * gv[j];
-            res             = std::fabs(gv[j + 1]);
-            k               = j + 1;
-            if (!std::isfinite(res) || !std::isfinite(nw))
+            k      = j + 1;
+            res    = ws->h_out[j].x;
+            status = int(ws->h_out[j].y);
+            if (status == 3)
               {
                 set_error("GMRES: non-finite Hessenberg entry");
                 *its_out = its;
                 return SINT_ERR_NO_CONVERGENCE;
               }
-            if (nw == 0.0 || res <= tol || its >= prm.l_max_iter || j == m - 1)
+            if (status != 0 || its >= prm.l_max_iter || j == m - 1)
               break;
-            if ((rc = axpby<R>(n, 1.0 / nw, w, 0.0, V + (long long)(j + 1) * n, s)))
+            if (!queued && (rc = enqueue(j + 1)))
               return rc;
+            res_prev2 = res_prev;
+            res_prev  = res;
           }
-        // back substitution H(0:k,0:k) y = g, then x += V y
+        // back substitution H(0:k,0:k) y = g on the host (k <= restart), then x += V y
+        {
+          cudaError_t e = cudaMemcpyAsync(ws->h_H, ws->d_H, sizeof(double) * ldh * k, cudaMemcpyDeviceToHost, s);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ws->h_H + ldh * ldh, ws->d_g, sizeof(double) * k, cudaMemcpyDeviceToHost, s);
+          if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+          if (e != cudaSuccess)
+            return cuda_fail(e, "GMRES: fetch Hessenberg");
+        }
+        const double *H = ws->h_H, *gv = ws->h_H + ldh * ldh;
         for (int i = k - 1; i >= 0; --i)
           {
             double sum = gv[i];
             for (int l = i + 1; l < k; ++l)
-              sum -= H[l * (m + 1) + i] * y[l];
-            y[i] = sum / H[i * (m + 1) + i];
+              sum -= H[l * ldh + i] * y[l];
+            y[i] = sum / H[i * ldh + i];
           }
         {
           cudaError_t e = cudaMemcpyAsync(ws->d_y, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s);

@@ -373,10 +373,10 @@ namespace sint
   }
 
   // scale = (base_c, 1/m_c, base_mu, 1/m_mu, base_eta, 1/m_eta),
-  // oscale = (k_c/m_c, k_mu/m_mu, k_eta/m_eta); base = (base_c, base_mu,
-  // base_eta, k_c, k_mu, k_eta).  A zero increment keeps scale 1.
+  // oscale = (k_c/(m_c dt), k_mu/(m_mu dt), k_eta/(m_eta dt)); base = (base_c,
+  // base_mu, base_eta, k_c, k_mu, k_eta).  A zero increment keeps 1/m = 1.
   __global__ void increment_scales_kernel(const unsigned *__restrict__ work, const float *__restrict__ base,
-                                          float *__restrict__ scale, float *__restrict__ oscale)
+                                          float dt, float *__restrict__ scale, float *__restrict__ oscale)
   {
     if (threadIdx.x != 0)
       return;
@@ -386,7 +386,7 @@ namespace sint
         const float inv = m > 1e-30f ? 1.f / m : 1.f;
         scale[2 * g]     = base[g];
         scale[2 * g + 1] = inv;
-        oscale[g]        = base[3 + g] * inv;
+        oscale[g]        = base[3 + g] * inv / dt;
       }
   }
 
@@ -564,10 +564,10 @@ int sint_nn_apply_guess_f64(const double *u_n, const double *u_nm1, int64_t bloc
 }
 
 int sint_nn_increment_scales_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int64_t n_nodes, int G,
-                                 float ratio, const float *base, unsigned *work, float *scale, float *oscale,
-                                 sint_stream_t s)
+                                 float ratio, float dt, const float *base, unsigned *work, float *scale,
+                                 float *oscale, sint_stream_t s)
 {
-  if (!u_n || !u_nm1 || !base || !work || !scale || !oscale || G < 1 || n_nodes < 1)
+  if (!u_n || !u_nm1 || !base || !work || !scale || !oscale || G < 1 || n_nodes < 1 || !(dt > 0.f))
     {
       set_error("sint_nn_increment_scales_f64: bad argument");
       return SINT_ERR_ARG;
@@ -578,7 +578,7 @@ int sint_nn_increment_scales_f64(const double *u_n, const double *u_nm1, int64_t
   increment_max_kernel<<<592, 256, 0, s>>>(u_n, u_nm1, block_stride, n_nodes, G, ratio, work);
   if (int rc = launch_err("sint_nn_increment_scales_f64"))
     return rc;
-  increment_scales_kernel<<<1, 32, 0, s>>>(work, base, scale, oscale);
+  increment_scales_kernel<<<1, 32, 0, s>>>(work, base, dt, scale, oscale);
   return launch_err("sint_nn_increment_scales_f64: scales");
 }
 

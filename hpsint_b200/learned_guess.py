@@ -120,11 +120,13 @@ class Normaliser:
     """Scales of the network's inputs and outputs.  Per state, m_c, m_mu and
     m_eta are the largest extrapolated increments |r (u_n - u_{n-1})| of c,
     mu and the eta_i over the mesh (computed on the device); the increments
-    enter divided by them, the values c, mu, eta times the fixed base scales,
-    and the output is the deviation from linear extrapolation divided by m
-    times the fixed gains.  base = (s_c, s_mu, s_eta, k_c, k_mu, k_eta): s the
-    reciprocal RMS of the values, k the reciprocal RMS of deviation / m over
-    the training triples, so every channel is O(1) whatever dt is."""
+    enter divided by them, the values c, mu, eta times the fixed base scales.
+    The output is the deviation from linear extrapolation divided by m dt_n
+    (dt_n the predicted step) times the fixed gains: for a smooth trajectory
+    that deviation is about dt_n J(u) r (u_n - u_{n-1}), so the scaled target
+    depends on the state and the normalised increment only.  base = (s_c,
+    s_mu, s_eta, k_c, k_mu, k_eta): s the reciprocal RMS of the values, k the
+    reciprocal RMS of deviation / (m dt) over the training triples."""
     base: list
 
     def device(self):
@@ -138,9 +140,10 @@ class IncrementScales:
     def __init__(self):
         self.work = torch.zeros(4, dtype=torch.int32, device="cuda")
 
-    def __call__(self, un, um, ld, n_nodes, G, ratio, base, scale, oscale):
-        L.check(L.lib().sint_nn_increment_scales_f64(_p(un), _p(um), ld, n_nodes, G, ratio, _p(base), _p(self.work),
-                                                     _p(scale), _p(oscale), _s()), "sint_nn_increment_scales_f64")
+    def __call__(self, un, um, ld, n_nodes, G, ratio, dt, base, scale, oscale):
+        L.check(L.lib().sint_nn_increment_scales_f64(_p(un), _p(um), ld, n_nodes, G, ratio, dt, _p(base),
+                                                     _p(self.work), _p(scale), _p(oscale), _s()),
+                "sint_nn_increment_scales_f64")
 
 
 def _triple_scales(tr, base, inc):
@@ -149,8 +152,8 @@ def _triple_scales(tr, base, inc):
     sc = torch.ones((K, 6), dtype=torch.float32, device="cuda")
     osc = torch.ones((K, 3), dtype=torch.float32, device="cuda")
     for k in range(1, K - 1):
-        inc(tr.states[k], tr.states[k - 1], tr.case.op.ld, tr.case.op.N, tr.case.G, tr.dts[k] / tr.dts[k - 1], base,
-            sc[k], osc[k])
+        inc(tr.states[k], tr.states[k - 1], tr.case.op.ld, tr.case.op.N, tr.case.G, tr.dts[k] / tr.dts[k - 1],
+            tr.dts[k], base, sc[k], osc[k])
     return sc, osc
 
 
@@ -172,7 +175,7 @@ def fit_normaliser(trajs, max_triples=400):
             dev = up - un - r * (un - um)
             for g, (i0, i1) in enumerate(((0, 1), (1, 2), (2, 2 + G))):
                 vsum[g] += float((un[i0:i1] ** 2).sum())
-                dsum[g] += float((dev[i0:i1] ** 2).sum()) * inv_m[k, g] ** 2
+                dsum[g] += float((dev[i0:i1] ** 2).sum()) * (inv_m[k, g] / tr.dts[k]) ** 2
                 cnt[g] += (i1 - i0) * N
             used += 1
     cnt = np.maximum(cnt, 1)
@@ -296,31 +299,36 @@ class Trainer:
         return c.lr_final + 0.5 * (c.lr - c.lr_final) * (1.0 + math.cos(math.pi * min(it, n) / max(n, 1)))
 
     def step(self, lr=None):
-        """One Adam step; returns the batch loss as a device scalar (no sync)."""
+        """One Adam step; returns (batch loss, loss of predicting zero = linear
+        extrapolation) as device scalars (no sync)."""
         G, b = self.fill_batch()
         B = self.cfg.batch
         yg, ys, cache = self.net.forward(b["xg"], b["xs"], B, G, keep=True)
         lg = self.net.mse(yg, b["tg"], b["wg"], b["dyg"])
         ls = self.net.mse(ys, b["ts"], b["ws"], b["dys"])
+        zg, zs = torch.zeros_like(b["tg"]), torch.zeros_like(b["ts"])
+        base = self.net.mse(zg, b["tg"], b["wg"], None) + self.net.mse(zs, b["ts"], b["ws"], None)
         self.net.zero_grad()
         self.net.backward(cache, b["dyg"], b["dys"], B, G)
         self.net.adam_step(lr=self.cfg.lr if lr is None else lr)
-        return lg + ls
+        return lg + ls, base
 
     def train(self, iterations=None, verbose=False):
         n = iterations if iterations is not None else self.cfg.iterations
         t0 = time.perf_counter()
-        acc, cnt = None, 0
+        acc, accb, cnt = None, None, 0
         for it in range(1, n + 1):
-            loss = self.step(self.lr_at(it - 1, n))
+            loss, base = self.step(self.lr_at(it - 1, n))
             acc = loss if acc is None else acc + loss
+            accb = base if accb is None else accb + base
             cnt += 1
             if it % self.cfg.log_every == 0 or it == n:
-                mean = float(acc.item()) / cnt
-                self.history.append((it, mean))
+                mean, mb = float(acc.item()) / cnt, float(accb.item()) / cnt
+                self.history.append((it, mean, mb))
                 if verbose:
-                    print(f"iter {it:6d}  loss {mean:.4e}  {time.perf_counter() - t0:.1f}s", flush=True)
-                acc, cnt = None, 0
+                    print(f"iter {it:6d}  loss {mean:.4e}  (zero prediction {mb:.4e})  "
+                          f"{time.perf_counter() - t0:.1f}s", flush=True)
+                acc, accb, cnt = None, None, 0
         torch.cuda.synchronize()
         return time.perf_counter() - t0
 
@@ -349,10 +357,16 @@ class LinearPredictor:
 
 class LearnedPredictor:
     """Whole-mesh inference: features of (u_{n-1}, u_n, r) -> net -> guess
-    u_n + r (u_n - u_{n-1}) + output / oscale.  FP32 network, FP64 guess."""
+    u_n + r (u_n - u_{n-1}) + output / oscale.  FP32 network, FP64 guess.
 
-    def __init__(self, op: SinteringOperatorGeneric, net: EquivariantNet, norm: Normaliser, tensor_cores=True):
-        self.op, self.net, self.tensor_cores = op, net, tensor_cores
+    safeguard: also form the linear guess, evaluate the residual of both
+    under the step's time weights (set by the integrator before it asks for
+    a guess) and keep the smaller, all on the device (no host sync), so the
+    guess is never worse than hpsint's linear predictor in residual norm."""
+
+    def __init__(self, op: SinteringOperatorGeneric, net: EquivariantNet, norm: Normaliser, tensor_cores=True,
+                 safeguard=False):
+        self.op, self.net, self.tensor_cores, self.safeguard = op, net, tensor_cores, safeguard
         self.base, self.inc = norm.device(), IncrementScales()
         self.scale = torch.ones(6, dtype=torch.float32, device="cuda")
         self.oscale = torch.ones(3, dtype=torch.float32, device="cuda")
@@ -364,6 +378,11 @@ class LearnedPredictor:
         self.xg, self.xs = f(G, 2, self.ny, self.nx), f(1, 4, self.ny, self.nx)
         self.guess = op.initialize_dof_vector()
         self.calls = 0
+        if safeguard:
+            self.linear = LinearPredictor(op)
+            self.r = op.initialize_dof_vector()
+            self.norms = torch.zeros(2, dtype=torch.float64, device="cuda")
+            self.picked_linear = torch.zeros(1, dtype=torch.float64, device="cuda")
 
     def __call__(self, history, dts, dt):
         if len(history) < 2 or not dts or dts[0] <= 0:
@@ -371,7 +390,7 @@ class LearnedPredictor:
         op, G = self.op, self.op.params.n_grains
         r = dt / dts[0]
         lib = L.lib()
-        self.inc(history[0], history[1], op.ld, op.N, G, r, self.base, self.scale, self.oscale)
+        self.inc(history[0], history[1], op.ld, op.N, G, r, dt, self.base, self.scale, self.oscale)
         L.check(lib.sint_nn_features_f64(_p(history[0]), _p(history[1]), op.ld, self.nx, self.ny, G, 0, 0, self.ny,
                                          self.nx, r, _p(self.scale), _p(self.xg), _p(self.xs), 0, _s()),
                 "sint_nn_features_f64")
@@ -379,6 +398,15 @@ class LearnedPredictor:
         L.check(lib.sint_nn_apply_guess_f64(_p(history[0]), _p(history[1]), op.ld, op.N, G, r, _p(self.oscale),
                                             _p(yg), _p(ys), _p(self.guess), _s()), "sint_nn_apply_guess_f64")
         self.calls += 1
+        if self.safeguard:
+            lin = self.linear(history, dts, dt)
+            n = self.guess.numel()
+            for i, g in enumerate((self.guess, lin)):
+                op.evaluate_nonlinear_residual(self.r, g, 2, history[:max(1, op.order)])
+                L.check(lib.sint_vec_norm2_f64(op._h, n, _p(self.r), _p(self.norms[i:]), _s()), "sint_vec_norm2_f64")
+            L.check(lib.sint_vec_select_f64(n, _p(self.guess), _p(lin), _p(self.norms[0:]), _p(self.norms[1:]),
+                                            _p(self.guess), _s()), "sint_vec_select_f64")
+            self.picked_linear += (self.norms[1] < self.norms[0]).double()
         return self.guess
 
 
@@ -389,8 +417,11 @@ ARMS = {
     "fp64_plain": (64, None),
     "fp64_linear": (64, "linear"),
     "fp64_learned": (64, "learned"),
+    "fp64_learned_safeguarded": (64, "learned_safeguarded"),
     "fp32_inner_plain": (32, None),
+    "fp32_inner_linear": (32, "linear"),
     "fp32_inner_learned": (32, "learned"),
+    "fp32_inner_learned_safeguarded": (32, "learned_safeguarded"),
 }
 
 
@@ -414,6 +445,10 @@ def run_arm(case, n_steps, inner_precision, predictor, dt_schedule=None, nl_rel_
     return case.op.to_host(ti.history[0]), ti.records, wall
 
 
+def _gmean(x):
+    return float(np.exp(np.mean(np.log(x)))) if len(x) else None
+
+
 def compare_arms(case, n_steps, net=None, norm=None, arms=None, warmup_steps=2):
     """Runs the arms on the same packing.  fp64_plain (hpsint's method: FP64,
     previous-solution guess, adaptive dt) runs first and fixes the time grid;
@@ -426,6 +461,7 @@ def compare_arms(case, n_steps, net=None, norm=None, arms=None, warmup_steps=2):
     preds = {"linear": LinearPredictor(case.op)}
     if net is not None:
         preds["learned"] = LearnedPredictor(case.op, net, norm)
+        preds["learned_safeguarded"] = LearnedPredictor(case.op, net, norm, safeguard=True)
     # warm-up: workspaces of both inner precisions, library load, first launches
     for prec in sorted({ARMS[a][0] for a in arms}):
         run_arm(case, warmup_steps, prec, None)
@@ -452,6 +488,11 @@ def compare_arms(case, n_steps, net=None, norm=None, arms=None, warmup_steps=2):
             "linear_iterations": int(sum(r.linear_iterations for r in recs)),
             "residual_evaluations": int(sum(r.residual_evaluations for r in recs)),
             "failed_tries": int(sum(r.failed_tries for r in recs)),
+            # guess quality: |R(guess)| / |R(u_n)| over the predicted steps (geometric mean, worst)
+            "guess_residual_ratio_gmean": _gmean([r.initial_residual / r.reference_residual for r in recs
+                                                  if r.reference_residual > 0]),
+            "guess_residual_ratio_max": max([r.initial_residual / r.reference_residual for r in recs
+                                             if r.reference_residual > 0], default=None),
             "max_abs_diff_c": float(np.abs(u[0] - ref[0]).max()),
             "max_abs_diff_eta": float(np.abs(u[2:] - ref[2:]).max()),
             "int_c_rel_change": float(abs(mass @ u[0] - c0) / abs(c0)),

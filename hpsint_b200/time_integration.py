@@ -44,6 +44,7 @@ class StepRecord:
     initial_residual: float = 0.0
     final_residual: float = 0.0
     accepted_wall_s: float = 0.0   # the successful attempt alone (wall_s includes failed tries)
+    reference_residual: float = 0.0  # |R(u_n)| of the step when a predicted guess was measured against it
 
 
 class TimeIntegrator:
@@ -108,6 +109,7 @@ class TimeIntegrator:
         hist = self.history[:len(wh)]
         self.op.evaluate_nonlinear_residual(self._r, self.history[0], 2, hist)
         ref = self.op.norm(self._r)
+        self._reference_residual = ref
         return replace(self.nl, nl_abs_tol=max(self.nl.nl_abs_tol, self.nl.nl_rel_tol * ref), nl_rel_tol=0.0)
 
     def step(self, u_out=None):
@@ -119,6 +121,7 @@ class TimeIntegrator:
             w0, wh = self._weights(self.dt)
             self.op.set_time_weights(w0, wh, 1.0)
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
+            self._reference_residual = 0.0
             data = self._stop_rule(wh) if guess is not None else None
             u = (guess if guess is not None else self.history[0]).clone()
             st = self.newton.solve(u, self.history[:len(wh)], raise_on_failure=False, data=data)
@@ -141,7 +144,7 @@ class TimeIntegrator:
         t1 = time.perf_counter()
         self.records.append(StepRecord(self.t, self.dt, st.newton_iterations, st.linear_iterations,
                                        st.residual_evaluations, tries, t1 - t0, st.initial_residual,
-                                       st.final_residual, t1 - t_try))
+                                       st.final_residual, t1 - t_try, self._reference_residual))
         self.history.insert(0, u)
         self.dts.insert(0, self.dt)
         keep = max(2, self.td.scheme_order)  # predictors use the last two states

@@ -193,6 +193,10 @@ int sint_vec_dot_f32(sint_ctx *ctx, int64_t n, const float *x, const float *y, d
 int sint_vec_norm2_f32(sint_ctx *ctx, int64_t n, const float *x, double *result, sint_stream_t stream);
 int sint_vec_f64_to_f32(int64_t n, const double *x, float *y, sint_stream_t stream);   /* FP32 shadow */
 int sint_vec_f32_to_f64(int64_t n, const float *x, double *y, sint_stream_t stream);
+/* out = (*norm_a <= *norm_b) ? a : b, decided on the device (norms are device
+ * scalars, e.g. from sint_vec_norm2_f64); out may alias a or b. */
+int sint_vec_select_f64(int64_t n, const double *a, const double *b, const double *norm_a, const double *norm_b,
+                        double *out, sint_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
 /* Nonlinear solve: DampedNewtonSolver (lac/solvers_nonlinear.h:236-394)     */
@@ -311,13 +315,14 @@ int sint_nn_apply_guess_f64(const double *u_n, const double *u_nm1, int64_t bloc
                             double *guess, sint_stream_t stream);
 
 /* Per-state scales of the network inputs and outputs: with m_c, m_mu, m_eta
- * the largest |ratio (u_n - u_{n-1})| of c, mu and any eta_i over the mesh,
- * scale = (base[0], 1/m_c, base[1], 1/m_mu, base[2], 1/m_eta) and
- * oscale = (base[3]/m_c, base[4]/m_mu, base[5]/m_eta) (device arrays; a zero
- * increment gives 1/m = 1).  work: 3 device unsigned ints of scratch. */
+ * the largest |ratio (u_n - u_{n-1})| of c, mu and any eta_i over the mesh and
+ * dt the step being predicted, scale = (base[0], 1/m_c, base[1], 1/m_mu,
+ * base[2], 1/m_eta) and oscale = (base[3], base[4], base[5]) / (m dt) per
+ * group (device arrays; a zero increment gives 1/m = 1).  work: 3 device
+ * unsigned ints of scratch. */
 int sint_nn_increment_scales_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int64_t n_nodes, int G,
-                                 float ratio, const float *base, unsigned *work, float *scale, float *oscale,
-                                 sint_stream_t stream);
+                                 float ratio, float dt, const float *base, unsigned *work, float *scale,
+                                 float *oscale, sint_stream_t stream);
 
 /* Measured FMA throughput of the current device in TFLOP/s (precision 64 or
  * 32): the denominator of the cell kernels' ALU roofline.  Synchronous. */
