@@ -54,6 +54,8 @@ def parse_args():
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
     ap.add_argument("--n3", type=int, default=192, help="cells per direction of the 3D solve workload")
+    ap.add_argument("--no-solve", action="store_true", help="skip the s/step comparison of the operator run")
+    ap.add_argument("--solve-compare-steps", type=int, default=40)
     ap.add_argument("--train-seeds", type=int, default=10)
     ap.add_argument("--train-steps", type=int, default=200, help="FP64 steps per training trajectory")
     ap.add_argument("--train-iters", type=int, default=4000)
@@ -61,7 +63,7 @@ def parse_args():
     ap.add_argument("--eval-steps", type=int, default=100)
     ap.add_argument("--cells", type=int, default=512)
     ap.add_argument("--circles", type=int, default=100)
-    ap.add_argument("--save-net", default=None, help="write the trained parameters (.pt) here")
+    ap.add_argument("--save-net", default=None, help="write the trained predictor (.npz) here")
     ap.add_argument("--solve-steps", type=int, default=100)
     return ap.parse_args()
 
@@ -247,6 +249,33 @@ def two_particle_solve(args):
     print(json.dumps(line), flush=True)
 
 
+def solve_comparison(n_steps):
+    """s/step of the metric's solve arms on a held-out 2D many-grain packing
+    (512^2 cells, 100 circles, seed 1000, scalar mobility, Newton 1e-8): the
+    plain FP64 solve (hpsint's method) fixes the time grid, the FP32-inner
+    arms replay it with the previous-solution, linear and safeguarded
+    learned guesses (the net trained by --workload learned2d on seeds 0..9,
+    hpsint_b200/weights/learned_guess_c4.npz)."""
+    from hpsint_b200 import learned_guess as LG
+    wpath = os.path.join(ROOT, "hpsint_b200", "weights", "learned_guess_c4.npz")
+    net, norm = LG.load_predictor(wpath)
+    case = LG.make_case(1000)
+    arms = ["fp64_plain", "fp32_inner_plain", "fp32_inner_linear", "fp32_inner_learned_safeguarded"]
+    res = LG.compare_arms(case, n_steps, net, norm, arms=arms)
+    plain = res["fp64_plain"]["s_per_step"]
+    pick = lambda key: {a: res[a].get(key) for a in arms if a in res}
+    return {"workload": f"2d-512x512-100-circles-G{case.G}-seed1000", "dofs": case.op.C * case.op.N,
+            "steps": n_steps, "unit": "s/step", "newton_tol": 1e-8,
+            "s_per_step": pick("s_per_step"),
+            "speedup_vs_fp64_plain": {a: plain / res[a]["s_per_step"] for a in arms if "s_per_step" in res.get(a, {})},
+            "newton_iterations": pick("newton_iterations"), "linear_iterations": pick("linear_iterations"),
+            "guess_residual_ratio_gmean": pick("guess_residual_ratio_gmean"),
+            "max_abs_diff_vs_fp64_plain": {a: max(res[a]["max_abs_diff_c"], res[a]["max_abs_diff_eta"])
+                                           for a in arms if "max_abs_diff_c" in res.get(a, {})},
+            "int_c_rel_change": pick("int_c_rel_change"),
+            "weights": "hpsint_b200/weights/learned_guess_c4.npz"}
+
+
 def mixed_precision_solve_3d(args):
     """3D mixed-precision solve: 192^3 Q1 cells at unit spacing, 51 spheres
     with lognormal radii (median 10, sigma 0.2) in a random sequential packing
@@ -339,7 +368,7 @@ def learned_guess_solve(args):
         train, n=args.cells, n_circles=args.circles, n_steps=args.train_steps, net_cfg=NetConfig(),
         train_cfg=LG.TrainConfig(iterations=args.train_iters), verbose=False)
     if args.save_net:
-        torch.save({"state": net.state_dict(), "base": norm.base}, args.save_net)
+        LG.save_predictor(args.save_net, net, norm)
     evals = []
     for seed in held:
         case = LG.make_case(seed, n=args.cells, n_circles=args.circles)
@@ -554,6 +583,10 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if world == 1 and not args.no_solve:
+        del ud, vd, dst, v32, dst32, hist, res, z32, d_src, pc
+        torch.cuda.empty_cache()
+        line["solve"] = solve_comparison(args.solve_compare_steps)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(u, v, G, tensorial, args.cpu_seconds, n)
     print(json.dumps(line), flush=True)

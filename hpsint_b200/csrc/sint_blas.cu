@@ -101,12 +101,44 @@ namespace sint
     return n % E == 0 && stride % E == 0 && aligned16(a) && aligned16(b);
   }
 
+  // Fused finish of a reduction: every block has written its partials
+  // (rows 0..m-1, NB_RED blocks each); the block that takes the last ticket
+  // sums each row in a fixed order (lane l adds blocks l, l + 32, ..., then a
+  // fixed butterfly), writes out[0..m) and resets the ticket.  The result does
+  // not depend on which block finishes last.
+  __device__ __forceinline__ void finish_if_last(const double *__restrict__ rows, int m, double *__restrict__ out,
+                                                 unsigned *ticket)
+  {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+      last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last)
+      return;
+    __threadfence();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = warp; j < m; j += RED_THREADS / 32)
+      {
+        double v = 0.0;
+        for (int b = lane; b < NB_RED; b += 32)
+          v += __ldcg(rows + (size_t)j * NB_RED + b);
+        v = warp_sum(v);
+        if (lane == 0)
+          out[j] = v;
+      }
+    if (threadIdx.x == 0)
+      *ticket = 0u;
+  }
+
   // partial[j * NB_RED + blockIdx.x] = sum over this block's chunks of w . V_j
   // (FP64 products and sums; m <= M).
   template <typename R, int M, int E>
   __global__ void __launch_bounds__(RED_THREADS)
     multidot_kernel(long long nc, const R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
-                    double *__restrict__ partial, const int *__restrict__ cond)
+                    double *__restrict__ partial, const int *__restrict__ cond, const double *__restrict__ rows,
+                    int m_total, double *__restrict__ out, unsigned *ticket)
   {
     if (cond && *cond == 0)
       return;
@@ -136,21 +168,8 @@ namespace sint
           if (threadIdx.x == 0)
             partial[j * NB_RED + blockIdx.x] = s;
         }
-  }
-
-  // out[j] = sum_b partial[j * NB_RED + b] (one block per j, fixed order)
-  __global__ void __launch_bounds__(RED_THREADS)
-    finish_kernel(const double *__restrict__ partial, double *__restrict__ out, const int *__restrict__ cond)
-  {
-    if (cond && *cond == 0)
-      return;
-    __shared__ double s_w[RED_THREADS / 32];
-    double            v = 0.0;
-    for (int b = threadIdx.x; b < NB_RED; b += RED_THREADS)
-      v += partial[blockIdx.x * NB_RED + b];
-    v = block_sum(v, s_w);
-    if (threadIdx.x == 0)
-      out[blockIdx.x] = v;
+    if (out)
+      finish_if_last(rows, m_total, out, ticket);
   }
 
   constexpr int MD = 16; // vectors per multidot / multiaxpy pass (accumulators in registers)
@@ -168,16 +187,17 @@ namespace sint
     const bool    pack = can_pack<R>(n, stride, w, V);
     for (int j0 = 0; j0 < m; j0 += MD)
       {
-        const int mm = m - j0 < MD ? m - j0 : MD;
-        double   *pp = c->red + (size_t)j0 * NB_RED;
+        const int mm   = m - j0 < MD ? m - j0 : MD;
+        double   *pp   = c->red + (size_t)j0 * NB_RED;
+        double   *outl = j0 + MD >= m ? out : nullptr; // the last pass sums all rows
         if (pack)
-          multidot_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, pp, cond);
+          multidot_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, pp, cond,
+                                                                   c->red, m, outl, c->red_ticket);
         else
-          multidot_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, pp, cond);
+          multidot_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, pp, cond,
+                                                                   c->red, m, outl, c->red_ticket);
         count_launches(1);
       }
-    finish_kernel<<<m, RED_THREADS, 0, s>>>(c->red, out, cond);
-    count_launches(1);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SINT_OK : cuda_fail(e, "multidot");
   }
@@ -217,7 +237,8 @@ namespace sint
   template <typename R, int M, int E>
   __global__ void __launch_bounds__(RED_THREADS)
     multiaxpy_kernel(long long nc, R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
-                     const double *__restrict__ coef, double *__restrict__ partial, const int *__restrict__ cond)
+                     const double *__restrict__ coef, double *__restrict__ partial, const int *__restrict__ cond,
+                     double *__restrict__ norm2_out, unsigned *ticket)
   {
     if (cond && *cond == 0)
       return;
@@ -252,6 +273,7 @@ namespace sint
         const double t = block_sum(nrm, s_w);
         if (threadIdx.x == 0)
           partial[blockIdx.x] = t;
+        finish_if_last(partial, 1, norm2_out, ticket);
       }
   }
 
@@ -265,17 +287,13 @@ namespace sint
       {
         const int mm   = m - j0 < MD ? m - j0 : MD;
         double   *part = (norm2_out && j0 + MD >= m) ? c->red : nullptr; // norm in the last pass
+        unsigned *tk   = c ? c->red_ticket : nullptr;
         if (pack)
           multiaxpy_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, coef + j0,
-                                                                    part, cond);
+                                                                    part, cond, norm2_out, tk);
         else
           multiaxpy_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, coef + j0,
-                                                                    part, cond);
-        count_launches(1);
-      }
-    if (norm2_out)
-      {
-        finish_kernel<<<1, RED_THREADS, 0, s>>>(c->red, norm2_out, cond);
+                                                                    part, cond, norm2_out, tk);
         count_launches(1);
       }
     const cudaError_t e = cudaGetLastError();

@@ -231,7 +231,10 @@ namespace sint
         return SINT_ERR_ARG;
       }
     for (int d = 0; d < 2; ++d)
-      make_divisor((unsigned)g.nt[d], g.mdiv[d], g.sdiv[d]);
+      {
+        make_divisor((unsigned)g.nt[d], g.mdiv[d], g.sdiv[d]);
+        make_divisor((unsigned)g.nn[d], g.mnode[d], g.snode[d]);
+      }
     // exact Q1 element Laplacian of the uniform cell: K_lm = kx[l xor m], built
     // from the 1D stiffness (1/h)[[1,-1],[-1,1]] and mass (h/6)[[2,1],[1,2]]
     for (int x = 0; x < 8; ++x)
@@ -328,16 +331,18 @@ int sint_create(const sint_mesh *mesh, const sint_params *params, sint_ctx **out
       (e = cudaMalloc(&c->pc_raw, pcsz * sizeof(double))) != cudaSuccess ||
       (e = cudaMalloc(&c->pc_inv64, pcsz * sizeof(double))) != cudaSuccess ||
       (e = cudaMalloc(&c->pc_inv32, pcsz * sizeof(float))) != cudaSuccess ||
-      (e = cudaMalloc(&c->red, sizeof(double) * (MAX_MULTIDOT + 1) * NB_RED)) != cudaSuccess)
+      (e = cudaMalloc(&c->red, sizeof(double) * ((MAX_MULTIDOT + 1) * NB_RED + RED_TICKETS))) != cudaSuccess)
     {
       const int rc = cuda_fail(e, "sint_create: cudaMalloc");
       sint_destroy(c);
       return rc;
     }
+  c->red_ticket = reinterpret_cast<unsigned *>(c->red + (MAX_MULTIDOT + 1) * NB_RED);
   // padding entries are part of every block vector; keep them defined
   if ((e = cudaMemset(c->lin64, 0, vec64)) != cudaSuccess || (e = cudaMemset(c->lin32, 0, vec64 / 2)) != cudaSuccess ||
       (e = cudaMemset(c->pc_inv64, 0, pcsz * sizeof(double))) != cudaSuccess ||
-      (e = cudaMemset(c->pc_inv32, 0, pcsz * sizeof(float))) != cudaSuccess)
+      (e = cudaMemset(c->pc_inv32, 0, pcsz * sizeof(float))) != cudaSuccess ||
+      (e = cudaMemset(c->red_ticket, 0, sizeof(double) * RED_TICKETS)) != cudaSuccess)
     {
       const int rc = cuda_fail(e, "sint_create: cudaMemset");
       sint_destroy(c);

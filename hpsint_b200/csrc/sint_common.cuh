@@ -81,6 +81,9 @@ namespace sint
     // n / nt[d] = (n * mdiv[d]) >> (32 + sdiv[d])
     unsigned long long mdiv[2];
     int                sdiv[2];
+    // the same for nn[0] and nn[1] (node index -> node coordinates; N < 2^31)
+    unsigned long long mnode[2];
+    int                snode[2];
   };
 
   // Granlund-Montgomery division by an invariant integer d >= 1: with
@@ -517,9 +520,21 @@ namespace sint
     if (idx >= g.N)
       return;
     int c[3];
-    c[0]             = int(idx % g.nn[0]);
-    c[1]             = int((idx / g.nn[0]) % g.nn[1]);
-    c[2]             = int(idx / ((long long)g.nn[0] * g.nn[1]));
+    if (g.N < (1ll << 31))
+      {
+        // multiply-shift instead of 64-bit division (most threads only classify their node)
+        const unsigned q0 = fast_div(unsigned(idx), g.mnode[0], g.snode[0]);
+        const unsigned q1 = fast_div(q0, g.mnode[1], g.snode[1]);
+        c[0]              = int(unsigned(idx) - q0 * unsigned(g.nn[0]));
+        c[1]              = int(q0 - q1 * unsigned(g.nn[1]));
+        c[2]              = int(q1);
+      }
+    else
+      {
+        c[0] = int(idx % g.nn[0]);
+        c[1] = int((idx / g.nn[0]) % g.nn[1]);
+        c[2] = int(idx / ((long long)g.nn[0] * g.nn[1]));
+      }
     const int TT[3]  = {T::TX, T::TY, T::TZ};
     int       nt[3]  = {1, 1, 1}; // number of candidate tiles per direction
     int       t0[3]  = {0, 0, 0}; // first candidate tile

@@ -17,6 +17,7 @@ namespace sint
   // Deterministic reductions: NB_RED fixed block partials, then one block.
   constexpr int NB_RED       = 592; // 4 x 148 SMs
   constexpr int MAX_MULTIDOT = 64;
+  constexpr int RED_TICKETS  = 1; // doubles after the partials holding the last-block ticket counter
 
   struct Workspace; // Newton/GMRES vectors, sint_newton.cu
 
@@ -41,7 +42,8 @@ namespace sint
     float  *pc_inv32 = nullptr;
     bool    has_pc   = false;
 
-    double *red = nullptr; // reduction partials: MAX_MULTIDOT x NB_RED doubles
+    double   *red        = nullptr; // reduction partials: (MAX_MULTIDOT + 1) x NB_RED doubles, then the ticket
+    unsigned *red_ticket = nullptr; // blocks of a reduction that finished (the last one sums; back to 0)
 
     // DampedNewtonSolver state that outlives one solve (solvers_nonlinear.h:390-391)
     unsigned history_newton_iterations      = 0;

@@ -500,6 +500,27 @@ def compare_arms(case, n_steps, net=None, norm=None, arms=None, warmup_steps=2):
     return out
 
 
+def save_predictor(path, net: EquivariantNet, norm: Normaliser):
+    """Trained parameters, architecture and normaliser as a NumPy .npz (no pickle)."""
+    cfg = net.cfg
+    np.savez(path, params=net.params.detach().cpu().numpy(), base=np.asarray(norm.base, np.float64),
+             cfg=np.asarray([cfg.width, cfg.layers, cfg.grain_in, cfg.shared_in, cfg.shared_out, cfg.seed],
+                            np.int64), slope=np.float64(cfg.slope))
+
+
+def load_predictor(path):
+    """(net, normaliser) from save_predictor's file."""
+    with np.load(path) as f:
+        w, layers, gi, si, so, seed = (int(x) for x in f["cfg"])
+        net = EquivariantNet(NetConfig(width=w, layers=layers, grain_in=gi, shared_in=si, shared_out=so,
+                                       slope=float(f["slope"]), seed=seed))
+        params = torch.as_tensor(f["params"], dtype=torch.float32)
+        if params.numel() != net.n_params:
+            raise ValueError(f"{path}: {params.numel()} parameters, the architecture needs {net.n_params}")
+        net.load_params(params)
+        return net, Normaliser([float(x) for x in f["base"]])
+
+
 def train_learned_guess(train_seeds, n=512, n_circles=100, n_steps=200, net_cfg=None, train_cfg=None,
                         verbose=False, rmin=6.0, rmax=12.0):
     """FP64 trajectories over train_seeds, normaliser, Adam training.
