@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["operator", "solve2d", "solve3d", "learned2d"], default="operator",
+    ap.add_argument("--workload", choices=["operator", "solve2d", "solve3d", "learned2d", "nnconv"], default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
     ap.add_argument("--n3", type=int, default=192, help="cells per direction of the 3D solve workload")
@@ -249,6 +249,44 @@ def two_particle_solve(args):
     print(json.dumps(line), flush=True)
 
 
+def nn_conv(args):
+    """The learned guess's hidden-layer convolution at inference size: 8 grain
+    streams of 513 x 513 nodes, 32 -> 32 channels, 3x3 (38.8 GFLOP): the
+    tcgen05 TF32 kernel and the FP32 kernel, CUDA-event time per call."""
+    import torch
+
+    from hpsint_b200 import predictor as P
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    G, H, W, C = 8, 513, 513, 32
+    gen = torch.Generator("cuda").manual_seed(0)
+    x = torch.randn((G, C, H, W), device="cuda", generator=gen)
+    w = torch.randn((C, C, 3, 3), device="cuda", generator=gen) * 0.1
+    b = torch.randn(C, device="cuda", generator=gen)
+    out = torch.empty_like(x)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flops = 2.0 * G * H * W * C * C * 9
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    ms_tc = timed(lambda: P.conv3x3_tc(x, w, b, out, status))
+    assert int(status.item()) == 0
+    ms_fp32 = timed(lambda: P.conv3x3(x, w, b, out))
+    print(json.dumps({"workload": "nn-conv3x3-8x32x513x513-to-32", "unit": "ms", "gflop": flops / 1e9,
+                      "tcgen05_tf32": {"ms": ms_tc, "tflops": flops / (ms_tc * 1e-3) / 1e12},
+                      "fp32_simt": {"ms": ms_fp32, "tflops": flops / (ms_fp32 * 1e-3) / 1e12}}), flush=True)
+
+
 def solve_comparison(n_steps):
     """s/step of the metric's solve arms on a held-out 2D many-grain packing
     (512^2 cells, 100 circles, seed 1000, scalar mobility, Newton 1e-8): the
@@ -409,6 +447,9 @@ def main():
         return
     if args.workload == "solve2d":
         two_particle_solve(args)
+        return
+    if args.workload == "nnconv":
+        nn_conv(args)
         return
     if args.workload == "solve3d":
         mixed_precision_solve_3d(args)

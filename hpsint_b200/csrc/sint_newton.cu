@@ -13,6 +13,7 @@
 // Jacobian-vector product and FP32 preconditioner, its Gram-Schmidt dot
 // products and norms accumulate in FP64 and its Hessenberg matrix is FP64.
 #include <cmath>
+#include <limits>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -33,7 +34,7 @@ namespace sint
     double   *h_s = nullptr; // pinned host mirror
     double   *d_y = nullptr; // device copy of the GMRES coefficients
     // device-resident Arnoldi state: Hessenberg matrix (column j at j * (restart + 1)),
-    // Givens rotations, rotated right-hand side g, scalars {|w|, tol}, the DGKS flag
+    // Givens rotations, rotated right-hand side g, scalars {|w|, tol}, the re-orthogonalisation flag
     double  *d_H = nullptr, *d_cs = nullptr, *d_sn = nullptr, *d_g = nullptr, *d_sc = nullptr;
     int     *d_flag = nullptr;
     double2 *d_out = nullptr, *h_out = nullptr; // per iteration {|g_{j+1}|, status}
@@ -175,10 +176,13 @@ namespace sint
       g[i] = i == 0 ? beta : 0.0;
   }
 
-  // after the first Gram-Schmidt pass: Hessenberg column j = h and the DGKS
-  // decision (second pass when the norm dropped by more than 30 %)
+  // after the first Gram-Schmidt pass: Hessenberg column j = h and deal.II's
+  // re-orthogonalisation test (Kelley 1995, as in SolverGMRES): once |w| after
+  // the pass falls below 10 sqrt(eps) of |w| before it, every later iteration
+  // of this solve takes a second pass (the flag is sticky).  thresh2 =
+  // 100 eps of the Krylov vectors' precision; |w|^2 before = |h|^2 + |w'|^2.
   __global__ void arnoldi_check_kernel(int j, int ldh, const double *__restrict__ d_s, double *__restrict__ H,
-                                       int *__restrict__ reorth)
+                                       double thresh2, int *__restrict__ reorth)
   {
     if (threadIdx.x != 0)
       return;
@@ -190,7 +194,8 @@ namespace sint
         hh += d_s[i] * d_s[i];
       }
     const double nw2 = d_s[MAX_MULTIDOT];
-    *reorth          = nw2 < 0.49 * (hh + nw2) ? 1 : 0;
+    if (nw2 < thresh2 * (hh + nw2))
+      *reorth = 1;
   }
 
   // after the (optional) second pass: |w|, Givens rotations, residual estimate.
@@ -237,8 +242,9 @@ namespace sint
   }
 
   // Restarted, left-preconditioned GMRES for J x = b with x0 = 0; classical
-  // Gram-Schmidt with a second pass when the first one loses more than 30%
-  // of the norm.  Returns SINT_OK / SINT_ERR_NO_CONVERGENCE; *its = iterations.
+  // Gram-Schmidt with deal.II's re-orthogonalisation test (second pass from
+  // the first iteration whose norm drops below 10 sqrt(eps) of its starting
+  // value on).  Returns SINT_OK / SINT_ERR_NO_CONVERGENCE; *its = iterations.
   //
   // Each Arnoldi iteration is a fixed sequence of kernels (J v, P^-1, fused
   // multi-dot, fused multi-axpy + norm, check, conditional second pass,
@@ -260,6 +266,14 @@ namespace sint
     int    its = 0, rc;
     double tol = 0.0;
     bool   first = true;
+    // 100 eps of the Krylov vectors' precision: (10 sqrt(eps))^2
+    const double reorth_thresh2 = 100.0 * double(std::numeric_limits<R>::epsilon());
+    {
+      // re-orthogonalisation starts off for every solve (deal.II: force_re_orthogonalization = false)
+      const cudaError_t e = cudaMemsetAsync(ws->d_flag, 0, sizeof(int), s);
+      if (e != cudaSuccess)
+        return cuda_fail(e, "GMRES: reset");
+    }
 
     auto enqueue = [&](int j) -> int {
       R  *vj = V + (long long)j * n;
@@ -268,7 +282,7 @@ namespace sint
           (r = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s)) ||
           (r = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s)))
         return r;
-      arnoldi_check_kernel<<<1, 32, 0, s>>>(j, ldh, ws->d_s, ws->d_H, ws->d_flag);
+      arnoldi_check_kernel<<<1, 32, 0, s>>>(j, ldh, ws->d_s, ws->d_H, reorth_thresh2, ws->d_flag);
       count_launches(1);
       if ((r = multidot_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_flag, s)) ||
           (r = multiaxpy_norm2_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, ws->d_flag, s)))
