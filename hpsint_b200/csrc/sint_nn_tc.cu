@@ -37,6 +37,7 @@ namespace sint
     constexpr int NMAX    = 32;             // output channels (TMEM columns)
     constexpr int TMEM_COLS = 32;           // smallest TMEM allocation
     constexpr int THREADS = 256;            // warps w and w + 4 read the same TMEM lanes, different columns
+    constexpr int CTAS_PER_SM = 2;
     constexpr int CIN_MAX = 32;
 
     __host__ __device__ constexpr int chunks_of(int cin) { return (cin + 7) / 8 * 2; } // 4-channel chunks, K padded to 8
@@ -114,7 +115,7 @@ namespace sint
     }
 
     template <int N>
-    __global__ void __launch_bounds__(THREADS, 2)
+    __global__ void __launch_bounds__(THREADS, CTAS_PER_SM)
       conv3x3_tc_kernel(const float *__restrict__ in, int B, int Cin, int H, int W, const float *__restrict__ w,
                         const float *__restrict__ bias, float *__restrict__ out, int Cout, int accumulate,
                         int *status)
@@ -169,6 +170,13 @@ namespace sint
       uint32_t phase = 0;
       bool     failed = false;
       int      buf = 0;
+      // this thread's epilogue columns never change: keep their biases in registers
+      constexpr int NH = N / 2;
+      const int     c0 = (warp >> 2) * NH;
+      float         bias_r[NH];
+#pragma unroll
+      for (int j = 0; j < NH; ++j)
+        bias_r[j] = (bias && c0 + j < Cout) ? bias[c0 + j] : 0.f;
       if (blockIdx.x < n_tiles)
         {
           int b, y0, x0;
@@ -226,8 +234,7 @@ namespace sint
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (pixels), columns (w / 4) N/2 .. + N/2 - 1
           {
-            constexpr int  NH   = N / 2;
-            const int      row  = 32 * (warp & 3) + lane, c0 = (warp >> 2) * NH;
+            const int      row  = 32 * (warp & 3) + lane;
             const uint32_t addr = taddr + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(c0);
             uint32_t       d[NH];
             if constexpr (NH == 16)
@@ -253,7 +260,7 @@ namespace sint
                     const int co = c0 + j;
                     if (co >= Cout)
                       break;
-                    float v = __uint_as_float(d[j]) + (bias ? bias[co] : 0.f);
+                    float v = __uint_as_float(d[j]) + bias_r[j];
                     if (accumulate)
                       v += ob[size_t(co) * HW];
                     ob[size_t(co) * HW] = v;
@@ -287,7 +294,7 @@ namespace
     auto       k        = tc::conv3x3_tc_kernel<N>;
     if (grid_cap == 0)
       {
-        int         dev = 0, sms = 0, per_sm = 0;
+        int         dev = 0, sms = 0;
         const int   smax = int(tc::smem_bytes(tc::chunks_of(tc::CIN_MAX), N));
         cudaError_t e    = cudaGetDevice(&dev);
         if (e == cudaSuccess)
@@ -296,11 +303,11 @@ namespace
           e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
         if (e == cudaSuccess) // all of the unified L1 / shared storage as shared memory
           e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e == cudaSuccess)
-          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tc::THREADS, smax);
         if (e != cudaSuccess)
           return cuda_fail(e, "sint_nn_conv3x3_tc_f32: setup");
-        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
+        // two CTAs per SM: the launch bound caps registers at 128 and the largest
+        // configuration takes 83 KB of shared memory, so both fit on every SM
+        grid_cap = sms * tc::CTAS_PER_SM;
       }
     const int       KC    = tc::chunks_of(Cin);
     const long long tiles = (long long)B * ((H + tc::TY - 1) / tc::TY) * ((W + tc::TX - 1) / tc::TX);
