@@ -54,6 +54,10 @@ def parse_args():
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
     ap.add_argument("--n3", type=int, default=192, help="cells per direction of the 3D solve workload")
+    ap.add_argument("--spheres", type=int, default=51, help="3D solve: number of spheres")
+    ap.add_argument("--median", type=float, default=10.0, help="3D solve: median sphere radius")
+    ap.add_argument("--sigma", type=float, default=0.2, help="3D solve: sigma of log radius")
+    ap.add_argument("--max-grains", type=int, default=10, help="3D solve: order-parameter budget")
     ap.add_argument("--no-solve", action="store_true", help="skip the s/step comparison of the operator run")
     ap.add_argument("--solve-compare-steps", type=int, default=40)
     ap.add_argument("--train-seeds", type=int, default=10)
@@ -197,9 +201,9 @@ def two_particle_solve(args):
     """2D two-particle sintering: 256 x 128 Q1 cells on [-40, 40] x [-20, 20],
     circles R = 10 at (+-10, 0), tanh width 2, G = 2, hpsint's default
     constants, BDF1 with dt0 = 1e-3 and hpsint's dt control, Newton relative
-    tolerance 1e-8.  Runs the plain FP64 solve and the FP32-inner solve from
-    the same state and reports s/step, iteration counts, and the FP32-inner
-    run's error against the FP64 run."""
+    tolerance 1e-8.  Runs the plain FP64 solve, then the FP32-inner solve from
+    the same state on the FP64 run's time grid, and reports s/step, iteration
+    counts, and the FP32-inner run's error against the FP64 run."""
     import torch
 
     import hpsint_b200 as hb
@@ -214,26 +218,30 @@ def two_particle_solve(args):
     wy = np.full(ny + 1, h[1]); wy[[0, -1]] *= 0.5
     mass = np.outer(wy, wx).ravel()  # lumped weights: int c_h = sum_n m_n c_n
 
-    runs = {}
+    runs, schedule = {}, None
     for label, prec in (("fp64", 64), ("fp32_inner", 32)):
         op = hb.SinteringOperatorGeneric(hb.Mesh(2, (nx, ny, 1), (h[0], h[1], 1.0)), hb.Params(2))
         ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec),
                             TimeIntegrationData(time_step_init=1e-3))
         ti.initialize(op.to_device(u0))
+        ti.run(2, dt_schedule=[1e-3, 1e-3])  # warm-up (discarded)
+        ti.initialize(op.to_device(u0))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ti.run(args.solve_steps)
+        ti.run(args.solve_steps, dt_schedule=schedule)  # the FP32-inner run replays the FP64 time grid
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+        if schedule is None:
+            schedule = [r.dt for r in ti.records]
         u = op.to_host(ti.history[0])
         runs[label] = dict(u=u, wall=wall, t=ti.t, rec=ti.records)
     ref, mp = runs["fp64"], runs["fp32_inner"]
-    n_common = min(len(ref["rec"]), len(mp["rec"]))
     line = {"metric": METRIC, "workload": "2d-two-particle-256x128-G2", "steps": args.solve_steps,
             "unit": "s/step", "higher_is_better": False, "dtype": "f64 Newton", "data": "synthetic"}
     for label, r in runs.items():
         recs = r["rec"]
         line[label] = {"s_per_step": r["wall"] / len(recs), "sim_time": r["t"],
+                       "s_per_accepted_attempt": sum(x.accepted_wall_s for x in recs) / len(recs),
                        "newton_iterations": sum(x.newton_iterations for x in recs),
                        "linear_iterations": sum(x.linear_iterations for x in recs),
                        "failed_tries": sum(x.failed_tries for x in recs), "final_dt": recs[-1].dt}
@@ -245,6 +253,8 @@ def two_particle_solve(args):
         "int_c_conservation_fp64": float(abs(mass @ ref["u"][0] - mass @ u0[0]) / abs(mass @ u0[0])),
         "int_c_conservation_fp32_inner": float(abs(mass @ mp["u"][0] - mass @ u0[0]) / abs(mass @ u0[0])),
         "speedup_s_per_step": (ref["wall"] / len(ref["rec"])) / (mp["wall"] / len(mp["rec"])),
+        "speedup_accepted_attempts": sum(x.accepted_wall_s for x in ref["rec"]) /
+                                     sum(x.accepted_wall_s for x in mp["rec"]),
     }
     print(json.dumps(line), flush=True)
 
@@ -331,7 +341,8 @@ def mixed_precision_solve_3d(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     n = args.n3
-    centers, radii, colours = P.lognormal_packing_3d(n=n)
+    centers, radii, colours = P.lognormal_packing_3d(n=n, n_spheres=args.spheres, median=args.median,
+                                                     sigma=args.sigma, max_grains=args.max_grains)
     G = int(colours.max()) + 1
     u0 = P.initial_state(3, (n, n, n), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), centers, radii, colours, width=2.0)
     w = np.ones(n + 1)
@@ -360,7 +371,7 @@ def mixed_precision_solve_3d(args):
         runs[label] = dict(u=u, wall=wall, recs=recs, c_int=c_int)
         del ti
     ref, mp = runs["fp64_inner"], runs["fp32_inner"]
-    line = {"metric": METRIC, "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-G{G}",
+    line = {"metric": METRIC, "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-median{args.median:g}-G{G}",
             "unit": "s/step", "higher_is_better": False, "dofs": op.C * op.N, "grains": G,
             "steps": args.solve_steps, "dtype": "f64 Newton", "data": "synthetic seeded packing",
             "mobility": "scalar" if args.scalar else "tensorial"}

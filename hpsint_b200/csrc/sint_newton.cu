@@ -40,6 +40,20 @@ namespace sint
     double2 *d_out = nullptr, *h_out = nullptr; // per iteration {|g_{j+1}|, status}
     double  *h_H   = nullptr;                   // pinned host copy of H and g at the end of a cycle
     cudaEvent_t ev[MAX_MULTIDOT] = {};
+    // The Krylov loop runs on a private non-blocking stream (joined to the
+    // caller's stream by two events) so that Arnoldi iteration j can be
+    // captured once as a CUDA graph and replayed; a graph is updated in place
+    // when a kernel argument it holds (the operator's physics: time weights,
+    // mobility) has changed since its capture.
+    cudaStream_t ps       = nullptr;
+    cudaEvent_t  join_in  = nullptr, join_out = nullptr;
+    struct IterGraph
+    {
+      cudaGraphExec_t exec  = nullptr;
+      Phys            key   = {};
+      int             nodes = 0;
+    } graphs[MAX_MULTIDOT];
+    bool warm = false; // one eager solve has run (lazy kernel set-up is done outside any capture)
   };
 
   int free_workspace(Ctx *c)
@@ -70,6 +84,15 @@ namespace sint
     for (cudaEvent_t &e : w->ev)
       if (e)
         cudaEventDestroy(e);
+    for (auto &g : w->graphs)
+      if (g.exec)
+        cudaGraphExecDestroy(g.exec);
+    if (w->join_in)
+      cudaEventDestroy(w->join_in);
+    if (w->join_out)
+      cudaEventDestroy(w->join_out);
+    if (w->ps)
+      cudaStreamDestroy(w->ps);
     delete w;
     c->ws = nullptr;
     return SINT_OK;
@@ -117,6 +140,14 @@ namespace sint
           free_workspace(c);
           return rc;
         }
+    if ((e = cudaStreamCreateWithFlags(&w->ps, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&w->join_in, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&w->join_out, cudaEventDisableTiming)) != cudaSuccess)
+      {
+        const int rc = cuda_fail(e, "newton workspace stream");
+        free_workspace(c);
+        return rc;
+      }
     // padding entries take part in dot products: keep every vector zeroed
     if ((e = cudaMemset(w->r, 0, n64)) != cudaSuccess || (e = cudaMemset(w->du, 0, n64)) != cudaSuccess ||
         (e = cudaMemset(w->tmp, 0, n64)) != cudaSuccess || (e = cudaMemset(w->V, 0, nr * (restart + 1))) != cudaSuccess ||
@@ -255,7 +286,7 @@ namespace sint
   // vector j + 2 and Hessenberg column j + 1, which the solution update
   // (columns 0..j) never reads.
   template <typename R>
-  static int gmres(Ctx *c, const sint_newton_params &prm, cudaStream_t s, int *its_out)
+  static int gmres_body(Ctx *c, const sint_newton_params &prm, cudaStream_t s, int *its_out)
   {
     Workspace      *ws = c->ws;
     const long long n  = ws->nvec;
@@ -275,7 +306,7 @@ namespace sint
         return cuda_fail(e, "GMRES: reset");
     }
 
-    auto enqueue = [&](int j) -> int {
+    auto enqueue_kernels = [&](int j) -> int {
       R  *vj = V + (long long)j * n;
       int r;
       if ((r = jvp<R>(c, t, vj, s)) || (r = prec<R>(c, w, t, s)) ||
@@ -292,10 +323,70 @@ namespace sint
       count_launches(1);
       if ((r = scale_by_device<R>(n, w, ws->d_sc, V + (long long)(j + 1) * n, s)))
         return r;
-      cudaError_t e = cudaMemcpyAsync(ws->h_out + j, ws->d_out + j, sizeof(double2), cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess)
-        e = cudaEventRecord(ws->ev[j], s);
+      const cudaError_t e =
+        cudaMemcpyAsync(ws->h_out + j, ws->d_out + j, sizeof(double2), cudaMemcpyDeviceToHost, s);
       return e == cudaSuccess ? SINT_OK : cuda_fail(e, "GMRES: enqueue");
+    };
+
+    // Iteration j: replay its graph (capture or update it first when needed),
+    // then record the event the host waits on.
+    auto enqueue = [&](int j) -> int {
+      int r = SINT_OK;
+      if (!ws->warm)
+        r = enqueue_kernels(j);
+      else
+        {
+          auto &g = ws->graphs[j];
+          if (!g.exec || std::memcmp(&g.key, &c->phys, sizeof(Phys)) != 0)
+            {
+              cudaGraph_t       graph = nullptr;
+              const long long   n0    = sint_kernel_launch_count();
+              cudaError_t       e     = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+              if (e != cudaSuccess)
+                return cuda_fail(e, "GMRES: begin capture");
+              const int rk = enqueue_kernels(j);
+              e            = cudaStreamEndCapture(s, &graph);
+              count_launches(-int(sint_kernel_launch_count() - n0)); // captured, not launched
+              if (rk != SINT_OK || e != cudaSuccess)
+                {
+                  if (graph)
+                    cudaGraphDestroy(graph);
+                  return rk != SINT_OK ? rk : cuda_fail(e, "GMRES: end capture");
+                }
+              size_t nn = 0;
+              cudaGraphGetNodes(graph, nullptr, &nn);
+              bool updated = false;
+              if (g.exec)
+                {
+                  cudaGraphExecUpdateResultInfo info;
+                  updated = cudaGraphExecUpdate(g.exec, graph, &info) == cudaSuccess;
+                  if (!updated)
+                    {
+                      cudaGetLastError(); // clear the update failure; instantiate anew
+                      cudaGraphExecDestroy(g.exec);
+                      g.exec = nullptr;
+                    }
+                }
+              if (!updated)
+                e = cudaGraphInstantiate(&g.exec, graph, 0);
+              cudaGraphDestroy(graph);
+              if (e != cudaSuccess)
+                {
+                  g.exec = nullptr;
+                  return cuda_fail(e, "GMRES: instantiate");
+                }
+              g.key   = c->phys;
+              g.nodes = int(nn);
+            }
+          const cudaError_t e = cudaGraphLaunch(g.exec, s);
+          if (e != cudaSuccess)
+            return cuda_fail(e, "GMRES: graph launch");
+          count_launches(g.nodes);
+        }
+      if (r != SINT_OK)
+        return r;
+      const cudaError_t e = cudaEventRecord(ws->ev[j], s);
+      return e == cudaSuccess ? SINT_OK : cuda_fail(e, "GMRES: record");
     };
 
     if ((rc = axpby<R>(n, 0.0, b, 0.0, x, s)))
@@ -427,6 +518,27 @@ namespace sint
             return SINT_ERR_NO_CONVERGENCE;
           }
       }
+  }
+
+  // GMRES on the workspace's private stream, ordered after and before the caller's stream.
+  template <typename R>
+  static int gmres(Ctx *c, const sint_newton_params &prm, cudaStream_t s, int *its_out)
+  {
+    Workspace  *ws = c->ws;
+    cudaError_t e  = cudaEventRecord(ws->join_in, s);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(ws->ps, ws->join_in, 0);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "GMRES: join");
+    const int rc = gmres_body<R>(c, prm, ws->ps, its_out);
+    e            = cudaEventRecord(ws->join_out, ws->ps);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(s, ws->join_out, 0);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "GMRES: join back");
+    if (rc == SINT_OK)
+      ws->warm = true;
+    return rc;
   }
 
   static int residual_norm(Ctx *c, double *r, double *out, cudaStream_t s)

@@ -118,7 +118,7 @@ namespace sint
     __global__ void __launch_bounds__(THREADS, CTAS_PER_SM)
       conv3x3_tc_kernel(const float *__restrict__ in, int B, int Cin, int H, int W, const float *__restrict__ w,
                         const float *__restrict__ bias, float *__restrict__ out, int Cout, int accumulate,
-                        int *status)
+                        const float *__restrict__ addend, int add_group, int act, float slope, int *status)
     {
       extern __shared__ __align__(1024) unsigned char smem_raw[];
       const int KC = chunks_of(Cin);                           // 4-channel chunks per tap
@@ -263,6 +263,10 @@ namespace sint
                     float v = __uint_as_float(d[j]) + bias_r[j];
                     if (accumulate)
                       v += ob[size_t(co) * HW];
+                    if (addend) // one addend image per group of add_group batch entries
+                      v += addend[(size_t(b / add_group) * Cout + co) * HW + y * W + x];
+                    if (act)
+                      v = v > 0.f ? v : slope * v;
                     ob[size_t(co) * HW] = v;
                   }
               }
@@ -288,7 +292,8 @@ namespace
 {
   template <int N>
   int launch_tc(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias, float *out, int Cout,
-                int accumulate, int *status, cudaStream_t s)
+                int accumulate, const float *addend, int add_group, int act, float slope, int *status,
+                cudaStream_t s)
   {
     static int grid_cap = 0;
     auto       k        = tc::conv3x3_tc_kernel<N>;
@@ -312,7 +317,8 @@ namespace
     const int       KC    = tc::chunks_of(Cin);
     const long long tiles = (long long)B * ((H + tc::TY - 1) / tc::TY) * ((W + tc::TX - 1) / tc::TX);
     const int       grid  = int(tiles < grid_cap ? tiles : grid_cap);
-    k<<<grid, tc::THREADS, tc::smem_bytes(KC, N), s>>>(in, B, Cin, H, W, w, bias, out, Cout, accumulate, status);
+    k<<<grid, tc::THREADS, tc::smem_bytes(KC, N), s>>>(in, B, Cin, H, W, w, bias, out, Cout, accumulate, addend,
+                                                       add_group, act, slope, status);
     count_launches(1);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SINT_OK : cuda_fail(e, "sint_nn_conv3x3_tc_f32");
@@ -321,17 +327,27 @@ namespace
 
 extern "C" {
 
+int sint_nn_conv3x3_tc_ex_f32(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias,
+                              float *out, int Cout, int accumulate, const float *addend, int addend_group,
+                              int leaky, float slope, int *status, sint_stream_t s)
+{
+  if (!in || !w || !out || !status || B < 1 || Cin < 1 || Cin > tc::CIN_MAX || Cout < 1 || Cout > tc::NMAX || H < 1 ||
+      W < 1 || (addend && (addend_group < 1 || B % addend_group != 0)))
+    {
+      set_error("sint_nn_conv3x3_tc_f32: bad argument (needs 1 <= Cin <= 32, 1 <= Cout <= 32, "
+                "addend_group dividing B)");
+      return SINT_ERR_ARG;
+    }
+  return Cout <= 16 ? launch_tc<16>(in, B, Cin, H, W, w, bias, out, Cout, accumulate, addend, addend_group, leaky,
+                                    slope, status, s)
+                    : launch_tc<32>(in, B, Cin, H, W, w, bias, out, Cout, accumulate, addend, addend_group, leaky,
+                                    slope, status, s);
+}
+
 int sint_nn_conv3x3_tc_f32(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias,
                            float *out, int Cout, int accumulate, int *status, sint_stream_t s)
 {
-  if (!in || !w || !out || !status || B < 1 || Cin < 1 || Cin > tc::CIN_MAX || Cout < 1 || Cout > tc::NMAX || H < 1 ||
-      W < 1)
-    {
-      set_error("sint_nn_conv3x3_tc_f32: bad argument (needs 1 <= Cin <= 32, 1 <= Cout <= 32)");
-      return SINT_ERR_ARG;
-    }
-  return Cout <= 16 ? launch_tc<16>(in, B, Cin, H, W, w, bias, out, Cout, accumulate, status, s)
-                    : launch_tc<32>(in, B, Cin, H, W, w, bias, out, Cout, accumulate, status, s);
+  return sint_nn_conv3x3_tc_ex_f32(in, B, Cin, H, W, w, bias, out, Cout, accumulate, nullptr, 1, 0, 0.f, status, s);
 }
 
 } // extern "C"

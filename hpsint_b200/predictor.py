@@ -54,6 +54,16 @@ def conv3x3_tc(x, w, bias, out, status, accumulate=False):
                                            _p(status), _s()), "sint_nn_conv3x3_tc_f32")
 
 
+def conv3x3_tc_ex(x, w, bias, out, status, accumulate=False, addend=None, addend_group=1, slope=None):
+    """conv3x3_tc with the fused inference epilogue: out = act(conv + bias (+ out) (+ addend[b // group]))
+    with act the leaky ReLU of `slope` (None: identity)."""
+    B, Cin, H, W = x.shape
+    Cout = w.shape[0]
+    L.check(L.lib().sint_nn_conv3x3_tc_ex_f32(_p(x), B, Cin, H, W, _p(w), _p(bias), _p(out), Cout, int(accumulate),
+                                              _p(addend), int(addend_group), int(slope is not None),
+                                              float(slope or 0.0), _p(status), _s()), "sint_nn_conv3x3_tc_ex_f32")
+
+
 def conv3x3_input_grad(dout, w, din, accumulate=False, wT=None):
     """din (+)= d(conv(x, w))/dx applied to dout (convolution with the flipped kernel)."""
     Cout, Cin = w.shape[0], w.shape[1]
@@ -178,6 +188,8 @@ class EquivariantNet:
         tensor_cores: run the convolutions on the tensor cores (TF32 products,
         FP32 accumulation; inference) instead of the FP32 kernel."""
         H, W = xs.shape[2], xs.shape[3]
+        if tensor_cores and not keep and max(max(d) for d in self.dims) <= 32:
+            return self._forward_fused(xg, xs, B, G, H, W)
         cache = []
         hg, hs = xg, xs
 
@@ -210,6 +222,29 @@ class EquivariantNet:
             else:
                 hg, hs = Zg, Zs
         return hg, hs, cache
+
+    def _forward_fused(self, xg, xs, B, G, H, W):
+        """Inference on the tensor cores with fused epilogues: per layer
+        P = sum_i h_i;  Q = B*P + C*s;  h_i <- act(A*h_i + a + Q)  (one conv);
+        s <- act(D*s + d + E*P)  (the activation in the second conv)."""
+        hg, hs = xg, xs
+        n = len(self.dims)
+        st = self.tc_status
+        for l, (cg, cs, go, so) in enumerate(self.dims):
+            w = self.w[l]
+            slope = self.cfg.slope if l < n - 1 else None
+            P = torch.empty((B, cg, H, W), dtype=torch.float32, device="cuda")
+            grain_sum(hg, B, G, P)
+            Q = torch.empty((B, go, H, W), dtype=torch.float32, device="cuda")
+            conv3x3_tc(P, w["B"], None, Q, st)
+            conv3x3_tc(hs, w["C"], None, Q, st, accumulate=True)
+            Zg = torch.empty((B * G, go, H, W), dtype=torch.float32, device="cuda")
+            conv3x3_tc_ex(hg, w["A"], w["a"], Zg, st, addend=Q, addend_group=G, slope=slope)
+            Zs = torch.empty((B, so, H, W), dtype=torch.float32, device="cuda")
+            conv3x3_tc(hs, w["D"], w["d"], Zs, st)
+            conv3x3_tc_ex(P, w["E"], None, Zs, st, accumulate=True, slope=slope)
+            hg, hs = Zg, Zs
+        return hg, hs, []
 
     # -- backward ------------------------------------------------------------
     def backward(self, cache, dyg, dys, B, G):

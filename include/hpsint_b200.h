@@ -269,6 +269,13 @@ int sint_nn_conv3x3_f32(const float *in, int B, int Cin, int H, int W, const flo
  * out (the output is then incomplete). */
 int sint_nn_conv3x3_tc_f32(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias,
                            float *out, int Cout, int accumulate, int *status, sint_stream_t stream);
+/* The same with a fused epilogue for inference: out = act(conv + bias
+ * (+ out if accumulate) (+ addend[b / addend_group] if addend)), act = leaky
+ * ReLU with `slope` if leaky != 0.  addend: [B / addend_group][Cout][H][W]
+ * (the shared-stream term broadcast to the grain streams). */
+int sint_nn_conv3x3_tc_ex_f32(const float *in, int B, int Cin, int H, int W, const float *w, const float *bias,
+                              float *out, int Cout, int accumulate, const float *addend, int addend_group,
+                              int leaky, float slope, int *status, sint_stream_t stream);
 /* wT[ci][co][8 - k] = w[co][ci][k]: the kernel whose convolution with the
  * output gradient is the input gradient. */
 int sint_nn_conv3x3_flip_f32(const float *w, int Cout, int Cin, float *wT, sint_stream_t stream);

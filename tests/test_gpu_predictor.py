@@ -123,3 +123,21 @@ def test_network_inference_on_tensor_cores():
     yg2, ys2, _ = net.forward(xg, xs, B, G, tensor_cores=True)
     net.check_tensor_cores()
     assert rel(yg2.cpu().numpy(), yg.cpu().numpy()) < 1e-2 and rel(ys2.cpu().numpy(), ys.cpu().numpy()) < 1e-2
+
+
+def test_tensor_core_conv_fused_epilogue():
+    """act(conv + bias + out + addend[b // group]) against the FP32 kernel and torch arithmetic."""
+    from hpsint_b200 import predictor as P
+    rng = np.random.default_rng(4)
+    Bg, grp, Cin, Cout, H, W = 6, 3, 32, 32, 19, 26
+    x, w, b = rng.normal(size=(Bg, Cin, H, W)), rng.normal(size=(Cout, Cin, 3, 3)), rng.normal(size=Cout)
+    q, o0 = rng.normal(size=(Bg // grp, Cout, H, W)), rng.normal(size=(Bg, Cout, H, W))
+    ref = dev(o0)
+    P.conv3x3(dev(x), dev(w), dev(b), ref, accumulate=True)
+    ref = ref + dev(q).repeat_interleave(grp, dim=0)
+    ref = torch.where(ref > 0, ref, 0.1 * ref)
+    out = dev(o0)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    P.conv3x3_tc_ex(dev(x), dev(w), dev(b), out, status, accumulate=True, addend=dev(q), addend_group=grp, slope=0.1)
+    assert int(status.item()) == 0
+    assert rel(out.cpu().numpy(), ref.cpu().numpy()) < 3e-3
