@@ -50,7 +50,8 @@ def parse_args():
     ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["operator", "solve2d", "solve3d", "learned2d", "nnconv"], default="operator",
+    ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "nnconv"],
+                    default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
     ap.add_argument("--n3", type=int, default=192, help="cells per direction of the 3D solve workload")
@@ -259,6 +260,49 @@ def two_particle_solve(args):
     print(json.dumps(line), flush=True)
 
 
+def operator_2d(args):
+    """The kernels of one FP32-inner Newton step on the 2D many-grain state
+    (512^2 cells, 100 circles, seed 0, G = 8, scalar mobility, 2.63 M DoFs,
+    BDF1 with dt = 1e-3): CUDA-event time per call of J v (FP64, FP32), the
+    residual and the FP32 block-Jacobi apply."""
+    import torch
+
+    from hpsint_b200 import learned_guess as LG
+    from hpsint_b200.operator import BlockPreconditioner2
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    case = LG.make_case(0)
+    op = case.op
+    op.set_time_weights(1.0 / DT, [-1.0 / DT], 1.0)
+    op.fill_quadrature_point_values(case.u0)
+    gen = torch.Generator("cuda").manual_seed(3)
+    v = torch.rand(case.u0.shape, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
+    v[:, op.N:] = 0
+    d = op.initialize_dof_vector()
+    v32, d32 = v.float(), d.float()
+    pc = BlockPreconditioner2(op)
+    pc.do_update()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    dofs = op.C * op.N
+    res = {"jvp_f64": timed(lambda: op.vmult(d, v)), "jvp_f32": timed(lambda: op.vmult(d32, v32)),
+           "residual_f64_bdf1": timed(lambda: op.evaluate_nonlinear_residual(d, case.u0, 2, [case.u0])),
+           "precond_apply_f32": timed(lambda: pc.vmult(d32, v32))}
+    print(json.dumps({"workload": f"2d-512x512-100-circles-G{case.G}-operator", "dofs": dofs, "unit": "ms",
+                      "ms": res, "gdofs": {k: dofs / (t * 1e-3) / 1e9 for k, t in res.items()}}), flush=True)
+
+
 def nn_conv(args):
     """The learned guess's hidden-layer convolution at inference size: 8 grain
     streams of 513 x 513 nodes, 32 -> 32 channels, 3x3 (38.8 GFLOP): the
@@ -458,6 +502,9 @@ def main():
         return
     if args.workload == "solve2d":
         two_particle_solve(args)
+        return
+    if args.workload == "operator2d":
+        operator_2d(args)
         return
     if args.workload == "nnconv":
         nn_conv(args)
