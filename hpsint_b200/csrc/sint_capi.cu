@@ -38,7 +38,7 @@ namespace sint
   cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, cudaStream_t s)
   {
     const long long nb = (g.N + 255) / 256;
-    combine_kernel<DIM, R><<<dim3((unsigned)nb), 256, 0, s>>>(g, ncomp, partial, dst);
+    combine_kernel<DIM, R><<<dim3((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u), 256, 0, s>>>(g, ncomp, partial, dst);
     count_launches(1);
     return cudaGetLastError();
   }

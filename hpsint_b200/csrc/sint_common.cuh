@@ -510,13 +510,16 @@ namespace sint
   }
 
   // Second pass of the scatter: nodes on an interior tile face sum the
-  // partials of the 2, 4 or 8 tiles that share them, in a fixed order.
+  // partials of the 2, 4 or 8 tiles that share them, in a fixed order.  One
+  // thread per (node, component): blockIdx.y is the component, so the
+  // partial loads of different components are independent.
   template <int DIM, typename R>
   __global__ void __launch_bounds__(256) combine_kernel(const Grid g, int ncomp, const R *__restrict__ partial,
                                                         R *__restrict__ dst)
   {
-    using T             = Tile<DIM>;
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    using T              = Tile<DIM>;
+    const long long idx  = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int       comp = blockIdx.y;
     if (idx >= g.N)
       return;
     int c[3];
@@ -558,7 +561,9 @@ namespace sint
       }
     if (!shared)
       return;
-    for (int comp = 0; comp < ncomp; ++comp)
+    // 2D: one component per thread (blockIdx.y); 3D: one thread loops over all components
+    const int c_end = DIM == 2 ? comp + 1 : ncomp;
+    for (int cp = DIM == 2 ? comp : 0; cp < c_end; ++cp)
       {
         R sum = R(0);
         for (int a = 0; a < nt[2]; ++a)
@@ -568,9 +573,9 @@ namespace sint
                 const int       ti = t0[0] + cc, tj = t0[1] + bb, tk = t0[2] + a;
                 const int       bx = lo[0] - cc * TT[0], by = lo[1] - bb * TT[1], bz = lo[2] - a * TT[2];
                 const long long tile = ti + (long long)g.nt[0] * (tj + (long long)g.nt[1] * tk);
-                sum += partial[(tile * ncomp + comp) * (long long)T::BOX + bx + T::BX * (by + T::BY * bz)];
+                sum += partial[(tile * ncomp + cp) * (long long)T::BOX + bx + T::BX * (by + T::BY * bz)];
               }
-        dst[comp * g.ld + idx] = sum;
+        dst[cp * g.ld + idx] = sum;
       }
   }
 } // namespace sint

@@ -364,10 +364,10 @@ namespace sint
   // software pipelined: block b handles tiles b, b + grid, ...; the node boxes
   // of the next tile are copied (cp.async) into the second half of a double
   // buffer while the current tile is computed.
-  // Two resident blocks per SM (<= 128 registers) unless the FP64 grain state
-  // of large G would spill; those run one block with up to 255 registers.
+  // Two resident blocks per SM (<= 128 registers) unless the 3D FP64 grain
+  // state of large G would spill; those run one block with up to 255 registers.
   template <int DIM, int G, bool TENS, typename R>
-  __global__ void __launch_bounds__(Tile<DIM>::THREADS, (sizeof(R) == 8 && G > 5) ? 1 : 2)
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, (DIM == 3 && sizeof(R) == 8 && G > 5) ? 1 : 2)
     jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
                R *__restrict__ dst, R *__restrict__ partial)
   {
@@ -423,7 +423,7 @@ namespace sint
   // do_evalute_history (:927-975) for WTD == 2: the weighted sum of the old
   // solutions is formed at the nodes while staging and evaluated at the points.
   template <int DIM, int G, bool TENS, int WTD>
-  __global__ void __launch_bounds__(Tile<DIM>::THREADS, G > 5 ? 1 : 2)
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, (DIM == 3 && G > 5) ? 1 : 2)
     residual_kernel(const Grid g, const Phys ph, const double *__restrict__ src, const double *__restrict__ h0,
                     const double *__restrict__ h1, const double *__restrict__ h2, double *__restrict__ dst,
                     double *__restrict__ partial)

@@ -8,11 +8,25 @@
 
 namespace sint
 {
+  // Dynamic shared memory above the 48 KB default, and a shared-memory
+  // carveout just large enough for two resident blocks (the rest of the
+  // unified storage stays L1), so that two blocks of up to ~100 KB fit.
   template <typename Kernel>
   inline cudaError_t prepare_smem(Kernel k, size_t bytes)
   {
     if (bytes > 48 * 1024)
-      return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+      {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        if (e != cudaSuccess)
+          return e;
+        int dev = 0, per_sm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+            (e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+          return e;
+        const size_t two = 2 * (bytes + 1024); // + the per-block reservation
+        const int    pct = two >= size_t(per_sm) ? 100 : int((two * 100 + per_sm - 1) / per_sm);
+        return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+      }
     return cudaSuccess;
   }
 
