@@ -365,9 +365,21 @@ namespace sint
   // of the next tile are copied (cp.async) into the second half of a double
   // buffer while the current tile is computed.
   // Two resident blocks per SM (<= 128 registers) unless the 3D FP64 grain
-  // state of large G would spill; those run one block with up to 255 registers.
+  // state of large G would spill (one block, up to 255 registers); the light
+  // 2D FP32 product runs three (<= 85 registers).
+  template <int DIM, int G, typename R>
+  constexpr int jvp_blocks_per_sm()
+  {
+    return (DIM == 3 && sizeof(R) == 8 && G > 5) ? 1 : (DIM == 2 && sizeof(R) == 4) ? 3 : 2;
+  }
+  template <int DIM, int G>
+  constexpr int residual_blocks_per_sm()
+  {
+    return (DIM == 3 && G > 5) ? 1 : 2;
+  }
+
   template <int DIM, int G, bool TENS, typename R>
-  __global__ void __launch_bounds__(Tile<DIM>::THREADS, (DIM == 3 && sizeof(R) == 8 && G > 5) ? 1 : 2)
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, jvp_blocks_per_sm<DIM, G, R>())
     jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
                R *__restrict__ dst, R *__restrict__ partial)
   {
@@ -423,7 +435,7 @@ namespace sint
   // do_evalute_history (:927-975) for WTD == 2: the weighted sum of the old
   // solutions is formed at the nodes while staging and evaluated at the points.
   template <int DIM, int G, bool TENS, int WTD>
-  __global__ void __launch_bounds__(Tile<DIM>::THREADS, (DIM == 3 && G > 5) ? 1 : 2)
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, residual_blocks_per_sm<DIM, G>())
     residual_kernel(const Grid g, const Phys ph, const double *__restrict__ src, const double *__restrict__ h0,
                     const double *__restrict__ h1, const double *__restrict__ h2, double *__restrict__ dst,
                     double *__restrict__ partial)

@@ -9,25 +9,22 @@
 namespace sint
 {
   // Dynamic shared memory above the 48 KB default, and a shared-memory
-  // carveout just large enough for two resident blocks (the rest of the
-  // unified storage stays L1), so that two blocks of up to ~100 KB fit.
+  // carveout just large enough for `blocks` resident blocks (the rest of the
+  // unified storage stays L1).
   template <typename Kernel>
-  inline cudaError_t prepare_smem(Kernel k, size_t bytes)
+  inline cudaError_t prepare_smem(Kernel k, size_t bytes, int blocks = 2)
   {
-    if (bytes > 48 * 1024)
-      {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-        if (e != cudaSuccess)
-          return e;
-        int dev = 0, per_sm = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
-            (e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
-          return e;
-        const size_t two = 2 * (bytes + 1024); // + the per-block reservation
-        const int    pct = two >= size_t(per_sm) ? 100 : int((two * 100 + per_sm - 1) / per_sm);
-        return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
-      }
-    return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    if (bytes > 48 * 1024 && (e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))) !=
+                               cudaSuccess)
+      return e;
+    int dev = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+      return e;
+    const size_t need = size_t(blocks) * (bytes + 1024); // + the per-block reservation
+    const int    pct  = need >= size_t(per_sm) ? 100 : int((need * 100 + per_sm - 1) / per_sm);
+    return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
   }
 
   template <int DIM, int G, bool TENS, typename R>
@@ -41,7 +38,7 @@ namespace sint
     cudaError_t  e        = cudaSuccess;
     if (grid_cap == 0)
       {
-        if ((e = prepare_smem(k, smem)) != cudaSuccess)
+        if ((e = prepare_smem(k, smem, jvp_blocks_per_sm<DIM, G, R>())) != cudaSuccess)
           return e;
         int dev = 0, sms = 0, per_sm = 0;
         if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
@@ -66,7 +63,7 @@ namespace sint
     cudaError_t   e        = cudaSuccess;
     if (grid_cap == 0)
       {
-        if ((e = prepare_smem(k, smem)) != cudaSuccess)
+        if ((e = prepare_smem(k, smem, residual_blocks_per_sm<DIM, G>())) != cudaSuccess)
           return e;
         int dev = 0, sms = 0, per_sm = 0;
         if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
