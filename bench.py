@@ -517,9 +517,10 @@ def main():
         return
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    from hpsint_b200 import replicas
+
+    w = replicas.from_env()
+    world, rank, local_rank = w.size, w.rank, w.local_rank
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -557,11 +558,8 @@ def main():
             fn()
         ev[1].record(stream)
         torch.cuda.synchronize()
-        ms = ev[0].elapsed_time(ev[1])
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        # the job's step time is the slowest rank's (replicas: no data-path collective)
+        ms = replicas.max_over_ranks(ev[0].elapsed_time(ev[1]), dist)
         return ms / steps
 
     # --- headline: FP64 Jacobian-vector product --------------------------------
