@@ -84,6 +84,49 @@ def test_newton_fp32_inner_matches_fp64():
     assert np.max(np.abs(u64 - u32)) < 1e-6
 
 
+@pytest.mark.parametrize("prec", [64, 32])
+def test_short_gmres_restart_reaches_the_same_step(prec):
+    """GMRES(3): many restart cycles per Newton step, the same converged step as GMRES(30)."""
+    u_old = two_particle_state(noise=1e-3)
+    u30, s30 = gpu_solve((40, 20), 2, u_old, 1e-2, nl_rel_tol=1e-10, nl_abs_tol=1e-16, inner_precision=prec)
+    u3, s3 = gpu_solve((40, 20), 2, u_old, 1e-2, nl_rel_tol=1e-10, nl_abs_tol=1e-16, inner_precision=prec,
+                       gmres_restart=3, l_max_iter=5000)
+    assert s30.status == 0 and s3.status == 0, (s30, s3)
+    assert s3.linear_iterations > 3 * s3.newton_iterations  # restarts happened
+    assert np.abs(u3 - u30).max() < 1e-7
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_graph_replayed_gmres_equals_a_fresh_solve(prec):
+    """After a first solve the Arnoldi iterations replay captured CUDA graphs,
+    updated when the time weights change; the result must be bitwise that of
+    a fresh context solving the same step eagerly."""
+    import hpsint_b200 as hb
+    u_old = two_particle_state(noise=1e-3)
+    data = hb.NonLinearData(nl_rel_tol=1e-10, nl_abs_tol=1e-16, inner_precision=prec)
+
+    def solve(op, dt):
+        op.set_time_weights(1.0 / dt, [-1.0 / dt], 1.0)
+        old = op.to_device(u_old)
+        u = old.clone()
+        newton = hb.DampedNewtonSolver(op, data)
+        newton.clear()  # same preconditioner-rebuild history as a fresh context
+        st = newton.solve(u, [old])
+        torch.cuda.synchronize()
+        return op.to_host(u), st
+
+    op = hb.SinteringOperatorGeneric(hb.Mesh(2, (40, 20, 1)), hb.Params(2))
+    solve(op, 1e-2)                  # eager (first solve of this context)
+    ua, sa = solve(op, 3e-3)         # graphs captured at dt = 3e-3
+    ub, sb = solve(op, 7e-3)         # graphs updated for dt = 7e-3
+    fresh_b, fsb = solve(hb.SinteringOperatorGeneric(hb.Mesh(2, (40, 20, 1)), hb.Params(2)), 7e-3)
+    uc, sc = solve(op, 3e-3)         # back to dt = 3e-3
+    assert sb.status == 0 and fsb.status == 0
+    assert (sb.newton_iterations, sb.linear_iterations) == (fsb.newton_iterations, fsb.linear_iterations)
+    assert np.array_equal(ub, fresh_b)
+    assert np.array_equal(uc, ua)
+
+
 def test_newton_3d_tensorial_converges():
     import hpsint_b200 as hb
     from hpsint_b200 import packings as P
