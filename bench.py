@@ -601,9 +601,32 @@ def main():
                 "sint_jvp_f64")
         h_dst.copy_(dst, non_blocking=True)
 
-    ms_e2e = time_loop(e2e_step, args.steps, args.warmup)
+    ms_e2e_serial = time_loop(e2e_step, args.steps, args.warmup)
     torch.cuda.synchronize()
     assert np.isfinite(h_dst[:, :op.N].numpy()).all()
+    # the same calls pipelined (copy-in / product / copy-out of consecutive steps overlap)
+    pipe = hb.HostJvpPipeline(op)
+    h_dsts = [torch.empty((op.C, op.ld), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    step_no = [0]
+
+    def e2e_pipelined():
+        pipe.submit(h_dsts[step_no[0] % 2], h_src)
+        step_no[0] += 1
+
+    for _ in range(args.warmup):
+        e2e_pipelined()
+    pipe.end(stream)
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    pipe.begin(stream)
+    for _ in range(args.steps):
+        e2e_pipelined()
+    pipe.end(stream)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = replicas.max_over_ranks(ev[0].elapsed_time(ev[1]), dist) / args.steps
+    assert torch.equal(h_dsts[0], h_dst)  # same product, bitwise
 
     # --- measured FMA throughput: denominator of the ALU roofline ---------------
     fma = {}
@@ -676,7 +699,10 @@ def main():
                          "frac": (flops / (ms_jvp64 * 1e-3) / 1e12 / fma[64]) if flops else None,
                          "flops_source": "executed FP64 add/mul/fma (fma = 2) of one ncu capture" if flops else None},
         "e2e": {"value": gdofs(ms_e2e) * world, "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                "d2h_bytes_per_step": nbytes},
+                "d2h_bytes_per_step": nbytes,
+                "note": "sint_jvp_f64 on pinned host vectors, copy-in / product / copy-out of consecutive "
+                        "steps overlapped on three streams (operator.HostJvpPipeline)",
+                "serial_value": gdofs(ms_e2e_serial) * world},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }

@@ -300,3 +300,75 @@ class DampedNewtonSolver:
 
     def clear(self):
         L.check(L.lib().sint_newton_clear(self.op._h), "sint_newton_clear")
+
+
+class HostJvpPipeline:
+    """J(u) v for vectors that live in (pinned) host memory, pipelined.
+
+    A caller whose vectors stay on the host (a CPU driver handing one vector
+    at a time to the GPU operator) pays a host-to-device copy, the product
+    and a device-to-host copy per call.  Here consecutive calls overlap: the
+    copy-in of call k + 1, the product of call k and the copy-out of call
+    k - 1 run on three streams with double-buffered device vectors, so the
+    throughput is set by the slowest of the three instead of their sum.
+    `submit` returns at once; `synchronize` waits for every submitted call.
+    Host buffers must be pinned (torch pin_memory) and stay untouched until
+    their call is synchronised.
+    """
+
+    def __init__(self, op: SinteringOperatorGeneric, depth=2):
+        if depth < 1:
+            raise ValueError("depth must be >= 1")
+        self.op = op
+        self.depth = depth
+        self.src = [op.initialize_dof_vector() for _ in range(depth)]
+        self.dst = [op.initialize_dof_vector() for _ in range(depth)]
+        self.s_in, self.s_jv, self.s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+        self.copied_in = [torch.cuda.Event() for _ in range(depth)]
+        self.computed = [torch.cuda.Event() for _ in range(depth)]
+        self.copied_out = [torch.cuda.Event() for _ in range(depth)]
+        self.k = 0
+        self.launched = [False] * depth
+        self.begin()
+
+    def submit(self, dst_host, src_host):
+        """Queue dst_host = J src_host (both pinned (C, block_stride) float64 CPU tensors)."""
+        i = self.k % self.depth
+        op = self.op
+        with torch.cuda.stream(self.s_in):
+            if self.launched[i]:
+                self.s_in.wait_event(self.computed[i])      # the product has read src[i]
+            self.src[i].copy_(src_host, non_blocking=True)
+            self.copied_in[i].record(self.s_in)
+        with torch.cuda.stream(self.s_jv):
+            self.s_jv.wait_event(self.copied_in[i])
+            if self.launched[i]:
+                self.s_jv.wait_event(self.copied_out[i])    # dst[i] was copied out
+            L.check(L.lib().sint_jvp_f64(op._h, _ptr(self.dst[i]), _ptr(self.src[i]),
+                                         ctypes.c_void_p(self.s_jv.cuda_stream)), "sint_jvp_f64")
+            self.computed[i].record(self.s_jv)
+        with torch.cuda.stream(self.s_out):
+            self.s_out.wait_event(self.computed[i])
+            dst_host.copy_(self.dst[i], non_blocking=True)
+            self.copied_out[i].record(self.s_out)
+        self.launched[i] = True
+        self.k += 1
+
+    def begin(self, stream=None):
+        """Order the pipeline after everything queued so far on `stream` (default: current)."""
+        ev = torch.cuda.Event()
+        ev.record(stream or torch.cuda.current_stream())
+        for s in (self.s_in, self.s_jv, self.s_out):
+            s.wait_event(ev)
+
+    def end(self, stream=None):
+        """Make `stream` (default: current) wait for every submitted call."""
+        stream = stream or torch.cuda.current_stream()
+        for s in (self.s_in, self.s_jv, self.s_out):
+            ev = torch.cuda.Event()
+            ev.record(s)
+            stream.wait_event(ev)
+
+    def synchronize(self):
+        for s in (self.s_in, self.s_jv, self.s_out):
+            s.synchronize()
