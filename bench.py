@@ -64,6 +64,7 @@ def parse_args():
     ap.add_argument("--train-seeds", type=int, default=10)
     ap.add_argument("--train-steps", type=int, default=200, help="FP64 steps per training trajectory")
     ap.add_argument("--train-iters", type=int, default=4000)
+    ap.add_argument("--smooth", type=float, default=4.0, help="learned2d: weight of the Laplacian error term")
     ap.add_argument("--eval-seeds", type=int, default=2)
     ap.add_argument("--eval-steps", type=int, default=100)
     ap.add_argument("--cells", type=int, default=512)
@@ -459,7 +460,7 @@ def learned_guess_solve(args):
     held = list(range(1000, 1000 + args.eval_seeds))
     net, norm, trainer, info = LG.train_learned_guess(
         train, n=args.cells, n_circles=args.circles, n_steps=args.train_steps, net_cfg=NetConfig(),
-        train_cfg=LG.TrainConfig(iterations=args.train_iters), verbose=False)
+        train_cfg=LG.TrainConfig(iterations=args.train_iters, smooth=args.smooth), verbose=False)
     if args.save_net:
         LG.save_predictor(args.save_net, net, norm)
     evals = []

@@ -103,6 +103,8 @@ SIGNATURES = {
     "sint_nn_conv3x3_tc_ex_f32": (_c_int, [_c_void, _c_int, _c_int, _c_int, _c_int, _c_void, _c_void, _c_void,
                                            _c_int, _c_int, _c_void, _c_int, _c_int, ctypes.c_float, _c_void,
                                            _c_void]),
+    "sint_nn_weighted_diff_f32": (_c_int, [_c_int64, _c_void, _c_void, _c_void, _c_void, _c_void]),
+    "sint_nn_mul_add_f32": (_c_int, [_c_int64, ctypes.c_float, _c_void, _c_void, _c_void, _c_void]),
     "sint_nn_increment_scales_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float,
                                               ctypes.c_float, _c_void, _c_void, _c_void, _c_void, _c_void]),
     "sint_nn_apply_guess_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,

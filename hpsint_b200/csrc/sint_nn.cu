@@ -227,6 +227,22 @@ namespace sint
   // Mean squared error over n elements, weights w (nullable): loss = sum w d^2 / n,
   // grad = 2 w d / n; block partial sums in double, summed by the host-side
   // second launch.
+  // out = w (p - t)   (w may be NULL = 1)
+  __global__ void weighted_diff_kernel(long long n, const float *__restrict__ p, const float *__restrict__ t,
+                                       const float *__restrict__ w, float *__restrict__ out)
+  {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      out[i] = (w ? w[i] : 1.f) * (p[i] - t[i]);
+  }
+
+  // y += alpha a x   (a may be NULL = 1)
+  __global__ void mul_add_kernel(long long n, float alpha, const float *__restrict__ a, const float *__restrict__ x,
+                                 float *__restrict__ y)
+  {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      y[i] += alpha * (a ? a[i] : 1.f) * x[i];
+  }
+
   __global__ void mse_kernel(long long n, const float *__restrict__ pred, const float *__restrict__ target,
                              const float *__restrict__ wt, float *__restrict__ grad, double *__restrict__ partial)
   {
@@ -502,6 +518,33 @@ int sint_nn_adam_f32(int64_t n, float *p, const float *g, float *m, float *v, fl
   const float c1 = 1.f - powf(beta1, float(step)), c2 = 1.f - powf(beta2, float(step));
   adam_kernel<<<1184, 256, 0, s>>>(n, p, g, m, v, lr, beta1, beta2, eps, c1, c2);
   return launch_err("sint_nn_adam_f32");
+}
+
+int sint_nn_weighted_diff_f32(int64_t n, const float *pred, const float *target, const float *weight, float *out,
+                              sint_stream_t s)
+{
+  if (!pred || !target || !out || n < 0)
+    {
+      set_error("sint_nn_weighted_diff_f32: bad argument");
+      return SINT_ERR_ARG;
+    }
+  if (n == 0)
+    return SINT_OK;
+  weighted_diff_kernel<<<1184, 256, 0, s>>>(n, pred, target, weight, out);
+  return launch_err("sint_nn_weighted_diff_f32");
+}
+
+int sint_nn_mul_add_f32(int64_t n, float alpha, const float *a, const float *x, float *y, sint_stream_t s)
+{
+  if (!x || !y || n < 0)
+    {
+      set_error("sint_nn_mul_add_f32: bad argument");
+      return SINT_ERR_ARG;
+    }
+  if (n == 0)
+    return SINT_OK;
+  mul_add_kernel<<<1184, 256, 0, s>>>(n, alpha, a, x, y);
+  return launch_err("sint_nn_mul_add_f32");
 }
 
 int64_t sint_nn_mse_workspace(void) { return 1184 + 1; }

@@ -196,6 +196,10 @@ class TrainConfig:
     lr_final: float = 1e-5    # cosine decay from lr to lr_final over the iterations (lr_final = lr: constant)
     seed: int = 0
     log_every: int = 100
+    # weight of the curvature term: mean of (5-point Laplacian of the masked
+    # error)^2, which penalises the high-frequency error the fourth-order
+    # Cahn-Hilliard operator amplifies in the Newton residual (0: plain MSE)
+    smooth: float = 4.0
 
 
 class WindowSampler:
@@ -298,6 +302,27 @@ class Trainer:
         c = self.cfg
         return c.lr_final + 0.5 * (c.lr - c.lr_final) * (1.0 + math.cos(math.pi * min(it, n) / max(n, 1)))
 
+    def _smooth_term(self, pred, target, weight, grad):
+        """lambda mean((Delta (w (pred - target)))^2); adds lambda 2/n w Delta(Delta(w e)) to grad
+        (grad may be None).  Delta: 5-point Laplacian with zero padding (a symmetric stencil, so
+        its transpose is itself), applied per channel by the FP32 conv kernel."""
+        from . import predictor as P
+        lam = self.cfg.smooth
+        H, W = pred.shape[-2], pred.shape[-1]
+        e = torch.empty_like(pred)
+        L.check(L.lib().sint_nn_weighted_diff_f32(pred.numel(), _p(pred), _p(target), _p(weight), _p(e), _s()),
+                "sint_nn_weighted_diff_f32")
+        lap = torch.empty_like(pred)
+        P.conv3x3(e.view(-1, 1, H, W), self._lap, None, lap.view(-1, 1, H, W))
+        g_l = torch.empty_like(pred) if grad is not None else None
+        loss = self.net.mse(lap, torch.zeros_like(lap), None, g_l)
+        if grad is not None:
+            q = torch.empty_like(pred)
+            P.conv3x3(g_l.view(-1, 1, H, W), self._lap, None, q.view(-1, 1, H, W))
+            L.check(L.lib().sint_nn_mul_add_f32(pred.numel(), lam, _p(weight), _p(q), _p(grad), _s()),
+                    "sint_nn_mul_add_f32")
+        return loss * lam
+
     def step(self, lr=None):
         """One Adam step; returns (batch loss, loss of predicting zero = linear
         extrapolation) as device scalars (no sync)."""
@@ -308,6 +333,13 @@ class Trainer:
         ls = self.net.mse(ys, b["ts"], b["ws"], b["dys"])
         zg, zs = torch.zeros_like(b["tg"]), torch.zeros_like(b["ts"])
         base = self.net.mse(zg, b["tg"], b["wg"], None) + self.net.mse(zs, b["ts"], b["ws"], None)
+        if self.cfg.smooth > 0:
+            if not hasattr(self, "_lap"):
+                self._lap = torch.tensor([[0.0, 1.0, 0.0], [1.0, -4.0, 1.0], [0.0, 1.0, 0.0]], dtype=torch.float32,
+                                         device="cuda").view(1, 1, 3, 3)
+            lg = lg + self._smooth_term(yg, b["tg"], b["wg"], b["dyg"])
+            ls = ls + self._smooth_term(ys, b["ts"], b["ws"], b["dys"])
+            base = base + self._smooth_term(zg, b["tg"], b["wg"], None) + self._smooth_term(zs, b["ts"], b["ws"], None)
         self.net.zero_grad()
         self.net.backward(cache, b["dyg"], b["dys"], B, G)
         self.net.adam_step(lr=self.cfg.lr if lr is None else lr)

@@ -296,6 +296,11 @@ int sint_nn_grain_bcast_add_f32(const float *Q, int B, int G, int64_t chw, float
 /* Adam (Kingma & Ba 2015) with bias correction at step >= 1 */
 int sint_nn_adam_f32(int64_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1,
                      float beta2, float eps, int step, sint_stream_t stream);
+/* out = w (pred - target) elementwise (weight may be NULL = 1) */
+int sint_nn_weighted_diff_f32(int64_t n, const float *pred, const float *target, const float *weight, float *out,
+                              sint_stream_t stream);
+/* y += alpha a x elementwise (a may be NULL = 1) */
+int sint_nn_mul_add_f32(int64_t n, float alpha, const float *a, const float *x, float *y, sint_stream_t stream);
 /* doubles of workspace sint_nn_mse_f32 needs */
 int64_t sint_nn_mse_workspace(void);
 /* loss[0] = sum w (pred - target)^2 / n (weight may be NULL = 1); grad (may be

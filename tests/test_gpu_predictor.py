@@ -141,3 +141,26 @@ def test_tensor_core_conv_fused_epilogue():
     P.conv3x3_tc_ex(dev(x), dev(w), dev(b), out, status, accumulate=True, addend=dev(q), addend_group=grp, slope=0.1)
     assert int(status.item()) == 0
     assert rel(out.cpu().numpy(), ref.cpu().numpy()) < 3e-3
+
+
+def test_curvature_loss_term_and_gradient_match_autograd():
+    """lambda mean((Laplacian(w (p - t)))^2) and its gradient in p, against torch autograd."""
+    import types
+    from hpsint_b200 import learned_guess as LG
+    from hpsint_b200 import predictor as P
+    rng = np.random.default_rng(11)
+    shape = (3, 2, 13, 17)
+    p, t, w = dev(rng.normal(size=shape)), dev(rng.normal(size=shape)), dev(rng.uniform(0, 1, shape))
+    grad = dev(rng.normal(size=shape))
+    g0 = grad.clone()
+    lam = 0.7
+    me = types.SimpleNamespace(cfg=types.SimpleNamespace(smooth=lam), net=P.EquivariantNet(P.NetConfig(width=4, layers=2)),
+                               _lap=torch.tensor([[0.0, 1, 0], [1, -4, 1], [0, 1, 0]], device="cuda").view(1, 1, 3, 3))
+    loss = LG.Trainer._smooth_term(me, p, t, w, grad)
+    pp = p.double().requires_grad_(True)
+    e = (w.double() * (pp - t.double())).view(-1, 1, 13, 17)
+    lap = torch.nn.functional.conv2d(e, me._lap.double(), padding=1)
+    ref = lam * (lap ** 2).mean()
+    ref.backward()
+    assert abs(float(loss.item()) - float(ref.item())) <= 1e-5 * float(ref.item())
+    assert rel((grad - g0).cpu().numpy(), pp.grad.cpu().numpy()) < 1e-5
