@@ -71,6 +71,8 @@ def parse_args():
     ap.add_argument("--circles", type=int, default=100)
     ap.add_argument("--save-net", default=None, help="write the trained predictor (.npz) here")
     ap.add_argument("--solve-steps", type=int, default=100)
+    ap.add_argument("--cut-off", type=float, default=0.0,
+                    help="solve3d: also run both solves with this GrainCutOffTolerance and time the cut-off J v")
     return ap.parse_args()
 
 
@@ -377,7 +379,10 @@ def mixed_precision_solve_3d(args):
     dt0 = 1e-4 and hpsint's dt control, Newton relative tolerance 1e-8.  The
     FP64-inner solve fixes the time grid; the FP32-inner solve (FP32 GMRES(30)
     vectors, Jacobian and block-Jacobi inside FP64 Newton) replays it.  Reports
-    s/step of both and the FP32-inner run's errors against the FP64-inner run."""
+    s/step of both and the FP32-inner run's errors against the FP64-inner run.
+    With --cut-off TOL both solves run again on the same grid with the grain
+    cut-off (GrainCutOffTolerance = TOL), and the J v throughput at the initial
+    state is timed with and without it."""
     import torch
 
     import hpsint_b200 as hb
@@ -396,10 +401,15 @@ def mixed_precision_solve_3d(args):
     u0d = op.to_device(u0)
     c0 = float(np.einsum("k,j,i,kji->", w, w, w, u0[0].reshape(n + 1, n + 1, n + 1)))
     del u0
+    operator_rates = cut_off_operator_rates(op, u0d, args.cut_off) if args.cut_off > 0 else None
+    arms = [("fp64_inner", 64, 0.0), ("fp32_inner", 32, 0.0)]
+    if args.cut_off > 0:
+        arms += [("fp64_inner_cut_off", 64, args.cut_off), ("fp32_inner_cut_off", 32, args.cut_off)]
     runs, schedule = {}, None
-    for label, prec in (("fp64_inner", 64), ("fp32_inner", 32)):
+    for label, prec, tol in arms:
+        op.set_component_mask(u0d, tol)  # 0 switches a previous arm's cut-off off
         ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec),
-                            TimeIntegrationData(time_step_init=1e-4))
+                            TimeIntegrationData(time_step_init=1e-4), grain_cut_off_tolerance=tol)
         ti.initialize(u0d)
         ti.run(2, dt_schedule=[1e-4, 1e-4])  # warm-up: workspaces, first launches (discarded)
         ti.initialize(u0d)
@@ -413,7 +423,7 @@ def mixed_precision_solve_3d(args):
         u = op.to_host(ti.history[0])
         c_int = float(np.einsum("k,j,i,kji->", w, w, w, u[0].reshape(n + 1, n + 1, n + 1)))
         recs = ti.records
-        runs[label] = dict(u=u, wall=wall, recs=recs, c_int=c_int)
+        runs[label] = dict(u=u, wall=wall, recs=recs, c_int=c_int, stats=list(ti.cut_off_statistics))
         del ti
     ref, mp = runs["fp64_inner"], runs["fp32_inner"]
     line = {"metric": METRIC, "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-median{args.median:g}-G{G}",
@@ -437,7 +447,56 @@ def mixed_precision_solve_3d(args):
         "speedup_accepted_attempts": sum(x.accepted_wall_s for x in ref["recs"]) /
                                      sum(x.accepted_wall_s for x in mp["recs"]),
     }
+    if args.cut_off > 0:
+        line["cut_off"] = {"tolerance": args.cut_off, "operator_at_initial_state": operator_rates}
+        for label in ("fp64_inner_cut_off", "fp32_inner_cut_off"):
+            r = runs[label]
+            st = np.sum(r["stats"], axis=0)
+            line["cut_off"][label] = {
+                "mean_relevant_grains_per_cell": float((np.arange(len(st)) * st).sum() / st.sum()),
+                "max_abs_diff_c_vs_fp64_inner": float(np.abs(r["u"][0] - ref["u"][0]).max()),
+                "max_abs_diff_eta_vs_fp64_inner": float(np.abs(r["u"][2:] - ref["u"][2:]).max()),
+                "speedup_s_per_step_vs_fp64_inner": (ref["wall"] / len(ref["recs"])) / (r["wall"] / len(r["recs"]))}
     print(json.dumps(line), flush=True)
+
+
+def cut_off_operator_rates(op, u, tol, reps=20):
+    """GDoF/s of the FP64/FP32 Jacobian-vector products and the residual at
+    state u, without and with the grain cut-off at tolerance tol (CUDA events
+    on the current stream, 3 warm-up calls)."""
+    import torch
+
+    op.set_time_weights(1e4, [-1e4], 1.0)
+    op.fill_quadrature_point_values(u)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    out = {}
+    stream = torch.cuda.current_stream()
+    for t in (0.0, tol):
+        op.set_component_mask(u, t)
+        for name, dt in (("jvp_f64", torch.float64), ("jvp_f32", torch.float32), ("residual_f64", None)):
+            if dt is None:
+                dst = op.initialize_dof_vector()
+                fn = lambda: op.evaluate_nonlinear_residual(dst, u, 2, [u])  # noqa: E731
+            else:
+                src = torch.rand((op.C, op.ld), dtype=dt, device="cuda", generator=gen) - 0.5
+                dst = op.initialize_dof_vector(dt)
+                fn = lambda: op.vmult(dst, src)  # noqa: E731
+            for _ in range(3):
+                fn()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(stream)
+            for _ in range(reps):
+                fn()
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            ms = ev[0].elapsed_time(ev[1]) / reps
+            out[f"{name}{'_cut_off' if t > 0 else ''}_gdofs"] = op.C * op.N / (ms * 1e-3) / 1e9
+        if t > 0:
+            st = op.component_mask_statistics()
+            out["mean_relevant_grains_per_cell"] = float((np.arange(len(st)) * st).sum() / st.sum())
+            out["cells_per_relevant_grain_count"] = st.tolist()
+    op.set_component_mask(u, 0.0)
+    return out
 
 
 def learned_guess_solve(args):

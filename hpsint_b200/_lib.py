@@ -65,6 +65,9 @@ SIGNATURES = {
     "sint_precond_apply_f32": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_ac_inverse_diagonal_f64": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_ch_blocks_f64": (_c_int, [_c_void, _c_void, _c_void]),
+    "sint_set_component_mask": (_c_int, [_c_void, _c_void, _c_double, _c_void]),
+    "sint_component_mask_statistics": (_c_int, [_c_void, P(_c_int64), _c_void]),
+    "sint_get_component_mask": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_vec_axpy_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_sadd_f64": (_c_int, [_c_int64, _c_double, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_scale_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void]),

@@ -55,11 +55,11 @@ namespace sint
     const bool t = c->params.tensorial != 0;
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_jvp<3, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, s)
-            : launch_jvp<3, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, s);
+      e = t ? launch_jvp<3, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s)
+            : launch_jvp<3, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s);
     else
-      e = t ? launch_jvp<2, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, s)
-            : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, s);
+      e = t ? launch_jvp<2, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s)
+            : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s);
     if (e != cudaSuccess)
       return e;
     return c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, s)
@@ -75,11 +75,11 @@ namespace sint
     const bool t = c->params.tensorial != 0;
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, s)
-            : launch_residual<3, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, s);
+      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s)
+            : launch_residual<3, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s);
     else
-      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, s)
-            : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, s);
+      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s)
+            : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s);
     if (e != cudaSuccess)
       return e;
     return c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, s)
@@ -91,11 +91,11 @@ namespace sint
     const bool t = c->params.tensorial != 0;
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_diag<3, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, s)
-            : launch_diag<3, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, s);
+      e = t ? launch_diag<3, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s)
+            : launch_diag<3, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s);
     else
-      e = t ? launch_diag<2, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, s)
-            : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, s);
+      e = t ? launch_diag<2, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s)
+            : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s);
     if (e != cudaSuccess)
       return e;
     return c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, s)
@@ -361,6 +361,7 @@ int sint_destroy(sint_ctx *c)
   cudaFree(c->lin64);
   cudaFree(c->lin32);
   cudaFree(c->partial);
+  cudaFree(c->mask);
   cudaFree(c->pc_raw);
   cudaFree(c->pc_inv64);
   cudaFree(c->pc_inv32);

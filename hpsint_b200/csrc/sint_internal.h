@@ -37,6 +37,14 @@ namespace sint
     double *partial       = nullptr; // tile-face partial sums of the cell kernels
     size_t  partial_bytes = 0;
 
+    // grain cut-off (SinteringOperatorData::set_component_mask,
+    // operator_sintering_data.h:149-298): bit i of mask[cell] set when grain
+    // i is relevant on the cell; the kernels use it while `cut` is set
+    uint16_t *mask    = nullptr;
+    long long n_cells = 0;
+    bool      cut     = false;
+    double    cut_tol = 0.0;
+
     double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
     double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
     float  *pc_inv32 = nullptr;
@@ -88,6 +96,8 @@ namespace sint
 
   // Validates and fills the operator description of c (no allocation).
   int describe_operator(const sint_mesh *mesh, const sint_params *params, Ctx *c);
+  // Cell masks the kernels use: c->mask with the cut-off on, else nullptr.
+  inline const uint16_t *active_mask(const Ctx *c) { return c->cut ? c->mask : nullptr; }
   // J v through the cell kernel + combine, with c->partial as scratch.
   template <typename R>
   cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s);

@@ -64,6 +64,14 @@ namespace sint
     __host__ __device__ static constexpr int src_eta(int i) { return 4 + G + i; }
     static constexpr int h_c = 2 + G;
     __host__ __device__ static constexpr int h_eta(int i) { return 3 + G + i; }
+    // grain of a phase-1 item (-1 for c and mu items)
+    __host__ __device__ static constexpr int grain(int it)
+    {
+      return (it >= lin_eta(0) && it < lin_eta(0) + G) ? it - lin_eta(0)
+             : (JVP && it >= src_eta(0)) ? it - src_eta(0)
+             : (!JVP && HIST && it >= h_eta(0)) ? it - h_eta(0)
+                                               : -1;
+    }
 
     // phase 1 item -> (buffer 0 = lin / state, 1 = src / history; component; value+gradient?)
     __device__ static void source(int it, int &buf, int &comp)
@@ -106,21 +114,44 @@ namespace sint
     }
   };
 
-  // Phase 1: evaluate all items of the tile.
-  template <int DIM, int G, bool TENS, bool JVP, bool HIST, typename R>
-  __device__ __forceinline__ void phase_evaluate(const R *box0, const R *box1, R *F, const CellConsts<DIM, R> &k)
+  // Phase 1: evaluate all items of the tile.  With the grain cut-off (CUT),
+  // the items of a grain absent on this thread's cell (bit clear in m) are
+  // zero; a warp that has no lane needing an item writes the zeros without
+  // evaluating.
+  template <int DIM, int G, bool TENS, bool JVP, bool HIST, typename R, bool CUT = false>
+  __device__ __forceinline__ void phase_evaluate(const R *box0, const R *box1, R *F, const CellConsts<DIM, R> &k,
+                                                 unsigned m = ~0u)
   {
     using T            = Tile<DIM>;
+    using SL           = Slots<DIM>;
     using FM           = FieldMap<DIM, G, TENS, JVP, HIST>;
     constexpr int NGRP = T::THREADS / T::CELLS;
     const int     cell = threadIdx.x % T::CELLS;
     const int     b0   = cell_box_base<DIM>(cell);
     for (int it = threadIdx.x / T::CELLS; it < FM::NITEMS; it += NGRP)
       {
+        bool absent = false;
+        if constexpr (CUT)
+          {
+            const int gr = FM::grain(it);
+            absent       = gr >= 0 && ((m >> gr) & 1u) == 0u;
+            if (!__any_sync(0xffffffffu, !absent))
+              {
+                const int ns = it < FM::NVG ? SL::VG : SL::V;
+                for (int sl = 0; sl < ns; ++sl)
+                  F[(FM::base(it) + sl) * T::CELLS + cell] = R(0);
+                continue;
+              }
+          }
         int buf = 0, comp = 0;
         FM::source(it, buf, comp);
         R u[1 << DIM];
         cell_nodes<DIM>((buf == 0 ? box0 : box1) + comp * T::BOX, b0, u);
+        if constexpr (CUT)
+          if (absent)
+#pragma unroll
+            for (int l = 0; l < (1 << DIM); ++l)
+              u[l] = R(0);
         if (it < FM::NVG)
           cell_eval_vg<DIM>(u, k, F, FM::base(it), cell);
         else
@@ -153,7 +184,7 @@ namespace sint
   // Phase 2 of the Jacobian product at point q of cell `cell`
   // (SinteringOperatorGenericQuad::operator(), generic.h:101-190).
   template <int DIM, int G, bool TENS, typename R>
-  __device__ __forceinline__ void jvp_point(const PhysR<R> &p, const R *F, R *P, int q, int cell)
+  __device__ __forceinline__ void jvp_point(const PhysR<R> &p, const R *F, R *P, int q, int cell, unsigned m = ~0u)
   {
     using FM = FieldMap<DIM, G, TENS, true, false>;
     R c, gc[DIM], gmu[DIM];
@@ -193,7 +224,7 @@ namespace sint
     // 1) c row (generic.h:120-134)
     {
       R gres[DIM];
-      apply_M_derivative<DIM, G, TENS>(p, c, gc, gmu, eta, geta, dc, gdc, gdmu, deta, gres);
+      apply_M_derivative<DIM, G, TENS>(p, c, gc, gmu, eta, geta, dc, gdc, gdmu, deta, gres, m);
       pstore<DIM>(P, 0, q, cell, dc * p.w0);
 #pragma unroll
       for (int d = 0; d < DIM; ++d)
@@ -231,7 +262,8 @@ namespace sint
   // Phase 2 of the residual at point q of cell `cell`
   // (SinteringOperatorGenericResidualQuad::operator(), generic.h:254-308).
   template <int DIM, int G, bool TENS, int WTD, typename R>
-  __device__ __forceinline__ void residual_point(const PhysR<R> &p, const R *F, R *P, int q, int cell)
+  __device__ __forceinline__ void residual_point(const PhysR<R> &p, const R *F, R *P, int q, int cell,
+                                                 unsigned m = ~0u)
   {
     using FM = FieldMap<DIM, G, TENS, false, WTD == 2>;
     R c, gc[DIM], mu, gmu[DIM];
@@ -265,7 +297,7 @@ namespace sint
       if constexpr (WTD == 2)
         v += fval<DIM>(F, FM::base(FM::h_c), q, cell);
       R gres[DIM];
-      apply_M<DIM, G, TENS>(p, c, eta, gc, geta, gmu, gres);
+      apply_M<DIM, G, TENS>(p, c, eta, gc, geta, gmu, gres, m);
       pstore<DIM>(P, 0, q, cell, v);
 #pragma unroll
       for (int d = 0; d < DIM; ++d)
@@ -295,9 +327,14 @@ namespace sint
   // contributions of cells outside the mesh (partial tiles) are zero.  `stiff`
   // holds the nodal values the constant-coefficient gradient terms act on
   // (component 0 = c for the mu row, component 2 + i = eta_i for the eta rows).
-  template <int DIM, int G, typename R>
+  // With the grain cut-off (CUT) the row of a grain absent on the cell is zero
+  // (do_vmult_range_no_template / do_evaluate_nonlinear_residual_nt,
+  // operator_sintering_generic.h:456-537, :1008-1081, assemble the relevant
+  // grains' rows only).
+  template <int DIM, int G, typename R, bool CUT = false>
   __device__ __forceinline__ void phase_integrate(const PhysR<R> &p, const Grid &g, const CellConsts<DIM, R> &k,
-                                                  const TileCoord &tc, const R *P, const R *stiff, R *K)
+                                                  const TileCoord &tc, const R *P, const R *stiff, R *K,
+                                                  unsigned m = ~0u)
   {
     using T            = Tile<DIM>;
     constexpr int NQ   = 1 << DIM;
@@ -308,6 +345,19 @@ namespace sint
     const bool    in   = cell_in_mesh<DIM>(cell, tc, g);
     for (int row = threadIdx.x / T::CELLS; row < C; row += NGRP)
       {
+        bool keep = in;
+        if constexpr (CUT)
+          if (row >= 2)
+            {
+              keep = keep && ((m >> (row - 2)) & 1u) != 0u;
+              if (!__any_sync(0xffffffffu, keep))
+                {
+#pragma unroll
+                  for (int l = 0; l < NQ; ++l)
+                    K[(row * NQ + l) * T::CP + cell] = R(0);
+                  continue;
+                }
+            }
         R r[NQ];
         if (row == 0)
           {
@@ -336,8 +386,23 @@ namespace sint
           }
 #pragma unroll
         for (int l = 0; l < NQ; ++l)
-          K[(row * NQ + l) * T::CP + cell] = in ? r[l] : R(0);
+          K[(row * NQ + l) * T::CP + cell] = keep ? r[l] : R(0);
       }
+  }
+
+  // Grain-cut-off mask of local cell `cell` of tile tc (one bit per grain,
+  // n[0] x n[1] x n[2] cells in lexicographic order); cells outside the mesh
+  // have no relevant grain.
+  template <int DIM>
+  __device__ __forceinline__ unsigned cell_mask(const uint16_t *__restrict__ mask, const Grid &g,
+                                                const TileCoord &tc, int cell)
+  {
+    using T      = Tile<DIM>;
+    const int cx = cell % T::TX, cy = (cell / T::TX) % T::TY, cz = cell / (T::TX * T::TY);
+    const int i = tc.o[0] + cx, j = tc.o[1] + cy, k = DIM == 3 ? tc.o[2] + cz : 0;
+    if (i >= g.n[0] || j >= g.n[1] || (DIM == 3 && k >= g.n[2]))
+      return 0u;
+    return mask[i + (long long)g.n[0] * (j + (long long)g.n[1] * k)];
   }
 
   template <int DIM, int G, bool TENS, bool JVP, bool HIST>
@@ -378,10 +443,11 @@ namespace sint
     return (DIM == 3 && G > 5) ? 1 : 2;
   }
 
-  template <int DIM, int G, bool TENS, typename R>
+  // CUT: grain cut-off with the per-cell masks `mask` (unused otherwise).
+  template <int DIM, int G, bool TENS, typename R, bool CUT>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS, jvp_blocks_per_sm<DIM, G, R>())
     jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
-               R *__restrict__ dst, R *__restrict__ partial)
+               R *__restrict__ dst, R *__restrict__ partial, const uint16_t *__restrict__ mask)
   {
     using T  = Tile<DIM>;
     using SM = ThreePhaseSmem<DIM, G, TENS, true, false>;
@@ -395,11 +461,15 @@ namespace sint
     const PhysR<R>           p(ph);
     const CellConsts<DIM, R> k(g);
     long long                tile = blockIdx.x;
+    unsigned                 m_cur = ~0u, m_next = ~0u; // this and the next tile's cell masks
     if (tile < g.n_tiles)
       {
-        const BoxNode<DIM> bn(g, tile_coord_of<DIM>(g, tile));
+        const TileCoord    tc0 = tile_coord_of<DIM>(g, tile);
+        const BoxNode<DIM> bn(g, tc0);
         load_box_async<DIM>(s_buf, lin, C, g, bn);
         load_box_async<DIM>(s_buf + C * T::BOX, src, C, g, bn);
+        if constexpr (CUT)
+          m_cur = cell_mask<DIM>(mask, g, tc0, threadIdx.x % T::CELLS);
       }
     cp_async_commit();
     for (int it = 0; tile < g.n_tiles; ++it, tile += gridDim.x)
@@ -408,21 +478,25 @@ namespace sint
         R              *nb   = s_buf + ((it + 1) & 1) * SM::BOXES;
         if (next < g.n_tiles)
           {
-            const BoxNode<DIM> bnn(g, tile_coord_of<DIM>(g, next));
+            const TileCoord    tcn = tile_coord_of<DIM>(g, next);
+            const BoxNode<DIM> bnn(g, tcn);
             load_box_async<DIM>(nb, lin, C, g, bnn);
             load_box_async<DIM>(nb + C * T::BOX, src, C, g, bnn);
+            if constexpr (CUT)
+              m_next = cell_mask<DIM>(mask, g, tcn, threadIdx.x % T::CELLS);
           }
         cp_async_commit();
         cp_async_wait<1>(); // this tile's group has landed (only the prefetch may be pending)
         __syncthreads();
         const TileCoord tc = tile_coord_of<DIM>(g, tile);
         const R        *cb = s_buf + (it & 1) * SM::BOXES;
-        phase_evaluate<DIM, G, TENS, true, false, R>(cb, cb + C * T::BOX, F, k);
+        phase_evaluate<DIM, G, TENS, true, false, R, CUT>(cb, cb + C * T::BOX, F, k, m_cur);
         __syncthreads();
-        jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS);
+        jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS, m_cur);
         __syncthreads();
-        phase_integrate<DIM, G, R>(p, g, k, tc, P, cb + C * T::BOX, K);
+        phase_integrate<DIM, G, R, CUT>(p, g, k, tc, P, cb + C * T::BOX, K, m_cur);
         __syncthreads();
+        m_cur = m_next;
         sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial);
         __syncthreads(); // K and this buffer are reused by the next iterations
       }
@@ -434,11 +508,11 @@ namespace sint
   // (operator_sintering_generic.h:254-308) with the history of
   // do_evalute_history (:927-975) for WTD == 2: the weighted sum of the old
   // solutions is formed at the nodes while staging and evaluated at the points.
-  template <int DIM, int G, bool TENS, int WTD>
+  template <int DIM, int G, bool TENS, int WTD, bool CUT>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS, residual_blocks_per_sm<DIM, G>())
     residual_kernel(const Grid g, const Phys ph, const double *__restrict__ src, const double *__restrict__ h0,
                     const double *__restrict__ h1, const double *__restrict__ h2, double *__restrict__ dst,
-                    double *__restrict__ partial)
+                    double *__restrict__ partial, const uint16_t *__restrict__ mask)
   {
     using R  = double;
     using T  = Tile<DIM>;
@@ -457,6 +531,7 @@ namespace sint
       {
         const TileCoord    tc = tile_coord_of<DIM>(g, tile);
         const BoxNode<DIM> bn(g, tc);
+        const unsigned     m  = CUT ? cell_mask<DIM>(mask, g, tc, threadIdx.x % T::CELLS) : ~0u;
         load_box<DIM>(s_u, src, C, g, bn);
         if constexpr (WTD == 2)
           {
@@ -478,11 +553,11 @@ namespace sint
                 }
           }
         __syncthreads();
-        phase_evaluate<DIM, G, TENS, false, WTD == 2, R>(s_u, s_h, F, k);
+        phase_evaluate<DIM, G, TENS, false, WTD == 2, R, CUT>(s_u, s_h, F, k, m);
         __syncthreads();
-        residual_point<DIM, G, TENS, WTD, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS);
+        residual_point<DIM, G, TENS, WTD, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS, m);
         __syncthreads();
-        phase_integrate<DIM, G, R>(p, g, k, tc, P, s_u, K);
+        phase_integrate<DIM, G, R, CUT>(p, g, k, tc, P, s_u, K, m);
         __syncthreads();
         sum_and_store<DIM>(K, C, g, tc, bn, dst, partial);
         __syncthreads();
@@ -505,10 +580,12 @@ namespace sint
     static constexpr int NCOEF = DIM * DIM + DIM + DIM * DIM + 1 + G;
   };
 
-  template <int DIM, int G, bool TENS>
+  // CUT: the grains absent on a cell (mask bit clear) have zero values there
+  // and no Allen-Cahn diagonal contribution from it (preconditioners.h:787-817).
+  template <int DIM, int G, bool TENS, bool CUT>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS)
     diag_kernel(const Grid g, const Phys ph, const double *__restrict__ lin, double *__restrict__ dst,
-                double *__restrict__ partial)
+                double *__restrict__ partial, const uint16_t *__restrict__ mask)
   {
     using R          = double;
     using T          = Tile<DIM>;
@@ -529,6 +606,7 @@ namespace sint
     const int        cell  = threadIdx.x / T::NQ;
     const int        b0    = cell_box_base<DIM>(cell);
     const bool       valid = cell_in_mesh<DIM>(cell, tc, g);
+    const unsigned   gmask = CUT ? cell_mask<DIM>(mask, g, tc, cell) : ~0u;
 
     {
       R c, gc[DIM], mu_unused, gmu[DIM];
@@ -538,7 +616,16 @@ namespace sint
       R geta[G][DIM];
 #pragma unroll
       for (int i = 0; i < G; ++i)
-        eval_vg<DIM>(s_lin + (2 + i) * T::BOX, b0, w, eta[i], geta[i]);
+        {
+          eval_vg<DIM>(s_lin + (2 + i) * T::BOX, b0, w, eta[i], geta[i]);
+          if (CUT && ((gmask >> i) & 1u) == 0u)
+            {
+              eta[i] = R(0);
+#pragma unroll
+              for (int d = 0; d < DIM; ++d)
+                geta[i][d] = R(0);
+            }
+        }
       R *cf = s_coef + threadIdx.x * LY::NCOEF;
       // mobility matrix: column e = apply_M(..., unit vector e)
 #pragma unroll
@@ -548,7 +635,7 @@ namespace sint
 #pragma unroll
           for (int d = 0; d < DIM; ++d)
             unit[d] = d == e ? R(1) : R(0);
-          apply_M<DIM, G, TENS>(p, c, eta, gc, geta, unit, col);
+          apply_M<DIM, G, TENS>(p, c, eta, gc, geta, unit, col, gmask);
 #pragma unroll
           for (int d = 0; d < DIM; ++d)
             cf[d * DIM + e] = col[d];
@@ -636,6 +723,10 @@ namespace sint
           for (int i = 0; i < G; ++i)
             acc[4 + i] += w.JxW * ((p.w0 + p.L * cf[2 * DIM * DIM + DIM + 1 + i]) * pp + p.L * p.kp * gg);
         }
+#pragma unroll
+      for (int i = 0; i < G; ++i)
+        if (CUT && ((gmask >> i) & 1u) == 0u)
+          acc[4 + i] = R(0);
 #pragma unroll
       for (int k = 0; k < LY::NOUT; ++k)
         store_contrib<DIM>(s_con, k, acc[k], valid);

@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "sint_common.cuh"
 
 namespace sint
@@ -13,17 +15,19 @@ namespace sint
   // Dynamic shared memory of the diagonal kernel (bytes).
   size_t smem_diag(int dim, int G);
 
+  // mask: per-cell grain masks of the grain cut-off, nullptr for the full operator
   template <int DIM, bool TENS, typename R>
   cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                         cudaStream_t s);
+                         const uint16_t *mask, cudaStream_t s);
 
   template <int DIM, bool TENS>
   cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
-                              const double *const *hist, double *dst, double *partial, cudaStream_t s);
+                              const double *const *hist, double *dst, double *partial, const uint16_t *mask,
+                              cudaStream_t s);
 
   template <int DIM, bool TENS>
   cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
-                          cudaStream_t s);
+                          const uint16_t *mask, cudaStream_t s);
 
   template <int DIM, typename R>
   cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, cudaStream_t s);

@@ -27,12 +27,12 @@ namespace sint
     return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
   }
 
-  template <int DIM, int G, bool TENS, typename R>
+  template <int DIM, int G, bool TENS, typename R, bool CUT>
   cudaError_t launch_jvp_g(const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                           cudaStream_t s)
+                           const uint16_t *mask, cudaStream_t s)
   {
     const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false>::TOTAL * sizeof(R);
-    auto         k    = jvp_kernel<DIM, G, TENS, R>;
+    auto         k    = jvp_kernel<DIM, G, TENS, R, CUT>;
     // persistent grid: as many blocks as are resident at once
     static int   grid_cap = 0;
     cudaError_t  e        = cudaSuccess;
@@ -48,17 +48,17 @@ namespace sint
         grid_cap = sms * (per_sm > 0 ? per_sm : 1);
       }
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
-    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial);
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, mask);
     count_launches(1);
     return cudaGetLastError();
   }
 
-  template <int DIM, int G, bool TENS, int WTD>
+  template <int DIM, int G, bool TENS, int WTD, bool CUT>
   cudaError_t launch_residual_g(const Grid &g, const Phys &p, const double *src, const double *const *hist,
-                                double *dst, double *partial, cudaStream_t s)
+                                double *dst, double *partial, const uint16_t *mask, cudaStream_t s)
   {
     const size_t  smem     = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2>::TOTAL * sizeof(double);
-    auto          k        = residual_kernel<DIM, G, TENS, WTD>;
+    auto          k        = residual_kernel<DIM, G, TENS, WTD, CUT>;
     static int    grid_cap = 0;
     cudaError_t   e        = cudaSuccess;
     if (grid_cap == 0)
@@ -76,21 +76,21 @@ namespace sint
     const double *h1     = (WTD == 2 && p.order > 1) ? hist[1] : nullptr;
     const double *h2     = (WTD == 2 && p.order > 2) ? hist[2] : nullptr;
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
-    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial);
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial, mask);
     count_launches(1);
     return cudaGetLastError();
   }
 
-  template <int DIM, int G, bool TENS>
+  template <int DIM, int G, bool TENS, bool CUT>
   cudaError_t launch_diag_g(const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
-                            cudaStream_t s)
+                            const uint16_t *mask, cudaStream_t s)
   {
     const size_t smem = smem_diag(DIM, G);
-    auto         k    = diag_kernel<DIM, G, TENS>;
+    auto         k    = diag_kernel<DIM, G, TENS, CUT>;
     cudaError_t  e    = prepare_smem(k, smem);
     if (e != cudaSuccess)
       return e;
-    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, dst, partial);
+    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, dst, partial, mask);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -113,44 +113,67 @@ namespace sint
       default: return cudaErrorInvalidValue;                                                                      \
     }
 
+  // mask == nullptr: the full operator; otherwise the grain cut-off with these cell masks
   template <int DIM, bool TENS, typename R>
   cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                         cudaStream_t s)
+                         const uint16_t *mask, cudaStream_t s)
   {
-#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R>(g, p, lin, src, dst, partial, s)
+    if (mask)
+      {
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, true>(g, p, lin, src, dst, partial, mask, s)
+        SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+      }
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, false>(g, p, lin, src, dst, partial, nullptr, s)
     SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
   }
 
-  template <int DIM, bool TENS>
-  cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
-                              const double *const *hist, double *dst, double *partial, cudaStream_t s)
+  template <int DIM, bool TENS, bool CUT>
+  cudaError_t launch_residual_c(int G, int wtd, const Grid &g, const Phys &p, const double *src,
+                                const double *const *hist, double *dst, double *partial, const uint16_t *mask,
+                                cudaStream_t s)
   {
     if (wtd == 0)
       {
-#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 0>(g, p, src, hist, dst, partial, s)
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 0, CUT>(g, p, src, hist, dst, partial, mask, s)
         SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
       }
     else if (wtd == 1)
       {
-#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 1>(g, p, src, hist, dst, partial, s)
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 1, CUT>(g, p, src, hist, dst, partial, mask, s)
         SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
       }
     else
       {
-#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 2>(g, p, src, hist, dst, partial, s)
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 2, CUT>(g, p, src, hist, dst, partial, mask, s)
         SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
       }
   }
 
   template <int DIM, bool TENS>
-  cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
-                          cudaStream_t s)
+  cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
+                              const double *const *hist, double *dst, double *partial, const uint16_t *mask,
+                              cudaStream_t s)
   {
-#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS>(g, p, lin, dst, partial, s)
+    return mask ? launch_residual_c<DIM, TENS, true>(G, wtd, g, p, src, hist, dst, partial, mask, s)
+                : launch_residual_c<DIM, TENS, false>(G, wtd, g, p, src, hist, dst, partial, nullptr, s);
+  }
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
+                          const uint16_t *mask, cudaStream_t s)
+  {
+    if (mask)
+      {
+#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS, true>(g, p, lin, dst, partial, mask, s)
+        SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+      }
+#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS, false>(g, p, lin, dst, partial, nullptr, s)
     SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
   }

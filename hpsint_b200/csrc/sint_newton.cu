@@ -44,16 +44,20 @@ namespace sint
     // caller's stream by two events) so that Arnoldi iteration j can be
     // captured once as a CUDA graph and replayed; a graph is updated in place
     // when a kernel argument it holds (the operator's physics: time weights,
-    // mobility) has changed since its capture.
+    // mobility) or the kernel set (grain cut-off on or off) has changed since
+    // its capture.
     cudaStream_t ps       = nullptr;
     cudaEvent_t  join_in  = nullptr, join_out = nullptr;
     struct IterGraph
     {
       cudaGraphExec_t exec  = nullptr;
       Phys            key   = {};
+      const uint16_t *mask  = nullptr; // cell masks the captured kernels read (nullptr: no cut-off)
       int             nodes = 0;
     } graphs[MAX_MULTIDOT];
-    bool warm = false; // one eager solve has run (lazy kernel set-up is done outside any capture)
+    // [FP32 Krylov vectors][grain cut-off]: one eager solve with this kernel
+    // set has run (lazy kernel set-up is done outside any capture)
+    bool warm[2][2] = {{false, false}, {false, false}};
   };
 
   int free_workspace(Ctx *c)
@@ -332,12 +336,12 @@ namespace sint
     // then record the event the host waits on.
     auto enqueue = [&](int j) -> int {
       int r = SINT_OK;
-      if (!ws->warm)
+      if (!ws->warm[sizeof(R) == 4][c->cut])
         r = enqueue_kernels(j);
       else
         {
           auto &g = ws->graphs[j];
-          if (!g.exec || std::memcmp(&g.key, &c->phys, sizeof(Phys)) != 0)
+          if (!g.exec || std::memcmp(&g.key, &c->phys, sizeof(Phys)) != 0 || g.mask != active_mask(c))
             {
               cudaGraph_t       graph = nullptr;
               const long long   n0    = sint_kernel_launch_count();
@@ -376,6 +380,7 @@ namespace sint
                   return cuda_fail(e, "GMRES: instantiate");
                 }
               g.key   = c->phys;
+              g.mask  = active_mask(c);
               g.nodes = int(nn);
             }
           const cudaError_t e = cudaGraphLaunch(g.exec, s);
@@ -537,7 +542,7 @@ namespace sint
     if (e != cudaSuccess)
       return cuda_fail(e, "GMRES: join back");
     if (rc == SINT_OK)
-      ws->warm = true;
+      ws->warm[sizeof(R) == 4][c->cut] = true;
     return rc;
   }
 

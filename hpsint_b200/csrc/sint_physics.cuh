@@ -89,6 +89,18 @@ namespace sint
     return n2 > R(1e-20) ? rcp_pos<R>(n2) : R(0);
   }
 
+  // Grain cut-off (operator_sintering_data.h:149-203): bit i of the cell mask m
+  // is set when grain i is relevant on the cell.  Absent grains enter the
+  // point physics with zero values and gradients, so a pair term of an absent
+  // grain is exactly zero; a warp skips the pair when no lane needs it.  The
+  // full operator passes m = ~0u, which folds every test away.
+  __device__ __forceinline__ bool pair_needed(unsigned m, int i, int j)
+  {
+    if (m == ~0u)
+      return true;
+    return __any_sync(0xffffffffu, ((m >> i) & (m >> j) & 1u) != 0u);
+  }
+
   template <typename R>
   __device__ __forceinline__ R phi_clamped(R c)
   {
@@ -100,7 +112,8 @@ namespace sint
   // scalar: mobility.h:439-472, tensorial: mobility.h:756-804
   template <int DIM, int G, bool TENS, typename R>
   __device__ __forceinline__ void apply_M(const PhysR<R> &p, R c, const R (&eta)[G], const R (&gc)[DIM],
-                                          const R (*geta)[DIM], const R (&gmu)[DIM], R (&out)[DIM])
+                                          const R (*geta)[DIM], const R (&gmu)[DIM], R (&out)[DIM],
+                                          unsigned m = ~0u)
   {
     const R phi = phi_clamped(c);
     if constexpr (!TENS)
@@ -140,6 +153,8 @@ namespace sint
 #pragma unroll
               for (int j = 0; j < i; ++j)
                 {
+                  if (!pair_needed(m, i, j))
+                    continue;
                   R dd[DIM];
 #pragma unroll
                   for (int d = 0; d < DIM; ++d)
@@ -167,7 +182,7 @@ namespace sint
   __device__ __forceinline__ void apply_M_derivative(const PhysR<R> &p, R c, const R (&gc)[DIM],
                                                      const R (&gmu)[DIM], const R (&eta)[G], const R (*geta)[DIM],
                                                      R dc, const R (&gdc)[DIM], const R (&gdmu)[DIM],
-                                                     const R (&deta)[G], R (&out)[DIM])
+                                                     const R (&deta)[G], R (&out)[DIM], unsigned m = ~0u)
   {
     const R phi = phi_clamped(c);
     const R omc = R(1) - c;
@@ -237,6 +252,8 @@ namespace sint
 #pragma unroll
               for (int j = 0; j < i; ++j)
                 {
+                  if (!pair_needed(m, i, j))
+                    continue;
                   R dd[DIM];
 #pragma unroll
                   for (int d = 0; d < DIM; ++d)

@@ -14,6 +14,7 @@ library's CUDA kernels.
 import ctypes
 from dataclasses import dataclass, field
 
+import numpy as np
 import torch
 
 from . import _lib as L
@@ -118,6 +119,7 @@ class SinteringOperatorGeneric:
         L.check(lib.sint_dof_layout(self._h, ctypes.byref(n), ctypes.byref(c), ctypes.byref(ld)), "sint_dof_layout")
         self.N, self.C, self.ld = n.value, c.value, ld.value
         self.order = 0
+        self.cut_off_tolerance = 0.0
 
     @classmethod
     def create(cls, mesh, params):
@@ -161,6 +163,36 @@ class SinteringOperatorGeneric:
         L.check(L.lib().sint_set_linearization_point(self._h, _ptr(src), _stream()), "sint_set_linearization_point")
 
     set_linearization_point = fill_quadrature_point_values
+
+    def set_component_mask(self, src, grain_use_cut_off_tolerance):
+        """Grain cut-off (SinteringOperatorData::set_component_mask,
+        operator_sintering_data.h:149-298): grain b is relevant on a cell when
+        max |eta_b| over the cell's nodes of `src` exceeds the tolerance; the
+        residual, the Jacobian products and the preconditioner then treat
+        every cell with its relevant grains only.  Tolerance 0 switches the
+        cut-off off (GrainCutOffTolerance, parameters.h:314)."""
+        tol = float(grain_use_cut_off_tolerance)
+        if tol != 0.0:
+            self._check_vec(src, torch.float64)
+        L.check(L.lib().sint_set_component_mask(self._h, _ptr(src) if tol != 0.0 else None, tol, _stream()),
+                "sint_set_component_mask")
+        self.cut_off_tolerance = tol
+
+    def component_mask_statistics(self):
+        """numpy array: entry k = number of cells with k relevant grains
+        (the "Cut-off statistic" of operator_sintering_data.h:236-296)."""
+        counts = (ctypes.c_int64 * (self.params.n_grains + 1))()
+        L.check(L.lib().sint_component_mask_statistics(self._h, counts, _stream()), "sint_component_mask_statistics")
+        return np.array(counts[:], dtype=np.int64)
+
+    def get_component_mask(self):
+        """Device tensor of the cell masks (int16 bit patterns; bit b = grain b relevant), cells x-fastest."""
+        n = 1
+        for d in range(self.mesh.dim):
+            n *= self.mesh.n_cells[d]
+        out = torch.empty(n, dtype=torch.int16, device="cuda")
+        L.check(L.lib().sint_get_component_mask(self._h, _ptr(out), _stream()), "sint_get_component_mask")
+        return out
 
     def evaluate_nonlinear_residual(self, dst, src, with_time_derivative=2, history=()):
         self._check_vec(dst, torch.float64)

@@ -8,6 +8,7 @@ asked to do:
   predictor hook                    sintering/driver.h:2001-2058 (initial Newton iterate)
   failure -> dt halving, restore    sintering/driver.h:2163-2202, :2489-2505
   dt growth after "good" steps      sintering/driver.h:2239-2243, :2387-2409
+  grain cut-off before each attempt sintering/driver.h:2212-2218
   defaults                          time_integration/time_integrator_parameters.h:32-36
 The solution stays on the device; a step is one sint_newton_solve call (or
 several after failures).
@@ -65,10 +66,14 @@ class TimeIntegrator:
                        nl_rel_tol * |R(u_n)|, so a better guess can only save
                        iterations, never loosen the answer.  Without a
                        predictor the two rules coincide.
+
+    grain_cut_off_tolerance != 0 (GrainCutOffTolerance, parameters.h:314)
+    sets the operator's grain cut-off from u_n before every step attempt, as
+    the driver does before make_step.
     """
 
     def __init__(self, op: SinteringOperatorGeneric, nl: NonLinearData = None, td: TimeIntegrationData = None,
-                 predictor=None, tolerance_base="initial_guess"):
+                 predictor=None, tolerance_base="initial_guess", grain_cut_off_tolerance=0.0):
         if tolerance_base not in ("initial_guess", "old_solution"):
             raise ValueError(f"tolerance_base must be 'initial_guess' or 'old_solution', not {tolerance_base!r}")
         self.op = op
@@ -77,6 +82,8 @@ class TimeIntegrator:
         self.newton = DampedNewtonSolver(op, self.nl)
         self.predictor = predictor
         self.tolerance_base = tolerance_base
+        self.grain_cut_off_tolerance = float(grain_cut_off_tolerance)
+        self.cut_off_statistics = []  # per accepted step: cells per number of relevant grains
         self._r = None
         self.history = []     # old solutions, most recent first (device tensors)
         self.dts = []         # accepted time steps, most recent first
@@ -120,6 +127,8 @@ class TimeIntegrator:
             t_try = time.perf_counter()
             w0, wh = self._weights(self.dt)
             self.op.set_time_weights(w0, wh, 1.0)
+            if self.grain_cut_off_tolerance != 0.0:
+                self.op.set_component_mask(self.history[0], self.grain_cut_off_tolerance)
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
             self._reference_residual = 0.0
             data = self._stop_rule(wh) if guess is not None else None
@@ -145,6 +154,8 @@ class TimeIntegrator:
         self.records.append(StepRecord(self.t, self.dt, st.newton_iterations, st.linear_iterations,
                                        st.residual_evaluations, tries, t1 - t0, st.initial_residual,
                                        st.final_residual, t1 - t_try, self._reference_residual))
+        if self.grain_cut_off_tolerance != 0.0:
+            self.cut_off_statistics.append(self.op.component_mask_statistics())
         self.history.insert(0, u)
         self.dts.insert(0, self.dt)
         keep = max(2, self.td.scheme_order)  # predictors use the last two states

@@ -174,6 +174,37 @@ int sint_ac_inverse_diagonal_f64(sint_ctx *ctx, double *inv_diag, sint_stream_t 
 int sint_ch_blocks_f64(sint_ctx *ctx, double *blocks, sint_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Grain cut-off: SinteringOperatorData::set_component_mask                 */
+/* (operator_sintering_data.h:149-298), called by the driver before every   */
+/* step attempt with the current solution when GrainCutOffTolerance != 0    */
+/* (driver.h:2212-2218, parameters.h:314, :421).                            */
+/* ---------------------------------------------------------------------- */
+
+/* Marks grain b relevant on a cell when max |eta_b| over the cell's nodes
+ * exceeds tol (u: C blocks of block_stride, device).  While set, the
+ * context's residual, both Jacobian-vector products, the preconditioner and
+ * the Newton solver restrict every cell to its relevant grains (the
+ * context-free sint_jvp_f64_noalloc always applies the full operator), as
+ * do_evaluate_nonlinear_residual_nt and
+ * do_vmult_range_no_template (operator_sintering_generic.h:456-537,
+ * :1008-1081) and the Allen-Cahn preconditioner block
+ * (preconditioners.h:787-817, :865-882) do: an absent grain contributes
+ * nothing to the cell's sums and its row receives nothing from the cell.
+ * The reference forms the union over the cells of one SIMD batch; this
+ * library keeps one set per cell.  tol == 0 switches the cut-off off;
+ * tol < 0 is SINT_ERR_ARG.  The first call allocates one uint16 per cell. */
+int sint_set_component_mask(sint_ctx *ctx, const double *u, double tol, sint_stream_t stream);
+
+/* The "Cut-off statistic" (operator_sintering_data.h:236-296): counts[k]
+ * (host, n_grains + 1 entries) = number of cells with k relevant grains.
+ * SINT_ERR_NOT_READY without a cut-off.  Synchronises `stream`. */
+int sint_component_mask_statistics(sint_ctx *ctx, int64_t *counts, sint_stream_t stream);
+
+/* Copies the cell masks (bit b = grain b relevant; n_cells[0] * n_cells[1]
+ * * n_cells[2] entries, x fastest) to the device array dst. */
+int sint_get_component_mask(const sint_ctx *ctx, uint16_t *dst, sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* BLAS-1 on block vectors: DynamicBlockVector                              */
 /* (include/pf-applications/lac/dynamic_block_vector.h:346-516).            */
 /* n = number of elements (C * block_stride for a whole block vector).      */

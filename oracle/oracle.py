@@ -51,12 +51,14 @@ def lib():
         L.oracle_free_energy.argtypes = [_c_double, _c_double, P(_c_double), _c_int, P(_c_double)]
         L.oracle_power_sum.argtypes = [P(_c_double), _c_int, _c_int]
         L.oracle_power_sum.restype = _c_double
+        U16 = P(ctypes.c_uint16)
         L.oracle_residual.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(P(_c_double)),
-                                      _c_int, P(_c_double), _c_int]
+                                      _c_int, U16, P(_c_double), _c_int]
         L.oracle_jvp.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double),
-                                 P(_c_double), _c_int]
-        L.oracle_ac_diagonal.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double), _c_int]
-        L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double), _c_int]
+                                 U16, P(_c_double), _c_int]
+        L.oracle_ac_diagonal.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
+        L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
+        L.oracle_grain_mask.argtypes = [P(Mesh), P(Params), P(_c_double), _c_double, U16]
         _lib = L
     return _lib
 
@@ -64,6 +66,18 @@ def lib():
 def _dptr(a):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(ctypes.POINTER(_c_double))
+
+
+def _mptr(mask, mesh):
+    """Cell-mask argument: None (every grain) or uint16 per cell."""
+    if mask is None:
+        return None, None
+    n = 1
+    for d in range(mesh.dim):
+        n *= mesh.n[d]
+    m = np.ascontiguousarray(mask, dtype=np.uint16).reshape(-1)
+    assert m.size == n, (m.size, n)
+    return m, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
 
 
 def make_mesh(dim, cells, h=(1.0, 1.0, 1.0)):
@@ -120,42 +134,63 @@ def power_sum(x, p):
     return lib().oracle_power_sum(_dptr(xs), len(xs), p)
 
 
-def residual(mesh, params, time, u, hist=(), with_td=2, threads=0):
+def n_cells(mesh):
+    n = 1
+    for d in range(mesh.dim):
+        n *= mesh.n[d]
+    return n
+
+
+def grain_mask(mesh, params, u, tol):
+    """Cell masks of the grain cut-off (uint16 per cell, bit b = grain b relevant)."""
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(C, N)
+    m = np.zeros(n_cells(mesh), dtype=np.uint16)
+    _check(lib().oracle_grain_mask(ctypes.byref(mesh), ctypes.byref(params), _dptr(u), float(tol),
+                                   m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))), "grain_mask")
+    return m
+
+
+def residual(mesh, params, time, u, hist=(), with_td=2, threads=0, mask=None):
     C, N = params.n_grains + 2, n_nodes(mesh)
     u = np.ascontiguousarray(u, dtype=np.float64).reshape(C, N)
     hs = [np.ascontiguousarray(h, dtype=np.float64).reshape(C, N) for h in hist]
     arr = (ctypes.POINTER(_c_double) * max(1, len(hs)))(*[_dptr(h) for h in hs])
     dst = np.zeros((C, N))
+    keep, mp = _mptr(mask, mesh)
     _check(lib().oracle_residual(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(u),
-                                 arr, with_td, _dptr(dst), threads or os.cpu_count()), "residual")
+                                 arr, with_td, mp, _dptr(dst), threads or os.cpu_count()), "residual")
     return dst
 
 
-def jvp(mesh, params, time, lin, src, threads=0):
+def jvp(mesh, params, time, lin, src, threads=0, mask=None):
     C, N = params.n_grains + 2, n_nodes(mesh)
     lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
     src = np.ascontiguousarray(src, dtype=np.float64).reshape(C, N)
     dst = np.zeros((C, N))
+    keep, mp = _mptr(mask, mesh)
     _check(lib().oracle_jvp(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin), _dptr(src),
-                            _dptr(dst), threads or os.cpu_count()), "jvp")
+                            mp, _dptr(dst), threads or os.cpu_count()), "jvp")
     return dst
 
 
-def ac_diagonal(mesh, params, time, lin, threads=0):
+def ac_diagonal(mesh, params, time, lin, threads=0, mask=None):
     C, N, G = params.n_grains + 2, n_nodes(mesh), params.n_grains
     lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
     d = np.zeros((G, N))
+    keep, mp = _mptr(mask, mesh)
     _check(lib().oracle_ac_diagonal(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
-                                    _dptr(d), threads or os.cpu_count()), "ac_diagonal")
+                                    mp, _dptr(d), threads or os.cpu_count()), "ac_diagonal")
     return d
 
 
-def ch_blocks(mesh, params, time, lin, threads=0):
+def ch_blocks(mesh, params, time, lin, threads=0, mask=None):
     C, N = params.n_grains + 2, n_nodes(mesh)
     lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
     b = np.zeros((4, N))
+    keep, mp = _mptr(mask, mesh)
     _check(lib().oracle_ch_blocks(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
-                                  _dptr(b), threads or os.cpu_count()), "ch_blocks")
+                                  mp, _dptr(b), threads or os.cpu_count()), "ch_blocks")
     return b
 
 

@@ -19,6 +19,14 @@
 // Cell loops are parallelised with OpenMP over 2^dim cell colours (parity of
 // the cell index in each direction); cells of one colour share no node, so
 // the scatter is race-free and the summation order deterministic.
+//
+// Grain cut-off: with a cell mask (one uint16 per cell, bit b = grain b
+// relevant, cells in lexicographic order) a cell gathers c, mu and its
+// relevant grains only, runs the point physics with that many grains and
+// scatters into those blocks only -- the src_view / vector_indices loops of
+// do_vmult_range_no_template and do_evaluate_nonlinear_residual_nt
+// (sintering/operator_sintering_generic.h:456-537, :1008-1081).  A null mask
+// keeps every grain.
 
 #include <algorithm>
 #include <cmath>
@@ -537,6 +545,22 @@ namespace
   {
     return Mobility{m->dim, p->Mvol, p->Mvap, p->Msurf, p->Mgb, p->L, p->tensorial != 0};
   }
+
+  // Blocks cell (i,j,k) works on: blk[0] = c, blk[1] = mu, blk[2..] = the
+  // relevant grains' blocks in increasing order (all grains without a mask).
+  // Returns the number of relevant grains.
+  inline int cell_blocks(const Geometry &geo, const uint16_t *mask, int G, int i, int j, int k, int *blk)
+  {
+    blk[0] = 0;
+    blk[1] = 1;
+    const unsigned m =
+      mask ? mask[int64_t(i) + int64_t(geo.n[0]) * (int64_t(j) + int64_t(geo.n[1]) * k)] : 0xffffffffu;
+    int n = 0;
+    for (int b = 0; b < G; ++b)
+      if ((m >> b) & 1u)
+        blk[2 + n++] = 2 + b;
+    return n;
+  }
 }
 
 extern "C" {
@@ -565,6 +589,38 @@ int oracle_free_energy(double A, double B, const double *state, int G, double *o
   return 0;
 }
 
+// SinteringOperatorData::set_component_mask (operator_sintering_data.h:149-203)
+// per cell: bit b of mask[cell] is set when the l-infinity norm of the cell's
+// nodal values of eta_b exceeds tol.  (The reference takes the union over the
+// cells of one SIMD batch; the restatement keeps one set per cell.)
+int oracle_grain_mask(const oracle_mesh *m, const oracle_params *p, const double *u, double tol, uint16_t *mask)
+{
+  if (int e = check_args(m, p))
+    return e;
+  if (!(tol >= 0.0))
+    return 1;
+  const Geometry geo(*m);
+  const int      G  = p->n_grains;
+  const int64_t  N  = geo.n_nodes;
+  const int      nk = geo.dim == 3 ? geo.n[2] : 1;
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < geo.n[1]; ++j)
+      for (int i = 0; i < geo.n[0]; ++i)
+        {
+          unsigned bits = 0;
+          for (int b = 0; b < G; ++b)
+            {
+              double norm = 0.0;
+              for (int l = 0; l < geo.nq; ++l)
+                norm = std::max(norm, std::fabs(u[(2 + b) * N + geo.node(i, j, k, l)]));
+              if (norm > tol)
+                bits |= 1u << b;
+            }
+          mask[int64_t(i) + int64_t(geo.n[0]) * (int64_t(j) + int64_t(geo.n[1]) * k)] = uint16_t(bits);
+        }
+  return 0;
+}
+
 // numerics/power_helper.h:31-45: sum_i x_i^p
 double oracle_power_sum(const double *x, int n, int p)
 {
@@ -587,7 +643,7 @@ double oracle_power_sum(const double *x, int n, int p)
 // sum_i w_hist[i] * hist[i], interpolated to the quadrature points.
 // dst is overwritten.
 int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *u,
-                    const double *const *hist, int with_td, double *dst, int n_threads)
+                    const double *const *hist, int with_td, const uint16_t *mask, double *dst, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
@@ -602,21 +658,24 @@ int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_t
   std::memset(dst, 0, sizeof(double) * C * N);
 
   coloured_cell_loop(geo, n_threads, [&](int i, int j, int k) {
-    double ul[MAXC][8], hl[MAXC][8];
-    double val[MAXC][8], hval[MAXC][8];
-    V3     grad[MAXC][8];
+    int       blk[MAXC];
+    const int G = cell_blocks(geo, mask, p->n_grains, i, j, k, blk), C = G + 2;
+    double    ul[MAXC][8], hl[MAXC][8];
+    double    val[MAXC][8], hval[MAXC][8];
+    V3        grad[MAXC][8];
     for (int l = 0; l < nq; ++l)
       {
         const int64_t gi = geo.node(i, j, k, l);
         for (int b = 0; b < C; ++b)
           {
-            ul[b][l] = u[b * N + gi];
+            ul[b][l] = u[blk[b] * N + gi];
             if (with_td == 2)
               {
                 // generic.h:947-966: weighted sum of the old solutions at the nodes
                 double s = 0.0;
                 for (int o = 0; o < t->order; ++o)
-                  s = (o == 0) ? hist[o][b * N + gi] * t->w_hist[o] : s + hist[o][b * N + gi] * t->w_hist[o];
+                  s = (o == 0) ? hist[o][blk[b] * N + gi] * t->w_hist[o]
+                               : s + hist[o][blk[b] * N + gi] * t->w_hist[o];
                 hl[b][l] = s;
               }
           }
@@ -634,7 +693,7 @@ int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_t
     V3     rg[MAXC][8];
     for (int q = 0; q < nq; ++q)
       {
-        double value[MAXC];
+        double value[MAXC] = {};
         V3     gradient[MAXC];
         for (int b = 0; b < C; ++b)
           {
@@ -672,7 +731,7 @@ int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_t
         double rl[8];
         integrate(geo, rv[b], rg[b], rl);
         for (int l = 0; l < nq; ++l)
-          dst[b * N + geo.node(i, j, k, l)] += rl[l];
+          dst[blk[b] * N + geo.node(i, j, k, l)] += rl[l];
       }
   });
   return 0;
@@ -686,7 +745,7 @@ int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_t
 // No constrained DoFs exist on these meshes (operator_base.h:294-353 is then
 // a plain cell loop).  dst is overwritten.
 int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *lin,
-               const double *src, double *dst, int n_threads)
+               const double *src, const uint16_t *mask, double *dst, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
@@ -699,16 +758,18 @@ int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *
   std::memset(dst, 0, sizeof(double) * C * N);
 
   coloured_cell_loop(geo, n_threads, [&](int i, int j, int k) {
-    double ll[MAXC][8], sl[MAXC][8];
-    double lval[MAXC][8], sval[MAXC][8];
-    V3     lgrad[MAXC][8], sgrad[MAXC][8];
+    int       blk[MAXC];
+    const int G = cell_blocks(geo, mask, p->n_grains, i, j, k, blk), C = G + 2;
+    double    ll[MAXC][8], sl[MAXC][8];
+    double    lval[MAXC][8], sval[MAXC][8];
+    V3        lgrad[MAXC][8], sgrad[MAXC][8];
     for (int l = 0; l < nq; ++l)
       {
         const int64_t gi = geo.node(i, j, k, l);
         for (int b = 0; b < C; ++b)
           {
-            ll[b][l] = lin[b * N + gi];
-            sl[b][l] = src[b * N + gi];
+            ll[b][l] = lin[blk[b] * N + gi];
+            sl[b][l] = src[blk[b] * N + gi];
           }
       }
     for (int b = 0; b < C; ++b)
@@ -720,7 +781,7 @@ int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *
     V3     rg[MAXC][8];
     for (int q = 0; q < nq; ++q)
       {
-        double lin_value[MAXC], value[MAXC];
+        double lin_value[MAXC] = {}, value[MAXC] = {};
         V3     lin_gradient[MAXC], gradient[MAXC];
         for (int b = 0; b < C; ++b)
           {
@@ -761,7 +822,7 @@ int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *
         double rl[8];
         integrate(geo, rv[b], rg[b], rl);
         for (int l = 0; l < nq; ++l)
-          dst[b * N + geo.node(i, j, k, l)] += rl[l];
+          dst[blk[b] * N + geo.node(i, j, k, l)] += rl[l];
       }
   });
   return 0;
@@ -775,20 +836,23 @@ int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *
 // coupling lands off the diagonal, so
 //   d_i(n) = sum_cells sum_q JxW [(w0 + L f_{eta_i eta_i}) phi_n^2 + L kappa_p |grad phi_n|^2].
 int oracle_ac_diagonal(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *lin,
-                       double *diag, int n_threads)
+                       const uint16_t *mask, double *diag, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
   const Geometry geo(*m);
-  const int      G = p->n_grains, C = G + 2, nq = geo.nq;
+  const int      G = p->n_grains, nq = geo.nq;
   const int64_t  N = geo.n_nodes;
   std::memset(diag, 0, sizeof(double) * G * N);
   coloured_cell_loop(geo, n_threads, [&](int i, int j, int k) {
-    double ll[MAXC][8], lval[MAXC][8];
-    V3     lgrad[MAXC][8];
+    // cut-off: absent grains add nothing (preconditioners.h:787-817)
+    int       blk[MAXC];
+    const int G = cell_blocks(geo, mask, p->n_grains, i, j, k, blk), C = G + 2;
+    double    ll[MAXC][8], lval[MAXC][8];
+    V3        lgrad[MAXC][8];
     for (int l = 0; l < nq; ++l)
       for (int b = 0; b < C; ++b)
-        ll[b][l] = lin[b * N + geo.node(i, j, k, l)];
+        ll[b][l] = lin[blk[b] * N + geo.node(i, j, k, l)];
     for (int b = 0; b < C; ++b)
       evaluate(geo, ll[b], lval[b], lgrad[b]);
     for (int ig = 0; ig < G; ++ig)
@@ -807,7 +871,7 @@ int oracle_ac_diagonal(const oracle_mesh *m, const oracle_params *p, const oracl
               const V3             gr  = (p->L * p->kappa_p) * dphi;
               d += geo.JxW * (vr * phi + dot(gr, dphi));
             }
-          diag[ig * N + geo.node(i, j, k, l)] += d;
+          diag[(blk[2 + ig] - 2) * N + geo.node(i, j, k, l)] += d;
         }
   });
   return 0;
@@ -818,21 +882,23 @@ int oracle_ac_diagonal(const oracle_mesh *m, const oracle_params *p, const oracl
 // restricted to (node n, node n):  blocks[0*N+n] = J_cc, [1*N+n] = J_c,mu,
 // [2*N+n] = J_mu,c, [3*N+n] = J_mu,mu  (row = tested equation, col = unknown).
 int oracle_ch_blocks(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *lin,
-                     double *blocks, int n_threads)
+                     const uint16_t *mask, double *blocks, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
   const Geometry geo(*m);
   const Mobility mob = make_mobility(m, p);
-  const int      G = p->n_grains, C = G + 2, nq = geo.nq;
+  const int      G = p->n_grains, nq = geo.nq;
   const int64_t  N = geo.n_nodes;
   std::memset(blocks, 0, sizeof(double) * 4 * N);
   coloured_cell_loop(geo, n_threads, [&](int i, int j, int k) {
-    double ll[MAXC][8], lval[MAXC][8];
-    V3     lgrad[MAXC][8];
+    int       blk[MAXC];
+    const int G = cell_blocks(geo, mask, p->n_grains, i, j, k, blk), C = G + 2;
+    double    ll[MAXC][8], lval[MAXC][8];
+    V3        lgrad[MAXC][8];
     for (int l = 0; l < nq; ++l)
       for (int b = 0; b < C; ++b)
-        ll[b][l] = lin[b * N + geo.node(i, j, k, l)];
+        ll[b][l] = lin[blk[b] * N + geo.node(i, j, k, l)];
     for (int b = 0; b < C; ++b)
       evaluate(geo, ll[b], lval[b], lgrad[b]);
     for (int l = 0; l < nq; ++l)

@@ -54,3 +54,60 @@ def block_rel_err(ours, ref):
         ne = np.linalg.norm(ours[b] - ref[b])
         errs.append(ne / nr if nr > 0 else ne)
     return max(errs)
+
+
+def particle_state(dim, cells, G, seed, width=1.0):
+    """A (C, N) packing state whose grains are localised: every grain owns one
+    or two round particles (tanh profile of the given interface width), c is
+    the largest eta, mu a smooth random field.  Far from a particle its eta
+    decays to ~1e-10 and below, so grain cut-off masks vary from cell to cell.
+    Each eta carries a smooth 5 % modulation of its own (keeping eta < 1, where
+    the clamp of the interpolation function is inactive): without it the
+    plateaus where particles of two grains overlap have gradients of ~1e-9, and
+    the direction of grad eta_i - grad eta_j that the tensorial mobility's
+    grain-boundary projector needs is rounding noise there (an ill-conditioned
+    state, not a test of the operator)."""
+    rng = np.random.default_rng(seed)
+    shape = [cells[d] + 1 for d in range(dim)]
+    axes = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
+    C = G + 2
+    u = np.zeros((C, int(np.prod(shape))))
+    etas = []
+    for g in range(G):
+        eta = np.zeros(shape)
+        for _ in range(int(rng.integers(1, 3))):
+            ctr = [rng.uniform(0, cells[d]) for d in range(dim)]
+            R = rng.uniform(1.0, 0.3 * min(cells[:dim]) + 1.0)
+            r = np.sqrt(sum((axes[d] - ctr[d]) ** 2 for d in range(dim)))
+            eta = np.maximum(eta, 0.5 * (1.0 - np.tanh((r - R) / (0.5 * width))))
+        k = rng.integers(1, 4, dim)
+        ph = rng.uniform(0, 2 * np.pi)
+        eta = eta * (0.95 + 0.05 * np.cos(sum(np.pi * k[d] * axes[d] / max(1, cells[d]) for d in range(dim)) + ph))
+        etas.append(eta)
+        u[2 + g] = np.transpose(eta).ravel()
+    u[0] = np.transpose(np.max(etas, axis=0)).ravel()
+    mu = np.zeros(shape)
+    for _ in range(3):
+        k = rng.integers(1, 4, dim)
+        ph = rng.uniform(0, 2 * np.pi, dim)
+        term = np.ones(shape)
+        for d in range(dim):
+            term = term * np.cos(np.pi * k[d] * axes[d] / max(1, cells[d]) + ph[d])
+        mu += rng.uniform(0.3, 1.0) * term
+    u[1] = np.transpose(mu).ravel() / 3.0
+    return u
+
+
+def grain_mask_numpy(dim, cells, G, u, tol):
+    """The cut-off rule restated in numpy: bit b set on a cell when the largest
+    |eta_b| over its nodes exceeds tol (cells x fastest)."""
+    shape = [cells[d] + 1 for d in range(dim)]
+    mask = np.zeros([cells[d] for d in range(dim)], dtype=np.uint16)
+    for b in range(G):
+        eta = np.abs(u[2 + b].reshape(list(reversed(shape))).T)  # index [x, y, (z)]
+        m = np.zeros([cells[d] for d in range(dim)])
+        for corner in range(1 << dim):
+            sl = tuple(slice((corner >> d) & 1, ((corner >> d) & 1) + cells[d]) for d in range(dim))
+            m = np.maximum(m, eta[sl])
+        mask |= ((m > tol).astype(np.uint16) << b)
+    return np.transpose(mask).ravel()
