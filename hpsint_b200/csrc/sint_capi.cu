@@ -35,17 +35,23 @@ namespace sint
   }
 
   template <int DIM, typename R>
-  cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, cudaStream_t s)
+  cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, const uint16_t *tile_mask,
+                             cudaStream_t s)
   {
     const long long nb = (g.N + 255) / 256;
-    combine_kernel<DIM, R><<<dim3((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u), 256, 0, s>>>(g, ncomp, partial, dst);
+    combine_kernel<DIM, R>
+      <<<dim3((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u), 256, 0, s>>>(g, ncomp, partial, dst, tile_mask);
     count_launches(1);
     return cudaGetLastError();
   }
-  template cudaError_t launch_combine<2, double>(int, const Grid &, const double *, double *, cudaStream_t);
-  template cudaError_t launch_combine<3, double>(int, const Grid &, const double *, double *, cudaStream_t);
-  template cudaError_t launch_combine<2, float>(int, const Grid &, const float *, float *, cudaStream_t);
-  template cudaError_t launch_combine<3, float>(int, const Grid &, const float *, float *, cudaStream_t);
+  template cudaError_t launch_combine<2, double>(int, const Grid &, const double *, double *, const uint16_t *,
+                                                 cudaStream_t);
+  template cudaError_t launch_combine<3, double>(int, const Grid &, const double *, double *, const uint16_t *,
+                                                 cudaStream_t);
+  template cudaError_t launch_combine<2, float>(int, const Grid &, const float *, float *, const uint16_t *,
+                                                cudaStream_t);
+  template cudaError_t launch_combine<3, float>(int, const Grid &, const float *, float *, const uint16_t *,
+                                                cudaStream_t);
 
   // --- dispatch over (dim, mobility) ---------------------------------------
   template <typename R>
@@ -55,15 +61,15 @@ namespace sint
     const bool t = c->params.tensorial != 0;
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_jvp<3, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s)
-            : launch_jvp<3, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s);
+      e = t ? launch_jvp<3, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s)
+            : launch_jvp<3, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s);
     else
-      e = t ? launch_jvp<2, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s)
-            : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_mask(c), s);
+      e = t ? launch_jvp<2, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s)
+            : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s);
     if (e != cudaSuccess)
       return e;
-    return c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, s)
-                            : launch_combine<2, R>(c->C, c->grid, part, dst, s);
+    return c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, active_tile_union(c), s)
+                            : launch_combine<2, R>(c->C, c->grid, part, dst, active_tile_union(c), s);
   }
 
   template cudaError_t dispatch_jvp<double>(const Ctx *, const double *, const double *, double *, cudaStream_t);
@@ -75,15 +81,15 @@ namespace sint
     const bool t = c->params.tensorial != 0;
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s)
-            : launch_residual<3, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s);
+      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s)
+            : launch_residual<3, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s);
     else
-      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s)
-            : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_mask(c), s);
+      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s)
+            : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s);
     if (e != cudaSuccess)
       return e;
-    return c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, s)
-                            : launch_combine<2, double>(c->C, c->grid, c->partial, dst, s);
+    return c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s)
+                            : launch_combine<2, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s);
   }
 
   static cudaError_t dispatch_diag(const Ctx *c, double *dst, cudaStream_t s)
@@ -98,8 +104,8 @@ namespace sint
             : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s);
     if (e != cudaSuccess)
       return e;
-    return c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, s)
-                            : launch_combine<2, double>(c->G + 4, c->grid, c->partial, dst, s);
+    return c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s)
+                            : launch_combine<2, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s);
   }
 
   // --- preconditioner point kernels ----------------------------------------
@@ -362,6 +368,12 @@ int sint_destroy(sint_ctx *c)
   cudaFree(c->lin32);
   cudaFree(c->partial);
   cudaFree(c->mask);
+  cudaFree(c->cut_tiles);
+  cudaFree(c->cut_grains);
+  cudaFree(c->cut_union);
+  cudaFree(c->tile_union);
+  cudaFree(c->cut_range);
+  cudaFree(c->cut_count);
   cudaFree(c->pc_raw);
   cudaFree(c->pc_inv64);
   cudaFree(c->pc_inv32);

@@ -145,6 +145,34 @@ namespace sint
     long long linear; // blockIdx.x
   };
 
+  // Grain cut-off, as the kernels see it.  Tiles are sorted into classes by
+  // the number of grains relevant on any of their cells: class k's tiles are
+  // tiles[range[k] .. range[k + 1]), and the kernel instantiated for k grains
+  // works on the compacted components (c, mu, eta_{l_0}, .., eta_{l_(k-1)})
+  // with the tile's grain list l packed four bits per grain in
+  // tile_grains[tile] -- the src_view of do_vmult_range_no_template
+  // (operator_sintering_generic.h:496-509) per tile instead of per cell batch.
+  // The arrays below `tiles` are in the sorted order of `tiles`.
+  struct CutTiles
+  {
+    const uint16_t           *cell_mask   = nullptr; // per cell: bit b = grain b relevant
+    const int                *tiles       = nullptr; // tile ids sorted by class
+    const unsigned long long *tile_grains = nullptr; // the tile's packed grain list
+    const uint16_t           *tile_mask   = nullptr; // the union of the tile's cell masks
+    const int                *range       = nullptr; // class offsets into tiles (n_grains + 2)
+    int                       c_all       = 0;       // components of the full operator
+  };
+
+  // Size of a per-grain array: at least one element (the grain cut-off runs
+  // tiles without any relevant grain through the G = 0 kernels).
+  __host__ __device__ constexpr int gdim(int G) { return G > 0 ? G : 1; }
+
+  // Component of the full vector behind compacted component b.
+  __device__ __forceinline__ int comp_of(int b, unsigned long long gl)
+  {
+    return b < 2 ? b : 2 + int((gl >> (4 * (b - 2))) & 15ull);
+  }
+
   template <int DIM>
   __device__ __forceinline__ TileCoord tile_coord(const Grid &g)
   {
@@ -200,16 +228,17 @@ namespace sint
   // Stage the node box of `ncomp` components of `src` (block stride g.ld) in
   // shared memory, layout s[comp * BOX + box_node]; nodes outside the mesh
   // read as zero.
+  // With `mapped`, box component b is component comp_of(b, gl) of src.
   template <int DIM, typename R, typename S>
   __device__ __forceinline__ void load_box(R *s, const S *__restrict__ src, int ncomp, const Grid &g,
-                                           const BoxNode<DIM> &bn)
+                                           const BoxNode<DIM> &bn, unsigned long long gl = 0, bool mapped = false)
   {
     using T = Tile<DIM>;
     if (!bn.active)
       return;
     const S *p = src + bn.gidx;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
-      s[comp * T::BOX + bn.b] = bn.inside ? R(p[comp * g.ld]) : R(0);
+      s[comp * T::BOX + bn.b] = bn.inside ? R(p[(mapped ? comp_of(comp, gl) : comp) * g.ld]) : R(0);
   }
 
   // Asynchronous global->shared copies (cp.async, sm_80+): the node box of the
@@ -237,14 +266,16 @@ namespace sint
   // buffer s (layout s[comp * BOX + box_node]).
   template <int DIM, typename R>
   __device__ __forceinline__ void load_box_async(R *s, const R *__restrict__ src, int ncomp, const Grid &g,
-                                                 const BoxNode<DIM> &bn)
+                                                 const BoxNode<DIM> &bn, unsigned long long gl = 0,
+                                                 bool mapped = false)
   {
     using T = Tile<DIM>;
     if (!bn.active)
       return;
     const R *p = bn.inside ? src + bn.gidx : src;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
-      cp_async_elem(s + comp * T::BOX + bn.b, bn.inside ? p + comp * g.ld : src, bn.inside);
+      cp_async_elem(s + comp * T::BOX + bn.b, bn.inside ? p + (mapped ? comp_of(comp, gl) : comp) * g.ld : src,
+                    bn.inside);
   }
 
   template <int DIM>
@@ -472,10 +503,16 @@ namespace sint
   // Step 5 of the data flow: sum the per-cell node contributions
   // s_con[comp * CS + l * CP + cell] of the tile per box node (fixed order),
   // write nodes owned by the tile to dst and the others to the tile's slot of
-  // the partial buffer (layout [tile][comp][BOX]).
+  // the partial buffer (layout [tile][comp][BOX]).  With `mapped` (grain
+  // cut-off), contribution row b belongs to component comp_of(b, gl) of the
+  // c_all components; the owned nodes of the grains absent from the tile
+  // (bit clear in tmask) are written as zero, their partial slots are left
+  // alone (the combine step skips them).
   template <int DIM, typename R>
   __device__ __forceinline__ void sum_and_store(const R *s_con, int ncomp, const Grid &g, const TileCoord &tc,
-                                                const BoxNode<DIM> &bn, R *__restrict__ dst, R *__restrict__ partial)
+                                                const BoxNode<DIM> &bn, R *__restrict__ dst, R *__restrict__ partial,
+                                                unsigned long long gl = 0, bool mapped = false, int c_all = 0,
+                                                unsigned tmask = 0)
   {
     using T = Tile<DIM>;
     if (!bn.active || !bn.inside)
@@ -495,7 +532,7 @@ namespace sint
                  (bn.by < T::TY || gj == g.n[1]);
     if (DIM == 3)
       owned = owned && (bn.bz > 0 || gk == 0) && (bn.bz < T::TZ || gk == g.n[2]);
-    R *out              = owned ? dst + bn.gidx : partial + tc.linear * ncomp * (long long)T::BOX + bn.b;
+    R *out = owned ? dst + bn.gidx : partial + tc.linear * (mapped ? c_all : ncomp) * (long long)T::BOX + bn.b;
     const long long ost = owned ? g.ld : (long long)T::BOX;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
       {
@@ -505,17 +542,23 @@ namespace sint
         for (int l = 0; l < T::NQ; ++l)
           if (ok[l])
             sum += sc[src_off[l]];
-        out[comp * ost] = sum;
+        out[(mapped ? comp_of(comp, gl) : comp) * ost] = sum;
       }
+    if (mapped && owned)
+      for (int comp = 2 + bn.grp; comp < c_all; comp += T::NG)
+        if (((tmask >> (comp - 2)) & 1u) == 0u)
+          out[comp * ost] = R(0);
   }
 
   // Second pass of the scatter: nodes on an interior tile face sum the
   // partials of the 2, 4 or 8 tiles that share them, in a fixed order.  One
   // thread per (node, component): blockIdx.y is the component, so the
   // partial loads of different components are independent.
+  // tile_mask (grain cut-off): a tile's partial of grain component 2 + b
+  // exists only when bit b of tile_mask[tile] is set; nullptr = all exist.
   template <int DIM, typename R>
   __global__ void __launch_bounds__(256) combine_kernel(const Grid g, int ncomp, const R *__restrict__ partial,
-                                                        R *__restrict__ dst)
+                                                        R *__restrict__ dst, const uint16_t *__restrict__ tile_mask)
   {
     using T              = Tile<DIM>;
     const long long idx  = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -573,6 +616,8 @@ namespace sint
                 const int       ti = t0[0] + cc, tj = t0[1] + bb, tk = t0[2] + a;
                 const int       bx = lo[0] - cc * TT[0], by = lo[1] - bb * TT[1], bz = lo[2] - a * TT[2];
                 const long long tile = ti + (long long)g.nt[0] * (tj + (long long)g.nt[1] * tk);
+                if (tile_mask && cp >= 2 && ((tile_mask[tile] >> (cp - 2)) & 1u) == 0u)
+                  continue;
                 sum += partial[(tile * ncomp + cp) * (long long)T::BOX + bx + T::BX * (by + T::BY * bz)];
               }
         dst[cp * g.ld + idx] = sum;

@@ -3,6 +3,15 @@
 // operator_sintering_data.h:149-298) that the residual, Jacobian and
 // preconditioner kernels restrict their grain terms to, and the statistic of
 // relevant-grain counts the reference prints with it.
+//
+// The reference dispatches every cell batch to the kernel instantiated for
+// its number of relevant grains (EXPAND_OPERATIONS_N_COMP_NT,
+// operator_sintering_generic.h:482-530).  Here the unit is a tile: tiles are
+// sorted into classes by the number of grains relevant on any of their
+// cells, and each class runs the kernels instantiated for that many grains
+// on the compacted components.  The class offsets stay on the device, so
+// the launch sequence of an operator call does not depend on the masks and
+// captured CUDA graphs stay valid when they change.
 #include <string>
 
 #include "sint_internal.h"
@@ -59,7 +68,103 @@ namespace sint
       atomicAdd(&counts[threadIdx.x], (unsigned long long)h[threadIdx.x]);
   }
 
+  // One thread per tile: the union of the masks of its cells inside the
+  // mesh, and the tile counted in the class of its number of grains.
+  __global__ void __launch_bounds__(256)
+    tile_union_kernel(const Grid g, const uint16_t *__restrict__ cell_mask, uint16_t *__restrict__ tile_union,
+                      unsigned *__restrict__ count)
+  {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.n_tiles)
+      return;
+    const int TX = g.dim == 3 ? Tile<3>::TX : Tile<2>::TX, TY = g.dim == 3 ? Tile<3>::TY : Tile<2>::TY,
+              TZ = g.dim == 3 ? Tile<3>::TZ : 1;
+    const int o0 = int(t % g.nt[0]) * TX, o1 = int((t / g.nt[0]) % g.nt[1]) * TY,
+              o2 = int(t / ((long long)g.nt[0] * g.nt[1])) * TZ;
+    unsigned u = 0;
+    for (int k = o2; k < o2 + TZ && k < g.n[2]; ++k)
+      for (int j = o1; j < o1 + TY && j < g.n[1]; ++j)
+        for (int i = o0; i < o0 + TX && i < g.n[0]; ++i)
+          u |= cell_mask[i + (long long)g.n[0] * (j + (long long)g.n[1] * k)];
+    tile_union[t] = (uint16_t)u;
+    atomicAdd(&count[__popc(u)], 1u);
+  }
+
+  // One thread: class offsets from the class sizes; the sizes become the
+  // scatter cursors.
+  __global__ void class_scan_kernel(int G, unsigned *__restrict__ count, int *__restrict__ range)
+  {
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+      return;
+    int acc = 0;
+    for (int k = 0; k <= SINT_MAX_GRAINS + 1; ++k)
+      {
+        range[k] = acc;
+        if (k <= G)
+          {
+            const unsigned n = count[k];
+            count[k]         = (unsigned)acc;
+            acc += (int)n;
+          }
+      }
+  }
+
+  // One thread per tile: its slot in its class (the order inside a class
+  // does not change any result: tiles write disjoint outputs).
+  __global__ void __launch_bounds__(256)
+    class_scatter_kernel(long long n_tiles, const uint16_t *__restrict__ tile_union, unsigned *__restrict__ cursor,
+                         int *__restrict__ tiles, unsigned long long *__restrict__ grains,
+                         uint16_t *__restrict__ sorted_union)
+  {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles)
+      return;
+    const unsigned     u   = tile_union[t];
+    const unsigned     pos = atomicAdd(&cursor[__popc(u)], 1u);
+    unsigned long long gl  = 0;
+    int                n   = 0;
+    for (int b = 0; b < SINT_MAX_GRAINS; ++b)
+      if ((u >> b) & 1u)
+        gl |= (unsigned long long)b << (4 * n++);
+    tiles[pos]        = (int)t;
+    grains[pos]       = gl;
+    sorted_union[pos] = (uint16_t)u;
+  }
+
   static long long cell_count(const Ctx *c) { return (long long)c->grid.n[0] * c->grid.n[1] * c->grid.n[2]; }
+
+  static int allocate_cut(Ctx *c)
+  {
+    const long long nt = c->grid.n_tiles;
+    c->n_cells         = cell_count(c);
+    cudaError_t e      = cudaSuccess;
+    if ((e = cudaMalloc(&c->mask, sizeof(uint16_t) * (size_t)c->n_cells)) != cudaSuccess ||
+        (e = cudaMalloc(&c->cut_tiles, sizeof(int) * (size_t)nt)) != cudaSuccess ||
+        (e = cudaMalloc(&c->cut_grains, sizeof(unsigned long long) * (size_t)nt)) != cudaSuccess ||
+        (e = cudaMalloc(&c->cut_union, sizeof(uint16_t) * (size_t)nt)) != cudaSuccess ||
+        (e = cudaMalloc(&c->tile_union, sizeof(uint16_t) * (size_t)nt)) != cudaSuccess ||
+        (e = cudaMalloc(&c->cut_range, sizeof(int) * (SINT_MAX_GRAINS + 2))) != cudaSuccess ||
+        (e = cudaMalloc(&c->cut_count, sizeof(unsigned) * (SINT_MAX_GRAINS + 1))) != cudaSuccess)
+      {
+        cudaFree(c->mask);
+        cudaFree(c->cut_tiles);
+        cudaFree(c->cut_grains);
+        cudaFree(c->cut_union);
+        cudaFree(c->tile_union);
+        cudaFree(c->cut_range);
+        cudaFree(c->cut_count);
+        c->mask = nullptr, c->cut_tiles = nullptr, c->cut_grains = nullptr, c->cut_union = nullptr;
+        c->tile_union = nullptr, c->cut_range = nullptr, c->cut_count = nullptr;
+        return cuda_fail(e, "sint_set_component_mask: allocation");
+      }
+    c->cut_view.cell_mask   = c->mask;
+    c->cut_view.tiles       = c->cut_tiles;
+    c->cut_view.tile_grains = c->cut_grains;
+    c->cut_view.tile_mask   = c->cut_union;
+    c->cut_view.range       = c->cut_range;
+    c->cut_view.c_all       = c->C;
+    return SINT_OK;
+  }
 } // namespace sint
 
 using namespace sint;
@@ -90,18 +195,20 @@ int sint_set_component_mask(sint_ctx *c, const double *u, double tol, sint_strea
     }
   cudaError_t e = cudaSuccess;
   if (!c->mask)
-    {
-      c->n_cells = cell_count(c);
-      if ((e = cudaMalloc(&c->mask, sizeof(uint16_t) * (size_t)c->n_cells)) != cudaSuccess)
-        {
-          c->mask = nullptr;
-          return cuda_fail(e, "sint_set_component_mask: allocation");
-        }
-    }
-  const long long nb = (c->n_cells + 255) / 256;
+    if (int rc = allocate_cut(c))
+      return rc;
+  const long long nb = (c->n_cells + 255) / 256, nbt = (c->grid.n_tiles + 255) / 256;
   grain_mask_kernel<<<dim3((unsigned)nb), 256, 0, stream>>>(c->grid, c->G, u, tol, c->mask);
-  count_launches(1);
-  if ((e = cudaGetLastError()) != cudaSuccess)
+  if ((e = cudaMemsetAsync(c->cut_count, 0, sizeof(unsigned) * (SINT_MAX_GRAINS + 1), stream)) == cudaSuccess)
+    {
+      tile_union_kernel<<<dim3((unsigned)nbt), 256, 0, stream>>>(c->grid, c->mask, c->tile_union, c->cut_count);
+      class_scan_kernel<<<1, 32, 0, stream>>>(c->G, c->cut_count, c->cut_range);
+      class_scatter_kernel<<<dim3((unsigned)nbt), 256, 0, stream>>>(c->grid.n_tiles, c->tile_union, c->cut_count,
+                                                                    c->cut_tiles, c->cut_grains, c->cut_union);
+      count_launches(4);
+      e = cudaGetLastError();
+    }
+  if (e != cudaSuccess)
     return cuda_fail(e, "sint_set_component_mask");
   c->cut     = true;
   c->cut_tol = tol;

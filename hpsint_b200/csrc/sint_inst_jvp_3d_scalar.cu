@@ -4,7 +4,7 @@
 namespace sint
 {
   template cudaError_t launch_jvp<3, false, double>(int, const Grid &, const Phys &, const double *, const double *,
-                                                   double *, double *, const uint16_t *, cudaStream_t);
+                                                   double *, double *, const CutTiles *, cudaStream_t);
   template cudaError_t launch_jvp<3, false, float>(int, const Grid &, const Phys &, const float *, const float *,
-                                                  float *, float *, const uint16_t *, cudaStream_t);
+                                                  float *, float *, const CutTiles *, cudaStream_t);
 } // namespace sint

@@ -4,5 +4,5 @@
 namespace sint
 {
   template cudaError_t launch_residual<3, true>(int, int, const Grid &, const Phys &, const double *,
-                                                const double *const *, double *, double *, const uint16_t *, cudaStream_t);
+                                                const double *const *, double *, double *, const CutTiles *, cudaStream_t);
 } // namespace sint

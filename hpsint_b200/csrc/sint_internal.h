@@ -44,6 +44,14 @@ namespace sint
     long long n_cells = 0;
     bool      cut     = false;
     double    cut_tol = 0.0;
+    // tiles sorted into classes by their number of relevant grains (device)
+    int                *cut_tiles  = nullptr; // tile ids, class by class
+    unsigned long long *cut_grains = nullptr; // their packed grain lists
+    uint16_t           *cut_union  = nullptr; // their union masks
+    uint16_t           *tile_union = nullptr; // union mask by tile id (combine step)
+    int                *cut_range  = nullptr; // class offsets, SINT_MAX_GRAINS + 2
+    unsigned           *cut_count  = nullptr; // class sizes / scatter cursors, SINT_MAX_GRAINS + 1
+    CutTiles            cut_view;             // the above as the kernels take them
 
     double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
     double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
@@ -96,8 +104,10 @@ namespace sint
 
   // Validates and fills the operator description of c (no allocation).
   int describe_operator(const sint_mesh *mesh, const sint_params *params, Ctx *c);
-  // Cell masks the kernels use: c->mask with the cut-off on, else nullptr.
+  // Cell masks / tile classes the kernels use: with the cut-off on, else nullptr.
   inline const uint16_t *active_mask(const Ctx *c) { return c->cut ? c->mask : nullptr; }
+  inline const CutTiles *active_cut(const Ctx *c) { return c->cut ? &c->cut_view : nullptr; }
+  inline const uint16_t *active_tile_union(const Ctx *c) { return c->cut ? c->tile_union : nullptr; }
   // J v through the cell kernel + combine, with c->partial as scratch.
   template <typename R>
   cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s);

@@ -192,8 +192,8 @@ namespace sint
     if constexpr (TENS)
       fgrad<DIM>(F, FM::base(FM::lin_c), q, cell, gc);
     fgrad<DIM>(F, FM::base(FM::lin_mu), q, cell, gmu);
-    R eta[G];
-    R geta[TENS ? G : 1][DIM];
+    R eta[gdim(G)];
+    R geta[TENS ? gdim(G) : 1][DIM];
 #pragma unroll
     for (int i = 0; i < G; ++i)
       {
@@ -207,7 +207,7 @@ namespace sint
       fgrad<DIM>(F, FM::base(FM::src_c), q, cell, gdc);
     dmu = fval<DIM>(F, FM::base(FM::src_mu), q, cell);
     fgrad<DIM>(F, FM::base(FM::src_mu), q, cell, gdmu);
-    R deta[G];
+    R deta[gdim(G)];
 #pragma unroll
     for (int i = 0; i < G; ++i)
       deta[i] = fval<DIM>(F, FM::base(FM::src_eta(i)), q, cell);
@@ -272,8 +272,8 @@ namespace sint
       fgrad<DIM>(F, FM::base(FM::lin_c), q, cell, gc);
     mu = fval<DIM>(F, FM::base(FM::lin_mu), q, cell);
     fgrad<DIM>(F, FM::base(FM::lin_mu), q, cell, gmu);
-    R eta[G];
-    R geta[TENS ? G : 1][DIM];
+    R eta[gdim(G)];
+    R geta[TENS ? gdim(G) : 1][DIM];
 #pragma unroll
     for (int i = 0; i < G; ++i)
       {
@@ -405,6 +405,18 @@ namespace sint
     return mask[i + (long long)g.n[0] * (j + (long long)g.n[1] * k)];
   }
 
+  // Cell mask m (bits = grains of the full operator) in the numbering of a
+  // tile's compacted grain list gl: bit k set when grain gl[k] is relevant.
+  template <int G>
+  __device__ __forceinline__ unsigned local_mask(unsigned m, unsigned long long gl)
+  {
+    unsigned r = 0;
+#pragma unroll
+    for (int kk = 0; kk < G; ++kk)
+      r |= ((m >> unsigned((gl >> (4 * kk)) & 15ull)) & 1u) << kk;
+    return r;
+  }
+
   template <int DIM, int G, bool TENS, bool JVP, bool HIST>
   struct ThreePhaseSmem
   {
@@ -443,11 +455,16 @@ namespace sint
     return (DIM == 3 && G > 5) ? 1 : 2;
   }
 
-  // CUT: grain cut-off with the per-cell masks `mask` (unused otherwise).
+  // CUT: grain cut-off.  The kernel instantiated for G grains runs over the
+  // tiles of class G, ct.tiles[ct.range[G] .. ct.range[G + 1]), on their
+  // compacted components (c, mu and the tile's G grains); a cell lacking one
+  // of the tile's grains treats it as absent.  The tile ids, grain lists and
+  // masks of the next tile are read one tile ahead, so their latency hides
+  // behind the current tile.
   template <int DIM, int G, bool TENS, typename R, bool CUT>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS, jvp_blocks_per_sm<DIM, G, R>())
     jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
-               R *__restrict__ dst, R *__restrict__ partial, const uint16_t *__restrict__ mask)
+               R *__restrict__ dst, R *__restrict__ partial, const CutTiles ct)
   {
     using T  = Tile<DIM>;
     using SM = ThreePhaseSmem<DIM, G, TENS, true, false>;
@@ -460,45 +477,92 @@ namespace sint
 
     const PhysR<R>           p(ph);
     const CellConsts<DIM, R> k(g);
-    long long                tile = blockIdx.x;
-    unsigned                 m_cur = ~0u, m_next = ~0u; // this and the next tile's cell masks
-    if (tile < g.n_tiles)
+    const int                cell = threadIdx.x % T::CELLS;
+    const long long          i0   = CUT ? (long long)ct.range[G] : 0;
+    const long long          i1   = CUT ? (long long)ct.range[G + 1] : g.n_tiles;
+    long long                idx  = i0 + blockIdx.x;
+    // current and next tile: id, grain list, union mask, this thread's cell mask
+    long long          tile = 0, t_next = 0;
+    unsigned long long gl = 0, gl_next = 0;
+    unsigned           tm = 0, tm_next = 0, m_glob = ~0u, m_glob_next = ~0u;
+    if constexpr (CUT)
+      {
+        if (idx < i1)
+          {
+            tile = ct.tiles[idx];
+            gl   = ct.tile_grains[idx];
+            tm   = ct.tile_mask[idx];
+          }
+        if (idx + gridDim.x < i1)
+          {
+            t_next  = ct.tiles[idx + gridDim.x];
+            gl_next = ct.tile_grains[idx + gridDim.x];
+            tm_next = ct.tile_mask[idx + gridDim.x];
+          }
+      }
+    else
+      tile = idx;
+    if (idx < i1)
       {
         const TileCoord    tc0 = tile_coord_of<DIM>(g, tile);
         const BoxNode<DIM> bn(g, tc0);
-        load_box_async<DIM>(s_buf, lin, C, g, bn);
-        load_box_async<DIM>(s_buf + C * T::BOX, src, C, g, bn);
+        load_box_async<DIM>(s_buf, lin, C, g, bn, gl, CUT);
+        load_box_async<DIM>(s_buf + C * T::BOX, src, C, g, bn, gl, CUT);
         if constexpr (CUT)
-          m_cur = cell_mask<DIM>(mask, g, tc0, threadIdx.x % T::CELLS);
+          m_glob = cell_mask<DIM>(ct.cell_mask, g, tc0, cell);
       }
     cp_async_commit();
-    for (int it = 0; tile < g.n_tiles; ++it, tile += gridDim.x)
+    for (int it = 0; idx < i1; ++it, idx += gridDim.x)
       {
-        const long long next = tile + gridDim.x;
+        const long long nidx = idx + gridDim.x;
         R              *nb   = s_buf + ((it + 1) & 1) * SM::BOXES;
-        if (next < g.n_tiles)
+        long long       t_nn = 0; // the tile after next (CUT)
+        unsigned long long gl_nn = 0;
+        unsigned           tm_nn = 0;
+        if (nidx < i1)
           {
-            const TileCoord    tcn = tile_coord_of<DIM>(g, next);
+            const long long    next = CUT ? t_next : nidx;
+            const TileCoord    tcn  = tile_coord_of<DIM>(g, next);
             const BoxNode<DIM> bnn(g, tcn);
-            load_box_async<DIM>(nb, lin, C, g, bnn);
-            load_box_async<DIM>(nb + C * T::BOX, src, C, g, bnn);
+            load_box_async<DIM>(nb, lin, C, g, bnn, gl_next, CUT);
+            load_box_async<DIM>(nb + C * T::BOX, src, C, g, bnn, gl_next, CUT);
             if constexpr (CUT)
-              m_next = cell_mask<DIM>(mask, g, tcn, threadIdx.x % T::CELLS);
+              {
+                m_glob_next = cell_mask<DIM>(ct.cell_mask, g, tcn, cell);
+                if (nidx + gridDim.x < i1)
+                  {
+                    t_nn  = ct.tiles[nidx + gridDim.x];
+                    gl_nn = ct.tile_grains[nidx + gridDim.x];
+                    tm_nn = ct.tile_mask[nidx + gridDim.x];
+                  }
+              }
           }
         cp_async_commit();
         cp_async_wait<1>(); // this tile's group has landed (only the prefetch may be pending)
         __syncthreads();
         const TileCoord tc = tile_coord_of<DIM>(g, tile);
         const R        *cb = s_buf + (it & 1) * SM::BOXES;
-        phase_evaluate<DIM, G, TENS, true, false, R, CUT>(cb, cb + C * T::BOX, F, k, m_cur);
+        const unsigned  m  = CUT ? local_mask<G>(m_glob, gl) : ~0u;
+        phase_evaluate<DIM, G, TENS, true, false, R, CUT>(cb, cb + C * T::BOX, F, k, m);
         __syncthreads();
-        jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS, m_cur);
+        jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, cell, m);
         __syncthreads();
-        phase_integrate<DIM, G, R, CUT>(p, g, k, tc, P, cb + C * T::BOX, K, m_cur);
+        phase_integrate<DIM, G, R, CUT>(p, g, k, tc, P, cb + C * T::BOX, K, m);
         __syncthreads();
-        m_cur = m_next;
-        sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial);
+        sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
         __syncthreads(); // K and this buffer are reused by the next iterations
+        if constexpr (CUT)
+          {
+            tile    = t_next;
+            gl      = gl_next;
+            tm      = tm_next;
+            m_glob  = m_glob_next;
+            t_next  = t_nn;
+            gl_next = gl_nn;
+            tm_next = tm_nn;
+          }
+        else
+          tile = nidx;
       }
     cp_async_wait<0>();
   }
@@ -508,11 +572,13 @@ namespace sint
   // (operator_sintering_generic.h:254-308) with the history of
   // do_evalute_history (:927-975) for WTD == 2: the weighted sum of the old
   // solutions is formed at the nodes while staging and evaluated at the points.
+  // CUT: the kernel for G grains runs over the tiles of class G on their
+  // compacted components, as the Jacobian product does.
   template <int DIM, int G, bool TENS, int WTD, bool CUT>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS, residual_blocks_per_sm<DIM, G>())
     residual_kernel(const Grid g, const Phys ph, const double *__restrict__ src, const double *__restrict__ h0,
                     const double *__restrict__ h1, const double *__restrict__ h2, double *__restrict__ dst,
-                    double *__restrict__ partial, const uint16_t *__restrict__ mask)
+                    double *__restrict__ partial, const CutTiles ct)
   {
     using R  = double;
     using T  = Tile<DIM>;
@@ -527,12 +593,17 @@ namespace sint
 
     const PhysR<R>           p(ph);
     const CellConsts<DIM, R> k(g);
-    for (long long tile = blockIdx.x; tile < g.n_tiles; tile += gridDim.x)
+    const long long          i0 = CUT ? (long long)ct.range[G] : 0;
+    const long long          i1 = CUT ? (long long)ct.range[G + 1] : g.n_tiles;
+    for (long long idx = i0 + blockIdx.x; idx < i1; idx += gridDim.x)
       {
-        const TileCoord    tc = tile_coord_of<DIM>(g, tile);
-        const BoxNode<DIM> bn(g, tc);
-        const unsigned     m  = CUT ? cell_mask<DIM>(mask, g, tc, threadIdx.x % T::CELLS) : ~0u;
-        load_box<DIM>(s_u, src, C, g, bn);
+        const long long          tile = CUT ? (long long)ct.tiles[idx] : idx;
+        const unsigned long long gl   = CUT ? ct.tile_grains[idx] : 0ull;
+        const unsigned           tm   = CUT ? ct.tile_mask[idx] : 0u;
+        const TileCoord          tc   = tile_coord_of<DIM>(g, tile);
+        const BoxNode<DIM>       bn(g, tc);
+        const unsigned m = CUT ? local_mask<G>(cell_mask<DIM>(ct.cell_mask, g, tc, threadIdx.x % T::CELLS), gl) : ~0u;
+        load_box<DIM>(s_u, src, C, g, bn, gl, CUT);
         if constexpr (WTD == 2)
           {
             // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966); mu has no history
@@ -542,7 +613,7 @@ namespace sint
                   R v = R(0);
                   if (comp != 1 && bn.inside)
                     {
-                      const long long off = comp * g.ld + bn.gidx;
+                      const long long off = (CUT ? comp_of(comp, gl) : comp) * g.ld + bn.gidx;
                       v                   = h0[off] * ph.w_hist[0];
                       if (ph.order > 1)
                         v += h1[off] * ph.w_hist[1];
@@ -559,7 +630,7 @@ namespace sint
         __syncthreads();
         phase_integrate<DIM, G, R, CUT>(p, g, k, tc, P, s_u, K, m);
         __syncthreads();
-        sum_and_store<DIM>(K, C, g, tc, bn, dst, partial);
+        sum_and_store<DIM>(K, C, g, tc, bn, dst, partial, gl, CUT, ct.c_all, tm);
         __syncthreads();
       }
   }

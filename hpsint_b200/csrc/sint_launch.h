@@ -15,22 +15,26 @@ namespace sint
   // Dynamic shared memory of the diagonal kernel (bytes).
   size_t smem_diag(int dim, int G);
 
-  // mask: per-cell grain masks of the grain cut-off, nullptr for the full operator
+  // cut: the grain cut-off's tile classes, nullptr for the full operator
   template <int DIM, bool TENS, typename R>
   cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                         const uint16_t *mask, cudaStream_t s);
+                         const CutTiles *cut, cudaStream_t s);
 
   template <int DIM, bool TENS>
   cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
-                              const double *const *hist, double *dst, double *partial, const uint16_t *mask,
+                              const double *const *hist, double *dst, double *partial, const CutTiles *cut,
                               cudaStream_t s);
 
+  // mask: the cut-off's per-cell grain masks, nullptr for the full operator
   template <int DIM, bool TENS>
   cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
                           const uint16_t *mask, cudaStream_t s);
 
+  // tile_mask: per tile id, the grains whose partials the tile wrote (grain
+  // cut-off); nullptr = every component of every tile
   template <int DIM, typename R>
-  cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, cudaStream_t s);
+  cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, const uint16_t *tile_mask,
+                             cudaStream_t s);
 
   // Counts kernel launches issued by this library.
   void count_launches(int n);

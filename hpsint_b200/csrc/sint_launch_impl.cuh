@@ -29,7 +29,7 @@ namespace sint
 
   template <int DIM, int G, bool TENS, typename R, bool CUT>
   cudaError_t launch_jvp_g(const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                           const uint16_t *mask, cudaStream_t s)
+                           const CutTiles &ct, cudaStream_t s)
   {
     const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false>::TOTAL * sizeof(R);
     auto         k    = jvp_kernel<DIM, G, TENS, R, CUT>;
@@ -48,14 +48,14 @@ namespace sint
         grid_cap = sms * (per_sm > 0 ? per_sm : 1);
       }
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
-    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, mask);
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, ct);
     count_launches(1);
     return cudaGetLastError();
   }
 
   template <int DIM, int G, bool TENS, int WTD, bool CUT>
   cudaError_t launch_residual_g(const Grid &g, const Phys &p, const double *src, const double *const *hist,
-                                double *dst, double *partial, const uint16_t *mask, cudaStream_t s)
+                                double *dst, double *partial, const CutTiles &ct, cudaStream_t s)
   {
     const size_t  smem     = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2>::TOTAL * sizeof(double);
     auto          k        = residual_kernel<DIM, G, TENS, WTD, CUT>;
@@ -76,7 +76,7 @@ namespace sint
     const double *h1     = (WTD == 2 && p.order > 1) ? hist[1] : nullptr;
     const double *h2     = (WTD == 2 && p.order > 2) ? hist[2] : nullptr;
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
-    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial, mask);
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial, ct);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -113,54 +113,97 @@ namespace sint
       default: return cudaErrorInvalidValue;                                                                      \
     }
 
-  // mask == nullptr: the full operator; otherwise the grain cut-off with these cell masks
+  // The same over the grain-count classes 0..12 of the grain cut-off.
+#define SINT_CLASS_SWITCH(K, CALL)                                                                                \
+  switch (K)                                                                                                      \
+    {                                                                                                             \
+      case 0: return CALL(0);                                                                                     \
+      case 1: return CALL(1);                                                                                     \
+      case 2: return CALL(2);                                                                                     \
+      case 3: return CALL(3);                                                                                     \
+      case 4: return CALL(4);                                                                                     \
+      case 5: return CALL(5);                                                                                     \
+      case 6: return CALL(6);                                                                                     \
+      case 7: return CALL(7);                                                                                     \
+      case 8: return CALL(8);                                                                                     \
+      case 9: return CALL(9);                                                                                     \
+      case 10: return CALL(10);                                                                                   \
+      case 11: return CALL(11);                                                                                   \
+      case 12: return CALL(12);                                                                                   \
+      default: return cudaErrorInvalidValue;                                                                      \
+    }
+
+  template <int DIM, bool TENS, typename R>
+  cudaError_t launch_jvp_class(int K, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
+                               const CutTiles &ct, cudaStream_t s)
+  {
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, true>(g, p, lin, src, dst, partial, ct, s)
+    SINT_CLASS_SWITCH(K, SINT_CALL)
+#undef SINT_CALL
+  }
+
+  // cut == nullptr: the full operator; otherwise the grain cut-off, one
+  // launch per grain-count class 0..G (classes without tiles return at once)
   template <int DIM, bool TENS, typename R>
   cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                         const uint16_t *mask, cudaStream_t s)
+                         const CutTiles *cut, cudaStream_t s)
   {
-    if (mask)
+    if (cut)
       {
-#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, true>(g, p, lin, src, dst, partial, mask, s)
-        SINT_G_SWITCH(SINT_CALL)
-#undef SINT_CALL
+        for (int K = 0; K <= G; ++K)
+          if (const cudaError_t e = launch_jvp_class<DIM, TENS, R>(K, g, p, lin, src, dst, partial, *cut, s))
+            return e;
+        return cudaSuccess;
       }
-#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, false>(g, p, lin, src, dst, partial, nullptr, s)
+    const CutTiles none;
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, false>(g, p, lin, src, dst, partial, none, s)
     SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+  }
+
+  // G = the grain count (full operator, 1..12) or the class (grain cut-off, 0..12)
+  template <int DIM, bool TENS, bool CUT, int WTD>
+  cudaError_t launch_residual_w(int G, const Grid &g, const Phys &p, const double *src, const double *const *hist,
+                                double *dst, double *partial, const CutTiles &ct, cudaStream_t s)
+  {
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, WTD, CUT>(g, p, src, hist, dst, partial, ct, s)
+    if constexpr (CUT)
+      {
+        SINT_CLASS_SWITCH(G, SINT_CALL)
+      }
+    else
+      {
+        SINT_G_SWITCH(SINT_CALL)
+      }
 #undef SINT_CALL
   }
 
   template <int DIM, bool TENS, bool CUT>
   cudaError_t launch_residual_c(int G, int wtd, const Grid &g, const Phys &p, const double *src,
-                                const double *const *hist, double *dst, double *partial, const uint16_t *mask,
+                                const double *const *hist, double *dst, double *partial, const CutTiles &ct,
                                 cudaStream_t s)
   {
     if (wtd == 0)
-      {
-#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 0, CUT>(g, p, src, hist, dst, partial, mask, s)
-        SINT_G_SWITCH(SINT_CALL)
-#undef SINT_CALL
-      }
-    else if (wtd == 1)
-      {
-#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 1, CUT>(g, p, src, hist, dst, partial, mask, s)
-        SINT_G_SWITCH(SINT_CALL)
-#undef SINT_CALL
-      }
-    else
-      {
-#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, 2, CUT>(g, p, src, hist, dst, partial, mask, s)
-        SINT_G_SWITCH(SINT_CALL)
-#undef SINT_CALL
-      }
+      return launch_residual_w<DIM, TENS, CUT, 0>(G, g, p, src, hist, dst, partial, ct, s);
+    if (wtd == 1)
+      return launch_residual_w<DIM, TENS, CUT, 1>(G, g, p, src, hist, dst, partial, ct, s);
+    return launch_residual_w<DIM, TENS, CUT, 2>(G, g, p, src, hist, dst, partial, ct, s);
   }
 
   template <int DIM, bool TENS>
   cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
-                              const double *const *hist, double *dst, double *partial, const uint16_t *mask,
+                              const double *const *hist, double *dst, double *partial, const CutTiles *cut,
                               cudaStream_t s)
   {
-    return mask ? launch_residual_c<DIM, TENS, true>(G, wtd, g, p, src, hist, dst, partial, mask, s)
-                : launch_residual_c<DIM, TENS, false>(G, wtd, g, p, src, hist, dst, partial, nullptr, s);
+    if (cut)
+      {
+        for (int K = 0; K <= G; ++K)
+          if (const cudaError_t e =
+                launch_residual_c<DIM, TENS, true>(K, wtd, g, p, src, hist, dst, partial, *cut, s))
+            return e;
+        return cudaSuccess;
+      }
+    return launch_residual_c<DIM, TENS, false>(G, wtd, g, p, src, hist, dst, partial, CutTiles(), s);
   }
 
   template <int DIM, bool TENS>

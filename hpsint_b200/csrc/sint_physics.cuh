@@ -111,7 +111,7 @@ namespace sint
   // Residual flux of the c row: M(c, eta, grad c, grad eta) grad mu
   // scalar: mobility.h:439-472, tensorial: mobility.h:756-804
   template <int DIM, int G, bool TENS, typename R>
-  __device__ __forceinline__ void apply_M(const PhysR<R> &p, R c, const R (&eta)[G], const R (&gc)[DIM],
+  __device__ __forceinline__ void apply_M(const PhysR<R> &p, R c, const R (&eta)[gdim(G)], const R (&gc)[DIM],
                                           const R (*geta)[DIM], const R (&gmu)[DIM], R (&out)[DIM],
                                           unsigned m = ~0u)
   {
@@ -180,9 +180,9 @@ namespace sint
   // grad dmu, deta).  scalar: mobility.h:476-534, tensorial: mobility.h:808-916
   template <int DIM, int G, bool TENS, typename R>
   __device__ __forceinline__ void apply_M_derivative(const PhysR<R> &p, R c, const R (&gc)[DIM],
-                                                     const R (&gmu)[DIM], const R (&eta)[G], const R (*geta)[DIM],
+                                                     const R (&gmu)[DIM], const R (&eta)[gdim(G)], const R (*geta)[DIM],
                                                      R dc, const R (&gdc)[DIM], const R (&gdmu)[DIM],
-                                                     const R (&deta)[G], R (&out)[DIM], unsigned m = ~0u)
+                                                     const R (&deta)[gdim(G)], R (&out)[DIM], unsigned m = ~0u)
   {
     const R phi = phi_clamped(c);
     const R omc = R(1) - c;
