@@ -888,8 +888,8 @@ int oracle_ch_blocks(const oracle_mesh *m, const oracle_params *p, const oracle_
     return e;
   const Geometry geo(*m);
   const Mobility mob = make_mobility(m, p);
-  const int      G = p->n_grains, nq = geo.nq;
-  const int64_t  N = geo.n_nodes;
+  const int      nq  = geo.nq;
+  const int64_t  N   = geo.n_nodes;
   std::memset(blocks, 0, sizeof(double) * 4 * N);
   coloured_cell_loop(geo, n_threads, [&](int i, int j, int k) {
     int       blk[MAXC];
