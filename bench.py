@@ -381,8 +381,10 @@ def mixed_precision_solve_3d(args):
     vectors, Jacobian and block-Jacobi inside FP64 Newton) replays it.  Reports
     s/step of both and the FP32-inner run's errors against the FP64-inner run.
     With --cut-off TOL both solves run again on the same grid with the grain
-    cut-off (GrainCutOffTolerance = TOL), and the J v throughput at the initial
-    state is timed with and without it."""
+    cut-off (GrainCutOffTolerance = TOL; block-Jacobi from the full operator),
+    the FP32-inner one once more with the preconditioner cut as well (the
+    reference's assembly), and the J v throughput at the initial state is
+    timed with and without the cut-off."""
     import torch
 
     import hpsint_b200 as hb
@@ -402,12 +404,15 @@ def mixed_precision_solve_3d(args):
     c0 = float(np.einsum("k,j,i,kji->", w, w, w, u0[0].reshape(n + 1, n + 1, n + 1)))
     del u0
     operator_rates = cut_off_operator_rates(op, u0d, args.cut_off) if args.cut_off > 0 else None
-    arms = [("fp64_inner", 64, 0.0), ("fp32_inner", 32, 0.0)]
+    # (label, Krylov precision, cut-off tolerance, preconditioner with the cut-off too)
+    arms = [("fp64_inner", 64, 0.0, False), ("fp32_inner", 32, 0.0, False)]
     if args.cut_off > 0:
-        arms += [("fp64_inner_cut_off", 64, args.cut_off), ("fp32_inner_cut_off", 32, args.cut_off)]
+        arms += [("fp64_inner_cut_off", 64, args.cut_off, False), ("fp32_inner_cut_off", 32, args.cut_off, False),
+                 ("fp32_inner_cut_off_cut_preconditioner", 32, args.cut_off, True)]
     runs, schedule = {}, None
-    for label, prec, tol in arms:
+    for label, prec, tol, cut_pc in arms:
         op.set_component_mask(u0d, tol)  # 0 switches a previous arm's cut-off off
+        op.set_preconditioner_cut_off(cut_pc)
         ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec),
                             TimeIntegrationData(time_step_init=1e-4), grain_cut_off_tolerance=tol)
         ti.initialize(u0d)
@@ -449,7 +454,7 @@ def mixed_precision_solve_3d(args):
     }
     if args.cut_off > 0:
         line["cut_off"] = {"tolerance": args.cut_off, "operator_at_initial_state": operator_rates}
-        for label in ("fp64_inner_cut_off", "fp32_inner_cut_off"):
+        for label in ("fp64_inner_cut_off", "fp32_inner_cut_off", "fp32_inner_cut_off_cut_preconditioner"):
             r = runs[label]
             st = np.sum(r["stats"], axis=0)
             line["cut_off"][label] = {

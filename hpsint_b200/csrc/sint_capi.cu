@@ -97,11 +97,11 @@ namespace sint
     const bool t = c->params.tensorial != 0;
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_diag<3, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s)
-            : launch_diag<3, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s);
+      e = t ? launch_diag<3, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s)
+            : launch_diag<3, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s);
     else
-      e = t ? launch_diag<2, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s)
-            : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, active_mask(c), s);
+      e = t ? launch_diag<2, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s)
+            : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s);
     if (e != cudaSuccess)
       return e;
     return c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s)

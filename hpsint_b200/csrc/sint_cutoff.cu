@@ -215,6 +215,17 @@ int sint_set_component_mask(sint_ctx *c, const double *u, double tol, sint_strea
   return SINT_OK;
 }
 
+int sint_set_preconditioner_cut_off(sint_ctx *c, int on)
+{
+  if (!c)
+    {
+      set_error("null context");
+      return SINT_ERR_ARG;
+    }
+  c->pc_cut = on != 0;
+  return SINT_OK;
+}
+
 int sint_component_mask_statistics(sint_ctx *c, int64_t *counts, sint_stream_t stream)
 {
   if (!c || !counts)

@@ -44,6 +44,7 @@ namespace sint
     long long n_cells = 0;
     bool      cut     = false;
     double    cut_tol = 0.0;
+    bool      pc_cut  = false; // preconditioner diagonals with the cut-off too (else from the full operator)
     // tiles sorted into classes by their number of relevant grains (device)
     int                *cut_tiles  = nullptr; // tile ids, class by class
     unsigned long long *cut_grains = nullptr; // their packed grain lists
@@ -106,6 +107,7 @@ namespace sint
   int describe_operator(const sint_mesh *mesh, const sint_params *params, Ctx *c);
   // Cell masks / tile classes the kernels use: with the cut-off on, else nullptr.
   inline const uint16_t *active_mask(const Ctx *c) { return c->cut ? c->mask : nullptr; }
+  inline const uint16_t *preconditioner_mask(const Ctx *c) { return c->pc_cut ? active_mask(c) : nullptr; }
   inline const CutTiles *active_cut(const Ctx *c) { return c->cut ? &c->cut_view : nullptr; }
   inline const uint16_t *active_tile_union(const Ctx *c) { return c->cut ? c->tile_union : nullptr; }
   // J v through the cell kernel + combine, with c->partial as scratch.

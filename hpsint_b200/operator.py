@@ -168,15 +168,22 @@ class SinteringOperatorGeneric:
         """Grain cut-off (SinteringOperatorData::set_component_mask,
         operator_sintering_data.h:149-298): grain b is relevant on a cell when
         max |eta_b| over the cell's nodes of `src` exceeds the tolerance; the
-        residual, the Jacobian products and the preconditioner then treat
-        every cell with its relevant grains only.  Tolerance 0 switches the
-        cut-off off (GrainCutOffTolerance, parameters.h:314)."""
+        residual and the Jacobian products then treat every cell with its
+        relevant grains only (the preconditioner too after
+        set_preconditioner_cut_off(True)).  Tolerance 0 switches the cut-off
+        off (GrainCutOffTolerance, parameters.h:314)."""
         tol = float(grain_use_cut_off_tolerance)
         if tol != 0.0:
             self._check_vec(src, torch.float64)
         L.check(L.lib().sint_set_component_mask(self._h, _ptr(src) if tol != 0.0 else None, tol, _stream()),
                 "sint_set_component_mask")
         self.cut_off_tolerance = tol
+
+    def set_preconditioner_cut_off(self, on):
+        """Build the block preconditioner with the grain cut-off too (the
+        reference's assembly, preconditioners.h:787-817) instead of from the
+        full operator (the default); takes effect at the next set-up."""
+        L.check(L.lib().sint_set_preconditioner_cut_off(self._h, int(bool(on))), "sint_set_preconditioner_cut_off")
 
     def component_mask_statistics(self):
         """numpy array: entry k = number of cells with k relevant grains

@@ -182,18 +182,30 @@ int sint_ch_blocks_f64(sint_ctx *ctx, double *blocks, sint_stream_t stream);
 
 /* Marks grain b relevant on a cell when max |eta_b| over the cell's nodes
  * exceeds tol (u: C blocks of block_stride, device).  While set, the
- * context's residual, both Jacobian-vector products, the preconditioner and
- * the Newton solver restrict every cell to its relevant grains (the
- * context-free sint_jvp_f64_noalloc always applies the full operator), as
+ * context's residual, both Jacobian-vector products and the Newton solver
+ * restrict every cell to its relevant grains (the context-free
+ * sint_jvp_f64_noalloc always applies the full operator), as
  * do_evaluate_nonlinear_residual_nt and
  * do_vmult_range_no_template (operator_sintering_generic.h:456-537,
  * :1008-1081) and the Allen-Cahn preconditioner block
  * (preconditioners.h:787-817, :865-882) do: an absent grain contributes
  * nothing to the cell's sums and its row receives nothing from the cell.
+ * The preconditioner's diagonals come from the full operator unless
+ * sint_set_preconditioner_cut_off switches the cut-off on for them too.
  * The reference forms the union over the cells of one SIMD batch; this
  * library keeps one set per cell.  tol == 0 switches the cut-off off;
  * tol < 0 is SINT_ERR_ARG.  The first call allocates one uint16 per cell. */
 int sint_set_component_mask(sint_ctx *ctx, const double *u, double tol, sint_stream_t stream);
+
+/* Whether sint_precond_setup applies the grain cut-off as well (on != 0):
+ * the Allen-Cahn diagonal then drops absent grains' contributions and empty
+ * diagonals invert to 1, as the reference's matrix-based block does
+ * (preconditioners.h:787-817, :865-882).  Default off: the block-Jacobi
+ * diagonals come from the full operator, which changes only how fast GMRES
+ * converges (at a grain's cut boundary the assembled-from-relevant-cells
+ * rows are poorly scaled by their partial diagonals), not the Newton system
+ * or its solution.  Takes effect at the next sint_precond_setup. */
+int sint_set_preconditioner_cut_off(sint_ctx *ctx, int on);
 
 /* The "Cut-off statistic" (operator_sintering_data.h:236-296): counts[k]
  * (host, n_grains + 1 entries) = number of cells with k relevant grains.

@@ -118,12 +118,16 @@ def test_cut_off_preconditioner_matches_oracle(case):
     op.set_time_weights(40.0, [-40.0], 1.0)
     op.fill_quadrature_point_values(ud)
     pc = hb.BlockPreconditioner2(op)
-    pc.do_update()
     T = O.make_time(40.0, 1.0, [-40.0])
     N = op.N
-    assert block_rel_err(pc.ch_blocks()[:, :N].cpu().numpy(), O.ch_blocks(om, p, T, u, mask=mask)) <= 1e-12
-    inv_ref = O.inverse_diagonal(O.ac_diagonal(om, p, T, u, mask=mask))
-    assert block_rel_err(pc.inverse_diagonal()[:, :N].cpu().numpy(), inv_ref) <= 1e-12
+    # default: the block-Jacobi diagonals of the full operator; switched on:
+    # the reference's cut-off assembly (preconditioners.h:787-817)
+    for cut_pc, m in ((False, None), (True, mask)):
+        op.set_preconditioner_cut_off(cut_pc)
+        pc.do_update()
+        assert block_rel_err(pc.ch_blocks()[:, :N].cpu().numpy(), O.ch_blocks(om, p, T, u, mask=m)) <= 1e-12
+        inv_ref = O.inverse_diagonal(O.ac_diagonal(om, p, T, u, mask=m))
+        assert block_rel_err(pc.inverse_diagonal()[:, :N].cpu().numpy(), inv_ref) <= 1e-12
 
 
 def test_tolerance_zero_restores_the_full_operator_bitwise():
