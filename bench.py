@@ -50,7 +50,8 @@ def parse_args():
     ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "nnconv"],
+    ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "nnconv",
+                                           "cutoff"],
                     default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
@@ -465,10 +466,35 @@ def mixed_precision_solve_3d(args):
     print(json.dumps(line), flush=True)
 
 
-def cut_off_operator_rates(op, u, tol, reps=20):
+def cut_off_operator(args):
+    """Operator throughput with and without the grain cut-off (tolerance
+    --cut-off, 1e-5 if unset) at the initial state of the 3D solve workload
+    (--n3, --spheres, --median, --sigma, --max-grains; C3 by default)."""
+    import torch
+
+    import hpsint_b200 as hb
+    from hpsint_b200 import packings as P
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, tol = args.n3, args.cut_off if args.cut_off > 0 else 1e-5
+    centers, radii, colours = P.lognormal_packing_3d(n=n, n_spheres=args.spheres, median=args.median,
+                                                     sigma=args.sigma, max_grains=args.max_grains)
+    G = int(colours.max()) + 1
+    u0 = P.initial_state(3, (n, n, n), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), centers, radii, colours, width=2.0)
+    op = hb.SinteringOperatorGeneric(hb.Mesh(3, (n, n, n)), hb.Params(**model_params(G, not args.scalar)))
+    u0d = op.to_device(u0)
+    del u0
+    rates = cut_off_operator_rates(op, u0d, tol, reps=args.steps, warmup=args.warmup)
+    print(json.dumps({"metric": "Jacobian-vec GDoF/s with and without the grain cut-off", "unit": "GDoF/s",
+                      "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-median{args.median:g}-G{G}",
+                      "dofs": op.C * op.N, "grains": G, "tolerance": tol, "steps": args.steps,
+                      "warmup": args.warmup, "data": "synthetic seeded packing", **rates}), flush=True)
+
+
+def cut_off_operator_rates(op, u, tol, reps=20, warmup=3):
     """GDoF/s of the FP64/FP32 Jacobian-vector products and the residual at
     state u, without and with the grain cut-off at tolerance tol (CUDA events
-    on the current stream, 3 warm-up calls)."""
+    on the current stream after `warmup` calls)."""
     import torch
 
     op.set_time_weights(1e4, [-1e4], 1.0)
@@ -486,7 +512,7 @@ def cut_off_operator_rates(op, u, tol, reps=20):
                 src = torch.rand((op.C, op.ld), dtype=dt, device="cuda", generator=gen) - 0.5
                 dst = op.initialize_dof_vector(dt)
                 fn = lambda: op.vmult(dst, src)  # noqa: E731
-            for _ in range(3):
+            for _ in range(warmup):
                 fn()
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             ev[0].record(stream)
@@ -576,6 +602,9 @@ def main():
         return
     if args.workload == "solve3d":
         mixed_precision_solve_3d(args)
+        return
+    if args.workload == "cutoff":
+        cut_off_operator(args)
         return
     if args.workload == "learned2d":
         learned_guess_solve(args)

@@ -604,22 +604,35 @@ namespace sint
       }
     if (!shared)
       return;
+    // the (up to 8) tiles sharing the node, in a fixed order: the node's slot
+    // in each tile's partials and the grains each tile wrote
+    long long slot[8];
+    unsigned  tm[8];
+    bool      has[8];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc)
+          {
+            const int k = 4 * a + 2 * bb + cc;
+            has[k]      = a < nt[2] && bb < nt[1] && cc < nt[0];
+            const int       ti = t0[0] + cc, tj = t0[1] + bb, tk = t0[2] + a;
+            const int       bx = lo[0] - cc * TT[0], by = lo[1] - bb * TT[1], bz = lo[2] - a * TT[2];
+            const long long tile = ti + (long long)g.nt[0] * (tj + (long long)g.nt[1] * tk);
+            slot[k] = tile * ncomp * (long long)T::BOX + bx + T::BX * (by + T::BY * bz);
+            tm[k]   = (has[k] && tile_mask) ? unsigned(tile_mask[tile]) : ~0u;
+          }
     // 2D: one component per thread (blockIdx.y); 3D: one thread loops over all components
     const int c_end = DIM == 2 ? comp + 1 : ncomp;
     for (int cp = DIM == 2 ? comp : 0; cp < c_end; ++cp)
       {
         R sum = R(0);
-        for (int a = 0; a < nt[2]; ++a)
-          for (int bb = 0; bb < nt[1]; ++bb)
-            for (int cc = 0; cc < nt[0]; ++cc)
-              {
-                const int       ti = t0[0] + cc, tj = t0[1] + bb, tk = t0[2] + a;
-                const int       bx = lo[0] - cc * TT[0], by = lo[1] - bb * TT[1], bz = lo[2] - a * TT[2];
-                const long long tile = ti + (long long)g.nt[0] * (tj + (long long)g.nt[1] * tk);
-                if (tile_mask && cp >= 2 && ((tile_mask[tile] >> (cp - 2)) & 1u) == 0u)
-                  continue;
-                sum += partial[(tile * ncomp + cp) * (long long)T::BOX + bx + T::BX * (by + T::BY * bz)];
-              }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (has[k] && (cp < 2 || ((tm[k] >> (cp - 2)) & 1u) != 0u))
+            sum += partial[slot[k] + cp * (long long)T::BOX];
         dst[cp * g.ld + idx] = sum;
       }
   }

@@ -443,16 +443,17 @@ namespace sint
   // buffer while the current tile is computed.
   // Two resident blocks per SM (<= 128 registers) unless the 3D FP64 grain
   // state of large G would spill (one block, up to 255 registers); the light
-  // 2D FP32 product runs three (<= 85 registers).
+  // 2D FP32 product runs three (<= 85 registers), and the grain cut-off's
+  // G = 0 class (c and mu only) four (<= 64 registers).
   template <int DIM, int G, typename R>
   constexpr int jvp_blocks_per_sm()
   {
-    return (DIM == 3 && sizeof(R) == 8 && G > 5) ? 1 : (DIM == 2 && sizeof(R) == 4) ? 3 : 2;
+    return G == 0 ? 4 : (DIM == 3 && sizeof(R) == 8 && G > 5) ? 1 : (DIM == 2 && sizeof(R) == 4) ? 3 : 2;
   }
   template <int DIM, int G>
   constexpr int residual_blocks_per_sm()
   {
-    return (DIM == 3 && G > 5) ? 1 : 2;
+    return G == 0 ? 4 : (DIM == 3 && G > 5) ? 1 : 2;
   }
 
   // CUT: grain cut-off.  The kernel instantiated for G grains runs over the
