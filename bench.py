@@ -72,6 +72,8 @@ def parse_args():
     ap.add_argument("--circles", type=int, default=100)
     ap.add_argument("--save-net", default=None, help="write the trained predictor (.npz) here")
     ap.add_argument("--solve-steps", type=int, default=100)
+    ap.add_argument("--arms", default=None,
+                    help="solve3d: comma-separated subset of the arms to run (default: all)")
     ap.add_argument("--cut-off", type=float, default=0.0,
                     help="solve3d: also run both solves with this GrainCutOffTolerance and time the cut-off J v")
     return ap.parse_args()
@@ -410,6 +412,11 @@ def mixed_precision_solve_3d(args):
     if args.cut_off > 0:
         arms += [("fp64_inner_cut_off", 64, args.cut_off, False), ("fp32_inner_cut_off", 32, args.cut_off, False),
                  ("fp32_inner_cut_off_cut_preconditioner", 32, args.cut_off, True)]
+    if args.arms:
+        keep = args.arms.split(",")
+        arms = [a for a in arms if a[0] in keep]
+        if not arms:
+            raise SystemExit(f"--arms {args.arms}: no such arm")
     runs, schedule = {}, None
     for label, prec, tol, cut_pc in arms:
         op.set_component_mask(u0d, tol)  # 0 switches a previous arm's cut-off off
@@ -431,7 +438,7 @@ def mixed_precision_solve_3d(args):
         recs = ti.records
         runs[label] = dict(u=u, wall=wall, recs=recs, c_int=c_int, stats=list(ti.cut_off_statistics))
         del ti
-    ref, mp = runs["fp64_inner"], runs["fp32_inner"]
+    ref, mp = runs.get("fp64_inner"), runs.get("fp32_inner")
     line = {"metric": METRIC, "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-median{args.median:g}-G{G}",
             "unit": "s/step", "higher_is_better": False, "dofs": op.C * op.N, "grains": G,
             "steps": args.solve_steps, "dtype": "f64 Newton", "data": "synthetic seeded packing",
@@ -445,17 +452,20 @@ def mixed_precision_solve_3d(args):
                        "failed_tries": sum(x.failed_tries for x in recs),
                        "max_final_residual": max(x.final_residual for x in recs),
                        "int_c_rel_change": abs(r["c_int"] - c0) / abs(c0)}
-    line["fp32_inner_vs_fp64_inner"] = {
-        "max_abs_diff_c": float(np.abs(mp["u"][0] - ref["u"][0]).max()),
-        "max_abs_diff_eta": float(np.abs(mp["u"][2:] - ref["u"][2:]).max()),
-        "speedup_s_per_step": (ref["wall"] / len(ref["recs"])) / (mp["wall"] / len(mp["recs"])),
-        # failed FP64 attempts (dt halvings) fix the grid the FP32 run replays; without their time:
-        "speedup_accepted_attempts": sum(x.accepted_wall_s for x in ref["recs"]) /
-                                     sum(x.accepted_wall_s for x in mp["recs"]),
-    }
-    if args.cut_off > 0:
+    if ref and mp:
+        line["fp32_inner_vs_fp64_inner"] = {
+            "max_abs_diff_c": float(np.abs(mp["u"][0] - ref["u"][0]).max()),
+            "max_abs_diff_eta": float(np.abs(mp["u"][2:] - ref["u"][2:]).max()),
+            "speedup_s_per_step": (ref["wall"] / len(ref["recs"])) / (mp["wall"] / len(mp["recs"])),
+            # failed FP64 attempts (dt halvings) fix the grid the FP32 run replays; without their time:
+            "speedup_accepted_attempts": sum(x.accepted_wall_s for x in ref["recs"]) /
+                                         sum(x.accepted_wall_s for x in mp["recs"]),
+        }
+    if args.cut_off > 0 and ref:
         line["cut_off"] = {"tolerance": args.cut_off, "operator_at_initial_state": operator_rates}
         for label in ("fp64_inner_cut_off", "fp32_inner_cut_off", "fp32_inner_cut_off_cut_preconditioner"):
+            if label not in runs:
+                continue
             r = runs[label]
             st = np.sum(r["stats"], axis=0)
             line["cut_off"][label] = {

@@ -94,6 +94,17 @@ namespace sint
 
   inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+  // Live chunks (grain cut-off): bit k of live is clear when elements
+  // [k * LIVE_CHUNK, (k + 1) * LIVE_CHUNK) of every Krylov vector are known
+  // to be zero; nullptr = all live.  A warp's packs never straddle a chunk.
+  __device__ __forceinline__ bool chunk_live(const uint32_t *__restrict__ live, long long elem)
+  {
+    if (!live)
+      return true;
+    const long long k = elem / LIVE_CHUNK;
+    return (live[k >> 5] >> (k & 31)) & 1u;
+  }
+
   template <typename R>
   inline bool can_pack(long long n, long long stride, const void *a, const void *b)
   {
@@ -138,7 +149,7 @@ namespace sint
   __global__ void __launch_bounds__(RED_THREADS)
     multidot_kernel(long long nc, const R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
                     double *__restrict__ partial, const int *__restrict__ cond, const double *__restrict__ rows,
-                    int m_total, double *__restrict__ out, unsigned *ticket)
+                    int m_total, double *__restrict__ out, unsigned *ticket, const uint32_t *__restrict__ live)
   {
     if (cond && *cond == 0)
       return;
@@ -149,6 +160,8 @@ namespace sint
       acc[j] = 0.0;
     for (long long c = (long long)blockIdx.x * RED_THREADS + threadIdx.x; c < nc; c += (long long)NB_RED * RED_THREADS)
       {
+        if (!chunk_live(live, c * E))
+          continue;
         const Pack<R, E> wi = ld_pack<R, E>(w, c);
 #pragma unroll
         for (int j = 0; j < M; ++j)
@@ -176,7 +189,7 @@ namespace sint
 
   template <typename R>
   static int launch_multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out,
-                             cudaStream_t s, const int *cond = nullptr)
+                             cudaStream_t s, const int *cond = nullptr, const uint32_t *live = nullptr)
   {
     if (m < 1 || m > MAX_MULTIDOT)
       {
@@ -192,10 +205,10 @@ namespace sint
         double   *outl = j0 + MD >= m ? out : nullptr; // the last pass sums all rows
         if (pack)
           multidot_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, pp, cond,
-                                                                   c->red, m, outl, c->red_ticket);
+                                                                   c->red, m, outl, c->red_ticket, live);
         else
           multidot_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, pp, cond,
-                                                                   c->red, m, outl, c->red_ticket);
+                                                                   c->red, m, outl, c->red_ticket, live);
         count_launches(1);
       }
     const cudaError_t e = cudaGetLastError();
@@ -203,25 +216,26 @@ namespace sint
   }
 
   template <typename R>
-  int multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, cudaStream_t s)
+  int multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, cudaStream_t s,
+               const uint32_t *live)
   {
-    return launch_multidot<R>(c, n, w, V, stride, m, out, s);
+    return launch_multidot<R>(c, n, w, V, stride, m, out, s, nullptr, live);
   }
   template int multidot<double>(Ctx *, long long, const double *, const double *, long long, int, double *,
-                                cudaStream_t);
+                                cudaStream_t, const uint32_t *);
   template int multidot<float>(Ctx *, long long, const float *, const float *, long long, int, double *,
-                               cudaStream_t);
+                               cudaStream_t, const uint32_t *);
 
   template <typename R>
   int multidot_if(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, const int *cond,
-                  cudaStream_t s)
+                  cudaStream_t s, const uint32_t *live)
   {
-    return launch_multidot<R>(c, n, w, V, stride, m, out, s, cond);
+    return launch_multidot<R>(c, n, w, V, stride, m, out, s, cond, live);
   }
   template int multidot_if<double>(Ctx *, long long, const double *, const double *, long long, int, double *,
-                                   const int *, cudaStream_t);
+                                   const int *, cudaStream_t, const uint32_t *);
   template int multidot_if<float>(Ctx *, long long, const float *, const float *, long long, int, double *,
-                                  const int *, cudaStream_t);
+                                  const int *, cudaStream_t, const uint32_t *);
 
   int dot_f64(Ctx *c, long long n, const double *x, const double *y, double *out, cudaStream_t s)
   {
@@ -238,7 +252,7 @@ namespace sint
   __global__ void __launch_bounds__(RED_THREADS)
     multiaxpy_kernel(long long nc, R *__restrict__ w, const R *__restrict__ V, long long stride, int m,
                      const double *__restrict__ coef, double *__restrict__ partial, const int *__restrict__ cond,
-                     double *__restrict__ norm2_out, unsigned *ticket)
+                     double *__restrict__ norm2_out, unsigned *ticket, const uint32_t *__restrict__ live)
   {
     if (cond && *cond == 0)
       return;
@@ -250,6 +264,8 @@ namespace sint
     double nrm = 0.0;
     for (long long c = (long long)blockIdx.x * RED_THREADS + threadIdx.x; c < nc; c += (long long)gridDim.x * RED_THREADS)
       {
+        if (!chunk_live(live, c * E)) // w and every V_j are zero there: w stays zero
+          continue;
         Pack<R, E> acc = ld_pack<R, E>(w, c);
 #pragma unroll
         for (int j = 0; j < M; ++j)
@@ -279,7 +295,8 @@ namespace sint
 
   template <typename R>
   static int launch_multiaxpy(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
-                              double *norm2_out, cudaStream_t s, const int *cond = nullptr)
+                              double *norm2_out, cudaStream_t s, const int *cond = nullptr,
+                              const uint32_t *live = nullptr)
   {
     constexpr int E    = pack_of<R>();
     const bool    pack = can_pack<R>(n, stride, w, V);
@@ -290,10 +307,10 @@ namespace sint
         unsigned *tk   = c ? c->red_ticket : nullptr;
         if (pack)
           multiaxpy_kernel<R, MD, E><<<NB_RED, RED_THREADS, 0, s>>>(n / E, w, V + j0 * stride, stride, mm, coef + j0,
-                                                                    part, cond, norm2_out, tk);
+                                                                    part, cond, norm2_out, tk, live);
         else
           multiaxpy_kernel<R, MD, 1><<<NB_RED, RED_THREADS, 0, s>>>(n, w, V + j0 * stride, stride, mm, coef + j0,
-                                                                    part, cond, norm2_out, tk);
+                                                                    part, cond, norm2_out, tk, live);
         count_launches(1);
       }
     const cudaError_t e = cudaGetLastError();
@@ -310,30 +327,31 @@ namespace sint
 
   template <typename R>
   int multiaxpy_norm2(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
-                      double *norm2_out, cudaStream_t s)
+                      double *norm2_out, cudaStream_t s, const uint32_t *live)
   {
-    return launch_multiaxpy<R>(c, n, w, V, stride, m, coef, norm2_out, s);
+    return launch_multiaxpy<R>(c, n, w, V, stride, m, coef, norm2_out, s, nullptr, live);
   }
   template int multiaxpy_norm2<double>(Ctx *, long long, double *, const double *, long long, int, const double *,
-                                       double *, cudaStream_t);
+                                       double *, cudaStream_t, const uint32_t *);
   template int multiaxpy_norm2<float>(Ctx *, long long, float *, const float *, long long, int, const double *,
-                                      double *, cudaStream_t);
+                                      double *, cudaStream_t, const uint32_t *);
 
   template <typename R>
   int multiaxpy_norm2_if(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
-                         double *norm2_out, const int *cond, cudaStream_t s)
+                         double *norm2_out, const int *cond, cudaStream_t s, const uint32_t *live)
   {
-    return launch_multiaxpy<R>(c, n, w, V, stride, m, coef, norm2_out, s, cond);
+    return launch_multiaxpy<R>(c, n, w, V, stride, m, coef, norm2_out, s, cond, live);
   }
   template int multiaxpy_norm2_if<double>(Ctx *, long long, double *, const double *, long long, int, const double *,
-                                          double *, const int *, cudaStream_t);
+                                          double *, const int *, cudaStream_t, const uint32_t *);
   template int multiaxpy_norm2_if<float>(Ctx *, long long, float *, const float *, long long, int, const double *,
-                                         double *, const int *, cudaStream_t);
+                                         double *, const int *, cudaStream_t, const uint32_t *);
 
   // y += sum_j coef[j] V_j
   template <typename R, int M, int E>
   __global__ void __launch_bounds__(256) lincomb_kernel(long long nc, R *__restrict__ y, const R *__restrict__ V,
-                                                        long long stride, int m, const double *__restrict__ coef)
+                                                        long long stride, int m, const double *__restrict__ coef,
+                                                        const uint32_t *__restrict__ live)
   {
     __shared__ R s_c[M];
     if (threadIdx.x < M)
@@ -341,6 +359,8 @@ namespace sint
     __syncthreads();
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x)
       {
+        if (!chunk_live(live, c * E)) // y and every V_j are zero there
+          continue;
         Pack<R, E> acc = ld_pack<R, E>(y, c);
 #pragma unroll
         for (int j = 0; j < M; ++j)
@@ -356,7 +376,8 @@ namespace sint
   }
 
   template <typename R>
-  int lincomb(long long n, R *y, const R *V, long long stride, int m, const double *coef, cudaStream_t s)
+  int lincomb(long long n, R *y, const R *V, long long stride, int m, const double *coef, cudaStream_t s,
+              const uint32_t *live)
   {
     constexpr int E    = pack_of<R>();
     const bool    pack = can_pack<R>(n, stride, y, V);
@@ -364,27 +385,35 @@ namespace sint
       {
         const int mm = m - j0 < MD ? m - j0 : MD;
         if (pack)
-          lincomb_kernel<R, MD, E><<<1184, 256, 0, s>>>(n / E, y, V + j0 * stride, stride, mm, coef + j0);
+          lincomb_kernel<R, MD, E><<<1184, 256, 0, s>>>(n / E, y, V + j0 * stride, stride, mm, coef + j0, live);
         else
-          lincomb_kernel<R, MD, 1><<<1184, 256, 0, s>>>(n, y, V + j0 * stride, stride, mm, coef + j0);
+          lincomb_kernel<R, MD, 1><<<1184, 256, 0, s>>>(n, y, V + j0 * stride, stride, mm, coef + j0, live);
         count_launches(1);
       }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SINT_OK : cuda_fail(e, "lincomb");
   }
-  template int lincomb<double>(long long, double *, const double *, long long, int, const double *, cudaStream_t);
-  template int lincomb<float>(long long, float *, const float *, long long, int, const double *, cudaStream_t);
+  template int lincomb<double>(long long, double *, const double *, long long, int, const double *, cudaStream_t,
+                               const uint32_t *);
+  template int lincomb<float>(long long, float *, const float *, long long, int, const double *, cudaStream_t,
+                              const uint32_t *);
 
   // y = b y + a x; a term whose factor is 0 is dropped, so NaN in an unused
   // operand does not spread.  With d_div: a = 1 / d_div[0] read on the device.
+  // Chunks that are not live are written as zero without reading.
   template <typename R, int E>
   __global__ void axpby_kernel(long long nc, R a, const R *__restrict__ x, R b, R *__restrict__ y,
-                               const double *__restrict__ d_div)
+                               const double *__restrict__ d_div, const uint32_t *__restrict__ live)
   {
     if (d_div)
       a = R(1.0 / d_div[0]);
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x)
       {
+        if (!chunk_live(live, c * E))
+          {
+            st_pack<R, E>(y, c, Pack<R, E>{});
+            continue;
+          }
         Pack<R, E> xv{}, yv{}, out;
         if (a != R(0))
           xv = ld_pack<R, E>(x, c);
@@ -398,33 +427,36 @@ namespace sint
   }
 
   template <typename R>
-  static int launch_axpby(long long n, double a, const R *x, double b, R *y, const double *d_div, cudaStream_t s)
+  static int launch_axpby(long long n, double a, const R *x, double b, R *y, const double *d_div, cudaStream_t s,
+                          const uint32_t *live = nullptr)
   {
     constexpr int E = pack_of<R>();
     if (can_pack<R>(n, 0, x, y))
-      axpby_kernel<R, E><<<1184, 256, 0, s>>>(n / E, R(a), x, R(b), y, d_div);
+      axpby_kernel<R, E><<<1184, 256, 0, s>>>(n / E, R(a), x, R(b), y, d_div, live);
     else
-      axpby_kernel<R, 1><<<1184, 256, 0, s>>>(n, R(a), x, R(b), y, d_div);
+      axpby_kernel<R, 1><<<1184, 256, 0, s>>>(n, R(a), x, R(b), y, d_div, live);
     count_launches(1);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SINT_OK : cuda_fail(e, "axpby");
   }
 
   template <typename R>
-  int axpby(long long n, double a, const R *x, double b, R *y, cudaStream_t s)
+  int axpby(long long n, double a, const R *x, double b, R *y, cudaStream_t s, const uint32_t *live)
   {
-    return launch_axpby<R>(n, a, x, b, y, nullptr, s);
+    return launch_axpby<R>(n, a, x, b, y, nullptr, s, live);
   }
-  template int axpby<double>(long long, double, const double *, double, double *, cudaStream_t);
-  template int axpby<float>(long long, double, const float *, double, float *, cudaStream_t);
+  template int axpby<double>(long long, double, const double *, double, double *, cudaStream_t, const uint32_t *);
+  template int axpby<float>(long long, double, const float *, double, float *, cudaStream_t, const uint32_t *);
 
   template <typename R>
-  int scale_by_device(long long n, const R *x, const double *d_div, R *y, cudaStream_t s)
+  int scale_by_device(long long n, const R *x, const double *d_div, R *y, cudaStream_t s, const uint32_t *live)
   {
-    return launch_axpby<R>(n, 1.0, x, 0.0, y, d_div, s);
+    return launch_axpby<R>(n, 1.0, x, 0.0, y, d_div, s, live);
   }
-  template int scale_by_device<double>(long long, const double *, const double *, double *, cudaStream_t);
-  template int scale_by_device<float>(long long, const float *, const double *, float *, cudaStream_t);
+  template int scale_by_device<double>(long long, const double *, const double *, double *, cudaStream_t,
+                                       const uint32_t *);
+  template int scale_by_device<float>(long long, const float *, const double *, float *, cudaStream_t,
+                                      const uint32_t *);
 
   template <typename S, typename D>
   __global__ void convert_kernel(long long n, const S *__restrict__ x, D *__restrict__ y)

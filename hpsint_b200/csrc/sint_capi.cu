@@ -374,6 +374,8 @@ int sint_destroy(sint_ctx *c)
   cudaFree(c->tile_union);
   cudaFree(c->cut_range);
   cudaFree(c->cut_count);
+  cudaFree(c->node_mask);
+  cudaFree(c->live);
   cudaFree(c->pc_raw);
   cudaFree(c->pc_inv64);
   cudaFree(c->pc_inv32);

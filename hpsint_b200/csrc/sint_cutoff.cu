@@ -131,7 +131,60 @@ namespace sint
     sorted_union[pos] = (uint16_t)u;
   }
 
+  // One thread per node: the grains relevant on any cell the node belongs to.
+  // A grain outside this set gets no residual, Jacobian or preconditioner
+  // entry at the node, so every GMRES vector is zero there.
+  __global__ void __launch_bounds__(256)
+    node_mask_kernel(const Grid g, const uint16_t *__restrict__ cell_mask, uint16_t *__restrict__ node_mask)
+  {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.N)
+      return;
+    const int i = int(n % g.nn[0]), j = int((n / g.nn[0]) % g.nn[1]), k = int(n / ((long long)g.nn[0] * g.nn[1]));
+    unsigned  u = 0;
+    for (int ck = k - 1; ck <= k; ++ck)
+      for (int cj = j - 1; cj <= j; ++cj)
+        for (int ci = i - 1; ci <= i; ++ci)
+          if (ci >= 0 && ci < g.n[0] && cj >= 0 && cj < g.n[1] && ck >= 0 && ck < g.n[2])
+            u |= cell_mask[ci + (long long)g.n[0] * (cj + (long long)g.n[1] * ck)];
+    node_mask[n] = (uint16_t)u;
+  }
+
+  // One warp per 32 chunks of LIVE_CHUNK elements of a block vector (C blocks
+  // of stride ld): the chunk is live when one of its elements is c or mu, or
+  // a grain relevant at its node.
+  __global__ void __launch_bounds__(256)
+    live_chunk_kernel(const Grid g, int C, const uint16_t *__restrict__ node_mask, uint32_t *__restrict__ live,
+                      long long n_words)
+  {
+    const long long word = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int       lane = threadIdx.x & 31;
+    if (word >= n_words)
+      return;
+    const long long n_elem = (long long)C * g.ld;
+    uint32_t        bits   = 0;
+    for (int k = 0; k < 32; ++k)
+      {
+        const long long e0 = (word * 32 + k) * LIVE_CHUNK;
+        bool            any = false;
+        for (long long e = e0 + lane; e < e0 + LIVE_CHUNK && e < n_elem; e += 32)
+          {
+            const long long b = e / g.ld, node = e - b * g.ld;
+            any = any || b < 2 || (node < g.N && ((node_mask[node] >> (b - 2)) & 1u) != 0u);
+          }
+        if (__any_sync(0xffffffffu, any))
+          bits |= 1u << k;
+      }
+    if (lane == 0)
+      live[word] = bits;
+  }
+
   static long long cell_count(const Ctx *c) { return (long long)c->grid.n[0] * c->grid.n[1] * c->grid.n[2]; }
+  static long long live_words(const Ctx *c)
+  {
+    const long long chunks = ((long long)c->C * c->ld + LIVE_CHUNK - 1) / LIVE_CHUNK;
+    return (chunks + 31) / 32;
+  }
 
   static int allocate_cut(Ctx *c)
   {
@@ -144,7 +197,9 @@ namespace sint
         (e = cudaMalloc(&c->cut_union, sizeof(uint16_t) * (size_t)nt)) != cudaSuccess ||
         (e = cudaMalloc(&c->tile_union, sizeof(uint16_t) * (size_t)nt)) != cudaSuccess ||
         (e = cudaMalloc(&c->cut_range, sizeof(int) * (SINT_MAX_GRAINS + 2))) != cudaSuccess ||
-        (e = cudaMalloc(&c->cut_count, sizeof(unsigned) * (SINT_MAX_GRAINS + 1))) != cudaSuccess)
+        (e = cudaMalloc(&c->cut_count, sizeof(unsigned) * (SINT_MAX_GRAINS + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&c->node_mask, sizeof(uint16_t) * (size_t)c->grid.N)) != cudaSuccess ||
+        (e = cudaMalloc(&c->live, sizeof(uint32_t) * (size_t)live_words(c))) != cudaSuccess)
       {
         cudaFree(c->mask);
         cudaFree(c->cut_tiles);
@@ -153,8 +208,11 @@ namespace sint
         cudaFree(c->tile_union);
         cudaFree(c->cut_range);
         cudaFree(c->cut_count);
+        cudaFree(c->node_mask);
+        cudaFree(c->live);
         c->mask = nullptr, c->cut_tiles = nullptr, c->cut_grains = nullptr, c->cut_union = nullptr;
-        c->tile_union = nullptr, c->cut_range = nullptr, c->cut_count = nullptr;
+        c->tile_union = nullptr, c->cut_range = nullptr, c->cut_count = nullptr, c->node_mask = nullptr;
+        c->live = nullptr;
         return cuda_fail(e, "sint_set_component_mask: allocation");
       }
     c->cut_view.cell_mask   = c->mask;
@@ -205,13 +263,27 @@ int sint_set_component_mask(sint_ctx *c, const double *u, double tol, sint_strea
       class_scan_kernel<<<1, 32, 0, stream>>>(c->G, c->cut_count, c->cut_range);
       class_scatter_kernel<<<dim3((unsigned)nbt), 256, 0, stream>>>(c->grid.n_tiles, c->tile_union, c->cut_count,
                                                                     c->cut_tiles, c->cut_grains, c->cut_union);
-      count_launches(4);
+      const long long nbn = (c->grid.N + 255) / 256, nw = live_words(c), nbw = (nw * 32 + 255) / 256;
+      node_mask_kernel<<<dim3((unsigned)nbn), 256, 0, stream>>>(c->grid, c->mask, c->node_mask);
+      live_chunk_kernel<<<dim3((unsigned)nbw), 256, 0, stream>>>(c->grid, c->C, c->node_mask, c->live, nw);
+      count_launches(6);
       e = cudaGetLastError();
     }
   if (e != cudaSuccess)
     return cuda_fail(e, "sint_set_component_mask");
   c->cut     = true;
   c->cut_tol = tol;
+  return SINT_OK;
+}
+
+int sint_set_cut_off_skip_zero_chunks(sint_ctx *c, int on)
+{
+  if (!c)
+    {
+      set_error("null context");
+      return SINT_ERR_ARG;
+    }
+  c->skip_zeros = on != 0;
   return SINT_OK;
 }
 

@@ -18,6 +18,9 @@ namespace sint
   constexpr int NB_RED       = 592; // 4 x 148 SMs
   constexpr int MAX_MULTIDOT = 64;
   constexpr int RED_TICKETS  = 1; // doubles after the partials holding the last-block ticket counter
+  // Elements per chunk of the grain cut-off's live-chunk map of Krylov vectors
+  // (a multiple of the 128 elements one warp's 16-byte packs cover).
+  constexpr long long LIVE_CHUNK = 1024;
 
   struct Workspace; // Newton/GMRES vectors, sint_newton.cu
 
@@ -53,6 +56,11 @@ namespace sint
     int                *cut_range  = nullptr; // class offsets, SINT_MAX_GRAINS + 2
     unsigned           *cut_count  = nullptr; // class sizes / scatter cursors, SINT_MAX_GRAINS + 1
     CutTiles            cut_view;             // the above as the kernels take them
+    // nodes: the grains relevant on any adjacent cell; Krylov vectors: chunks
+    // of LIVE_CHUNK elements that can be non-zero under the cut-off
+    uint16_t *node_mask  = nullptr;
+    uint32_t *live       = nullptr;
+    bool      skip_zeros = true; // GMRES skips the chunks that are not live
 
     double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
     double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
@@ -69,35 +77,41 @@ namespace sint
     Workspace *ws = nullptr;
   };
 
-  // Reductions (sint_blas.cu); `out` is a device pointer.
+  // Reductions (sint_blas.cu); `out` is a device pointer.  `live` (grain
+  // cut-off, GMRES vectors only): chunks whose bit is clear are zero in every
+  // operand; read-only and update kernels skip them, kernels that produce a
+  // vector write zeros there.  nullptr = everything live.
   int dot_f64(Ctx *c, long long n, const double *x, const double *y, double *out, cudaStream_t s);
   int dot_f32(Ctx *c, long long n, const float *x, const float *y, double *out, cudaStream_t s);
   // out[i] = <w, V + i * stride> for i < m (FP64 accumulation)
   template <typename R>
-  int multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, cudaStream_t s);
+  int multidot(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, cudaStream_t s,
+               const uint32_t *live = nullptr);
   // w -= sum_i coef[i] * (V + i * stride), coef on the device
   template <typename R>
   int multiaxpy(long long n, R *w, const R *V, long long stride, int m, const double *coef, cudaStream_t s);
   // w -= sum_i coef[i] * V_i and norm2_out[0] = |w|^2 after the update (device scalar)
   template <typename R>
   int multiaxpy_norm2(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
-                      double *norm2_out, cudaStream_t s);
+                      double *norm2_out, cudaStream_t s, const uint32_t *live = nullptr);
   // the same two, skipped on the device when *cond == 0 (launched unconditionally, decided on the GPU)
   template <typename R>
   int multidot_if(Ctx *c, long long n, const R *w, const R *V, long long stride, int m, double *out, const int *cond,
-                  cudaStream_t s);
+                  cudaStream_t s, const uint32_t *live = nullptr);
   template <typename R>
   int multiaxpy_norm2_if(Ctx *c, long long n, R *w, const R *V, long long stride, int m, const double *coef,
-                         double *norm2_out, const int *cond, cudaStream_t s);
+                         double *norm2_out, const int *cond, cudaStream_t s, const uint32_t *live = nullptr);
   // y = x / d_div[0] (divisor on the device)
   template <typename R>
-  int scale_by_device(long long n, const R *x, const double *d_div, R *y, cudaStream_t s);
+  int scale_by_device(long long n, const R *x, const double *d_div, R *y, cudaStream_t s,
+                      const uint32_t *live = nullptr);
   // y = a * x + b * y  (a, b on the host)
   template <typename R>
-  int axpby(long long n, double a, const R *x, double b, R *y, cudaStream_t s);
+  int axpby(long long n, double a, const R *x, double b, R *y, cudaStream_t s, const uint32_t *live = nullptr);
   // y = sum_i y_i-combination: y = x + sum_i coef[i] * V_i (coef on the device), FP32/FP64 V
   template <typename R>
-  int lincomb(long long n, R *y, const R *V, long long stride, int m, const double *coef, cudaStream_t s);
+  int lincomb(long long n, R *y, const R *V, long long stride, int m, const double *coef, cudaStream_t s,
+              const uint32_t *live = nullptr);
   template <typename S, typename D>
   int convert(long long n, const S *x, D *y, cudaStream_t s);
 
@@ -110,6 +124,7 @@ namespace sint
   inline const uint16_t *preconditioner_mask(const Ctx *c) { return c->pc_cut ? active_mask(c) : nullptr; }
   inline const CutTiles *active_cut(const Ctx *c) { return c->cut ? &c->cut_view : nullptr; }
   inline const uint16_t *active_tile_union(const Ctx *c) { return c->cut ? c->tile_union : nullptr; }
+  inline const uint32_t *active_live(const Ctx *c) { return (c->cut && c->skip_zeros) ? c->live : nullptr; }
   // J v through the cell kernel + combine, with c->partial as scratch.
   template <typename R>
   cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s);

@@ -297,6 +297,10 @@ namespace sint
     const int       m  = ws->restart, ldh = m + 1;
     R              *V = static_cast<R *>(ws->V), *w = static_cast<R *>(ws->w), *t = static_cast<R *>(ws->t);
     R              *b = static_cast<R *>(ws->b), *x = static_cast<R *>(ws->x);
+    // grain cut-off: every GMRES vector is zero on the DoFs no relevant cell
+    // touches (no residual, Jacobian or preconditioner entry reaches them),
+    // so the BLAS steps skip those chunks; results are bitwise the same
+    const uint32_t *live = active_live(c);
     std::vector<double> y(m, 0.0);
     int    its = 0, rc;
     double tol = 0.0;
@@ -314,18 +318,18 @@ namespace sint
       R  *vj = V + (long long)j * n;
       int r;
       if ((r = jvp<R>(c, t, vj, s)) || (r = prec<R>(c, w, t, s)) ||
-          (r = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s)) ||
-          (r = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s)))
+          (r = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s, live)) ||
+          (r = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s, live)))
         return r;
       arnoldi_check_kernel<<<1, 32, 0, s>>>(j, ldh, ws->d_s, ws->d_H, reorth_thresh2, ws->d_flag);
       count_launches(1);
-      if ((r = multidot_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_flag, s)) ||
-          (r = multiaxpy_norm2_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, ws->d_flag, s)))
+      if ((r = multidot_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_flag, s, live)) ||
+          (r = multiaxpy_norm2_if<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, ws->d_flag, s, live)))
         return r;
       arnoldi_finish_kernel<<<1, 32, 0, s>>>(j, ldh, ws->d_s, ws->d_H, ws->d_cs, ws->d_sn, ws->d_g, ws->d_flag,
                                              ws->d_sc, ws->d_out);
       count_launches(1);
-      if ((r = scale_by_device<R>(n, w, ws->d_sc, V + (long long)(j + 1) * n, s)))
+      if ((r = scale_by_device<R>(n, w, ws->d_sc, V + (long long)(j + 1) * n, s, live)))
         return r;
       const cudaError_t e =
         cudaMemcpyAsync(ws->h_out + j, ws->d_out + j, sizeof(double2), cudaMemcpyDeviceToHost, s);
@@ -394,7 +398,7 @@ namespace sint
       return e == cudaSuccess ? SINT_OK : cuda_fail(e, "GMRES: record");
     };
 
-    if ((rc = axpby<R>(n, 0.0, b, 0.0, x, s)))
+    if ((rc = axpby<R>(n, 0.0, b, 0.0, x, s, live)))
       return rc;
     for (;;)
       {
@@ -406,10 +410,10 @@ namespace sint
           }
         else
           {
-            if ((rc = jvp<R>(c, t, x, s)) || (rc = axpby<R>(n, 1.0, b, -1.0, t, s)) || (rc = prec<R>(c, w, t, s)))
+            if ((rc = jvp<R>(c, t, x, s)) || (rc = axpby<R>(n, 1.0, b, -1.0, t, s, live)) || (rc = prec<R>(c, w, t, s)))
               return rc;
           }
-        if ((rc = multidot<R>(c, n, w, w, 0, 1, ws->d_s, s)) || (rc = fetch(ws, 1, s)))
+        if ((rc = multidot<R>(c, n, w, w, 0, 1, ws->d_s, s, live)) || (rc = fetch(ws, 1, s)))
           return rc;
         const double beta = std::sqrt(ws->h_s[0]);
         if (!std::isfinite(beta))
@@ -439,7 +443,7 @@ namespace sint
             *its_out = its;
             return SINT_ERR_NO_CONVERGENCE;
           }
-        if ((rc = axpby<R>(n, 1.0 / beta, w, 0.0, V, s)))
+        if ((rc = axpby<R>(n, 1.0 / beta, w, 0.0, V, s, live)))
           return rc;
         gmres_cycle_init_kernel<<<1, 64, 0, s>>>(m, beta, ws->d_g);
         count_launches(1);
@@ -505,7 +509,7 @@ namespace sint
           cudaError_t e = cudaMemcpyAsync(ws->d_y, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s);
           if (e != cudaSuccess)
             return cuda_fail(e, "GMRES: upload y");
-          if ((rc = lincomb<R>(n, x, V, n, k, ws->d_y, s)))
+          if ((rc = lincomb<R>(n, x, V, n, k, ws->d_y, s, live)))
             return rc;
           // y lives in a host vector that the next cycle overwrites
           if ((e = cudaStreamSynchronize(s)) != cudaSuccess)

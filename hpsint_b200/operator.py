@@ -185,6 +185,12 @@ class SinteringOperatorGeneric:
         full operator (the default); takes effect at the next set-up."""
         L.check(L.lib().sint_set_preconditioner_cut_off(self._h, int(bool(on))), "sint_set_preconditioner_cut_off")
 
+    def set_cut_off_skip_zero_chunks(self, on):
+        """Under the cut-off the device GMRES skips the chunks of its vectors
+        that are zero by construction (default on; results are bitwise the
+        same either way)."""
+        L.check(L.lib().sint_set_cut_off_skip_zero_chunks(self._h, int(bool(on))), "sint_set_cut_off_skip_zero_chunks")
+
     def component_mask_statistics(self):
         """numpy array: entry k = number of cells with k relevant grains
         (the "Cut-off statistic" of operator_sintering_data.h:236-296)."""

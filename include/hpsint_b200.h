@@ -207,6 +207,14 @@ int sint_set_component_mask(sint_ctx *ctx, const double *u, double tol, sint_str
  * or its solution.  Takes effect at the next sint_precond_setup. */
 int sint_set_preconditioner_cut_off(sint_ctx *ctx, int on);
 
+/* Whether the device GMRES (sint_newton_solve) skips, under the cut-off, the
+ * chunks of its vectors that are zero by construction: a grain's DoF at a
+ * node none of whose cells has the grain relevant receives no residual,
+ * Jacobian or preconditioner entry.  Results are bitwise the same either
+ * way; default on (no counterpart in the reference, whose vectors are dense
+ * as well). */
+int sint_set_cut_off_skip_zero_chunks(sint_ctx *ctx, int on);
+
 /* The "Cut-off statistic" (operator_sintering_data.h:236-296): counts[k]
  * (host, n_grains + 1 entries) = number of cells with k relevant grains.
  * SINT_ERR_NOT_READY without a cut-off.  Synchronises `stream`. */

@@ -186,3 +186,26 @@ def test_newton_solve_with_cut_off():
     for u in (full, cut):
         assert abs(w @ u[0] - m0) <= 1e-8 * abs(m0)
     assert np.max(np.abs(cut - full)) <= 1e-3
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_skipping_zero_chunks_changes_nothing(prec):
+    """Under the cut-off, GMRES skips the chunks of its vectors that no
+    relevant cell reaches; the solves must be bitwise the same without it."""
+    import hpsint_b200 as hb
+    from hpsint_b200.time_integration import TimeIntegrationData, TimeIntegrator
+    dim, cells, G = 3, (24, 20, 16), 5
+    u0 = particle_state(dim, cells, G, seed=23, width=1.0)
+    out = []
+    for skip in (True, False):
+        op, _ = make_op(dim, cells, G, True)
+        op.set_cut_off_skip_zero_chunks(skip)
+        ti = TimeIntegrator(op, hb.NonLinearData(inner_precision=prec), TimeIntegrationData(time_step_init=1e-4),
+                            grain_cut_off_tolerance=1e-3)
+        ti.initialize(op.to_device(u0))
+        u = ti.run(4, dt_schedule=[1e-4] * 4)
+        out.append((op.to_host(u), [(r.newton_iterations, r.linear_iterations) for r in ti.records],
+                    ti.cut_off_statistics[-1]))
+    assert out[0][2][0] > 0  # cells without any relevant grain exist
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
