@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "nnconv",
-                                           "cutoff"],
+                                           "cutoff", "tracker"],
                     default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
@@ -501,6 +501,61 @@ def cut_off_operator(args):
                       "warmup": args.warmup, "data": "synthetic seeded packing", **rates}), flush=True)
 
 
+def grain_tracker_detection(args):
+    """Grain-tracker particle detection (flood fill, measures, centers, radii,
+    maxima; threshold_lower 0.01) of every order parameter of the 3D solve
+    workload's initial state (--n3, --spheres, ...; C3 by default): device
+    time per tracker call (all order parameters, CUDA events, after --warmup
+    calls), against the oracle's flood fill and properties on one host core,
+    whose particle ids and counts must agree."""
+    import torch
+
+    import hpsint_b200 as hb
+    from hpsint_b200 import grain_tracker as GT
+    from hpsint_b200 import packings as P
+    from oracle import oracle as O
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = args.n3
+    centers, radii, colours = P.lognormal_packing_3d(n=n, n_spheres=args.spheres, median=args.median,
+                                                     sigma=args.sigma, max_grains=args.max_grains)
+    G = int(colours.max()) + 1
+    u0 = P.initial_state(3, (n, n, n), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), centers, radii, colours, width=2.0)
+    op = hb.SinteringOperatorGeneric(hb.Mesh(3, (n, n, n)), hb.Params(**model_params(G, not args.scalar)))
+    ud = op.to_device(u0)
+    thr = 0.01
+
+    def call():
+        return [GT.detect_particles(op, ud, b, thr) for b in range(G)]
+
+    for _ in range(args.warmup):
+        call()
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(args.steps):
+        parts = call()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    gpu_ms = ev[0].elapsed_time(ev[1]) / args.steps
+    om = O.make_mesh(3, [n, n, n], (1.0, 1.0, 1.0))
+    t0 = time.perf_counter()
+    ref = [O.grain_segments(om, u0[2 + b], thr) for b in range(G)]
+    props = [O.segment_properties(om, u0[2 + b], ids, k) for b, (ids, k) in enumerate(ref)]
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    agree = all(p.n_particles == k and np.array_equal(p.ids.cpu().numpy(), ids) for p, (ids, k) in zip(parts, ref))
+    max_rel = max([float(np.max(np.abs(p.radii - q[:, 4]) / q[:, 4])) for p, q in zip(parts, props) if len(q)],
+                  default=0.0)
+    print(json.dumps({"metric": "grain-tracker particle detection, ms per tracker call", "unit": "ms",
+                      "higher_is_better": False,
+                      "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-G{G}", "cells": n ** 3,
+                      "order_parameters": G, "threshold_lower": thr, "steps": args.steps, "warmup": args.warmup,
+                      "gpu_ms_per_call": gpu_ms, "cpu_oracle_ms_per_call": cpu_ms, "cpu_cores": 1,
+                      "particles": [p.n_particles for p in parts], "ids_equal_oracle": bool(agree),
+                      "max_rel_radius_diff_vs_oracle": max_rel, "data": "synthetic seeded packing"}), flush=True)
+
+
 def cut_off_operator_rates(op, u, tol, reps=20, warmup=3):
     """GDoF/s of the FP64/FP32 Jacobian-vector products and the residual at
     state u, without and with the grain cut-off at tolerance tol (CUDA events
@@ -615,6 +670,9 @@ def main():
         return
     if args.workload == "cutoff":
         cut_off_operator(args)
+        return
+    if args.workload == "tracker":
+        grain_tracker_detection(args)
         return
     if args.workload == "learned2d":
         learned_guess_solve(args)

@@ -69,6 +69,8 @@ SIGNATURES = {
     "sint_component_mask_statistics": (_c_int, [_c_void, P(_c_int64), _c_void]),
     "sint_set_preconditioner_cut_off": (_c_int, [_c_void, _c_int]),
     "sint_set_cut_off_skip_zero_chunks": (_c_int, [_c_void, _c_int]),
+    "sint_grain_segments": (_c_int, [_c_void, _c_void, _c_double, _c_void, P(_c_int), _c_void]),
+    "sint_grain_segment_properties": (_c_int, [_c_void, _c_void, _c_void, _c_int, P(_c_double), _c_void]),
     "sint_get_component_mask": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_vec_axpy_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_sadd_f64": (_c_int, [_c_int64, _c_double, _c_double, _c_void, _c_void, _c_void]),

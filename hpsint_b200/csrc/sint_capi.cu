@@ -376,6 +376,10 @@ int sint_destroy(sint_ctx *c)
   cudaFree(c->cut_count);
   cudaFree(c->node_mask);
   cudaFree(c->live);
+  cudaFree(c->seg_parent);
+  cudaFree(c->seg_blocks);
+  cudaFree(c->seg_acc);
+  cudaFree(c->seg_error);
   cudaFree(c->pc_raw);
   cudaFree(c->pc_inv64);
   cudaFree(c->pc_inv32);

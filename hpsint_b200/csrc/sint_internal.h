@@ -62,6 +62,14 @@ namespace sint
     uint32_t *live       = nullptr;
     bool      skip_zeros = true; // GMRES skips the chunks that are not live
 
+    // grain-tracker particle detection (sint_tracker.cu): union-find parents
+    // per cell, per-block root counts, accumulators per particle, error flag
+    int                *seg_parent  = nullptr;
+    int                *seg_blocks  = nullptr;
+    unsigned long long *seg_acc     = nullptr;
+    int                 seg_acc_cap = 0;
+    int                *seg_error   = nullptr;
+
     double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
     double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
     float  *pc_inv32 = nullptr;

@@ -1,0 +1,84 @@
+"""Grain-tracker particle detection on the device.
+
+Mirrors the detection half of hpsint's GrainTracker::Tracker
+(include/pf-applications/grain_tracker/tracker.h:1195-1300) for one order
+parameter:
+  detect_local_particle_groups  distributed_stitching.h:41-100, :441-480
+                                (run_flooding: cells whose largest nodal value
+                                exceeds threshold_lower, face-connected)
+  compute_particles_info        distributed_stitching.h:264-320
+  compute_particles_radii       distributed_stitching.h:322-360
+  compute_particles_max_values  distributed_stitching.h:217-258
+The labelling runs in the library's CUDA kernels (union-find with
+deterministic smallest-cell roots); the tracker's matching of particles to
+grains and its remapping decisions stay with the caller, on the small
+per-particle tables these functions return.
+"""
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+@dataclass
+class Particles:
+    """Particles of one order parameter: ids (device int32 tensor per cell, -1 =
+    none, cells x fastest) and per particle measure, center, radius, max value."""
+    ids: torch.Tensor
+    n_particles: int
+    measures: np.ndarray = None
+    centers: np.ndarray = None
+    radii: np.ndarray = None
+    max_values: np.ndarray = None
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _n_cells(op):
+    n = 1
+    for d in range(op.mesh.dim):
+        n *= int(op.mesh.n_cells[d])
+    return n
+
+
+def detect_local_particle_groups(op, eta, threshold_lower=0.01):
+    """Label the particles of the order parameter whose nodal values are the
+    device tensor `eta` (N values, e.g. one block of a block vector)."""
+    if eta.dtype != torch.float64 or not eta.is_cuda or not eta.is_contiguous():
+        raise ValueError("eta must be a contiguous float64 CUDA tensor")
+    if eta.numel() < op.N:
+        raise ValueError(f"eta holds {eta.numel()} values, the mesh has {op.N} nodes")
+    ids = torch.empty(_n_cells(op), dtype=torch.int32, device="cuda")
+    n = ctypes.c_int()
+    L.check(L.lib().sint_grain_segments(op._h, ctypes.c_void_p(eta.data_ptr()), float(threshold_lower),
+                                        ctypes.c_void_p(ids.data_ptr()), ctypes.byref(n), _stream()),
+            "sint_grain_segments")
+    return Particles(ids, n.value)
+
+
+def compute_particles_properties(op, eta, particles):
+    """Fill measures, centers, radii and max values of `particles` (the
+    spherical grain representation)."""
+    dim, n = op.mesh.dim, particles.n_particles
+    props = np.zeros((n, 3 + dim))
+    if n:
+        L.check(L.lib().sint_grain_segment_properties(
+            op._h, ctypes.c_void_p(eta.data_ptr()), ctypes.c_void_p(particles.ids.data_ptr()), n,
+            props.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream()), "sint_grain_segment_properties")
+    particles.measures = props[:, 0].copy()
+    particles.centers = props[:, 1:1 + dim].copy()
+    particles.radii = props[:, 1 + dim].copy()
+    particles.max_values = props[:, 2 + dim].copy()
+    return particles
+
+
+def detect_particles(op, u, order_parameter, threshold_lower=0.01):
+    """Particles of order parameter `order_parameter` of the block vector u
+    (the tracker's per-order-parameter loop body, tracker.h:1207-1300)."""
+    eta = u[2 + order_parameter]
+    return compute_particles_properties(op, eta, detect_local_particle_groups(op, eta, threshold_lower))

@@ -225,6 +225,33 @@ int sint_component_mask_statistics(sint_ctx *ctx, int64_t *counts, sint_stream_t
 int sint_get_component_mask(const sint_ctx *ctx, uint16_t *dst, sint_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Grain tracker: particle detection of one order parameter                 */
+/* (GrainTracker::Tracker, grain_tracker/tracker.h:1195-1300).              */
+/* ---------------------------------------------------------------------- */
+
+/* run_flooding / detect_local_particle_groups
+ * (grain_tracker/distributed_stitching.h:41-100, :441-480): a cell belongs
+ * to a particle when the largest of its nodal values of `eta` (one block, N
+ * values, device) exceeds threshold_lower (GrainTrackerData::threshold_lower,
+ * default 0.01, sintering/parameters.h:98); particles are face-connected
+ * sets of such cells.  particle_ids (device, n_cells[0] * n_cells[1] *
+ * n_cells[2] ints, x fastest) receives each cell's particle number or -1;
+ * particles are numbered in the order a lexicographic cell loop reaches them
+ * (the reference numbers them in deal.II's cell order, and renumbers across
+ * processes).  *n_particles (host) = their number.  Synchronises `stream`. */
+int sint_grain_segments(sint_ctx *ctx, const double *eta, double threshold_lower, int *particle_ids,
+                        int *n_particles, sint_stream_t stream);
+
+/* The spherical representation's particle properties, per particle (host,
+ * n_particles rows of 3 + dim doubles): measure, center[dim] (measure-
+ * weighted cell centers, compute_particles_info, distributed_stitching.h:
+ * 264-320), radius (largest |cell barycenter - center| + cell diameter / 2,
+ * compute_particles_radii, :322-360) and the largest nodal value (the
+ * particle max_value of run_flooding, :77-86).  Synchronises `stream`. */
+int sint_grain_segment_properties(sint_ctx *ctx, const double *eta, const int *particle_ids, int n_particles,
+                                  double *props, sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* BLAS-1 on block vectors: DynamicBlockVector                              */
 /* (include/pf-applications/lac/dynamic_block_vector.h:346-516).            */
 /* n = number of elements (C * block_stride for a whole block vector).      */

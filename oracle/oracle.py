@@ -59,6 +59,9 @@ def lib():
         L.oracle_ac_diagonal.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
         L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
         L.oracle_grain_mask.argtypes = [P(Mesh), P(Params), P(_c_double), _c_double, U16]
+        L.oracle_grain_segments.argtypes = [P(Mesh), P(_c_double), _c_double, P(_c_int), P(_c_int)]
+        L.oracle_segment_properties.argtypes = [P(Mesh), P(_c_double), P(_c_double), P(_c_int), _c_int,
+                                                P(_c_double)]
         _lib = L
     return _lib
 
@@ -198,3 +201,26 @@ def inverse_diagonal(d):
     """operator_base.h:386-388: 1/d where |d| > 1e-10, else 1."""
     d = np.asarray(d, dtype=np.float64)
     return np.where(np.abs(d) > 1.0e-10, 1.0 / np.where(d == 0, 1.0, d), 1.0)
+
+
+def grain_segments(mesh, eta, threshold_lower):
+    """Particles of one order parameter (nodal values eta, length N): cell ids
+    (int32 per cell, -1 = none) and the number of particles."""
+    eta = np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)
+    ids = np.zeros(n_cells(mesh), dtype=np.int32)
+    n = ctypes.c_int()
+    _check(lib().oracle_grain_segments(ctypes.byref(mesh), _dptr(eta), float(threshold_lower),
+                                       ids.ctypes.data_as(ctypes.POINTER(_c_int)), ctypes.byref(n)), "grain_segments")
+    return ids, n.value
+
+
+def segment_properties(mesh, eta, ids, n_particles, origin=(0.0, 0.0, 0.0)):
+    """(n_particles, 3 + dim): measure, center, radius, max value per particle."""
+    eta = np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)
+    ids = np.ascontiguousarray(ids, dtype=np.int32)
+    org = np.ascontiguousarray(origin, dtype=np.float64)
+    props = np.zeros((n_particles, 3 + mesh.dim))
+    _check(lib().oracle_segment_properties(ctypes.byref(mesh), _dptr(org), _dptr(eta),
+                                           ids.ctypes.data_as(ctypes.POINTER(_c_int)), int(n_particles),
+                                           _dptr(props)), "segment_properties")
+    return props

@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -940,6 +941,135 @@ int oracle_ch_blocks(const oracle_mesh *m, const oracle_params *p, const oracle_
           blocks[e * N + gi] += J[e];
       }
   });
+  return 0;
+}
+
+// GrainTracker particle detection for one order parameter on one process:
+// run_flooding / detect_local_particle_groups
+// (grain_tracker/distributed_stitching.h:41-100, :441-480).  A cell belongs
+// to a particle when the largest of its nodal values exceeds threshold_lower;
+// particles are the face-connected sets of such cells, numbered in the order
+// the lexicographic cell loop (x fastest) first reaches them.  ids[cell] =
+// particle number or -1; *n_particles = their number.
+int oracle_grain_segments(const oracle_mesh *m, const double *eta, double threshold_lower, int *ids,
+                          int *n_particles)
+{
+  if (!m || (m->dim != 2 && m->dim != 3) || !eta || !ids || !n_particles)
+    return 1;
+  const Geometry geo(*m);
+  const int64_t  nc = geo.n_cells;
+  auto cell_max = [&](int64_t c) {
+    const int i = int(c % geo.n[0]), j = int((c / geo.n[0]) % geo.n[1]), k = int(c / (int64_t(geo.n[0]) * geo.n[1]));
+    double mx = -std::numeric_limits<double>::infinity();
+    for (int l = 0; l < geo.nq; ++l)
+      mx = std::max(mx, eta[geo.node(i, j, k, l)]);
+    return mx;
+  };
+  std::vector<char> flag(nc);
+  for (int64_t c = 0; c < nc; ++c)
+    {
+      flag[c] = cell_max(c) > threshold_lower;
+      ids[c]  = -1;
+    }
+  const int64_t stride[3] = {1, geo.n[0], int64_t(geo.n[0]) * geo.n[1]};
+  int           count     = 0;
+  std::vector<int64_t> stack;
+  for (int64_t c0 = 0; c0 < nc; ++c0)
+    {
+      if (!flag[c0] || ids[c0] >= 0)
+        continue;
+      ids[c0] = count;
+      stack.assign(1, c0);
+      while (!stack.empty())
+        {
+          const int64_t c = stack.back();
+          stack.pop_back();
+          const int co[3] = {int(c % geo.n[0]), int((c / geo.n[0]) % geo.n[1]),
+                             int(c / (int64_t(geo.n[0]) * geo.n[1]))};
+          for (int d = 0; d < geo.dim; ++d)
+            for (int s = -1; s <= 1; s += 2)
+              {
+                const int cd = co[d] + s;
+                if (cd < 0 || cd >= geo.n[d])
+                  continue; // cell->at_boundary(face)
+                const int64_t nb = c + s * stride[d];
+                if (flag[nb] && ids[nb] < 0)
+                  {
+                    ids[nb] = count;
+                    stack.push_back(nb);
+                  }
+              }
+        }
+      ++count;
+    }
+  *n_particles = count;
+  return 0;
+}
+
+// Particle properties of the spherical representation, per particle
+// [measure, center[dim], radius, max value]: compute_particles_info
+// (distributed_stitching.h:264-320: measure-weighted cell centers),
+// compute_particles_radii (:322-360: max over the cells of the distance from
+// the center to the cell's barycenter plus half its diameter) and the
+// particle maxima of run_flooding (:77-86).  origin = lower corner of the mesh.
+int oracle_segment_properties(const oracle_mesh *m, const double *origin, const double *eta, const int *ids,
+                              int n_particles, double *props)
+{
+  if (!m || (m->dim != 2 && m->dim != 3) || !origin || !eta || !ids || !props || n_particles < 0)
+    return 1;
+  const Geometry geo(*m);
+  const int      dim = geo.dim, nf = 3 + dim;
+  double         vol = 1.0, diam2 = 0.0;
+  for (int d = 0; d < dim; ++d)
+    {
+      vol *= geo.h[d];
+      diam2 += geo.h[d] * geo.h[d];
+    }
+  const double        half_diam = 0.5 * std::sqrt(diam2);
+  std::vector<double> sum(int64_t(n_particles) * (1 + dim), 0.0);
+  for (int p = 0; p < n_particles; ++p)
+    {
+      props[p * nf + 1 + dim] = 0.0;
+      props[p * nf + 2 + dim] = -std::numeric_limits<double>::infinity();
+    }
+  auto center_of = [&](int64_t c, double *x) {
+    const int co[3] = {int(c % geo.n[0]), int((c / geo.n[0]) % geo.n[1]), int(c / (int64_t(geo.n[0]) * geo.n[1]))};
+    for (int d = 0; d < dim; ++d)
+      x[d] = origin[d] + (co[d] + 0.5) * geo.h[d];
+  };
+  for (int64_t c = 0; c < geo.n_cells; ++c)
+    {
+      const int p = ids[c];
+      if (p < 0)
+        continue;
+      if (p >= n_particles)
+        return 1;
+      double x[3];
+      center_of(c, x);
+      sum[int64_t(p) * (1 + dim)] += vol;
+      for (int d = 0; d < dim; ++d)
+        sum[int64_t(p) * (1 + dim) + 1 + d] += x[d] * vol;
+      const int i = int(c % geo.n[0]), j = int((c / geo.n[0]) % geo.n[1]), k = int(c / (int64_t(geo.n[0]) * geo.n[1]));
+      for (int l = 0; l < geo.nq; ++l)
+        props[p * nf + 2 + dim] = std::max(props[p * nf + 2 + dim], eta[geo.node(i, j, k, l)]);
+    }
+  for (int p = 0; p < n_particles; ++p)
+    {
+      props[p * nf] = sum[int64_t(p) * (1 + dim)];
+      for (int d = 0; d < dim; ++d)
+        props[p * nf + 1 + d] = sum[int64_t(p) * (1 + dim) + 1 + d] / sum[int64_t(p) * (1 + dim)];
+    }
+  for (int64_t c = 0; c < geo.n_cells; ++c)
+    {
+      const int p = ids[c];
+      if (p < 0)
+        continue;
+      double x[3], r2 = 0.0;
+      center_of(c, x);
+      for (int d = 0; d < dim; ++d)
+        r2 += (x[d] - props[p * nf + 1 + d]) * (x[d] - props[p * nf + 1 + d]);
+      props[p * nf + 1 + dim] = std::max(props[p * nf + 1 + dim], std::sqrt(r2) + half_diam);
+    }
   return 0;
 }
 

@@ -19,6 +19,10 @@ Sources (paths inside the hpsint project):
       power sums
   tests/tangent_generic_{scalar,tensorial}.cc + .mpirun=1.output
       tolerances of the analytic-vs-finite-difference tangent check
+  tests/grain_tracker_elliptical.{cc,mpirun=4.output}
+      grain-tracker segments (center, radius, max value) of the spherical
+      representation; the mesh, the indicator field and the threshold are
+      re-typed below from the .cc (lines cited), the segments are parsed
 """
 import json
 import os
@@ -64,6 +68,21 @@ def parse_power_sum(path):
         if m and "sums" in res[section]:
             res[section]["sums"].setdefault(m.group(1), float(m.group(2)))
     return res
+
+
+def parse_tracker_segments(path, section):
+    """Segments printed after the `section` header line (up to the next blank line)."""
+    segs, on = [], False
+    for line in open(path).read().splitlines():
+        if line.startswith(section):
+            on = True
+            continue
+        if on and not line.strip():
+            break
+        m = re.match(r"^\s+segment: center = (\S+) (\S+) \| radius = (\S+) \| max_value = (\S+)$", line)
+        if on and m:
+            segs.append([float(x) for x in m.groups()])
+    return segs
 
 
 def main(ref):
@@ -117,6 +136,19 @@ def main(ref):
                 "tensorial": open(os.path.join(t, "tangent_generic_tensorial.mpirun=1.output")).read().splitlines()[0],
             },
         },
+    }
+    # grain_tracker_elliptical.cc:56-60 (indicator of an ellipse and a circle,
+    # interpolated at the nodes), :81-93 ([0, 9]^2, 10 x 10 subdivisions, 3
+    # global refinements -> 80 x 80 cells), :124 (threshold_lower)
+    golden["grain_tracker_spherical"] = {
+        "mesh": {"dim": 2, "cells": [80, 80], "lower": [0.0, 0.0], "upper": [9.0, 9.0]},
+        "ellipse": {"center": [4.0, 2.0], "semi_axes": [3.0, 1.0], "inclusive": True},
+        "circle": {"center": [4.0, 6.5], "radius": 1.5, "inclusive": False},
+        "threshold_lower": 1e-15,
+        # [center x, center y, radius, max value], in the order printed
+        "segments": parse_tracker_segments(os.path.join(t, "grain_tracker_elliptical.mpirun=4.output"),
+                                           "Spherical grain representation"),
+        "digits": 6,
     }
     with open(os.path.join(HERE, "hpsint_goldens.json"), "w") as f:
         json.dump(golden, f, indent=1)

@@ -111,3 +111,21 @@ def grain_mask_numpy(dim, cells, G, u, tol):
             m = np.maximum(m, eta[sl])
         mask |= ((m > tol).astype(np.uint16) << b)
     return np.transpose(mask).ravel()
+
+
+def tracker_golden_field(g):
+    """The nodal field of grain_tracker_elliptical.cc: 1 inside the ellipse or
+    the circle, 0 elsewhere, on the golden's uniform mesh (nodes x fastest).
+    Returns (dim, cells, h, origin, eta)."""
+    mesh = g["mesh"]
+    cells = mesh["cells"]
+    h = [(mesh["upper"][d] - mesh["lower"][d]) / cells[d] for d in range(2)]
+    xs = mesh["lower"][0] + np.arange(cells[0] + 1) * h[0]
+    ys = mesh["lower"][1] + np.arange(cells[1] + 1) * h[1]
+    X, Y = np.meshgrid(xs, ys, indexing="xy")  # rows = y: x fastest when raveled
+    e, c = g["ellipse"], g["circle"]
+    q = ((X - e["center"][0]) / e["semi_axes"][0]) ** 2 + ((Y - e["center"][1]) / e["semi_axes"][1]) ** 2
+    in_e = q <= 1.0 if e["inclusive"] else q < 1.0
+    r = np.sqrt((X - c["center"][0]) ** 2 + (Y - c["center"][1]) ** 2)
+    in_c = r <= c["radius"] if c["inclusive"] else r < c["radius"]
+    return 2, cells, h, mesh["lower"], np.where(in_e | in_c, 1.0, 0.0).ravel()

@@ -129,3 +129,23 @@ def test_free_energy_derivatives_are_consistent():
         for j in range(G):
             if i != j:
                 assert np.isclose(fd(2 + j, "df_detai", i), r["d2f_detaidetaj"][i, j], rtol=1e-6, atol=1e-8)
+
+
+def test_grain_tracker_segments_match_hpsint_golden(goldens):
+    """grain_tracker_elliptical.cc, spherical representation: the flood fill
+    (distributed_stitching.h:41-100) finds the two grains, and their centers,
+    radii and maxima (:264-395) agree with hpsint's to the printed digits."""
+    from helpers import tracker_golden_field
+    g = goldens["grain_tracker_spherical"]
+    dim, cells, h, origin, eta = tracker_golden_field(g)
+    mesh = O.make_mesh(dim, list(cells) + [0], list(h) + [1.0])
+    ids, n = O.grain_segments(mesh, eta, g["threshold_lower"])
+    assert n == len(g["segments"])
+    props = O.segment_properties(mesh, eta, ids, n, list(origin) + [0.0])
+    ours = sorted([list(p[1:3]) + [p[3], p[4]] for p in props])
+    ref = sorted(g["segments"])
+    rtol = 0.5 * 10.0 ** (1 - g["digits"])
+    for a, b in zip(ours, ref):
+        assert np.allclose(a, b, rtol=rtol, atol=0), (a, b)
+    # every cell of a particle is face-connected to it and above the threshold
+    assert set(np.unique(ids)) == {-1, 0, 1}
