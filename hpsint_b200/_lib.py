@@ -69,6 +69,7 @@ SIGNATURES = {
     "sint_component_mask_statistics": (_c_int, [_c_void, P(_c_int64), _c_void]),
     "sint_set_preconditioner_cut_off": (_c_int, [_c_void, _c_int]),
     "sint_set_cut_off_skip_zero_chunks": (_c_int, [_c_void, _c_int]),
+    "sint_cut_off_freeze": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_grain_segments": (_c_int, [_c_void, _c_void, _c_double, _c_void, P(_c_int), _c_void]),
     "sint_grain_segment_properties": (_c_int, [_c_void, _c_void, _c_void, _c_int, P(_c_double), _c_void]),
     "sint_get_component_mask": (_c_int, [_c_void, _c_void, _c_void]),

@@ -179,6 +179,19 @@ namespace sint
       live[word] = bits;
   }
 
+  // u <- u_old on the grain DoFs no relevant cell reaches (node_mask bit clear).
+  __global__ void __launch_bounds__(256) cut_off_freeze_kernel(const Grid g, int G, const uint16_t *__restrict__ node_mask,
+                                                               double *__restrict__ u, const double *__restrict__ u_old)
+  {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.N)
+      return;
+    const unsigned m = node_mask[n];
+    for (int b = 0; b < G; ++b)
+      if (((m >> b) & 1u) == 0u)
+        u[(2 + b) * g.ld + n] = u_old[(2 + b) * g.ld + n];
+  }
+
   static long long cell_count(const Ctx *c) { return (long long)c->grid.n[0] * c->grid.n[1] * c->grid.n[2]; }
   static long long live_words(const Ctx *c)
   {
@@ -274,6 +287,25 @@ int sint_set_component_mask(sint_ctx *c, const double *u, double tol, sint_strea
   c->cut     = true;
   c->cut_tol = tol;
   return SINT_OK;
+}
+
+int sint_cut_off_freeze(sint_ctx *c, double *u, const double *u_old, sint_stream_t stream)
+{
+  if (!c || !u || !u_old)
+    {
+      set_error("sint_cut_off_freeze: null argument");
+      return SINT_ERR_ARG;
+    }
+  if (!c->cut)
+    {
+      set_error("sint_cut_off_freeze: no grain cut-off set");
+      return SINT_ERR_NOT_READY;
+    }
+  cut_off_freeze_kernel<<<dim3((unsigned)((c->grid.N + 255) / 256)), 256, 0, stream>>>(c->grid, c->G, c->node_mask,
+                                                                                       u, u_old);
+  count_launches(1);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SINT_OK : cuda_fail(e, "sint_cut_off_freeze");
 }
 
 int sint_set_cut_off_skip_zero_chunks(sint_ctx *c, int on)

@@ -444,16 +444,20 @@ class LearnedPredictor:
 
 # --- evaluation -------------------------------------------------------------------------
 
+GRAIN_CUT_OFF = 1e-5  # GrainCutOffTolerance of the *_cut_off arms
+
 ARMS = {
-    # label: (inner precision, predictor)
-    "fp64_plain": (64, None),
-    "fp64_linear": (64, "linear"),
-    "fp64_learned": (64, "learned"),
-    "fp64_learned_safeguarded": (64, "learned_safeguarded"),
-    "fp32_inner_plain": (32, None),
-    "fp32_inner_linear": (32, "linear"),
-    "fp32_inner_learned": (32, "learned"),
-    "fp32_inner_learned_safeguarded": (32, "learned_safeguarded"),
+    # label: (inner precision, predictor, grain cut-off tolerance)
+    "fp64_plain": (64, None, 0.0),
+    "fp64_linear": (64, "linear", 0.0),
+    "fp64_learned": (64, "learned", 0.0),
+    "fp64_learned_safeguarded": (64, "learned_safeguarded", 0.0),
+    "fp32_inner_plain": (32, None, 0.0),
+    "fp32_inner_linear": (32, "linear", 0.0),
+    "fp32_inner_learned": (32, "learned", 0.0),
+    "fp32_inner_learned_safeguarded": (32, "learned_safeguarded", 0.0),
+    "fp32_inner_linear_cut_off": (32, "linear", GRAIN_CUT_OFF),
+    "fp32_inner_learned_safeguarded_cut_off": (32, "learned_safeguarded", GRAIN_CUT_OFF),
 }
 
 
@@ -463,11 +467,13 @@ def lumped_mass_2d(nodes):
     return np.outer(w, w).ravel()
 
 
-def run_arm(case, n_steps, inner_precision, predictor, dt_schedule=None, nl_rel_tol=1e-8):
-    """One solve of n_steps from case.u0; returns (final state on the host, records, wall seconds)."""
+def run_arm(case, n_steps, inner_precision, predictor, dt_schedule=None, nl_rel_tol=1e-8, cut_off=0.0):
+    """One solve of n_steps from case.u0 (with the grain cut-off when
+    cut_off > 0); returns (final state on the host, records, wall seconds)."""
     nl = NonLinearData(nl_rel_tol=nl_rel_tol, inner_precision=inner_precision)
+    case.op.set_component_mask(case.u0, cut_off)  # 0: switch a previous arm's cut-off off
     ti = TimeIntegrator(case.op, nl, TimeIntegrationData(time_step_init=1e-3), predictor=predictor,
-                        tolerance_base="old_solution")
+                        tolerance_base="old_solution", grain_cut_off_tolerance=cut_off)
     ti.initialize(case.u0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -495,18 +501,18 @@ def compare_arms(case, n_steps, net=None, norm=None, arms=None, warmup_steps=2):
         preds["learned"] = LearnedPredictor(case.op, net, norm)
         preds["learned_safeguarded"] = LearnedPredictor(case.op, net, norm, safeguard=True)
     # warm-up: workspaces of both inner precisions, library load, first launches
-    for prec in sorted({ARMS[a][0] for a in arms}):
-        run_arm(case, warmup_steps, prec, None)
+    for prec, cut in sorted({(ARMS[a][0], ARMS[a][2]) for a in arms}):
+        run_arm(case, warmup_steps, prec, None, cut_off=cut)
     mass = lumped_mass_2d(case.nodes)
     u0 = case.op.to_host(case.u0)
     c0 = float(mass @ u0[0])
     out, ref, schedule = {}, None, None
     for a in arms:
-        prec, kind = ARMS[a]
+        prec, kind, cut = ARMS[a]
         if kind is not None and kind not in preds:
             continue
         try:
-            u, recs, wall = run_arm(case, n_steps, prec, preds.get(kind), schedule)
+            u, recs, wall = run_arm(case, n_steps, prec, preds.get(kind), schedule, cut_off=cut)
         except L.SintError as e:
             out[a] = {"failed": str(e)}
             continue

@@ -191,6 +191,13 @@ class SinteringOperatorGeneric:
         same either way)."""
         L.check(L.lib().sint_set_cut_off_skip_zero_chunks(self._h, int(bool(on))), "sint_set_cut_off_skip_zero_chunks")
 
+    def cut_off_freeze(self, u, u_old):
+        """u <- u_old on the DoFs the grain cut-off takes out of the system (a
+        grain at a node none of whose cells has it relevant)."""
+        self._check_vec(u, torch.float64)
+        self._check_vec(u_old, torch.float64)
+        L.check(L.lib().sint_cut_off_freeze(self._h, _ptr(u), _ptr(u_old), _stream()), "sint_cut_off_freeze")
+
     def component_mask_statistics(self):
         """numpy array: entry k = number of cells with k relevant grains
         (the "Cut-off statistic" of operator_sintering_data.h:236-296)."""

@@ -69,7 +69,8 @@ class TimeIntegrator:
 
     grain_cut_off_tolerance != 0 (GrainCutOffTolerance, parameters.h:314)
     sets the operator's grain cut-off from u_n before every step attempt, as
-    the driver does before make_step.
+    the driver does before make_step; a predicted guess keeps u_n on the DoFs
+    the cut-off takes out of the system (they have no equation this step).
     """
 
     def __init__(self, op: SinteringOperatorGeneric, nl: NonLinearData = None, td: TimeIntegrationData = None,
@@ -130,6 +131,9 @@ class TimeIntegrator:
             if self.grain_cut_off_tolerance != 0.0:
                 self.op.set_component_mask(self.history[0], self.grain_cut_off_tolerance)
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
+            if guess is not None and self.grain_cut_off_tolerance != 0.0:
+                # DoFs outside the cut-off's reach have no equation this step: keep their old values
+                self.op.cut_off_freeze(guess, self.history[0])
             self._reference_residual = 0.0
             data = self._stop_rule(wh) if guess is not None else None
             u = (guess if guess is not None else self.history[0]).clone()

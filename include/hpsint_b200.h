@@ -207,6 +207,15 @@ int sint_set_component_mask(sint_ctx *ctx, const double *u, double tol, sint_str
  * or its solution.  Takes effect at the next sint_precond_setup. */
 int sint_set_preconditioner_cut_off(sint_ctx *ctx, int on);
 
+/* Copies u_old into u (both C blocks, device) on the DoFs the cut-off takes
+ * out of the system: grain b at a node none of whose cells has b relevant.
+ * Those DoFs get no residual, Jacobian or preconditioner entry, so Newton
+ * keeps whatever the initial guess holds there; a caller that starts Newton
+ * from a predicted guess (the reference's predictor hook, driver.h:2001-2058)
+ * calls this so they keep their old values instead of the extrapolation (no
+ * counterpart in the reference).  SINT_ERR_NOT_READY without a cut-off. */
+int sint_cut_off_freeze(sint_ctx *ctx, double *u, const double *u_old, sint_stream_t stream);
+
 /* Whether the device GMRES (sint_newton_solve) skips, under the cut-off, the
  * chunks of its vectors that are zero by construction: a grain's DoF at a
  * node none of whose cells has the grain relevant receives no residual,

@@ -209,3 +209,31 @@ def test_skipping_zero_chunks_changes_nothing(prec):
     assert out[0][2][0] > 0  # cells without any relevant grain exist
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.parametrize("dim,cells", [(2, (37, 21)), (3, (13, 11, 9))])
+def test_cut_off_freeze_keeps_old_values_outside_the_cut(dim, cells):
+    """Grain b at a node none of whose cells has b relevant gets no equation;
+    cut_off_freeze puts the old value back there and touches nothing else."""
+    G, tol = 5, 1e-3
+    op, p = make_op(dim, cells, G, True)
+    u_old = particle_state(dim, cells, G, seed=41)
+    guess = u_old + 0.01 * (random_state(dim, cells, G, seed=42, smooth=False) - 0.5)
+    op.set_component_mask(op.to_device(u_old), tol)
+    g = op.to_device(guess)
+    op.cut_off_freeze(g, op.to_device(u_old))
+    got = op.to_host(g)
+    # node activity from the oracle's cell masks
+    mask = O.grain_mask(oracle_mesh(dim, cells), p, u_old, tol).reshape([cells[d] for d in reversed(range(dim))])
+    node = np.zeros([cells[d] + 1 for d in reversed(range(dim))], dtype=np.uint16)
+    for corner in range(1 << dim):
+        sl = tuple(slice((corner >> (dim - 1 - a)) & 1, ((corner >> (dim - 1 - a)) & 1) + mask.shape[a])
+                   for a in range(dim))
+        node[sl] |= mask
+    node = node.ravel()
+    for b in range(G):
+        live = ((node >> b) & 1).astype(bool)
+        assert np.array_equal(got[2 + b][~live], u_old[2 + b][~live])
+        assert np.array_equal(got[2 + b][live], guess[2 + b][live])
+        assert (~live).any() and live.any()
+    assert np.array_equal(got[:2], guess[:2])
