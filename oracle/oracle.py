@@ -28,6 +28,11 @@ class Params(ctypes.Structure):
                 ("Mgb", _c_double), ("L", _c_double), ("tensorial", _c_int)]
 
 
+class Advection(ctypes.Structure):
+    _fields_ = [("cell_segments", ctypes.POINTER(_c_int)), ("segments", ctypes.POINTER(_c_double)),
+                ("n_segments", _c_int), ("origin", _c_double * 3)]
+
+
 class Time(ctypes.Structure):
     _fields_ = [("w0", _c_double), ("w_alg", _c_double), ("order", _c_int),
                 ("w_hist", _c_double * 4)]
@@ -53,9 +58,9 @@ def lib():
         L.oracle_power_sum.restype = _c_double
         U16 = P(ctypes.c_uint16)
         L.oracle_residual.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(P(_c_double)),
-                                      _c_int, U16, P(_c_double), _c_int]
+                                      _c_int, U16, P(Advection), P(_c_double), _c_int]
         L.oracle_jvp.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double),
-                                 U16, P(_c_double), _c_int]
+                                 U16, P(Advection), P(_c_double), _c_int]
         L.oracle_ac_diagonal.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
         L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
         L.oracle_grain_mask.argtypes = [P(Mesh), P(Params), P(_c_double), _c_double, U16]
@@ -154,26 +159,44 @@ def grain_mask(mesh, params, u, tol):
     return m
 
 
-def residual(mesh, params, time, u, hist=(), with_td=2, threads=0, mask=None):
+def _adv(adv, mesh):
+    """Advection argument: None or (cell_segments (G, n_cells) int, segments (S, 9), origin)."""
+    if adv is None:
+        return None, None
+    seg = np.ascontiguousarray(adv[0], dtype=np.int32)
+    data = np.ascontiguousarray(adv[1], dtype=np.float64).reshape(-1, 9)
+    a = Advection()
+    a.cell_segments = seg.ctypes.data_as(ctypes.POINTER(_c_int))
+    a.segments = data.ctypes.data_as(ctypes.POINTER(_c_double))
+    a.n_segments = data.shape[0]
+    org = list(adv[2]) + [0.0] * (3 - len(adv[2]))
+    for d in range(3):
+        a.origin[d] = float(org[d])
+    return (seg, data), ctypes.byref(a)
+
+
+def residual(mesh, params, time, u, hist=(), with_td=2, threads=0, mask=None, advection=None):
     C, N = params.n_grains + 2, n_nodes(mesh)
     u = np.ascontiguousarray(u, dtype=np.float64).reshape(C, N)
     hs = [np.ascontiguousarray(h, dtype=np.float64).reshape(C, N) for h in hist]
     arr = (ctypes.POINTER(_c_double) * max(1, len(hs)))(*[_dptr(h) for h in hs])
     dst = np.zeros((C, N))
     keep, mp = _mptr(mask, mesh)
+    keep_a, ap = _adv(advection, mesh)
     _check(lib().oracle_residual(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(u),
-                                 arr, with_td, mp, _dptr(dst), threads or os.cpu_count()), "residual")
+                                 arr, with_td, mp, ap, _dptr(dst), threads or os.cpu_count()), "residual")
     return dst
 
 
-def jvp(mesh, params, time, lin, src, threads=0, mask=None):
+def jvp(mesh, params, time, lin, src, threads=0, mask=None, advection=None):
     C, N = params.n_grains + 2, n_nodes(mesh)
     lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
     src = np.ascontiguousarray(src, dtype=np.float64).reshape(C, N)
     dst = np.zeros((C, N))
     keep, mp = _mptr(mask, mesh)
+    keep_a, ap = _adv(advection, mesh)
     _check(lib().oracle_jvp(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin), _dptr(src),
-                            mp, _dptr(dst), threads or os.cpu_count()), "jvp")
+                            mp, ap, _dptr(dst), threads or os.cpu_count()), "jvp")
     return dst
 
 

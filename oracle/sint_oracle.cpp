@@ -227,6 +227,20 @@ typedef struct
   int    tensorial;
 } oracle_params;
 
+// Advection (rigid-body motion) data: cell_segments[b * n_cells + cell] =
+// segment of order parameter b the cell belongs to (-1: none); segments[9 s
+// ..] = translational velocity (3), angular velocity (3; z only in 2D) and
+// center (3) of segment s, so the velocity at x is v_t + w x (x - center)
+// (AdvectionMechanism::calc_translation_velocity / calc_rotation_velocity,
+// sintering/advection.h:330-352).  origin = lower corner of the mesh.
+typedef struct
+{
+  const int    *cell_segments;
+  const double *segments;
+  int           n_segments;
+  double        origin[3];
+} oracle_advection;
+
 typedef struct
 {
   double w0;        // primary BDF weight  (time_integrator_data.h:150-154)
@@ -547,6 +561,31 @@ namespace
     return Mobility{m->dim, p->Mvol, p->Mvap, p->Msurf, p->Mgb, p->L, p->tensorial != 0};
   }
 
+  // Advection velocity of grain b at quadrature point q of cell (i,j,k); false
+  // when the cell belongs to no segment of b (AdvectionVelocityData::
+  // has_velocity / get_velocity, sintering/advection.h:225-263).
+  inline bool advection_velocity(const oracle_advection *a, const Geometry &geo, int b, int i, int j, int k, int q,
+                                 V3 &v)
+  {
+    if (!a)
+      return false;
+    const int64_t cell = int64_t(i) + int64_t(geo.n[0]) * (int64_t(j) + int64_t(geo.n[1]) * k);
+    const int     s    = a->cell_segments[int64_t(b) * geo.n_cells + cell];
+    if (s < 0)
+      return false;
+    const double *d     = a->segments + 9 * int64_t(s);
+    const double  gp[2] = {0.5 - 0.5 / std::sqrt(3.0), 0.5 + 0.5 / std::sqrt(3.0)};
+    const int     co[3] = {i, j, k};
+    double        r[3]  = {0.0, 0.0, 0.0};
+    for (int e = 0; e < geo.dim; ++e)
+      r[e] = a->origin[e] + (co[e] + gp[(q >> e) & 1]) * geo.h[e] - d[6 + e];
+    // v_t + w x r
+    v[0] = d[0] + d[4] * r[2] - d[5] * r[1];
+    v[1] = d[1] + d[5] * r[0] - d[3] * r[2];
+    v[2] = geo.dim == 3 ? d[2] + d[3] * r[1] - d[4] * r[0] : 0.0;
+    return true;
+  }
+
   // Blocks cell (i,j,k) works on: blk[0] = c, blk[1] = mu, blk[2..] = the
   // relevant grains' blocks in increasing order (all grains without a mask).
   // Returns the number of relevant grains.
@@ -644,7 +683,8 @@ double oracle_power_sum(const double *x, int n, int p)
 // sum_i w_hist[i] * hist[i], interpolated to the quadrature points.
 // dst is overwritten.
 int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *u,
-                    const double *const *hist, int with_td, const uint16_t *mask, double *dst, int n_threads)
+                    const double *const *hist, int with_td, const uint16_t *mask, const oracle_advection *adv,
+                    double *dst, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
@@ -726,6 +766,16 @@ int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_t
             rv[2 + ig][q] = v;
             rg[2 + ig][q] = (p->L * p->kappa_p) * gradient[2 + ig];
           }
+        // generic.h:1015-1036: advection of c and eta_i with grain i's velocity
+        for (int ig = 0; ig < G; ++ig)
+          {
+            V3 vel;
+            if (advection_velocity(adv, geo, blk[2 + ig] - 2, i, j, k, q, vel))
+              {
+                rg[0][q]      = rg[0][q] - vel * value[0];
+                rg[2 + ig][q] = rg[2 + ig][q] - vel * value[2 + ig];
+              }
+          }
       }
     for (int b = 0; b < C; ++b)
       {
@@ -746,7 +796,7 @@ int oracle_residual(const oracle_mesh *m, const oracle_params *p, const oracle_t
 // No constrained DoFs exist on these meshes (operator_base.h:294-353 is then
 // a plain cell loop).  dst is overwritten.
 int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *lin,
-               const double *src, const uint16_t *mask, double *dst, int n_threads)
+               const double *src, const uint16_t *mask, const oracle_advection *adv, double *dst, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
@@ -812,6 +862,16 @@ int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *
             gradient_result[ig + 2] = (p->L * p->kappa_p) * gradient[ig + 2];
           }
         apply_d2f_detaidetaj(p->B, p->L, lin_etas, G, value + 2, value_result + 2);
+        // generic.h:167-177: advection with the (frozen) grain velocities
+        for (int ig = 0; ig < G; ++ig)
+          {
+            V3 vel;
+            if (advection_velocity(adv, geo, blk[2 + ig] - 2, i, j, k, q, vel))
+              {
+                gradient_result[0]      = gradient_result[0] - vel * value[0];
+                gradient_result[ig + 2] = gradient_result[ig + 2] - vel * value[ig + 2];
+              }
+          }
         for (int b = 0; b < C; ++b)
           {
             rv[b][q] = value_result[b];
