@@ -73,6 +73,7 @@ SIGNATURES = {
     "sint_grain_segments": (_c_int, [_c_void, _c_void, _c_double, _c_void, P(_c_int), _c_void]),
     "sint_grain_segment_properties": (_c_int, [_c_void, _c_void, _c_void, _c_int, P(_c_double), _c_void]),
     "sint_get_component_mask": (_c_int, [_c_void, _c_void, _c_void]),
+    "sint_set_advection": (_c_int, [_c_void, _c_void, _c_void, _c_int, _c_void]),
     "sint_vec_axpy_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_sadd_f64": (_c_int, [_c_int64, _c_double, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_scale_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void]),

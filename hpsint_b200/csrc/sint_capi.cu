@@ -58,14 +58,16 @@ namespace sint
   cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s)
   {
     R *part = reinterpret_cast<R *>(c->partial);
-    const bool t = c->params.tensorial != 0;
+    const bool      t   = c->params.tensorial != 0;
+    const CutTiles *cut = active_cut(c);
+    const AdvData  *adv = active_adv(c);
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_jvp<3, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s)
-            : launch_jvp<3, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s);
+      e = t ? launch_jvp<3, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, cut, adv, s)
+            : launch_jvp<3, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, cut, adv, s);
     else
-      e = t ? launch_jvp<2, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s)
-            : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, active_cut(c), s);
+      e = t ? launch_jvp<2, true, R>(c->G, c->grid, c->phys, lin, src, dst, part, cut, adv, s)
+            : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, cut, adv, s);
     if (e != cudaSuccess)
       return e;
     return c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, active_tile_union(c), s)
@@ -78,14 +80,16 @@ namespace sint
   static cudaError_t dispatch_residual(const Ctx *c, int wtd, const double *src, const double *const *hist,
                                        double *dst, cudaStream_t s)
   {
-    const bool t = c->params.tensorial != 0;
+    const bool      t   = c->params.tensorial != 0;
+    const CutTiles *cut = active_cut(c);
+    const AdvData  *adv = active_adv(c);
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s)
-            : launch_residual<3, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s);
+      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s)
+            : launch_residual<3, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s);
     else
-      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s)
-            : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, active_cut(c), s);
+      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s)
+            : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s);
     if (e != cudaSuccess)
       return e;
     return c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s)
@@ -380,6 +384,9 @@ int sint_destroy(sint_ctx *c)
   cudaFree(c->seg_blocks);
   cudaFree(c->seg_acc);
   cudaFree(c->seg_error);
+  cudaFree(c->adv_cells);
+  cudaFree(c->adv_segments);
+  cudaFree(c->adv_error);
   cudaFree(c->pc_raw);
   cudaFree(c->pc_inv64);
   cudaFree(c->pc_inv32);

@@ -234,6 +234,38 @@ namespace sint
       }
   }
 
+  // Values at the NQ points in registers: vq[q] = sum_l phi_l(x_q) u_l, one
+  // direction at a time.
+  template <int DIM, typename R>
+  __device__ __forceinline__ void cell_values(const R (&u)[1 << DIM], const CellConsts<DIM, R> &k,
+                                              R (&vq)[1 << DIM])
+  {
+    constexpr int NQ = 1 << DIM;
+    const R       xq[2] = {k.x0, k.x1};
+    R             a[NQ];
+#pragma unroll
+    for (int l = 0; l < NQ; ++l)
+      a[l] = u[l];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      {
+        // a is indexed by point bits below d and node bits from d on
+        R b[NQ];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i)
+          {
+            const int lo = i & ~(1 << d), hi = i | (1 << d);
+            b[i]         = a[lo] + xq[(i >> d) & 1] * (a[hi] - a[lo]);
+          }
+#pragma unroll
+        for (int i = 0; i < NQ; ++i)
+          a[i] = b[i];
+      }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      vq[q] = a[q];
+  }
+
   // 1D contraction of a point pair (a at x_0, b at x_1) with phi_l:
   // l = 0 -> x_1 a + x_0 b, l = 1 -> x_0 a + x_1 b
   template <typename R>

@@ -173,12 +173,15 @@ namespace sint
   {
     const int    *cell_segments = nullptr;
     const double *segments      = nullptr;
+    int           n_segments    = 0;
+    int           reserved      = 0; // explicit padding: the struct is compared bytewise
     double        origin[3]     = {0.0, 0.0, 0.0};
   };
 
   // Velocity of grain b at quadrature point q (bit d of q = upper Gauss point
   // in direction d) of the cell with global coordinates cc; false when the
-  // cell belongs to no segment of b.
+  // cell belongs to no segment of b (an id outside 0..n_segments - 1 counts
+  // as none).
   template <int DIM, typename R>
   __device__ __forceinline__ bool advection_velocity(const AdvData &a, const Grid &g, const int (&cc)[3], int q,
                                                      int b, R (&v)[DIM])
@@ -186,7 +189,7 @@ namespace sint
     const long long n_cells = (long long)g.n[0] * g.n[1] * g.n[2];
     const long long cell    = cc[0] + (long long)g.n[0] * (cc[1] + (long long)g.n[1] * cc[2]);
     const int       s       = a.cell_segments[b * n_cells + cell];
-    if (s < 0)
+    if (s < 0 || s >= a.n_segments)
       return false;
     const double *d      = a.segments + 9 * (long long)s;
     const double  lo     = 0.5 - 0.5 / sqrt(3.0), hi = 0.5 + 0.5 / sqrt(3.0);

@@ -4,7 +4,9 @@
 namespace sint
 {
   template cudaError_t launch_jvp<2, false, double>(int, const Grid &, const Phys &, const double *, const double *,
-                                                   double *, double *, const CutTiles *, cudaStream_t);
+                                                   double *, double *, const CutTiles *, const AdvData *,
+                                                   cudaStream_t);
   template cudaError_t launch_jvp<2, false, float>(int, const Grid &, const Phys &, const float *, const float *,
-                                                  float *, float *, const CutTiles *, cudaStream_t);
+                                                  float *, float *, const CutTiles *, const AdvData *,
+                                                  cudaStream_t);
 } // namespace sint

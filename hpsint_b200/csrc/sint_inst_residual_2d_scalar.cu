@@ -4,5 +4,6 @@
 namespace sint
 {
   template cudaError_t launch_residual<2, false>(int, int, const Grid &, const Phys &, const double *,
-                                                const double *const *, double *, double *, const CutTiles *, cudaStream_t);
+                                                const double *const *, double *, double *, const CutTiles *,
+                                                const AdvData *, cudaStream_t);
 } // namespace sint

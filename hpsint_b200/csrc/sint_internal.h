@@ -70,6 +70,15 @@ namespace sint
     int                 seg_acc_cap = 0;
     int                *seg_error   = nullptr;
 
+    // advection (sint_set_advection): the grains' segment of every cell and
+    // the segments' velocities and centers, copied from the caller
+    bool    adv          = false;
+    int    *adv_cells    = nullptr; // G x n_cells
+    double *adv_segments = nullptr; // adv_seg_cap x 9
+    int      adv_seg_cap = 0;
+    unsigned *adv_error  = nullptr; // count of invalid ids (sint_set_advection)
+    AdvData  adv_view;              // the above as the kernels take them
+
     double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
     double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
     float  *pc_inv32 = nullptr;
@@ -133,6 +142,7 @@ namespace sint
   inline const CutTiles *active_cut(const Ctx *c) { return c->cut ? &c->cut_view : nullptr; }
   inline const uint16_t *active_tile_union(const Ctx *c) { return c->cut ? c->tile_union : nullptr; }
   inline const uint32_t *active_live(const Ctx *c) { return (c->cut && c->skip_zeros) ? c->live : nullptr; }
+  inline const AdvData  *active_adv(const Ctx *c) { return c->adv ? &c->adv_view : nullptr; }
   // J v through the cell kernel + combine, with c->partial as scratch.
   template <typename R>
   cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s);

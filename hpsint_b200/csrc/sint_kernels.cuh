@@ -323,6 +323,55 @@ namespace sint
       }
   }
 
+  // Global coordinates of local cell `cell` of tile tc; false outside the mesh.
+  template <int DIM>
+  __device__ __forceinline__ bool cell_global(int cell, const TileCoord &tc, const Grid &g, int (&cc)[3])
+  {
+    using T = Tile<DIM>;
+    cc[0]   = tc.o[0] + cell % T::TX;
+    cc[1]   = tc.o[1] + (cell / T::TX) % T::TY;
+    cc[2]   = DIM == 3 ? tc.o[2] + cell / (T::TX * T::TY) : 0;
+    return cc[0] < g.n[0] && cc[1] < g.n[1] && (DIM == 2 || cc[2] < g.n[2]);
+  }
+
+  // Advection of the c row at point q (phase 2, after the point physics):
+  // the c flux loses v_i c for every grain i with a velocity on the cell, one
+  // grain after the other (operator_sintering_generic.h:1015-1036 for the
+  // residual, :167-177 for J v, where c is the direction's value).  With the
+  // grain cut-off only the cell's relevant grains move it (AdvectionVelocityData
+  // maps order parameters through the relevant-grain table,
+  // sintering/advection.h:225-245); gl maps the compacted grain k to its order
+  // parameter.
+  template <int DIM, int G, typename R, bool CUT>
+  __device__ __forceinline__ void advect_c_point(const AdvData &a, const Grid &g, const TileCoord &tc, const R *F,
+                                                 int c_base, R *P, int q, int cell, unsigned m,
+                                                 unsigned long long gl)
+  {
+    int cc[3];
+    if (!cell_global<DIM>(cell, tc, g, cc))
+      return;
+    const R c = fval<DIM>(F, c_base, q, cell);
+    R       flux[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      flux[d] = P[((1 + d) * Slots<DIM>::NQ + q) * Tile<DIM>::CELLS + cell];
+#pragma unroll 1
+    for (int i = 0; i < G; ++i)
+      {
+        if (CUT && ((m >> i) & 1u) == 0u)
+          continue;
+        const int b = CUT ? int((gl >> (4 * i)) & 15ull) : i;
+        R         v[DIM];
+        if (advection_velocity<DIM>(a, g, cc, q, b, v))
+#pragma unroll
+          for (int d = 0; d < DIM; ++d)
+            flux[d] = flux[d] - v[d] * c;
+      }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      P[((1 + d) * Slots<DIM>::NQ + q) * Tile<DIM>::CELLS + cell] = flux[d];
+  }
+
   // Phase 3: integrate every row of every cell into K[(row * NQ + l) * CP + cell];
   // contributions of cells outside the mesh (partial tiles) are zero.  `stiff`
   // holds the nodal values the constant-coefficient gradient terms act on
@@ -330,11 +379,14 @@ namespace sint
   // With the grain cut-off (CUT) the row of a grain absent on the cell is zero
   // (do_vmult_range_no_template / do_evaluate_nonlinear_residual_nt,
   // operator_sintering_generic.h:456-537, :1008-1081, assemble the relevant
-  // grains' rows only).
-  template <int DIM, int G, typename R, bool CUT = false>
+  // grains' rows only).  ADV: the eta_i row of a grain with a velocity on the
+  // cell gains the flux -v_i eta_i (operator_sintering_generic.h:1015-1036,
+  // :167-177), eta_i interpolated from the same nodal values `stiff` holds.
+  template <int DIM, int G, typename R, bool CUT = false, bool ADV = false>
   __device__ __forceinline__ void phase_integrate(const PhysR<R> &p, const Grid &g, const CellConsts<DIM, R> &k,
                                                   const TileCoord &tc, const R *P, const R *stiff, R *K,
-                                                  unsigned m = ~0u)
+                                                  unsigned m = ~0u, const AdvData *adv = nullptr,
+                                                  unsigned long long gl = 0ull)
   {
     using T            = Tile<DIM>;
     constexpr int NQ   = 1 << DIM;
@@ -371,6 +423,37 @@ namespace sint
                   gg[d][q] = P[((1 + d) * NQ + q) * T::CELLS + cell];
               }
             cell_integrate_vg<DIM>(v, gg, k, r);
+          }
+        else if (ADV && row >= 2)
+          {
+            R v[NQ], u[NQ], gg[DIM][NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+              {
+                v[q] = P[((DIM + row) * NQ + q) * T::CELLS + cell];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                  gg[d][q] = R(0);
+              }
+            cell_nodes<DIM>(stiff + row * T::BOX, b0, u);
+            int cc[3];
+            if (cell_global<DIM>(cell, tc, g, cc))
+              {
+                const int b = CUT ? int((gl >> (4 * (row - 2))) & 15ull) : row - 2;
+                R         e[NQ];
+                cell_values<DIM>(u, k, e);
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                  {
+                    R vel[DIM];
+                    if (advection_velocity<DIM>(*adv, g, cc, q, b, vel))
+#pragma unroll
+                      for (int d = 0; d < DIM; ++d)
+                        gg[d][q] = -(vel[d] * e[q]);
+                  }
+              }
+            cell_integrate_vg<DIM>(v, gg, k, r);
+            cell_stiffness_add<DIM>(p.L * p.kp, u, g, r);
           }
         else
           {
@@ -462,10 +545,11 @@ namespace sint
   // of the tile's grains treats it as absent.  The tile ids, grain lists and
   // masks of the next tile are read one tile ahead, so their latency hides
   // behind the current tile.
-  template <int DIM, int G, bool TENS, typename R, bool CUT>
+  // ADV: with the advection terms of the grains' rigid-body velocities.
+  template <int DIM, int G, bool TENS, typename R, bool CUT, bool ADV = false>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS, jvp_blocks_per_sm<DIM, G, R>())
     jvp_kernel(const Grid g, const Phys ph, const R *__restrict__ lin, const R *__restrict__ src,
-               R *__restrict__ dst, R *__restrict__ partial, const CutTiles ct)
+               R *__restrict__ dst, R *__restrict__ partial, const CutTiles ct, const AdvData adv)
   {
     using T  = Tile<DIM>;
     using SM = ThreePhaseSmem<DIM, G, TENS, true, false>;
@@ -547,8 +631,14 @@ namespace sint
         phase_evaluate<DIM, G, TENS, true, false, R, CUT>(cb, cb + C * T::BOX, F, k, m);
         __syncthreads();
         jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, cell, m);
+        if constexpr (ADV)
+          {
+            using FM = FieldMap<DIM, G, TENS, true, false>;
+            advect_c_point<DIM, G, R, CUT>(adv, g, tc, F, FM::base(FM::src_c), P, threadIdx.x / T::CELLS, cell, m,
+                                           gl);
+          }
         __syncthreads();
-        phase_integrate<DIM, G, R, CUT>(p, g, k, tc, P, cb + C * T::BOX, K, m);
+        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, cb + C * T::BOX, K, m, &adv, gl);
         __syncthreads();
         sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
         __syncthreads(); // K and this buffer are reused by the next iterations
@@ -575,11 +665,12 @@ namespace sint
   // solutions is formed at the nodes while staging and evaluated at the points.
   // CUT: the kernel for G grains runs over the tiles of class G on their
   // compacted components, as the Jacobian product does.
-  template <int DIM, int G, bool TENS, int WTD, bool CUT>
+  // ADV: with the advection terms of the grains' rigid-body velocities.
+  template <int DIM, int G, bool TENS, int WTD, bool CUT, bool ADV = false>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS, residual_blocks_per_sm<DIM, G>())
     residual_kernel(const Grid g, const Phys ph, const double *__restrict__ src, const double *__restrict__ h0,
                     const double *__restrict__ h1, const double *__restrict__ h2, double *__restrict__ dst,
-                    double *__restrict__ partial, const CutTiles ct)
+                    double *__restrict__ partial, const CutTiles ct, const AdvData adv)
   {
     using R  = double;
     using T  = Tile<DIM>;
@@ -628,8 +719,14 @@ namespace sint
         phase_evaluate<DIM, G, TENS, false, WTD == 2, R, CUT>(s_u, s_h, F, k, m);
         __syncthreads();
         residual_point<DIM, G, TENS, WTD, R>(p, F, P, threadIdx.x / T::CELLS, threadIdx.x % T::CELLS, m);
+        if constexpr (ADV)
+          {
+            using FM = FieldMap<DIM, G, TENS, false, WTD == 2>;
+            advect_c_point<DIM, G, R, CUT>(adv, g, tc, F, FM::base(FM::lin_c), P, threadIdx.x / T::CELLS,
+                                           threadIdx.x % T::CELLS, m, gl);
+          }
         __syncthreads();
-        phase_integrate<DIM, G, R, CUT>(p, g, k, tc, P, s_u, K, m);
+        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, s_u, K, m, &adv, gl);
         __syncthreads();
         sum_and_store<DIM>(K, C, g, tc, bn, dst, partial, gl, CUT, ct.c_all, tm);
         __syncthreads();

@@ -15,15 +15,26 @@ namespace sint
   // Dynamic shared memory of the diagonal kernel (bytes).
   size_t smem_diag(int dim, int G);
 
-  // cut: the grain cut-off's tile classes, nullptr for the full operator
+  // cut: the grain cut-off's tile classes, nullptr for the full operator;
+  // adv: the grains' rigid-body velocities, nullptr for no advection
   template <int DIM, bool TENS, typename R>
   cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                         const CutTiles *cut, cudaStream_t s);
+                         const CutTiles *cut, const AdvData *adv, cudaStream_t s);
 
   template <int DIM, bool TENS>
   cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
                               const double *const *hist, double *dst, double *partial, const CutTiles *cut,
-                              cudaStream_t s);
+                              const AdvData *adv, cudaStream_t s);
+
+  // The same with the advection terms (instantiated in sint_inst_adv_*.cu).
+  template <int DIM, bool TENS, typename R>
+  cudaError_t launch_jvp_adv(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
+                             const CutTiles *cut, const AdvData &adv, cudaStream_t s);
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_residual_adv(int G, int wtd, const Grid &g, const Phys &p, const double *src,
+                                  const double *const *hist, double *dst, double *partial, const CutTiles *cut,
+                                  const AdvData &adv, cudaStream_t s);
 
   // mask: the cut-off's per-cell grain masks, nullptr for the full operator
   template <int DIM, bool TENS>

@@ -27,12 +27,12 @@ namespace sint
     return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
   }
 
-  template <int DIM, int G, bool TENS, typename R, bool CUT>
+  template <int DIM, int G, bool TENS, typename R, bool CUT, bool ADV>
   cudaError_t launch_jvp_g(const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                           const CutTiles &ct, cudaStream_t s)
+                           const CutTiles &ct, const AdvData &adv, cudaStream_t s)
   {
     const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false>::TOTAL * sizeof(R);
-    auto         k    = jvp_kernel<DIM, G, TENS, R, CUT>;
+    auto         k    = jvp_kernel<DIM, G, TENS, R, CUT, ADV>;
     // persistent grid: as many blocks as are resident at once
     static int   grid_cap = 0;
     cudaError_t  e        = cudaSuccess;
@@ -48,17 +48,18 @@ namespace sint
         grid_cap = sms * (per_sm > 0 ? per_sm : 1);
       }
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
-    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, ct);
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, ct, adv);
     count_launches(1);
     return cudaGetLastError();
   }
 
-  template <int DIM, int G, bool TENS, int WTD, bool CUT>
+  template <int DIM, int G, bool TENS, int WTD, bool CUT, bool ADV>
   cudaError_t launch_residual_g(const Grid &g, const Phys &p, const double *src, const double *const *hist,
-                                double *dst, double *partial, const CutTiles &ct, cudaStream_t s)
+                                double *dst, double *partial, const CutTiles &ct, const AdvData &adv,
+                                cudaStream_t s)
   {
     const size_t  smem     = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2>::TOTAL * sizeof(double);
-    auto          k        = residual_kernel<DIM, G, TENS, WTD, CUT>;
+    auto          k        = residual_kernel<DIM, G, TENS, WTD, CUT, ADV>;
     static int    grid_cap = 0;
     cudaError_t   e        = cudaSuccess;
     if (grid_cap == 0)
@@ -76,7 +77,7 @@ namespace sint
     const double *h1     = (WTD == 2 && p.order > 1) ? hist[1] : nullptr;
     const double *h2     = (WTD == 2 && p.order > 2) ? hist[2] : nullptr;
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
-    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial, ct);
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, src, h0, h1, h2, dst, partial, ct, adv);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -133,40 +134,54 @@ namespace sint
       default: return cudaErrorInvalidValue;                                                                      \
     }
 
-  template <int DIM, bool TENS, typename R>
+  template <int DIM, bool TENS, typename R, bool ADV>
   cudaError_t launch_jvp_class(int K, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                               const CutTiles &ct, cudaStream_t s)
+                               const CutTiles &ct, const AdvData &adv, cudaStream_t s)
   {
-#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, true>(g, p, lin, src, dst, partial, ct, s)
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, true, ADV>(g, p, lin, src, dst, partial, ct, adv, s)
     SINT_CLASS_SWITCH(K, SINT_CALL)
 #undef SINT_CALL
   }
 
   // cut == nullptr: the full operator; otherwise the grain cut-off, one
-  // launch per grain-count class 0..G (classes without tiles return at once)
-  template <int DIM, bool TENS, typename R>
-  cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
-                         const CutTiles *cut, cudaStream_t s)
+  // launch per grain-count class 0..G (classes without tiles return at once).
+  // ADV: the kernels with the advection terms.
+  template <int DIM, bool TENS, typename R, bool ADV>
+  cudaError_t launch_jvp_impl(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
+                              const CutTiles *cut, const AdvData &adv, cudaStream_t s)
   {
     if (cut)
       {
         for (int K = 0; K <= G; ++K)
-          if (const cudaError_t e = launch_jvp_class<DIM, TENS, R>(K, g, p, lin, src, dst, partial, *cut, s))
+          if (const cudaError_t e =
+                launch_jvp_class<DIM, TENS, R, ADV>(K, g, p, lin, src, dst, partial, *cut, adv, s))
             return e;
         return cudaSuccess;
       }
     const CutTiles none;
-#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, false>(g, p, lin, src, dst, partial, none, s)
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, false, ADV>(g, p, lin, src, dst, partial, none, adv, s)
     SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
   }
 
-  // G = the grain count (full operator, 1..12) or the class (grain cut-off, 0..12)
-  template <int DIM, bool TENS, bool CUT, int WTD>
-  cudaError_t launch_residual_w(int G, const Grid &g, const Phys &p, const double *src, const double *const *hist,
-                                double *dst, double *partial, const CutTiles &ct, cudaStream_t s)
+  // The advection kernels are instantiated in their own translation units
+  // (launch_jvp_adv, launch_residual_adv).
+  template <int DIM, bool TENS, typename R>
+  cudaError_t launch_jvp(int G, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
+                         const CutTiles *cut, const AdvData *adv, cudaStream_t s)
   {
-#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, WTD, CUT>(g, p, src, hist, dst, partial, ct, s)
+    if (adv)
+      return launch_jvp_adv<DIM, TENS, R>(G, g, p, lin, src, dst, partial, cut, *adv, s);
+    return launch_jvp_impl<DIM, TENS, R, false>(G, g, p, lin, src, dst, partial, cut, AdvData(), s);
+  }
+
+  // G = the grain count (full operator, 1..12) or the class (grain cut-off, 0..12)
+  template <int DIM, bool TENS, bool CUT, int WTD, bool ADV>
+  cudaError_t launch_residual_w(int G, const Grid &g, const Phys &p, const double *src, const double *const *hist,
+                                double *dst, double *partial, const CutTiles &ct, const AdvData &adv,
+                                cudaStream_t s)
+  {
+#define SINT_CALL(GG) launch_residual_g<DIM, GG, TENS, WTD, CUT, ADV>(g, p, src, hist, dst, partial, ct, adv, s)
     if constexpr (CUT)
       {
         SINT_CLASS_SWITCH(G, SINT_CALL)
@@ -178,32 +193,42 @@ namespace sint
 #undef SINT_CALL
   }
 
-  template <int DIM, bool TENS, bool CUT>
+  template <int DIM, bool TENS, bool CUT, bool ADV>
   cudaError_t launch_residual_c(int G, int wtd, const Grid &g, const Phys &p, const double *src,
                                 const double *const *hist, double *dst, double *partial, const CutTiles &ct,
-                                cudaStream_t s)
+                                const AdvData &adv, cudaStream_t s)
   {
     if (wtd == 0)
-      return launch_residual_w<DIM, TENS, CUT, 0>(G, g, p, src, hist, dst, partial, ct, s);
+      return launch_residual_w<DIM, TENS, CUT, 0, ADV>(G, g, p, src, hist, dst, partial, ct, adv, s);
     if (wtd == 1)
-      return launch_residual_w<DIM, TENS, CUT, 1>(G, g, p, src, hist, dst, partial, ct, s);
-    return launch_residual_w<DIM, TENS, CUT, 2>(G, g, p, src, hist, dst, partial, ct, s);
+      return launch_residual_w<DIM, TENS, CUT, 1, ADV>(G, g, p, src, hist, dst, partial, ct, adv, s);
+    return launch_residual_w<DIM, TENS, CUT, 2, ADV>(G, g, p, src, hist, dst, partial, ct, adv, s);
   }
 
-  template <int DIM, bool TENS>
-  cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
-                              const double *const *hist, double *dst, double *partial, const CutTiles *cut,
-                              cudaStream_t s)
+  template <int DIM, bool TENS, bool ADV>
+  cudaError_t launch_residual_impl(int G, int wtd, const Grid &g, const Phys &p, const double *src,
+                                   const double *const *hist, double *dst, double *partial, const CutTiles *cut,
+                                   const AdvData &adv, cudaStream_t s)
   {
     if (cut)
       {
         for (int K = 0; K <= G; ++K)
           if (const cudaError_t e =
-                launch_residual_c<DIM, TENS, true>(K, wtd, g, p, src, hist, dst, partial, *cut, s))
+                launch_residual_c<DIM, TENS, true, ADV>(K, wtd, g, p, src, hist, dst, partial, *cut, adv, s))
             return e;
         return cudaSuccess;
       }
-    return launch_residual_c<DIM, TENS, false>(G, wtd, g, p, src, hist, dst, partial, CutTiles(), s);
+    return launch_residual_c<DIM, TENS, false, ADV>(G, wtd, g, p, src, hist, dst, partial, CutTiles(), adv, s);
+  }
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_residual(int G, int wtd, const Grid &g, const Phys &p, const double *src,
+                              const double *const *hist, double *dst, double *partial, const CutTiles *cut,
+                              const AdvData *adv, cudaStream_t s)
+  {
+    if (adv)
+      return launch_residual_adv<DIM, TENS>(G, wtd, g, p, src, hist, dst, partial, cut, *adv, s);
+    return launch_residual_impl<DIM, TENS, false>(G, wtd, g, p, src, hist, dst, partial, cut, AdvData(), s);
   }
 
   template <int DIM, bool TENS>

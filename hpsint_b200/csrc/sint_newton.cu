@@ -53,11 +53,12 @@ namespace sint
       cudaGraphExec_t exec  = nullptr;
       Phys            key   = {};
       const uint16_t *mask  = nullptr; // cell masks the captured kernels read (nullptr: no cut-off)
+      AdvData         adv   = {};      // advection tables the captured kernels read (none: null pointers)
       int             nodes = 0;
     } graphs[MAX_MULTIDOT];
-    // [FP32 Krylov vectors][grain cut-off]: one eager solve with this kernel
-    // set has run (lazy kernel set-up is done outside any capture)
-    bool warm[2][2] = {{false, false}, {false, false}};
+    // [FP32 Krylov vectors][grain cut-off][advection]: one eager solve with
+    // this kernel set has run (lazy kernel set-up is done outside any capture)
+    bool warm[2][2][2] = {};
   };
 
   int free_workspace(Ctx *c)
@@ -340,12 +341,14 @@ namespace sint
     // then record the event the host waits on.
     auto enqueue = [&](int j) -> int {
       int r = SINT_OK;
-      if (!ws->warm[sizeof(R) == 4][c->cut])
+      const AdvData adv = c->adv ? c->adv_view : AdvData();
+      if (!ws->warm[sizeof(R) == 4][c->cut][c->adv])
         r = enqueue_kernels(j);
       else
         {
           auto &g = ws->graphs[j];
-          if (!g.exec || std::memcmp(&g.key, &c->phys, sizeof(Phys)) != 0 || g.mask != active_mask(c))
+          if (!g.exec || std::memcmp(&g.key, &c->phys, sizeof(Phys)) != 0 || g.mask != active_mask(c) ||
+              std::memcmp(&g.adv, &adv, sizeof(AdvData)) != 0)
             {
               cudaGraph_t       graph = nullptr;
               const long long   n0    = sint_kernel_launch_count();
@@ -385,6 +388,7 @@ namespace sint
                 }
               g.key   = c->phys;
               g.mask  = active_mask(c);
+              g.adv   = adv;
               g.nodes = int(nn);
             }
           const cudaError_t e = cudaGraphLaunch(g.exec, s);
@@ -546,7 +550,7 @@ namespace sint
     if (e != cudaSuccess)
       return cuda_fail(e, "GMRES: join back");
     if (rc == SINT_OK)
-      ws->warm[sizeof(R) == 4][c->cut] = true;
+      ws->warm[sizeof(R) == 4][c->cut][c->adv] = true;
     return rc;
   }
 

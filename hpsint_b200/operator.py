@@ -214,6 +214,32 @@ class SinteringOperatorGeneric:
         L.check(L.lib().sint_get_component_mask(self._h, _ptr(out), _stream()), "sint_get_component_mask")
         return out
 
+    def set_advection(self, cell_segments, segments):
+        """Rigid-body motion of the grains (AdvectionMechanism,
+        sintering/advection.h:297-520): the residual and J v gain the terms
+        -(v_i c, grad phi) in the c row and -(v_i eta_i, grad phi) in the
+        eta_i rows.  cell_segments: device int32 tensor (n_grains, n_cells),
+        the segment of each order parameter a cell belongs to or -1;
+        segments: device float64 tensor (n_segments, 9) = translational
+        velocity, angular velocity (z only in 2D), center.  None switches
+        advection off.  The tables are copied."""
+        if cell_segments is None:
+            L.check(L.lib().sint_set_advection(self._h, None, None, 0, _stream()), "sint_set_advection")
+            return
+        n_cells = 1
+        for d in range(self.mesh.dim):
+            n_cells *= self.mesh.n_cells[d]
+        if (cell_segments.dtype != torch.int32 or not cell_segments.is_cuda or not cell_segments.is_contiguous()
+                or cell_segments.numel() != self.params.n_grains * n_cells):
+            raise ValueError(f"cell_segments must be a contiguous int32 CUDA tensor of {self.params.n_grains} x "
+                             f"{n_cells} ids")
+        if (segments.dtype != torch.float64 or not segments.is_cuda or not segments.is_contiguous()
+                or segments.numel() % 9 != 0):
+            raise ValueError("segments must be a contiguous float64 CUDA tensor of n_segments x 9 values")
+        n_seg = segments.numel() // 9
+        L.check(L.lib().sint_set_advection(self._h, _ptr(cell_segments), _ptr(segments) if n_seg else None, n_seg,
+                                           _stream()), "sint_set_advection")
+
     def evaluate_nonlinear_residual(self, dst, src, with_time_derivative=2, history=()):
         self._check_vec(dst, torch.float64)
         self._check_vec(src, torch.float64)

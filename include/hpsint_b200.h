@@ -261,6 +261,30 @@ int sint_grain_segment_properties(sint_ctx *ctx, const double *eta, const int *p
                                   double *props, sint_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Advection: rigid-body motion of the grains (AdvectionMechanism,          */
+/* sintering/advection.h:297-520).  Replaces the AdvectionMechanism the     */
+/* operator is constructed with (operator_sintering_generic.h:347-361).     */
+
+/* Sets the grains' velocities for the residual and J v of this context
+ * (operator_sintering_generic.h:167-177, :1015-1036: the c row gains
+ * -(v_i c, grad phi) and the eta_i row -(v_i eta_i, grad phi) for every
+ * grain i with a velocity on the cell).
+ *   cell_segments  DEVICE, n_grains x n_cells int32 (cells x fastest): the
+ *                  segment (particle) of order parameter b that cell belongs
+ *                  to, -1 for none (AdvectionMechanism::cell_index_values,
+ *                  advection.h:411-446)
+ *   segments       DEVICE, n_segments x 9 doubles: translational velocity
+ *                  (3), angular velocity (3; only z is used in 2D) and
+ *                  center (3) of each segment; the velocity at x is
+ *                  v_t + w x (x - center) (calc_translation_velocity /
+ *                  calc_rotation_velocity, advection.h:330-352)
+ * Both are copied (the caller may free or reuse its buffers); ids outside
+ * [-1, n_segments) are an error.  cell_segments == NULL switches advection
+ * off.  Synchronises `stream` (the id check). */
+int sint_set_advection(sint_ctx *ctx, const int32_t *cell_segments, const double *segments, int n_segments,
+                       sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* BLAS-1 on block vectors: DynamicBlockVector                              */
 /* (include/pf-applications/lac/dynamic_block_vector.h:346-516).            */
 /* n = number of elements (C * block_stride for a whole block vector).      */

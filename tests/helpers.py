@@ -129,3 +129,22 @@ def tracker_golden_field(g):
     r = np.sqrt((X - c["center"][0]) ** 2 + (Y - c["center"][1]) ** 2)
     in_c = r <= c["radius"] if c["inclusive"] else r < c["radius"]
     return 2, cells, h, mesh["lower"], np.where(in_e | in_c, 1.0, 0.0).ravel()
+
+
+def advection_data(dim, cells, G, seed, n_seg_per_grain=2, scale=1.0):
+    """Random segment assignment (-1 on about a third of the cells) and random
+    segment velocities/centers."""
+    rng = np.random.default_rng(seed)
+    n_cells = int(np.prod(cells))
+    S = G * n_seg_per_grain
+    seg = np.full((G, n_cells), -1, dtype=np.int32)
+    for b in range(G):
+        pick = rng.integers(0, n_seg_per_grain, n_cells) + b * n_seg_per_grain
+        seg[b] = np.where(rng.uniform(size=n_cells) < 0.67, pick, -1)
+    data = np.zeros((S, 9))
+    data[:, 0:3] = scale * rng.normal(size=(S, 3))
+    data[:, 3:6] = 0.2 * scale * rng.normal(size=(S, 3))
+    data[:, 6:9] = rng.uniform(0, 4, size=(S, 3))
+    if dim == 2:
+        data[:, 2] = 0.0
+    return seg, data

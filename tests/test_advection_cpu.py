@@ -16,29 +16,10 @@ import itertools
 import numpy as np
 import pytest
 
-from helpers import oracle_mesh, random_state
+from helpers import advection_data, oracle_mesh, random_state
 from oracle import oracle as O
 
 GP = (0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0))
-
-
-def advection_data(dim, cells, G, seed, n_seg_per_grain=2, scale=1.0):
-    """Random segment assignment (-1 on about a third of the cells) and random
-    segment velocities/centers."""
-    rng = np.random.default_rng(seed)
-    n_cells = int(np.prod(cells))
-    S = G * n_seg_per_grain
-    seg = np.full((G, n_cells), -1, dtype=np.int32)
-    for b in range(G):
-        pick = rng.integers(0, n_seg_per_grain, n_cells) + b * n_seg_per_grain
-        seg[b] = np.where(rng.uniform(size=n_cells) < 0.67, pick, -1)
-    data = np.zeros((S, 9))
-    data[:, 0:3] = scale * rng.normal(size=(S, 3))
-    data[:, 3:6] = 0.2 * scale * rng.normal(size=(S, 3))
-    data[:, 6:9] = rng.uniform(0, 4, size=(S, 3))
-    if dim == 2:
-        data[:, 2] = 0.0
-    return seg, data
 
 
 def numpy_advection(dim, cells, h, origin, u, seg, data):

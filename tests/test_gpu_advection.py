@@ -1,0 +1,270 @@
+"""Advection (grain rigid-body motion) on the GPU against the CPU oracle.
+
+The residual and Jacobian products with given segment velocities meet the
+full operator's tolerances (FP64 1e-12 per-block relative, FP32 2e-5 against
+the oracle at FP32-rounded inputs), alone and under the grain cut-off;
+switching advection off gives back the operator bit for bit; the device
+Newton solve with advection converges to the oracle's step; graph-replayed
+solves read the current velocities.
+"""
+import numpy as np
+import pytest
+
+from helpers import advection_data, block_rel_err, oracle_mesh, particle_state, random_state
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+ORIGIN = (1.5, -2.0, 0.25)
+H = (0.9, 1.1, 1.0)
+
+
+def make_op(dim, cells, G, tensorial, h=H, origin=ORIGIN):
+    import hpsint_b200 as hb
+    mesh = hb.Mesh(dim, tuple(cells) + (1,) * (3 - len(cells)), tuple(h), tuple(origin))
+    om = O.make_mesh(dim, list(cells) + [0] * (3 - dim), h)
+    return hb.SinteringOperatorGeneric(mesh, hb.Params(G, tensorial=tensorial)), O.make_params(G, tensorial=tensorial), om
+
+
+def set_adv(op, seg, data):
+    op.set_advection(torch.from_numpy(seg).cuda().contiguous(), torch.from_numpy(data).cuda().contiguous())
+
+
+CASES = [
+    # dim, cells, G, tensorial
+    (2, (37, 21), 3, True),
+    (2, (37, 21), 4, False),
+    (2, (30, 26), 9, True),
+    (3, (13, 11, 9), 5, True),
+    (3, (13, 11, 9), 3, False),
+    (3, (11, 9, 10), 9, True),
+]
+
+
+def ids(c):
+    return f"{c[0]}d-G{c[2]}-{'tens' if c[3] else 'scal'}"
+
+
+@pytest.mark.parametrize("case", CASES, ids=[ids(c) for c in CASES])
+def test_residual_and_jacobian_match_oracle(case):
+    dim, cells, G, tens = case
+    op, p, om = make_op(dim, cells, G, tens)
+    u = particle_state(dim, cells, G, seed=41)
+    old = particle_state(dim, cells, G, seed=41, width=1.2)
+    src = random_state(dim, cells, G, seed=42, smooth=False) - 0.5
+    seg, data = advection_data(dim, cells, G, seed=43, scale=5.0)
+    set_adv(op, seg, data)
+    adv = (seg, data, ORIGIN)
+    op.set_time_weights(20.0, [-20.0], 1.0)
+    T = O.make_time(20.0, 1.0, [-20.0])
+    ud = op.to_device(u)
+    r = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(r, ud, 2, [op.to_device(old)])
+    op.fill_quadrature_point_values(ud)
+    j = op.initialize_dof_vector()
+    op.vmult(j, op.to_device(src))
+    torch.cuda.synchronize()
+    r_ref = O.residual(om, p, T, u, [old], 2, advection=adv)
+    j_ref = O.jvp(om, p, T, u, src, advection=adv)
+    assert block_rel_err(op.to_host(r), r_ref) <= 1e-12
+    assert block_rel_err(op.to_host(j), j_ref) <= 1e-12
+    # advection changed the result
+    assert block_rel_err(j_ref, O.jvp(om, p, T, u, src)) > 1e-6
+    assert block_rel_err(r_ref, O.residual(om, p, T, u, [old], 2)) > 1e-6
+    # residual without the time derivative (with_time_derivative 0) too
+    r0 = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(r0, ud, 0)
+    torch.cuda.synchronize()
+    assert block_rel_err(op.to_host(r0), O.residual(om, p, T, u, [], 0, advection=adv)) <= 1e-12
+
+
+@pytest.mark.parametrize("case", CASES[:4], ids=[ids(c) for c in CASES[:4]])
+def test_jacobian_f32_close_to_oracle(case):
+    dim, cells, G, tens = case
+    op, p, om = make_op(dim, cells, G, tens)
+    u = particle_state(dim, cells, G, seed=44).astype(np.float32).astype(np.float64)
+    src = (random_state(dim, cells, G, seed=45, smooth=False) - 0.5).astype(np.float32).astype(np.float64)
+    seg, data = advection_data(dim, cells, G, seed=46, scale=5.0)
+    set_adv(op, seg, data)
+    op.set_time_weights(20.0, [-20.0], 1.0)
+    op.fill_quadrature_point_values(op.to_device(u))
+    j = op.initialize_dof_vector(torch.float32)
+    op.vmult(j, op.to_device(src, torch.float32))
+    torch.cuda.synchronize()
+    j_ref = O.jvp(om, p, O.make_time(20.0, 1.0, [-20.0]), u, src, advection=(seg, data, ORIGIN))
+    assert block_rel_err(op.to_host(j), j_ref) <= 2e-5
+
+
+@pytest.mark.parametrize("case", [CASES[0], CASES[3], CASES[5]], ids=[ids(c) for c in (CASES[0], CASES[3], CASES[5])])
+def test_advection_under_the_cut_off(case):
+    dim, cells, G, tens = case
+    op, p, om = make_op(dim, cells, G, tens)
+    u = particle_state(dim, cells, G, seed=47)
+    src = random_state(dim, cells, G, seed=48, smooth=False) - 0.5
+    seg, data = advection_data(dim, cells, G, seed=49, scale=5.0)
+    ud = op.to_device(u)
+    op.set_component_mask(ud, 1e-3)
+    mask = O.grain_mask(om, p, u, 1e-3)
+    set_adv(op, seg, data)
+    adv = (seg, data, ORIGIN)
+    op.set_time_weights(20.0, [-20.0], 1.0)
+    T = O.make_time(20.0, 1.0, [-20.0])
+    r = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(r, ud, 2, [ud])
+    op.fill_quadrature_point_values(ud)
+    j = op.initialize_dof_vector()
+    op.vmult(j, op.to_device(src))
+    torch.cuda.synchronize()
+    assert block_rel_err(op.to_host(r), O.residual(om, p, T, u, [u], 2, mask=mask, advection=adv)) <= 1e-12
+    assert block_rel_err(op.to_host(j), O.jvp(om, p, T, u, src, mask=mask, advection=adv)) <= 1e-12
+
+
+def test_switching_advection_off_is_the_plain_operator():
+    dim, cells, G, tens = 3, (13, 11, 9), 4, True
+    op, p, om = make_op(dim, cells, G, tens)
+    u = particle_state(dim, cells, G, seed=50)
+    src = random_state(dim, cells, G, seed=51, smooth=False) - 0.5
+    ud, sd = op.to_device(u), op.to_device(src)
+    op.set_time_weights(20.0, [-20.0], 1.0)
+    op.fill_quadrature_point_values(ud)
+    j0 = op.initialize_dof_vector()
+    op.vmult(j0, sd)
+    seg, data = advection_data(dim, cells, G, seed=52)
+    set_adv(op, seg, data)
+    j1 = op.initialize_dof_vector()
+    op.vmult(j1, sd)
+    op.set_advection(None, None)
+    j2 = op.initialize_dof_vector()
+    op.vmult(j2, sd)
+    # no segment anywhere: the advection kernels add nothing
+    set_adv(op, np.full_like(seg, -1), data)
+    j3 = op.initialize_dof_vector()
+    op.vmult(j3, sd)
+    torch.cuda.synchronize()
+    assert torch.equal(j0, j2)
+    assert not torch.equal(j0, j1)
+    assert torch.equal(j0, j3)
+
+
+def test_invalid_segment_ids_are_rejected():
+    import hpsint_b200 as hb
+    dim, cells, G = 2, (10, 8), 2
+    op, p, om = make_op(dim, cells, G, False)
+    seg, data = advection_data(dim, cells, G, seed=53)
+    bad = seg.copy()
+    bad[1, 17] = data.shape[0]  # one past the last segment
+    with pytest.raises(hb.SintError):
+        set_adv(op, bad, data)
+    bad[1, 17] = -2
+    with pytest.raises(hb.SintError):
+        set_adv(op, bad, data)
+    set_adv(op, seg, data)  # a valid table is accepted afterwards
+
+
+def _two_particles(cells, R=6.0):
+    from hpsint_b200 import packings as P
+    nx, ny = cells
+    c = np.array([[nx / 2 - R + 0.5, ny / 2], [nx / 2 + R - 0.5, ny / 2]])
+    return P.initial_state(2, cells, (1.0, 1.0), (0.0, 0.0), c, np.array([R, R]), np.array([0, 1]), width=2.0,
+                           noise=1e-3, seed=3)
+
+
+def _two_particle_advection(cells, R=6.0, vx=2.0, w=0.3):
+    """Grain 0 translates towards grain 1, grain 1 rotates about its center;
+    each grain's segment covers the cells of its half of the mesh."""
+    nx, ny = cells
+    n_cells = nx * ny
+    seg = np.full((2, n_cells), -1, dtype=np.int32)
+    ci = np.arange(n_cells) % nx
+    seg[0, ci < nx // 2] = 0
+    seg[1, ci >= nx // 2] = 1
+    data = np.zeros((2, 9))
+    data[0, 0] = vx
+    data[0, 6:8] = (nx / 2 - R + 0.5, ny / 2)
+    data[1, 5] = w
+    data[1, 6:8] = (nx / 2 + R - 0.5, ny / 2)
+    return seg, data
+
+
+def _cpu_newton(mesh, P, T, u_old, adv, tol_rel=1e-12, max_it=30):
+    from scipy.sparse.linalg import LinearOperator, gmres
+    u = u_old.copy()
+    C, N = u.shape
+    r0 = None
+    for _ in range(max_it):
+        r = O.residual(mesh, P, T, u, [u_old], 2, advection=adv)
+        nr = np.linalg.norm(r)
+        r0 = nr if r0 is None else r0
+        if nr <= tol_rel * r0 or nr < 1e-14:
+            return u
+        lin = u.copy()
+        J = LinearOperator((C * N, C * N),
+                           matvec=lambda v: O.jvp(mesh, P, T, lin, v.reshape(C, N), advection=adv).ravel())
+        du, info = gmres(J, -r.ravel(), rtol=1e-13, atol=0.0, restart=300, maxiter=50)
+        u = u + du.reshape(C, N)
+    raise RuntimeError("CPU Newton did not converge")
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_newton_with_advection_matches_cpu_newton(prec):
+    import hpsint_b200 as hb
+    cells, G, dt = (40, 20), 2, 1e-2
+    u_old = _two_particles(cells)
+    seg, data = _two_particle_advection(cells)
+    adv = (seg, data, (0.0, 0.0, 0.0))
+    mesh = oracle_mesh(2, cells)
+    P = O.make_params(G, tensorial=True)
+    T = O.make_time(1.0 / dt, 1.0, [-1.0 / dt])
+    ref = _cpu_newton(mesh, P, T, u_old, adv)
+    op = hb.SinteringOperatorGeneric(hb.Mesh(2, tuple(cells) + (1,)), hb.Params(G, tensorial=True))
+    op.set_time_weights(1.0 / dt, [-1.0 / dt], 1.0)
+    set_adv(op, seg, data)
+    old = op.to_device(u_old)
+    u = old.clone()
+    st = hb.DampedNewtonSolver(op, hb.NonLinearData(nl_rel_tol=1e-10, nl_abs_tol=1e-16, l_rel_tol=1e-4,
+                                                    nl_max_iter=20, inner_precision=prec)).solve(u, [old])
+    torch.cuda.synchronize()
+    assert st.status == 0
+    assert np.max(np.abs(op.to_host(u) - ref)) < (1e-7 if prec == 64 else 1e-6)
+    # advection moved the step away from the plain one
+    plain = O.residual(mesh, P, T, ref, [u_old], 2)
+    assert np.linalg.norm(plain) > 1e-3 * np.linalg.norm(O.residual(mesh, P, T, u_old, [u_old], 2))
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_graph_replayed_solve_reads_the_current_velocities(prec):
+    """The second solve replays the GMRES graphs captured in the first one;
+    new velocities in the same tables must give bitwise the result of a
+    fresh context."""
+    import hpsint_b200 as hb
+    cells, G, dt = (40, 20), 2, 1e-2
+    u_old = _two_particles(cells)
+    seg, data = _two_particle_advection(cells)
+    data2 = data.copy()
+    data2[0, 0], data2[1, 5] = -1.5, -0.4
+
+    def solve(op, d):
+        set_adv(op, seg, d)
+        old = op.to_device(u_old)
+        u = old.clone()
+        st = hb.DampedNewtonSolver(op, hb.NonLinearData(nl_rel_tol=1e-9, nl_abs_tol=1e-16,
+                                                        inner_precision=prec)).solve(u, [old])
+        torch.cuda.synchronize()
+        assert st.status == 0
+        return u
+
+    def new_op():
+        op = hb.SinteringOperatorGeneric(hb.Mesh(2, tuple(cells) + (1,)), hb.Params(G, tensorial=True))
+        op.set_time_weights(1.0 / dt, [-1.0 / dt], 1.0)
+        return op
+
+    op = new_op()
+    solve(op, data)
+    solve(op, data)  # graphs captured by now
+    replayed = solve(op, data2)
+    fresh_op = new_op()
+    solve(fresh_op, data2)
+    fresh = solve(fresh_op, data2)
+    assert torch.equal(replayed, fresh)
