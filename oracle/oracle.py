@@ -67,6 +67,11 @@ def lib():
         L.oracle_grain_segments.argtypes = [P(Mesh), P(_c_double), _c_double, P(_c_int), P(_c_int)]
         L.oracle_segment_properties.argtypes = [P(Mesh), P(_c_double), P(_c_double), P(_c_int), _c_int,
                                                 P(_c_double)]
+        L.oracle_advection_forces.argtypes = [P(Mesh), P(Params), P(_c_double), P(_c_double), U16, P(_c_int),
+                                              P(_c_double), _c_int, _c_double, _c_double, _c_double, _c_double,
+                                              P(_c_double)]
+        L.oracle_advection_velocities.argtypes = [_c_int, P(_c_double), P(_c_double), _c_int, _c_double,
+                                                  _c_double, P(_c_double)]
         _lib = L
     return _lib
 
@@ -247,3 +252,33 @@ def segment_properties(mesh, eta, ids, n_particles, origin=(0.0, 0.0, 0.0)):
                                            ids.ctypes.data_as(ctypes.POINTER(_c_int)), int(n_particles),
                                            _dptr(props)), "segment_properties")
     return props
+
+
+def advection_forces(mesh, params, u, cell_segments, centers, origin=(0.0, 0.0, 0.0), k=1.0, cgb=0.0, ceq=1.0,
+                     smoothening=0.0, mask=None):
+    """(n_segments, 1 + dim + (3 or 1)): volume, force, torque per segment
+    (AdvectionOperatorGeneric::evaluate_forces)."""
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(C, N)
+    seg = np.ascontiguousarray(cell_segments, dtype=np.int32)
+    cen = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+    org = np.ascontiguousarray(list(origin) + [0.0] * (3 - len(origin)), dtype=np.float64)
+    nc = 1 + mesh.dim + (3 if mesh.dim == 3 else 1)
+    out = np.zeros((cen.shape[0], nc))
+    keep, mp = _mptr(mask, mesh)
+    _check(lib().oracle_advection_forces(ctypes.byref(mesh), ctypes.byref(params), _dptr(org), _dptr(u), mp,
+                                         seg.ctypes.data_as(ctypes.POINTER(_c_int)), _dptr(cen), cen.shape[0],
+                                         float(k), float(cgb), float(ceq), float(smoothening), _dptr(out)),
+           "advection_forces")
+    return out
+
+
+def advection_velocities(dim, vft, centers, mt, mr):
+    """(n_segments, 9) velocity table (translation, angular velocity, center)
+    from volumes, forces and torques (AdvectionMechanism)."""
+    vft = np.ascontiguousarray(vft, dtype=np.float64)
+    cen = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((cen.shape[0], 9))
+    _check(lib().oracle_advection_velocities(int(dim), _dptr(vft), _dptr(cen), cen.shape[0], float(mt), float(mr),
+                                             _dptr(out)), "advection_velocities")
+    return out

@@ -1133,4 +1133,132 @@ int oracle_segment_properties(const oracle_mesh *m, const double *origin, const 
   return 0;
 }
 
+// AdvectionOperatorGeneric::evaluate_forces / do_evaluate_forces
+// (sintering/operator_advection.h:86-373): for every cell and every relevant
+// grain i whose order parameter has a segment s on the cell, with the
+// quadrature points x_q of the cell,
+//   volume_s += sum_q eta_i JxW
+//   force_s  += sum_q sum_{j != i relevant} dF_ij JxW,
+//               dF_ij = k (c - ceq) f(eta_i eta_j) (grad eta_i - grad eta_j)
+//   torque_s += sum_q sum_j (x_q - center_s) x dF_ij JxW
+// with f(p) = 1 / (1 + exp(-smoothening (p - cgb))) (cgb > 0, smoothening
+// > 0), [p > cgb] (cgb > 0) or 4 p (cgb <= 0), and hpsint's cross products
+// (include/pf-applications/base/tensor.h:62-84: in 2D the scalar
+// a[1] b[0] - a[0] b[1]).  out: n_segments rows of 1 + dim + (dim == 3 ? 3 :
+// 1) values (volume, force, torque), overwritten; cells in lexicographic
+// order, grains in increasing order.  centers: n_segments x 3.
+int oracle_advection_forces(const oracle_mesh *m, const oracle_params *p, const double *origin, const double *u,
+                            const uint16_t *mask, const int *cell_segments, const double *centers, int n_segments,
+                            double k_stiff, double cgb, double ceq, double smoothening, double *out)
+{
+  if (int e = check_args(m, p))
+    return e;
+  if (!origin || !u || !cell_segments || n_segments < 0 || (n_segments > 0 && (!centers || !out)))
+    return 1;
+  const Geometry geo(*m);
+  const int      dim = geo.dim, nt = dim == 3 ? 3 : 1, nc = 1 + dim + nt, nq = geo.nq;
+  const int64_t  N = geo.n_nodes;
+  std::fill(out, out + int64_t(n_segments) * nc, 0.0);
+  const double gp[2] = {0.5 - 0.5 / std::sqrt(3.0), 0.5 + 0.5 / std::sqrt(3.0)};
+  for (int k = 0; k < geo.n[2]; ++k)
+    for (int j = 0; j < geo.n[1]; ++j)
+      for (int i = 0; i < geo.n[0]; ++i)
+        {
+          const int64_t cell = int64_t(i) + int64_t(geo.n[0]) * (int64_t(j) + int64_t(geo.n[1]) * k);
+          int           blk[MAXC];
+          const int     G = cell_blocks(geo, mask, p->n_grains, i, j, k, blk), C = G + 2;
+          double        val[MAXC][8];
+          V3            grad[MAXC][8];
+          for (int b = 0; b < C; ++b)
+            {
+              double ul[8];
+              for (int l = 0; l < nq; ++l)
+                ul[l] = u[blk[b] * N + geo.node(i, j, k, l)];
+              evaluate(geo, ul, val[b], grad[b]);
+            }
+          const int co[3] = {i, j, k};
+          for (int ig = 0; ig < G; ++ig)
+            {
+              const int s = cell_segments[int64_t(blk[2 + ig] - 2) * geo.n_cells + cell];
+              if (s < 0)
+                continue;
+              if (s >= n_segments)
+                return 1;
+              double *o = out + int64_t(s) * nc;
+              for (int q = 0; q < nq; ++q)
+                {
+                  double r[3] = {0.0, 0.0, 0.0};
+                  for (int e = 0; e < dim; ++e)
+                    r[e] = origin[e] + (co[e] + gp[(q >> e) & 1]) * geo.h[e] - centers[3 * int64_t(s) + e];
+                  const double c = val[0][q], ei = val[2 + ig][q];
+                  double       force[3] = {0.0, 0.0, 0.0}, torque[3] = {0.0, 0.0, 0.0};
+                  for (int jg = 0; jg < G; ++jg)
+                    {
+                      if (jg == ig)
+                        continue;
+                      double f = ei * val[2 + jg][q];
+                      if (cgb > 0.0)
+                        f = smoothening > 0.0 ? 1.0 / (1.0 + std::exp(-smoothening * (f - cgb))) : (f > cgb ? 1.0 : 0.0);
+                      else
+                        f *= 4.0;
+                      const double w = k_stiff * (c - ceq) * f;
+                      double       dF[3];
+                      for (int e = 0; e < 3; ++e)
+                        dF[e] = (grad[2 + ig][q][e] - grad[2 + jg][q][e]) * w;
+                      for (int e = 0; e < dim; ++e)
+                        force[e] += dF[e];
+                      if (dim == 3)
+                        {
+                          torque[0] += r[1] * dF[2] - r[2] * dF[1];
+                          torque[1] += r[2] * dF[0] - r[0] * dF[2];
+                          torque[2] += r[0] * dF[1] - r[1] * dF[0];
+                        }
+                      else
+                        torque[0] += r[1] * dF[0] - r[0] * dF[1];
+                    }
+                  o[0] += ei * geo.JxW;
+                  for (int e = 0; e < dim; ++e)
+                    o[1 + e] += force[e] * geo.JxW;
+                  for (int e = 0; e < nt; ++e)
+                    o[1 + dim + e] += torque[e] * geo.JxW;
+                }
+            }
+        }
+  return 0;
+}
+
+// AdvectionMechanism::calc_translation_velocity / calc_rotation_velocity
+// (sintering/advection.h:330-352): per segment the velocity table the
+// residual and J v read: v_t = mt force / volume, w = mr torque / volume (the
+// z component in 2D, cross(r) = torque (-r[1], r[0]), advection.h:105-113),
+// center.  A segment without volume gets no velocity.  vft: n_segments rows
+// of 1 + dim + (dim == 3 ? 3 : 1) values; centers: n_segments x 3; segments:
+// n_segments x 9 (overwritten).
+int oracle_advection_velocities(int dim, const double *vft, const double *centers, int n_segments, double mt,
+                                double mr, double *segments)
+{
+  if ((dim != 2 && dim != 3) || n_segments < 0 || (n_segments > 0 && (!vft || !centers || !segments)))
+    return 1;
+  const int nt = dim == 3 ? 3 : 1, nc = 1 + dim + nt;
+  for (int s = 0; s < n_segments; ++s)
+    {
+      const double *d = vft + int64_t(s) * nc;
+      double       *o = segments + 9 * int64_t(s);
+      for (int e = 0; e < 9; ++e)
+        o[e] = 0.0;
+      for (int e = 0; e < 3; ++e)
+        o[6 + e] = centers[3 * int64_t(s) + e];
+      if (!(d[0] > 0.0))
+        continue;
+      for (int e = 0; e < dim; ++e)
+        o[e] = mt * d[1 + e] / d[0];
+      if (dim == 3)
+        for (int e = 0; e < 3; ++e)
+          o[3 + e] = mr * d[1 + dim + e] / d[0];
+      else
+        o[5] = mr * d[1 + dim] / d[0];
+    }
+  return 0;
+}
+
 } // extern "C"

@@ -23,6 +23,10 @@ Sources (paths inside the hpsint project):
       grain-tracker segments (center, radius, max value) of the spherical
       representation; the mesh, the indicator field and the threshold are
       re-typed below from the .cc (lines cited), the segments are parsed
+  tests/advection_mechanism_data.{cc,output}
+      advection velocities (translation, rotation, total) of three grain
+      segments at the cell barycenters of a 4 x 4 mesh; mt and mr are re-typed
+      from the .cc, volumes/forces/torques/centers and velocities are parsed
 """
 import json
 import os
@@ -83,6 +87,30 @@ def parse_tracker_segments(path, section):
         if on and m:
             segs.append([float(x) for x in m.groups()])
     return segs
+
+
+def parse_advection(path):
+    """advection_mechanism_data output: the grain data and centers, then per
+    cell batch and order parameter the velocities; deal.II prints a
+    vectorized 2D tensor as x of both lanes, then y of both lanes."""
+    out = {"batches": []}
+    for line in open(path).read().splitlines():
+        if line.startswith("grains_data:"):
+            out["grains_data"] = [float(x) for x in line.split(":")[1].split()]
+        elif line.startswith("grain_center:"):
+            out["grain_center"] = [float(x) for x in line.split(":")[1].split()]
+        elif line.startswith("cell_batch"):
+            out["batches"].append([])
+        else:
+            m = re.match(r"^\s+op = (\d+) \| has_velocity = (\d) \| trans_vel = (.*) \| rot_vel = (.*) \| "
+                         r"tot_vel = (.*)$", line)
+            if m:
+                out["batches"][-1].append({
+                    "op": int(m.group(1)), "has_velocity": int(m.group(2)),
+                    "trans_vel": [float(x) for x in m.group(3).split()],
+                    "rot_vel": [float(x) for x in m.group(4).split()],
+                    "tot_vel": [float(x) for x in m.group(5).split()]})
+    return out
 
 
 def main(ref):
@@ -150,6 +178,14 @@ def main(ref):
                                            "Spherical grain representation"),
         "digits": 6,
     }
+    # advection_mechanism_data.cc:38-46 (2D, [0, 1]^2, 2 global refinements
+    # -> 4 x 4 cells, 2 lanes per cell batch), :72-73 (mt, mr), :104-116 (one
+    # segment per order parameter: volume 1 + (i + 1) i, force (1 + i, 0),
+    # torque 1 + i, center (i, i)); the velocities are parsed
+    adv = parse_advection(os.path.join(t, "advection_mechanism_data.output"))
+    adv.update({"dim": 2, "cells": [4, 4], "h": [0.25, 0.25], "lanes": 2, "mt": 1.0, "mr": 1.0,
+                "n_comp_volume_force_torque": 4, "digits": 6})
+    golden["advection_mechanism_data"] = adv
     with open(os.path.join(HERE, "hpsint_goldens.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print("wrote", os.path.join(HERE, "hpsint_goldens.json"))

@@ -136,3 +136,128 @@ def test_mask_and_advection_together():
     a = O.residual(om, p, T, u, [u], 2, mask=mask, advection=(seg, data, (0, 0, 0)))
     b_ = O.residual(om, p, T, u, [u], 2, mask=mask, advection=(seg_m, data, (0, 0, 0)))
     assert np.array_equal(a, b_)
+
+
+# --- the advection mechanism: forces, torques, volumes and the velocity table
+
+
+def test_velocities_match_golden(goldens):
+    """AdvectionMechanism's velocities (advection_mechanism_data golden):
+    three segments with volume, force, torque and center, velocities at the
+    cell barycenters of a 4 x 4 mesh of [0, 1]^2, mt = mr = 1."""
+    g = goldens["advection_mechanism_data"]
+    nc = g["n_comp_volume_force_torque"]
+    vft = np.array(g["grains_data"]).reshape(-1, nc)
+    S = vft.shape[0]
+    centers = np.zeros((S, 3))
+    centers[:, :2] = np.array(g["grain_center"]).reshape(S, 2)
+    table = O.advection_velocities(2, vft, centers, g["mt"], g["mr"])
+    lanes = g["lanes"]
+    for batch in g["batches"]:
+        # op 0: center (0, 0) and mr torque / volume = 1, so its rotation
+        # velocity (-y, x) gives the lanes' evaluation points
+        rot0 = np.array(batch[0]["rot_vel"]).reshape(2, lanes)
+        pts = np.stack([rot0[1], -rot0[0]], axis=1)
+        assert np.allclose(pts / g["h"][0] % 1.0, 0.5, atol=1e-5)  # cell barycenters
+        for entry in batch:
+            s = entry["op"]
+            assert entry["has_velocity"] == 1
+            vt = np.tile(table[s, 0:2], (lanes, 1))
+            r = pts - table[s, 6:8]
+            vr = table[s, 5] * np.stack([-r[:, 1], r[:, 0]], axis=1)
+            for ours, key in ((vt, "trans_vel"), (vr, "rot_vel"), (vt + vr, "tot_vel")):
+                ref = np.array(entry[key]).reshape(2, lanes).T
+                assert np.allclose(ours, ref, rtol=1e-5, atol=1e-6), (s, key, ours, ref)
+
+
+def numpy_forces(dim, cells, h, origin, u, seg, centers, k, cgb, ceq, smoothening, mask=None):
+    G = u.shape[0] - 2
+    nn = [c + 1 for c in cells]
+    nt = 3 if dim == 3 else 1
+    out = np.zeros((centers.shape[0], 1 + dim + nt))
+    corners = list(itertools.product((0, 1), repeat=dim))
+    for cc in itertools.product(*[range(c) for c in reversed(cells)]):
+        cc = tuple(reversed(cc))
+        cell = sum(cc[d] * int(np.prod(cells[:d])) for d in range(dim))
+        rel = [b for b in range(G) if mask is None or (int(mask[cell]) >> b) & 1]
+        nodes = [sum((cc[d] + a[d]) * int(np.prod(nn[:d])) for d in range(dim)) for a in corners]
+        for qb in itertools.product((0, 1), repeat=dim):
+            xi = [GP[qb[d]] for d in range(dim)]
+            w = np.prod([h[d] for d in range(dim)]) / 2 ** dim
+            N = np.array([np.prod([xi[d] if a[d] else 1 - xi[d] for d in range(dim)]) for a in corners])
+            dN = np.zeros((len(corners), dim))
+            for kk, a in enumerate(corners):
+                for d in range(dim):
+                    f = (1.0 if a[d] else -1.0) / h[d]
+                    for e in range(dim):
+                        if e != d:
+                            f *= xi[e] if a[e] else 1 - xi[e]
+                    dN[kk, d] = f
+            x = np.array([origin[d] + (cc[d] + xi[d]) * h[d] for d in range(dim)])
+            val = u[:, nodes] @ N
+            grad = u[:, nodes] @ dN
+            for i in rel:
+                s = seg[i, cell]
+                if s < 0:
+                    continue
+                r = x - centers[s, :dim]
+                out[s, 0] += w * val[2 + i]
+                for j in rel:
+                    if j == i:
+                        continue
+                    p = val[2 + i] * val[2 + j]
+                    if cgb > 0:
+                        f = 1 / (1 + np.exp(-smoothening * (p - cgb))) if smoothening > 0 else float(p > cgb)
+                    else:
+                        f = 4 * p
+                    dF = k * (val[0] - ceq) * f * (grad[2 + i] - grad[2 + j])
+                    out[s, 1:1 + dim] += w * dF
+                    if dim == 3:
+                        out[s, 4:7] += w * np.cross(r, dF)
+                    else:
+                        out[s, 3] += w * (r[1] * dF[0] - r[0] * dF[1])  # tensor.h:62-66
+    return out
+
+
+@pytest.mark.parametrize("dim,cells,G", [(2, (7, 6), 3), (3, (4, 3, 3), 3)])
+@pytest.mark.parametrize("cgb,smoothening", [(0.0, 0.0), (0.14, 0.0), (0.14, 40.0)])
+def test_forces_match_independent_quadrature(dim, cells, G, cgb, smoothening):
+    h = (0.7, 1.3, 0.9)
+    origin = (1.5, -2.0, 0.25)
+    om, p = O.make_mesh(dim, list(cells) + [0] * (3 - dim), h), O.make_params(G)
+    u = random_state(dim, cells, G, seed=21)
+    seg, data = advection_data(dim, cells, G, seed=22)
+    centers = data[:, 6:9]
+    ref = numpy_forces(dim, cells, h, origin, u, seg, centers, 2.5, cgb, 0.9, smoothening)
+    got = O.advection_forces(om, p, u, seg, centers, origin, 2.5, cgb, 0.9, smoothening)
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-13 * np.abs(ref).max())
+    assert np.abs(ref[:, 1:]).max() > 1e-3  # non-trivial forces
+    # under the grain cut-off only the relevant grains act
+    mask = np.random.default_rng(23).integers(0, 1 << G, int(np.prod(cells))).astype(np.uint16)
+    ref_m = numpy_forces(dim, cells, h, origin, u, seg, centers, 2.5, cgb, 0.9, smoothening, mask)
+    got_m = O.advection_forces(om, p, u, seg, centers, origin, 2.5, cgb, 0.9, smoothening, mask=mask)
+    assert np.allclose(got_m, ref_m, rtol=1e-12, atol=1e-13 * np.abs(ref_m).max())
+
+
+@pytest.mark.parametrize("dim,cells", [(2, (12, 10)), (3, (6, 5, 5))])
+def test_forces_balance(dim, cells):
+    """With every grain one segment over the whole mesh, the pair forces
+    cancel (dF_ji = -dF_ij with the symmetric 4 eta_i eta_j weight), and so do
+    the torques about a common center."""
+    G = 3
+    om, p = oracle_mesh(dim, cells), O.make_params(G)
+    u = random_state(dim, cells, G, seed=24)
+    n_cells = int(np.prod(cells))
+    seg = np.repeat(np.arange(G, dtype=np.int32)[:, None], n_cells, axis=1)
+    centers = np.tile([1.0, 2.0, 0.5], (G, 1))
+    f = O.advection_forces(om, p, u, seg, centers, (0, 0, 0), 3.0, 0.0, 0.8, 0.0)
+    scale = np.abs(f[:, 1:]).max()
+    assert scale > 1e-3
+    assert np.abs(f[:, 1:].sum(axis=0)).max() < 1e-12 * scale
+    # volumes: the integral of each eta (Q1 basis functions integrate to the trapezoidal weights)
+    w = np.ones(1)
+    for d in range(dim):
+        wd = np.ones(cells[d] + 1)
+        wd[[0, -1]] = 0.5
+        w = np.kron(wd, w)
+    assert np.allclose(f[:, 0], u[2:] @ w, rtol=1e-13)
