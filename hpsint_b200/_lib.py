@@ -31,6 +31,11 @@ class SintParams(ctypes.Structure):
                 ("Mgb", _c_double), ("L", _c_double), ("tensorial", _c_int)]
 
 
+class SintAdvectionParams(ctypes.Structure):
+    _fields_ = [("k", _c_double), ("cgb", _c_double), ("ceq", _c_double), ("smoothening", _c_double),
+                ("mt", _c_double), ("mr", _c_double)]
+
+
 class SintNewtonParams(ctypes.Structure):
     _fields_ = [("nl_max_iter", _c_int), ("nl_abs_tol", _c_double), ("nl_rel_tol", _c_double),
                 ("l_max_iter", _c_int), ("l_abs_tol", _c_double), ("l_rel_tol", _c_double),
@@ -74,6 +79,8 @@ SIGNATURES = {
     "sint_grain_segment_properties": (_c_int, [_c_void, _c_void, _c_void, _c_int, P(_c_double), _c_void]),
     "sint_get_component_mask": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_set_advection": (_c_int, [_c_void, _c_void, _c_void, _c_int, _c_void]),
+    "sint_set_advection_mechanism": (_c_int, [_c_void, _c_void, _c_void, _c_int, P(SintAdvectionParams), _c_void]),
+    "sint_advection_forces": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_vec_axpy_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_sadd_f64": (_c_int, [_c_int64, _c_double, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_scale_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void]),

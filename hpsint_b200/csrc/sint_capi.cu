@@ -387,6 +387,11 @@ int sint_destroy(sint_ctx *c)
   cudaFree(c->adv_cells);
   cudaFree(c->adv_segments);
   cudaFree(c->adv_error);
+  cudaFree(c->adv_centers);
+  cudaFree(c->adv_vft);
+  cudaFree(c->adv_off);
+  cudaFree(c->adv_items);
+  cudaFree(c->adv_slots);
   cudaFree(c->pc_raw);
   cudaFree(c->pc_inv64);
   cudaFree(c->pc_inv32);
@@ -480,6 +485,11 @@ int sint_residual_f64(sint_ctx *c, double *dst, const double *src, const double 
         if (int e = check_vec(hist[i], "hist[i]"))
           return e;
     }
+  // the advection mechanism moves the grains with the forces of this state
+  // (ResidualWrapperAdvection::evaluate_for_residual, residual_wrapper.h:58-64)
+  if (c->adv_mech)
+    if (int rc = advection_update(c, src, stream))
+      return rc;
   const cudaError_t e = dispatch_residual(c, with_time_derivative, src, hist, dst, stream);
   if (e != cudaSuccess)
     return cuda_fail(e, "sint_residual_f64");

@@ -72,12 +72,23 @@ namespace sint
 
     // advection (sint_set_advection): the grains' segment of every cell and
     // the segments' velocities and centers, copied from the caller
-    bool    adv          = false;
-    int    *adv_cells    = nullptr; // G x n_cells
-    double *adv_segments = nullptr; // adv_seg_cap x 9
-    int      adv_seg_cap = 0;
-    unsigned *adv_error  = nullptr; // count of invalid ids (sint_set_advection)
-    AdvData  adv_view;              // the above as the kernels take them
+    bool      adv          = false;
+    int      *adv_cells    = nullptr; // G x n_cells
+    double   *adv_segments = nullptr; // n_segments x 9 (velocity table)
+    long long adv_seg_cap  = 0;       // capacities in elements
+    unsigned *adv_error    = nullptr; // count of invalid ids
+    AdvData   adv_view;               // the above as the kernels take them
+    // the advection mechanism (sint_set_advection_mechanism): the table is
+    // recomputed from the forces of every residual evaluation's state
+    bool                  adv_mech      = false;
+    sint_advection_params adv_prm       = {};
+    double               *adv_centers   = nullptr; // n_segments x 3
+    double               *adv_vft       = nullptr; // n_segments x (volume, force, torque)
+    long long            *adv_off       = nullptr; // segment offsets (S + 1) and totals (S)
+    unsigned             *adv_items     = nullptr; // (b, cell) items sorted by segment
+    double               *adv_slots     = nullptr; // per-tile pieces of the force sums
+    long long             adv_n_valid   = 0;       // items with a segment
+    long long adv_cen_cap = 0, adv_vft_cap = 0, adv_off_cap = 0, adv_items_cap = 0, adv_slots_cap = 0;
 
     double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
     double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
@@ -143,6 +154,10 @@ namespace sint
   inline const uint16_t *active_tile_union(const Ctx *c) { return c->cut ? c->tile_union : nullptr; }
   inline const uint32_t *active_live(const Ctx *c) { return (c->cut && c->skip_zeros) ? c->live : nullptr; }
   inline const AdvData  *active_adv(const Ctx *c) { return c->adv ? &c->adv_view : nullptr; }
+
+  // The advection mechanism's update before a residual evaluation: forces of
+  // u, then the velocity table (sint_advection.cu).
+  int advection_update(Ctx *c, const double *u, cudaStream_t s);
   // J v through the cell kernel + combine, with c->partial as scratch.
   template <typename R>
   cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s);

@@ -226,6 +226,49 @@ class SinteringOperatorGeneric:
         if cell_segments is None:
             L.check(L.lib().sint_set_advection(self._h, None, None, 0, _stream()), "sint_set_advection")
             return
+        self._check_segments(cell_segments)
+        if (segments.dtype != torch.float64 or not segments.is_cuda or not segments.is_contiguous()
+                or segments.numel() % 9 != 0):
+            raise ValueError("segments must be a contiguous float64 CUDA tensor of n_segments x 9 values")
+        n_seg = segments.numel() // 9
+        L.check(L.lib().sint_set_advection(self._h, _ptr(cell_segments), _ptr(segments) if n_seg else None, n_seg,
+                                           _stream()), "sint_set_advection")
+
+    def set_advection_mechanism(self, cell_segments, centers, k, cgb, ceq, smoothening, mt, mr):
+        """The advection mechanism (AdvectionMechanism + AdvectionOperatorGeneric,
+        sintering/advection.h, operator_advection.h): every residual evaluation
+        first computes each segment's volume, force and torque from its state
+        and moves the grain with v_t = mt F / V, w = mr T / V about its center;
+        J v uses the velocities of the latest residual evaluation.
+        cell_segments: device int32 (n_grains, n_cells), -1 = none; centers:
+        device float64 (n_segments, 3).  None switches advection off."""
+        if cell_segments is None:
+            L.check(L.lib().sint_set_advection_mechanism(self._h, None, None, 0, None, _stream()),
+                    "sint_set_advection_mechanism")
+            return
+        self._check_segments(cell_segments)
+        if (centers.dtype != torch.float64 or not centers.is_cuda or not centers.is_contiguous()
+                or centers.numel() % 3 != 0):
+            raise ValueError("centers must be a contiguous float64 CUDA tensor of n_segments x 3 values")
+        n_seg = centers.numel() // 3
+        prm = L.SintAdvectionParams(float(k), float(cgb), float(ceq), float(smoothening), float(mt), float(mr))
+        L.check(L.lib().sint_set_advection_mechanism(self._h, _ptr(cell_segments), _ptr(centers) if n_seg else None,
+                                                     n_seg, ctypes.byref(prm), _stream()),
+                "sint_set_advection_mechanism")
+        self._n_segments = n_seg
+
+    def advection_forces(self, u):
+        """Volume, force and torque of every segment at state u (device
+        float64 tensor (n_segments, 1 + dim + (3 or 1))); also updates the
+        velocities J v uses."""
+        self._check_vec(u, torch.float64)
+        nc = 7 if self.mesh.dim == 3 else 4
+        out = torch.zeros((getattr(self, "_n_segments", 0), nc), dtype=torch.float64, device="cuda")
+        L.check(L.lib().sint_advection_forces(self._h, _ptr(u), _ptr(out) if out.numel() else None, _stream()),
+                "sint_advection_forces")
+        return out
+
+    def _check_segments(self, cell_segments):
         n_cells = 1
         for d in range(self.mesh.dim):
             n_cells *= self.mesh.n_cells[d]
@@ -233,12 +276,6 @@ class SinteringOperatorGeneric:
                 or cell_segments.numel() != self.params.n_grains * n_cells):
             raise ValueError(f"cell_segments must be a contiguous int32 CUDA tensor of {self.params.n_grains} x "
                              f"{n_cells} ids")
-        if (segments.dtype != torch.float64 or not segments.is_cuda or not segments.is_contiguous()
-                or segments.numel() % 9 != 0):
-            raise ValueError("segments must be a contiguous float64 CUDA tensor of n_segments x 9 values")
-        n_seg = segments.numel() // 9
-        L.check(L.lib().sint_set_advection(self._h, _ptr(cell_segments), _ptr(segments) if n_seg else None, n_seg,
-                                           _stream()), "sint_set_advection")
 
     def evaluate_nonlinear_residual(self, dst, src, with_time_derivative=2, history=()):
         self._check_vec(dst, torch.float64)

@@ -284,6 +284,37 @@ int sint_grain_segment_properties(sint_ctx *ctx, const double *eta, const int *p
 int sint_set_advection(sint_ctx *ctx, const int32_t *cell_segments, const double *segments, int n_segments,
                        sint_stream_t stream);
 
+/* Parameters of the advection mechanism (AdvectionData,
+ * sintering/parameters.h:719-745): Wang stiffness k, grain-boundary
+ * threshold cgb, equilibrium concentration ceq, smoothening of the
+ * grain-boundary filter, translation and rotation factors mt and mr. */
+typedef struct
+{
+  double k, cgb, ceq, smoothening, mt, mr;
+} sint_advection_params;
+
+/* The advection mechanism with state-dependent velocities: every residual
+ * evaluation of the context (sint_residual_f64 and the device Newton's)
+ * first evaluates the segments' volumes, forces and torques from its input
+ * state (AdvectionOperatorGeneric::evaluate_forces, operator_advection.h:
+ * 86-373) and turns them into the velocity table (v_t = mt F / V,
+ * w = mr T / V); J v uses the table of the latest evaluation, as
+ * ResidualWrapperAdvection does (residual_wrapper.h:36-84).
+ *   cell_segments  DEVICE, n_grains x n_cells int32 as for sint_set_advection
+ *   centers        DEVICE, n_segments x 3: the segment centers (the grain
+ *                  tracker's), about which torques and rotations are taken
+ * Sums are deterministic (a fixed order independent of thread scheduling).
+ * Synchronises `stream`.  cell_segments == NULL switches advection off;
+ * sint_set_advection replaces the mechanism by fixed velocities. */
+int sint_set_advection_mechanism(sint_ctx *ctx, const int32_t *cell_segments, const double *centers, int n_segments,
+                                 const sint_advection_params *params, sint_stream_t stream);
+
+/* Evaluates the forces of the state u and updates the velocity table; with
+ * vft != NULL also copies the per-segment volume, force and torque to it
+ * (DEVICE, n_segments rows of 1 + dim + (dim == 3 ? 3 : 1) doubles; 2D
+ * torque = hpsint's scalar cross product r[1] F[0] - r[0] F[1]). */
+int sint_advection_forces(sint_ctx *ctx, const double *u, double *vft, sint_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* BLAS-1 on block vectors: DynamicBlockVector                              */
 /* (include/pf-applications/lac/dynamic_block_vector.h:346-516).            */

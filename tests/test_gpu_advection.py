@@ -268,3 +268,139 @@ def test_graph_replayed_solve_reads_the_current_velocities(prec):
     solve(fresh_op, data2)
     fresh = solve(fresh_op, data2)
     assert torch.equal(replayed, fresh)
+
+
+# --- the advection mechanism: forces from the state, velocities from forces
+
+MECH = dict(k=2.5, cgb=0.0, ceq=0.9, smoothening=0.0, mt=0.3, mr=0.2)
+
+
+def set_mech(op, seg, centers, **kw):
+    prm = dict(MECH, **kw)
+    op.set_advection_mechanism(torch.from_numpy(seg).cuda().contiguous(),
+                               torch.from_numpy(np.ascontiguousarray(centers)).cuda().contiguous(), **prm)
+    return prm
+
+
+MECH_CASES = [
+    # dim, cells, G, cgb, smoothening
+    (2, (37, 21), 4, 0.0, 0.0),
+    (2, (30, 26), 9, 0.14, 40.0),
+    (3, (13, 11, 9), 5, 0.14, 0.0),
+    (3, (11, 9, 10), 9, 0.0, 0.0),
+]
+
+
+@pytest.mark.parametrize("case", MECH_CASES, ids=[f"{c[0]}d-G{c[2]}-cgb{c[3]}-s{c[4]}" for c in MECH_CASES])
+def test_forces_and_velocities_match_oracle(case):
+    dim, cells, G, cgb, sm = case
+    op, p, om = make_op(dim, cells, G, True)
+    u = particle_state(dim, cells, G, seed=61)
+    seg, data = advection_data(dim, cells, G, seed=62, n_seg_per_grain=3)
+    centers = data[:, 6:9].copy()
+    prm = set_mech(op, seg, centers, cgb=cgb, smoothening=sm)
+    ud = op.to_device(u)
+    vft = op.advection_forces(ud).cpu().numpy()
+    ref = O.advection_forces(om, p, u, seg, centers, ORIGIN, prm["k"], cgb, prm["ceq"], sm)
+    scale = np.abs(ref).max(axis=0, keepdims=True)
+    assert np.all(np.abs(vft - ref) <= 1e-12 * scale + 1e-300)
+    # the residual then moves the grains with the oracle's velocities for those forces
+    table = O.advection_velocities(dim, ref, centers, prm["mt"], prm["mr"])
+    op.set_time_weights(20.0, [-20.0], 1.0)
+    r = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(r, ud, 2, [ud])
+    op.fill_quadrature_point_values(ud)
+    src = random_state(dim, cells, G, seed=63, smooth=False) - 0.5
+    j = op.initialize_dof_vector()
+    op.vmult(j, op.to_device(src))
+    torch.cuda.synchronize()
+    T = O.make_time(20.0, 1.0, [-20.0])
+    adv = (seg, table, ORIGIN)
+    assert block_rel_err(op.to_host(r), O.residual(om, p, T, u, [u], 2, advection=adv)) <= 1e-11
+    assert block_rel_err(op.to_host(j), O.jvp(om, p, T, u, src, advection=adv)) <= 1e-11
+
+
+def test_forces_under_the_cut_off_and_determinism():
+    dim, cells, G = 3, (14, 9, 10), 6
+    op, p, om = make_op(dim, cells, G, True)
+    u = particle_state(dim, cells, G, seed=64)
+    seg, data = advection_data(dim, cells, G, seed=65)
+    centers = data[:, 6:9].copy()
+    ud = op.to_device(u)
+    op.set_component_mask(ud, 1e-3)
+    prm = set_mech(op, seg, centers)
+    a = op.advection_forces(ud)
+    b = op.advection_forces(ud)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)  # fixed summation order
+    ref = O.advection_forces(om, p, u, seg, centers, ORIGIN, prm["k"], 0.0, prm["ceq"], 0.0,
+                             mask=O.grain_mask(om, p, u, 1e-3))
+    scale = np.abs(ref).max(axis=0, keepdims=True)
+    assert np.all(np.abs(a.cpu().numpy() - ref) <= 1e-12 * scale + 1e-300)
+
+
+def test_segments_spanning_many_tiles():
+    """One segment per grain over the whole mesh: the per-segment sums run
+    over hundreds of tiles of the sorted item list."""
+    dim, cells, G = 3, (40, 36, 30), 3
+    op, p, om = make_op(dim, cells, G, False)
+    u = particle_state(dim, cells, G, seed=66)
+    n_cells = int(np.prod(cells))
+    seg = np.repeat(np.arange(G, dtype=np.int32)[:, None], n_cells, axis=1)
+    seg[1, ::7] = -1  # holes
+    centers = np.array([[10.0, 12.0, 9.0], [25.0, 20.0, 15.0], [30.0, 5.0, 20.0]])
+    prm = set_mech(op, seg, centers)
+    vft = op.advection_forces(op.to_device(u)).cpu().numpy()
+    ref = O.advection_forces(om, p, u, seg, centers, ORIGIN, prm["k"], 0.0, prm["ceq"], 0.0)
+    scale = np.abs(ref).max(axis=0, keepdims=True)
+    assert np.all(np.abs(vft - ref) <= 1e-12 * scale + 1e-300)
+
+
+def _mech_cpu_newton(mesh, P, T, u_old, seg, centers, prm, tol_rel=1e-12, max_it=40):
+    """Newton on R(u; v(u)) with J v at frozen velocities, as the device solve."""
+    from scipy.sparse.linalg import LinearOperator, gmres
+    u = u_old.copy()
+    C, N = u.shape
+    r0 = None
+    for _ in range(max_it):
+        vft = O.advection_forces(mesh, P, u, seg, centers, (0, 0, 0), prm["k"], prm["cgb"], prm["ceq"],
+                                 prm["smoothening"])
+        adv = (seg, O.advection_velocities(2, vft, centers, prm["mt"], prm["mr"]), (0.0, 0.0, 0.0))
+        r = O.residual(mesh, P, T, u, [u_old], 2, advection=adv)
+        nr = np.linalg.norm(r)
+        r0 = nr if r0 is None else r0
+        if nr <= tol_rel * r0 or nr < 1e-14:
+            return u
+        lin = u.copy()
+        J = LinearOperator((C * N, C * N),
+                           matvec=lambda v: O.jvp(mesh, P, T, lin, v.reshape(C, N), advection=adv).ravel())
+        du, info = gmres(J, -r.ravel(), rtol=1e-13, atol=0.0, restart=300, maxiter=50)
+        u = u + du.reshape(C, N)
+    raise RuntimeError("CPU Newton did not converge")
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_newton_with_the_mechanism_matches_cpu_newton(prec):
+    import hpsint_b200 as hb
+    cells, G, dt = (40, 20), 2, 1e-2
+    u_old = _two_particles(cells)
+    seg, data = _two_particle_advection(cells)
+    centers = data[:, 6:9].copy()
+    prm = dict(MECH, mt=5.0, mr=5.0)
+    mesh = oracle_mesh(2, cells)
+    P = O.make_params(G, tensorial=True)
+    T = O.make_time(1.0 / dt, 1.0, [-1.0 / dt])
+    ref = _mech_cpu_newton(mesh, P, T, u_old, seg, centers, prm)
+    op = hb.SinteringOperatorGeneric(hb.Mesh(2, tuple(cells) + (1,)), hb.Params(G, tensorial=True))
+    op.set_time_weights(1.0 / dt, [-1.0 / dt], 1.0)
+    op.set_advection_mechanism(torch.from_numpy(seg).cuda(), torch.from_numpy(centers).cuda(), **prm)
+    old = op.to_device(u_old)
+    u = old.clone()
+    st = hb.DampedNewtonSolver(op, hb.NonLinearData(nl_rel_tol=1e-10, nl_abs_tol=1e-16, l_rel_tol=1e-4,
+                                                    nl_max_iter=30, inner_precision=prec)).solve(u, [old])
+    torch.cuda.synchronize()
+    assert st.status == 0
+    assert np.max(np.abs(op.to_host(u) - ref)) < (1e-7 if prec == 64 else 1e-6)
+    # the forces moved the grains: the step differs from the one without advection
+    vft = op.advection_forces(u).cpu().numpy()
+    assert np.abs(vft[:, 1:3]).max() > 0.0
