@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "nnconv",
-                                           "cutoff", "tracker"],
+                                           "cutoff", "tracker", "advection"],
                     default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
                          "learned2d: train the learned guess on 2D many-grain packings and compare s/step")
@@ -558,6 +558,86 @@ def grain_tracker_detection(args):
                       "max_rel_radius_diff_vs_oracle": max_rel, "data": "synthetic seeded packing"}), flush=True)
 
 
+def advection_operator(args):
+    """The operator with the advection mechanism at the initial state of the
+    3D solve workload (--n3, --spheres, ...; C3 by default): segments = the
+    particles of every order parameter (device tracker), k = 2.5, cgb = 0,
+    ceq = 0.9, mt = mr = 1.  Reports the set-up (tracker + segment sort), the
+    force evaluation, and J v / residual throughput with and without
+    advection, also under the grain cut-off (--cut-off, 1e-5 if unset)."""
+    import torch
+
+    import hpsint_b200 as hb
+    from hpsint_b200 import grain_tracker as GT
+    from hpsint_b200 import packings as P
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, tol = args.n3, args.cut_off if args.cut_off > 0 else 1e-5
+    centers, radii, colours = P.lognormal_packing_3d(n=n, n_spheres=args.spheres, median=args.median,
+                                                     sigma=args.sigma, max_grains=args.max_grains)
+    G = int(colours.max()) + 1
+    u0 = P.initial_state(3, (n, n, n), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), centers, radii, colours, width=2.0)
+    op = hb.SinteringOperatorGeneric(hb.Mesh(3, (n, n, n)), hb.Params(**model_params(G, not args.scalar)))
+    u = op.to_device(u0)
+    del u0
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps, warmup):
+        for _ in range(warmup):
+            fn()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(reps):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / reps
+
+    prm = dict(k=2.5, cgb=0.0, ceq=0.9, smoothening=0.0, mt=1.0, mr=1.0)
+
+    def set_up():
+        seg, cen, owners = GT.advection_segments(op, u, 0.01)
+        op.set_advection_mechanism(seg, cen, **prm)
+        return owners
+
+    owners = set_up()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        set_up()
+    torch.cuda.synchronize()
+    setup_ms = (time.perf_counter() - t0) * 1e3 / 3
+    forces_ms = timed(lambda: op.advection_forces(u), args.steps, args.warmup)
+    out = {"setup_ms_wall": setup_ms, "forces_ms": forces_ms, "segments": len(owners)}
+    op.set_time_weights(1e4, [-1e4], 1.0)
+    op.fill_quadrature_point_values(u)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    dst64, dst32 = op.initialize_dof_vector(), op.initialize_dof_vector(torch.float32)
+    src64 = torch.rand((op.C, op.ld), dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    src32 = src64.float()
+    dofs = op.C * op.N
+    for cut in (0.0, tol):
+        op.set_component_mask(u, cut)
+        for adv in (False, True):
+            if adv:
+                set_up()
+            else:
+                op.set_advection_mechanism(None, None, **prm)
+            tag = ("_advection" if adv else "") + ("_cut_off" if cut > 0 else "")
+            out["jvp_f64" + tag + "_gdofs"] = dofs / timed(lambda: op.vmult(dst64, src64), args.steps,
+                                                           args.warmup) / 1e6
+            out["jvp_f32" + tag + "_gdofs"] = dofs / timed(lambda: op.vmult(dst32, src32), args.steps,
+                                                           args.warmup) / 1e6
+            out["residual_f64" + tag + "_gdofs"] = dofs / timed(
+                lambda: op.evaluate_nonlinear_residual(dst64, u, 2, [u]), args.steps, args.warmup) / 1e6
+    op.set_component_mask(u, 0.0)
+    print(json.dumps({"metric": "operator GDoF/s with the advection mechanism", "unit": "GDoF/s",
+                      "workload": f"3d-{n}^3-{len(radii)}-lognormal-spheres-G{G}", "dofs": dofs, "grains": G,
+                      "cut_off_tolerance": tol, "advection": prm, "steps": args.steps, "warmup": args.warmup,
+                      "note": "residual with advection includes the force evaluation from its state",
+                      "data": "synthetic seeded packing", **out}), flush=True)
+
+
 def cut_off_operator_rates(op, u, tol, reps=20, warmup=3):
     """GDoF/s of the FP64/FP32 Jacobian-vector products and the residual at
     state u, without and with the grain cut-off at tolerance tol (CUDA events
@@ -673,6 +753,8 @@ def main():
     if args.workload == "cutoff":
         cut_off_operator(args)
         return
+    if args.workload == "advection":
+        return advection_operator(args)
     if args.workload == "tracker":
         grain_tracker_detection(args)
         return

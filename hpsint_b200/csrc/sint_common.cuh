@@ -165,10 +165,11 @@ namespace sint
 
   // Advection (rigid-body motion of the grains), as the kernels see it:
   // cell_segments[b * n_cells + cell] = segment of order parameter b the cell
-  // belongs to (-1: none); segments[9 s ..] = translational velocity (3),
-  // angular velocity (3; z only in 2D) and center (3) of segment s.  Grain b
-  // moves with v_t + w x (x - center) on the cells of its segment
-  // (AdvectionVelocityData::get_velocity, sintering/advection.h:247-263).
+  // belongs to (-1: none; ids >= n_segments count as none); segments[9 s ..]
+  // = translational velocity (3), angular velocity (3; z only in 2D) and
+  // center (3) of segment s.  Grain b moves with v_t + w x (x - center) on
+  // the cells of its segment (AdvectionVelocityData::get_velocity,
+  // sintering/advection.h:247-263).
   struct AdvData
   {
     const int    *cell_segments = nullptr;
@@ -177,32 +178,6 @@ namespace sint
     int           reserved      = 0; // explicit padding: the struct is compared bytewise
     double        origin[3]     = {0.0, 0.0, 0.0};
   };
-
-  // Velocity of grain b at quadrature point q (bit d of q = upper Gauss point
-  // in direction d) of the cell with global coordinates cc; false when the
-  // cell belongs to no segment of b (an id outside 0..n_segments - 1 counts
-  // as none).
-  template <int DIM, typename R>
-  __device__ __forceinline__ bool advection_velocity(const AdvData &a, const Grid &g, const int (&cc)[3], int q,
-                                                     int b, R (&v)[DIM])
-  {
-    const long long n_cells = (long long)g.n[0] * g.n[1] * g.n[2];
-    const long long cell    = cc[0] + (long long)g.n[0] * (cc[1] + (long long)g.n[1] * cc[2]);
-    const int       s       = a.cell_segments[b * n_cells + cell];
-    if (s < 0 || s >= a.n_segments)
-      return false;
-    const double *d      = a.segments + 9 * (long long)s;
-    const double  lo     = 0.5 - 0.5 / sqrt(3.0), hi = 0.5 + 0.5 / sqrt(3.0);
-    double        r[3]   = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int e = 0; e < DIM; ++e)
-      r[e] = a.origin[e] + (cc[e] + (((q >> e) & 1) ? hi : lo)) * g.h[e] - d[6 + e];
-    v[0] = R(d[0] + d[4] * r[2] - d[5] * r[1]);
-    v[1] = R(d[1] + d[5] * r[0] - d[3] * r[2]);
-    if constexpr (DIM == 3)
-      v[2] = R(d[2] + d[3] * r[1] - d[4] * r[0]);
-    return true;
-  }
 
   // Size of a per-grain array: at least one element (the grain cut-off runs
   // tiles without any relevant grain through the G = 0 kernels).

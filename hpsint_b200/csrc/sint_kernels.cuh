@@ -334,42 +334,102 @@ namespace sint
     return cc[0] < g.n[0] && cc[1] < g.n[1] && (DIM == 2 || cc[2] < g.n[2]);
   }
 
+  // Advection coefficients of one tile, staged once per tile before phase 1
+  // (AdvectionVelocityData::reinit, sintering/advection.h:185-222): for
+  // grain k (the tile's k-th grain under the cut-off) and local cell `cell`,
+  // item i = k * CELLS + cell: vel[6 i ..] = the velocity at the cell's lower
+  // corner and the angular velocity, has[i] = 1 when the grain has a segment
+  // on the cell.  The velocity at point q is then vel + w x (x_q - corner).
+  template <int DIM, int G, typename R, bool CUT>
+  __device__ __forceinline__ void adv_stage(const AdvData &a, const Grid &g, const TileCoord &tc,
+                                            unsigned long long gl, R *vel, unsigned char *has)
+  {
+    using T                 = Tile<DIM>;
+    const long long n_cells = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (int it = threadIdx.x; it < G * T::CELLS; it += T::THREADS)
+      {
+        const int k = it / T::CELLS, cell = it % T::CELLS;
+        int       cc[3];
+        int       s = -1;
+        if (cell_global<DIM>(cell, tc, g, cc))
+          {
+            const int b = CUT ? int((gl >> (4 * k)) & 15ull) : k;
+            s           = a.cell_segments[b * n_cells + cc[0] + (long long)g.n[0] * (cc[1] + (long long)g.n[1] * cc[2])];
+            if (s >= a.n_segments)
+              s = -1;
+          }
+        has[it] = s >= 0;
+        if (s >= 0)
+          {
+            const double *d    = a.segments + 9 * (long long)s;
+            double        r[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int e = 0; e < DIM; ++e)
+              r[e] = a.origin[e] + cc[e] * g.h[e] - d[6 + e];
+            R *o = vel + 6 * it;
+            o[0] = R(d[0] + d[4] * r[2] - d[5] * r[1]);
+            o[1] = R(d[1] + d[5] * r[0] - d[3] * r[2]);
+            o[2] = R(d[2] + d[3] * r[1] - d[4] * r[0]);
+            o[3] = R(d[3]);
+            o[4] = R(d[4]);
+            o[5] = R(d[5]);
+          }
+      }
+  }
+
+  // Velocity of staged item `it` at point q (offset dq from the cell corner).
+  template <int DIM, typename R>
+  __device__ __forceinline__ void adv_velocity(const R *vel, int it, const R (&dq)[3], R (&v)[DIM])
+  {
+    const R *w = vel + 6 * it;
+    v[0]       = w[0] + (w[4] * dq[2] - w[5] * dq[1]);
+    v[1]       = w[1] + (w[5] * dq[0] - w[3] * dq[2]);
+    if constexpr (DIM == 3)
+      v[2] = w[2] + (w[3] * dq[1] - w[4] * dq[0]);
+  }
+
+  template <int DIM, typename R>
+  __device__ __forceinline__ void adv_offset(const CellConsts<DIM, R> &k, const Grid &g, int q, R (&dq)[3])
+  {
+#pragma unroll
+    for (int e = 0; e < 3; ++e)
+      dq[e] = e < DIM ? (((q >> e) & 1) ? k.x1 : k.x0) * R(g.h[e]) : R(0);
+  }
+
   // Advection of the c row at point q (phase 2, after the point physics):
   // the c flux loses v_i c for every grain i with a velocity on the cell, one
   // grain after the other (operator_sintering_generic.h:1015-1036 for the
   // residual, :167-177 for J v, where c is the direction's value).  With the
   // grain cut-off only the cell's relevant grains move it (AdvectionVelocityData
   // maps order parameters through the relevant-grain table,
-  // sintering/advection.h:225-245); gl maps the compacted grain k to its order
-  // parameter.
+  // sintering/advection.h:225-245).
   template <int DIM, int G, typename R, bool CUT>
-  __device__ __forceinline__ void advect_c_point(const AdvData &a, const Grid &g, const TileCoord &tc, const R *F,
-                                                 int c_base, R *P, int q, int cell, unsigned m,
-                                                 unsigned long long gl)
+  __device__ __forceinline__ void advect_c_point(const CellConsts<DIM, R> &k, const Grid &g, const R *F, int c_base,
+                                                 R *P, int q, int cell, unsigned m, const R *vel,
+                                                 const unsigned char *has)
   {
-    int cc[3];
-    if (!cell_global<DIM>(cell, tc, g, cc))
-      return;
+    using T = Tile<DIM>;
+    R     dq[3];
+    adv_offset<DIM>(k, g, q, dq);
     const R c = fval<DIM>(F, c_base, q, cell);
     R       flux[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d)
-      flux[d] = P[((1 + d) * Slots<DIM>::NQ + q) * Tile<DIM>::CELLS + cell];
+      flux[d] = P[((1 + d) * Slots<DIM>::NQ + q) * T::CELLS + cell];
 #pragma unroll 1
     for (int i = 0; i < G; ++i)
       {
-        if (CUT && ((m >> i) & 1u) == 0u)
+        if ((CUT && ((m >> i) & 1u) == 0u) || !has[i * T::CELLS + cell])
           continue;
-        const int b = CUT ? int((gl >> (4 * i)) & 15ull) : i;
-        R         v[DIM];
-        if (advection_velocity<DIM>(a, g, cc, q, b, v))
+        R v[DIM];
+        adv_velocity<DIM>(vel, i * T::CELLS + cell, dq, v);
 #pragma unroll
-          for (int d = 0; d < DIM; ++d)
-            flux[d] = flux[d] - v[d] * c;
+        for (int d = 0; d < DIM; ++d)
+          flux[d] = flux[d] - v[d] * c;
       }
 #pragma unroll
     for (int d = 0; d < DIM; ++d)
-      P[((1 + d) * Slots<DIM>::NQ + q) * Tile<DIM>::CELLS + cell] = flux[d];
+      P[((1 + d) * Slots<DIM>::NQ + q) * T::CELLS + cell] = flux[d];
   }
 
   // Phase 3: integrate every row of every cell into K[(row * NQ + l) * CP + cell];
@@ -381,12 +441,13 @@ namespace sint
   // operator_sintering_generic.h:456-537, :1008-1081, assemble the relevant
   // grains' rows only).  ADV: the eta_i row of a grain with a velocity on the
   // cell gains the flux -v_i eta_i (operator_sintering_generic.h:1015-1036,
-  // :167-177), eta_i interpolated from the same nodal values `stiff` holds.
+  // :167-177), eta_i interpolated from the same nodal values `stiff` holds;
+  // warps in which no cell of the row moves keep the value-only integration.
   template <int DIM, int G, typename R, bool CUT = false, bool ADV = false>
   __device__ __forceinline__ void phase_integrate(const PhysR<R> &p, const Grid &g, const CellConsts<DIM, R> &k,
                                                   const TileCoord &tc, const R *P, const R *stiff, R *K,
-                                                  unsigned m = ~0u, const AdvData *adv = nullptr,
-                                                  unsigned long long gl = 0ull)
+                                                  unsigned m = ~0u, const R *vel = nullptr,
+                                                  const unsigned char *has = nullptr)
   {
     using T            = Tile<DIM>;
     constexpr int NQ   = 1 << DIM;
@@ -424,7 +485,7 @@ namespace sint
               }
             cell_integrate_vg<DIM>(v, gg, k, r);
           }
-        else if (ADV && row >= 2)
+        else if (ADV && row >= 2 && __any_sync(0xffffffffu, has[(row - 2) * T::CELLS + cell] != 0))
           {
             R v[NQ], u[NQ], gg[DIM][NQ];
 #pragma unroll
@@ -436,20 +497,20 @@ namespace sint
                   gg[d][q] = R(0);
               }
             cell_nodes<DIM>(stiff + row * T::BOX, b0, u);
-            int cc[3];
-            if (cell_global<DIM>(cell, tc, g, cc))
+            const int it = (row - 2) * T::CELLS + cell;
+            if (has[it])
               {
-                const int b = CUT ? int((gl >> (4 * (row - 2))) & 15ull) : row - 2;
-                R         e[NQ];
+                R e[NQ];
                 cell_values<DIM>(u, k, e);
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
                   {
-                    R vel[DIM];
-                    if (advection_velocity<DIM>(*adv, g, cc, q, b, vel))
+                    R dq[3], vq[DIM];
+                    adv_offset<DIM>(k, g, q, dq);
+                    adv_velocity<DIM>(vel, it, dq, vq);
 #pragma unroll
-                      for (int d = 0; d < DIM; ++d)
-                        gg[d][q] = -(vel[d] * e[q]);
+                    for (int d = 0; d < DIM; ++d)
+                      gg[d][q] = -(vq[d] * e[q]);
                   }
               }
             cell_integrate_vg<DIM>(v, gg, k, r);
@@ -500,7 +561,7 @@ namespace sint
     return r;
   }
 
-  template <int DIM, int G, bool TENS, bool JVP, bool HIST>
+  template <int DIM, int G, bool TENS, bool JVP, bool HIST, bool ADV = false>
   struct ThreePhaseSmem
   {
     using T                     = Tile<DIM>;
@@ -512,8 +573,12 @@ namespace sint
     static constexpr int P_SIZE = (DIM + 2 + G) * NQ * T::CELLS;   // point results
     static constexpr int K_SIZE = C * NQ * T::CP;
     static_assert(K_SIZE <= F_SIZE, "node contributions must fit in the point-field buffer");
+    // staged advection coefficients (adv_stage): 6 values and one flag byte
+    // per (grain, cell); the flags are counted in 4-byte elements
+    static constexpr int ADV_VEL = ADV ? 6 * G * T::CELLS : 0;
+    static constexpr int ADV_HAS = ADV ? (G * T::CELLS + 3) / 4 : 0;
     // elements: the JVP double-buffers its boxes, the residual does not
-    static constexpr int TOTAL = (JVP ? 2 : 1) * BOXES + F_SIZE + P_SIZE;
+    static constexpr int TOTAL = (JVP ? 2 : 1) * BOXES + F_SIZE + P_SIZE + ADV_VEL + ADV_HAS;
   };
 
   // -------------------------------------------------------------------------
@@ -552,13 +617,15 @@ namespace sint
                R *__restrict__ dst, R *__restrict__ partial, const CutTiles ct, const AdvData adv)
   {
     using T  = Tile<DIM>;
-    using SM = ThreePhaseSmem<DIM, G, TENS, true, false>;
+    using SM = ThreePhaseSmem<DIM, G, TENS, true, false, ADV>;
     constexpr int C = G + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *s_buf = reinterpret_cast<R *>(smem_raw); // 2 x BOXES
     R *F     = s_buf + 2 * SM::BOXES;
     R *P     = F + SM::F_SIZE;
     R *K     = F; // aliases the point fields, dead after phase 2
+    R *A_vel = P + SM::P_SIZE;
+    unsigned char *A_has = reinterpret_cast<unsigned char *>(A_vel + SM::ADV_VEL);
 
     const PhysR<R>           p(ph);
     const CellConsts<DIM, R> k(g);
@@ -628,17 +695,19 @@ namespace sint
         const TileCoord tc = tile_coord_of<DIM>(g, tile);
         const R        *cb = s_buf + (it & 1) * SM::BOXES;
         const unsigned  m  = CUT ? local_mask<G>(m_glob, gl) : ~0u;
+        if constexpr (ADV)
+          adv_stage<DIM, G, R, CUT>(adv, g, tc, gl, A_vel, A_has);
         phase_evaluate<DIM, G, TENS, true, false, R, CUT>(cb, cb + C * T::BOX, F, k, m);
         __syncthreads();
         jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, cell, m);
         if constexpr (ADV)
           {
             using FM = FieldMap<DIM, G, TENS, true, false>;
-            advect_c_point<DIM, G, R, CUT>(adv, g, tc, F, FM::base(FM::src_c), P, threadIdx.x / T::CELLS, cell, m,
-                                           gl);
+            advect_c_point<DIM, G, R, CUT>(k, g, F, FM::base(FM::src_c), P, threadIdx.x / T::CELLS, cell, m, A_vel,
+                                           A_has);
           }
         __syncthreads();
-        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, cb + C * T::BOX, K, m, &adv, gl);
+        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, cb + C * T::BOX, K, m, A_vel, A_has);
         __syncthreads();
         sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
         __syncthreads(); // K and this buffer are reused by the next iterations
@@ -674,7 +743,7 @@ namespace sint
   {
     using R  = double;
     using T  = Tile<DIM>;
-    using SM = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2>;
+    using SM = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2, ADV>;
     constexpr int C = G + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *s_u = reinterpret_cast<R *>(smem_raw);
@@ -682,6 +751,8 @@ namespace sint
     R *F   = s_u + SM::BOXES;
     R *P   = F + SM::F_SIZE;
     R *K   = F;
+    R *A_vel = P + SM::P_SIZE;
+    unsigned char *A_has = reinterpret_cast<unsigned char *>(A_vel + SM::ADV_VEL);
 
     const PhysR<R>           p(ph);
     const CellConsts<DIM, R> k(g);
@@ -715,6 +786,8 @@ namespace sint
                   s_h[comp * T::BOX + bn.b] = v;
                 }
           }
+        if constexpr (ADV)
+          adv_stage<DIM, G, R, CUT>(adv, g, tc, gl, A_vel, A_has);
         __syncthreads();
         phase_evaluate<DIM, G, TENS, false, WTD == 2, R, CUT>(s_u, s_h, F, k, m);
         __syncthreads();
@@ -722,11 +795,11 @@ namespace sint
         if constexpr (ADV)
           {
             using FM = FieldMap<DIM, G, TENS, false, WTD == 2>;
-            advect_c_point<DIM, G, R, CUT>(adv, g, tc, F, FM::base(FM::lin_c), P, threadIdx.x / T::CELLS,
-                                           threadIdx.x % T::CELLS, m, gl);
+            advect_c_point<DIM, G, R, CUT>(k, g, F, FM::base(FM::lin_c), P, threadIdx.x / T::CELLS,
+                                           threadIdx.x % T::CELLS, m, A_vel, A_has);
           }
         __syncthreads();
-        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, s_u, K, m, &adv, gl);
+        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, s_u, K, m, A_vel, A_has);
         __syncthreads();
         sum_and_store<DIM>(K, C, g, tc, bn, dst, partial, gl, CUT, ct.c_all, tm);
         __syncthreads();

@@ -31,7 +31,7 @@ namespace sint
   cudaError_t launch_jvp_g(const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
                            const CutTiles &ct, const AdvData &adv, cudaStream_t s)
   {
-    const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false>::TOTAL * sizeof(R);
+    const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false, ADV>::TOTAL * sizeof(R);
     auto         k    = jvp_kernel<DIM, G, TENS, R, CUT, ADV>;
     // persistent grid: as many blocks as are resident at once
     static int   grid_cap = 0;
@@ -58,7 +58,7 @@ namespace sint
                                 double *dst, double *partial, const CutTiles &ct, const AdvData &adv,
                                 cudaStream_t s)
   {
-    const size_t  smem     = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2>::TOTAL * sizeof(double);
+    const size_t  smem     = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2, ADV>::TOTAL * sizeof(double);
     auto          k        = residual_kernel<DIM, G, TENS, WTD, CUT, ADV>;
     static int    grid_cap = 0;
     cudaError_t   e        = cudaSuccess;

@@ -82,3 +82,27 @@ def detect_particles(op, u, order_parameter, threshold_lower=0.01):
     (the tracker's per-order-parameter loop body, tracker.h:1207-1300)."""
     eta = u[2 + order_parameter]
     return compute_particles_properties(op, eta, detect_local_particle_groups(op, eta, threshold_lower))
+
+
+def advection_segments(op, u, threshold_lower=0.01):
+    """Segments for the advection mechanism from the state u: every particle
+    of every order parameter is one segment (the tracker's grain segments,
+    tracker.h:1207-1300, with the particle centers as segment centers).
+    Returns (cell_segments: device int32 (n_grains, n_cells), -1 = none;
+    centers: device float64 (n_segments, 3); owners: list of (order
+    parameter, particle) per segment)."""
+    G = op.params.n_grains
+    n_cells = _n_cells(op)
+    seg = torch.full((G, n_cells), -1, dtype=torch.int32, device="cuda")
+    centers, owners, base = [], [], 0
+    for b in range(G):
+        parts = detect_particles(op, u, b, threshold_lower)
+        if parts.n_particles:
+            seg[b] = torch.where(parts.ids >= 0, parts.ids + base, parts.ids)
+            c = np.zeros((parts.n_particles, 3))
+            c[:, :op.mesh.dim] = parts.centers
+            centers.append(c)
+            owners += [(b, p) for p in range(parts.n_particles)]
+            base += parts.n_particles
+    cen = np.concatenate(centers) if centers else np.zeros((0, 3))
+    return seg, torch.from_numpy(cen).cuda(), owners

@@ -9,6 +9,8 @@ asked to do:
   failure -> dt halving, restore    sintering/driver.h:2163-2202, :2489-2505
   dt growth after "good" steps      sintering/driver.h:2239-2243, :2387-2409
   grain cut-off before each attempt sintering/driver.h:2212-2218
+  advection: tracker segments, then  sintering/driver.h:1000-1030, :2205-2224 (the
+    forces in every residual        tracker runs before the step), residual_wrapper.h:36-84
   defaults                          time_integration/time_integrator_parameters.h:32-36
 The solution stays on the device; a step is one sint_newton_solve call (or
 several after failures).
@@ -31,6 +33,19 @@ class TimeIntegrationData:
     growth_factor: float = 1.2
     desirable_newton_iterations: int = 5
     desirable_linear_iterations: int = 100
+
+
+@dataclass
+class AdvectionData:
+    """AdvectionData (sintering/parameters.h:719-745) plus the tracker's
+    threshold_lower that defines the grain segments."""
+    k: float = 20.0
+    cgb: float = 0.1
+    ceq: float = 1.0
+    smoothening: float = 0.0
+    mt: float = 1.0
+    mr: float = 1.0
+    threshold_lower: float = 0.01
 
 
 @dataclass
@@ -71,10 +86,16 @@ class TimeIntegrator:
     sets the operator's grain cut-off from u_n before every step attempt, as
     the driver does before make_step; a predicted guess keeps u_n on the DoFs
     the cut-off takes out of the system (they have no equation this step).
+
+    advection (AdvectionData) enables the advection mechanism: before every
+    step attempt the particles of every order parameter of u_n become the
+    segments (device labelling), and every residual evaluation of the solve
+    moves them with the forces of its own state.
     """
 
     def __init__(self, op: SinteringOperatorGeneric, nl: NonLinearData = None, td: TimeIntegrationData = None,
-                 predictor=None, tolerance_base="initial_guess", grain_cut_off_tolerance=0.0):
+                 predictor=None, tolerance_base="initial_guess", grain_cut_off_tolerance=0.0,
+                 advection: AdvectionData = None):
         if tolerance_base not in ("initial_guess", "old_solution"):
             raise ValueError(f"tolerance_base must be 'initial_guess' or 'old_solution', not {tolerance_base!r}")
         self.op = op
@@ -85,6 +106,8 @@ class TimeIntegrator:
         self.tolerance_base = tolerance_base
         self.grain_cut_off_tolerance = float(grain_cut_off_tolerance)
         self.cut_off_statistics = []  # per accepted step: cells per number of relevant grains
+        self.advection = advection
+        self.advection_forces = []    # per accepted step: (owners, volume/force/torque per segment at u_n+1)
         self._r = None
         self.history = []     # old solutions, most recent first (device tensors)
         self.dts = []         # accepted time steps, most recent first
@@ -102,6 +125,12 @@ class TimeIntegrator:
         self.dt = self.td.time_step_init
         self.records = []
         self.newton.clear()
+
+    def _set_advection(self):
+        from .grain_tracker import advection_segments
+        a = self.advection
+        seg, centers, self._owners = advection_segments(self.op, self.history[0], a.threshold_lower)
+        self.op.set_advection_mechanism(seg, centers, a.k, a.cgb, a.ceq, a.smoothening, a.mt, a.mr)
 
     def _weights(self, dt):
         order = min(self.td.scheme_order, len(self.history))
@@ -130,6 +159,8 @@ class TimeIntegrator:
             self.op.set_time_weights(w0, wh, 1.0)
             if self.grain_cut_off_tolerance != 0.0:
                 self.op.set_component_mask(self.history[0], self.grain_cut_off_tolerance)
+            if self.advection is not None:
+                self._set_advection()
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
             if guess is not None and self.grain_cut_off_tolerance != 0.0:
                 # DoFs outside the cut-off's reach have no equation this step: keep their old values
@@ -160,6 +191,8 @@ class TimeIntegrator:
                                        st.final_residual, t1 - t_try, self._reference_residual))
         if self.grain_cut_off_tolerance != 0.0:
             self.cut_off_statistics.append(self.op.component_mask_statistics())
+        if self.advection is not None:
+            self.advection_forces.append((self._owners, self.op.advection_forces(u).cpu().numpy()))
         self.history.insert(0, u)
         self.dts.insert(0, self.dt)
         keep = max(2, self.td.scheme_order)  # predictors use the last two states
