@@ -81,6 +81,7 @@ SIGNATURES = {
     "sint_set_advection": (_c_int, [_c_void, _c_void, _c_void, _c_int, _c_void]),
     "sint_set_advection_mechanism": (_c_int, [_c_void, _c_void, _c_void, _c_int, P(SintAdvectionParams), _c_void]),
     "sint_advection_forces": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
+    "sint_advection_check_courant": (_c_int, [_c_void, _c_double, P(_c_int), _c_void]),
     "sint_vec_axpy_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_sadd_f64": (_c_int, [_c_int64, _c_double, _c_double, _c_void, _c_void, _c_void]),
     "sint_vec_scale_f64": (_c_int, [_c_int64, _c_double, _c_void, _c_void]),

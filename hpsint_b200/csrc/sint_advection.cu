@@ -2,6 +2,7 @@
 // the per-segment velocities the residual and J v kernels read
 // (AdvectionMechanism, sintering/advection.h:297-520; the terms themselves are
 // in the cell kernels).
+#include <cmath>
 #include <cstdint>
 #include <string>
 
@@ -373,6 +374,41 @@ namespace sint
       }
   }
 
+  // CFLChecker::check_courant (sintering/cfl_checker.h:62-128): flags any
+  // (cell, relevant grain with a velocity, point) with |v| dt >= diameter.
+  __global__ void adv_courant_kernel(Grid g, int G, const uint16_t *__restrict__ mask, AdvData a, double dt,
+                                     double diam, unsigned *__restrict__ bad)
+  {
+    const long long n_cells = (long long)g.n[0] * g.n[1] * g.n[2];
+    const long long it      = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (it >= n_cells * G)
+      return;
+    const int       b    = int(it / n_cells);
+    const long long cell = it - b * n_cells;
+    if (mask && ((mask[cell] >> b) & 1u) == 0u)
+      return;
+    const int s = a.cell_segments[it];
+    if (s < 0 || s >= a.n_segments)
+      return;
+    const int     co[3] = {int(cell % g.n[0]), int((cell / g.n[0]) % g.n[1]), int(cell / ((long long)g.n[0] * g.n[1]))};
+    const double *d     = a.segments + 9 * (long long)s;
+    const double  gp[2] = {0.5 - 0.5 / sqrt(3.0), 0.5 + 0.5 / sqrt(3.0)};
+    for (int q = 0; q < (1 << g.dim); ++q)
+      {
+        double r[3] = {0.0, 0.0, 0.0};
+        for (int e = 0; e < g.dim; ++e)
+          r[e] = a.origin[e] + (co[e] + gp[(q >> e) & 1]) * g.h[e] - d[6 + e];
+        const double v0 = d[0] + d[4] * r[2] - d[5] * r[1];
+        const double v1 = d[1] + d[5] * r[0] - d[3] * r[2];
+        const double v2 = g.dim == 3 ? d[2] + d[3] * r[1] - d[4] * r[0] : 0.0;
+        if (!(sqrt(v0 * v0 + v1 * v1 + v2 * v2) * dt < diam))
+          {
+            atomicOr(bad, 1u);
+            return;
+          }
+      }
+  }
+
   // Velocity table with zero velocities at the given centers.
   __global__ void adv_init_table_kernel(int S, const double *__restrict__ centers, double *__restrict__ table)
   {
@@ -611,5 +647,38 @@ int sint_advection_forces(sint_ctx *c, const double *u, double *vft, sint_stream
     if (const cudaError_t e = cudaMemcpyAsync(vft, c->adv_vft, sizeof(double) * (size_t)nc * S,
                                               cudaMemcpyDeviceToDevice, stream))
       return cuda_fail(e, "sint_advection_forces: copy");
+  return SINT_OK;
+}
+
+int sint_advection_check_courant(sint_ctx *c, double dt, int *ok, sint_stream_t stream)
+{
+  if (!c || !ok || !(dt >= 0.0))
+    {
+      set_error("sint_advection_check_courant: null argument or negative dt");
+      return SINT_ERR_ARG;
+    }
+  if (!c->adv)
+    {
+      set_error("sint_advection_check_courant: no advection set");
+      return SINT_ERR_NOT_READY;
+    }
+  const long long n_items = (long long)c->grid.n[0] * c->grid.n[1] * c->grid.n[2] * c->G;
+  double          diam2   = 0.0;
+  for (int d = 0; d < c->grid.dim; ++d)
+    diam2 += c->grid.h[d] * c->grid.h[d];
+  unsigned    bad = 0;
+  cudaError_t e   = cudaMemsetAsync(c->adv_error, 0, sizeof(unsigned), stream);
+  if (e == cudaSuccess)
+    {
+      adv_courant_kernel<<<dim3((unsigned)((n_items + 255) / 256)), 256, 0, stream>>>(
+        c->grid, c->G, active_mask(c), c->adv_view, dt, std::sqrt(diam2), c->adv_error);
+      count_launches(1);
+      if ((e = cudaGetLastError()) == cudaSuccess &&
+          (e = cudaMemcpyAsync(&bad, c->adv_error, sizeof(unsigned), cudaMemcpyDeviceToHost, stream)) == cudaSuccess)
+        e = cudaStreamSynchronize(stream);
+    }
+  if (e != cudaSuccess)
+    return cuda_fail(e, "sint_advection_check_courant");
+  *ok = bad ? 0 : 1;
   return SINT_OK;
 }

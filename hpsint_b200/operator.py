@@ -268,6 +268,14 @@ class SinteringOperatorGeneric:
                 "sint_advection_forces")
         return out
 
+    def check_courant(self, dt):
+        """CFLChecker::check_courant with the current velocities: True when
+        |v| dt < cell diameter everywhere a grain moves."""
+        ok = ctypes.c_int()
+        L.check(L.lib().sint_advection_check_courant(self._h, float(dt), ctypes.byref(ok), _stream()),
+                "sint_advection_check_courant")
+        return bool(ok.value)
+
     def _check_segments(self, cell_segments):
         n_cells = 1
         for d in range(self.mesh.dim):

@@ -46,6 +46,7 @@ class AdvectionData:
     mt: float = 1.0
     mr: float = 1.0
     threshold_lower: float = 0.01
+    check_courant: bool = False   # CFLChecker before every step attempt (driver.h:2219-2226)
 
 
 @dataclass
@@ -126,11 +127,26 @@ class TimeIntegrator:
         self.records = []
         self.newton.clear()
 
+    def _halve_or_raise(self):
+        self.dt *= 0.5
+        self.newton.clear()
+        if self.dt <= self.td.time_step_min:
+            last = self.failures[-1]
+            raise L.SintError(8, "TimeIntegrator.step",
+                              f"Minimum timestep size exceeded, solution failed! (t = {self.t:.6g}, last "
+                              f"Newton status {last[2]}: {last[3]})")
+
     def _set_advection(self):
+        """Segments from u_n and the mechanism; False when the Courant check
+        (AdvectionData.check_courant) fails at the current dt."""
         from .grain_tracker import advection_segments
         a = self.advection
         seg, centers, self._owners = advection_segments(self.op, self.history[0], a.threshold_lower)
         self.op.set_advection_mechanism(seg, centers, a.k, a.cgb, a.ceq, a.smoothening, a.mt, a.mr)
+        if a.check_courant:
+            self.op.advection_forces(self.history[0])
+            return self.op.check_courant(self.dt)
+        return True
 
     def _weights(self, dt):
         order = min(self.td.scheme_order, len(self.history))
@@ -159,8 +175,13 @@ class TimeIntegrator:
             self.op.set_time_weights(w0, wh, 1.0)
             if self.grain_cut_off_tolerance != 0.0:
                 self.op.set_component_mask(self.history[0], self.grain_cut_off_tolerance)
-            if self.advection is not None:
-                self._set_advection()
+            if self.advection is not None and not self._set_advection():
+                # ExcCourantConditionViolated -> process_failure (driver.h:2219-2227, :2498-2501)
+                tries += 1
+                self.failures.append((self.t, self.dt, -1, "The Courant condition was violated. The advection "
+                                      "velocity is too high.", 0, 0, 0.0, 0.0))
+                self._halve_or_raise()
+                continue
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
             if guess is not None and self.grain_cut_off_tolerance != 0.0:
                 # DoFs outside the cut-off's reach have no equation this step: keep their old values
@@ -176,13 +197,7 @@ class TimeIntegrator:
             tries += 1
             self.failures.append((self.t, self.dt, st.status, L.last_error(), st.newton_iterations,
                                   st.linear_iterations, st.initial_residual, st.final_residual))
-            self.dt *= 0.5
-            self.newton.clear()
-            if self.dt <= self.td.time_step_min:
-                last = self.failures[-1]
-                raise L.SintError(8, "TimeIntegrator.step",
-                                  f"Minimum timestep size exceeded, solution failed! (t = {self.t:.6g}, last "
-                                  f"Newton status {last[2]}: {last[3]})")
+            self._halve_or_raise()
         torch.cuda.synchronize()
         self.t += self.dt
         t1 = time.perf_counter()

@@ -315,6 +315,13 @@ int sint_set_advection_mechanism(sint_ctx *ctx, const int32_t *cell_segments, co
  * torque = hpsint's scalar cross product r[1] F[0] - r[0] F[1]). */
 int sint_advection_forces(sint_ctx *ctx, const double *u, double *vft, sint_stream_t stream);
 
+/* CFLChecker::check_courant (sintering/cfl_checker.h:62-128) with the
+ * current velocity table: *ok = 1 when |v| dt < cell diameter at every
+ * quadrature point of every cell for every (relevant) grain with a
+ * velocity there, else 0 (the driver then throws
+ * ExcCourantConditionViolated).  Synchronises `stream`. */
+int sint_advection_check_courant(sint_ctx *ctx, double dt, int *ok, sint_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* BLAS-1 on block vectors: DynamicBlockVector                              */
 /* (include/pf-applications/lac/dynamic_block_vector.h:346-516).            */

@@ -72,6 +72,7 @@ def lib():
                                               P(_c_double)]
         L.oracle_advection_velocities.argtypes = [_c_int, P(_c_double), P(_c_double), _c_int, _c_double,
                                                   _c_double, P(_c_double)]
+        L.oracle_advection_courant.argtypes = [P(Mesh), P(Params), U16, P(Advection), _c_double]
         _lib = L
     return _lib
 
@@ -282,3 +283,13 @@ def advection_velocities(dim, vft, centers, mt, mr):
     _check(lib().oracle_advection_velocities(int(dim), _dptr(vft), _dptr(cen), cen.shape[0], float(mt), float(mr),
                                              _dptr(out)), "advection_velocities")
     return out
+
+
+def advection_courant(mesh, params, advection, dt, mask=None):
+    """CFLChecker::check_courant: True when |v| dt < cell diameter everywhere."""
+    keep, mp = _mptr(mask, mesh)
+    keep_a, ap = _adv(advection, mesh)
+    r = lib().oracle_advection_courant(ctypes.byref(mesh), ctypes.byref(params), mp, ap, float(dt))
+    if r < 0:
+        raise ValueError("advection_courant: bad arguments")
+    return bool(r)

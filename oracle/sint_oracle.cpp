@@ -1227,6 +1227,37 @@ int oracle_advection_forces(const oracle_mesh *m, const oracle_params *p, const 
   return 0;
 }
 
+// CFLChecker::check_courant (sintering/cfl_checker.h:62-128): returns 1 when
+// |v| dt < cell diameter for every relevant grain with a velocity at every
+// quadrature point of every cell, else 0 (-1 on bad arguments).
+int oracle_advection_courant(const oracle_mesh *m, const oracle_params *p, const uint16_t *mask,
+                             const oracle_advection *adv, double dt)
+{
+  if (check_args(m, p) || !adv)
+    return -1;
+  const Geometry geo(*m);
+  double         diam2 = 0.0;
+  for (int d = 0; d < geo.dim; ++d)
+    diam2 += geo.h[d] * geo.h[d];
+  const double diam = std::sqrt(diam2);
+  for (int k = 0; k < geo.n[2]; ++k)
+    for (int j = 0; j < geo.n[1]; ++j)
+      for (int i = 0; i < geo.n[0]; ++i)
+        {
+          int       blk[MAXC];
+          const int G = cell_blocks(geo, mask, p->n_grains, i, j, k, blk);
+          for (int ig = 0; ig < G; ++ig)
+            for (int q = 0; q < geo.nq; ++q)
+              {
+                V3 v;
+                if (advection_velocity(adv, geo, blk[2 + ig] - 2, i, j, k, q, v) &&
+                    !(std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * dt < diam))
+                  return 0;
+              }
+        }
+  return 1;
+}
+
 // AdvectionMechanism::calc_translation_velocity / calc_rotation_velocity
 // (sintering/advection.h:330-352): per segment the velocity table the
 // residual and J v read: v_t = mt force / volume, w = mr torque / volume (the

@@ -1,4 +1,6 @@
 """Shared helpers of the test-suite: random sintering states, parity metrics."""
+import itertools
+
 import numpy as np
 
 from oracle import oracle as O
@@ -148,3 +150,30 @@ def advection_data(dim, cells, G, seed, n_seg_per_grain=2, scale=1.0):
     if dim == 2:
         data[:, 2] = 0.0
     return seg, data
+
+
+def max_speed(dim, cells, h, origin, seg, data, mask=None):
+    """Largest |v| over the quadrature points of every (cell, grain) with a segment."""
+    n_cells = int(np.prod(cells))
+    idx = np.arange(n_cells)
+    co = np.stack([idx % cells[0], (idx // cells[0]) % cells[1],
+                   idx // (cells[0] * cells[1]) if dim == 3 else np.zeros_like(idx)], axis=1)
+    vmax = 0.0
+    for b in range(seg.shape[0]):
+        sel = seg[b] >= 0
+        if mask is not None:
+            sel &= ((mask >> b) & 1).astype(bool)
+        s = seg[b, sel]
+        for qb in itertools.product((0, 1), repeat=dim):
+            x = np.zeros((s.size, 3))
+            for d in range(dim):
+                x[:, d] = origin[d] + (co[sel, d] + (0.5 + (qb[d] - 0.5) / np.sqrt(3.0))) * h[d]
+            r = x - data[s, 6:9]
+            if dim == 2:
+                r[:, 2] = 0.0
+            v = data[s, 0:3] + np.cross(data[s, 3:6], r)
+            if dim == 2:
+                v[:, 2] = 0.0
+            if v.size:
+                vmax = max(vmax, float(np.sqrt((v ** 2).sum(axis=1)).max()))
+    return vmax

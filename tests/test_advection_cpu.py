@@ -16,7 +16,7 @@ import itertools
 import numpy as np
 import pytest
 
-from helpers import advection_data, oracle_mesh, random_state
+from helpers import advection_data, max_speed, oracle_mesh, random_state
 from oracle import oracle as O
 
 GP = (0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0))
@@ -261,3 +261,25 @@ def test_forces_balance(dim, cells):
         wd[[0, -1]] = 0.5
         w = np.kron(wd, w)
     assert np.allclose(f[:, 0], u[2:] @ w, rtol=1e-13)
+
+
+@pytest.mark.parametrize("dim,cells,G", [(2, (9, 7), 3), (3, (5, 4, 4), 3)])
+def test_courant_check(dim, cells, G):
+    """CFLChecker::check_courant: violated exactly when |v| dt reaches the
+    cell diameter somewhere a relevant grain moves."""
+    h = (0.7, 1.3, 0.9)
+    om, p = O.make_mesh(dim, list(cells) + [0] * (3 - dim), h), O.make_params(G)
+    seg, data = advection_data(dim, cells, G, seed=31)
+    adv = (seg, data, (0.5, -1.0, 0.0))
+    diam = np.sqrt(sum(h[d] ** 2 for d in range(dim)))
+    dt_crit = diam / max_speed(dim, cells, h, adv[2], seg, data)
+    assert O.advection_courant(om, p, adv, dt_crit * (1 - 1e-9))
+    assert not O.advection_courant(om, p, adv, dt_crit * (1 + 1e-9))
+    # no segments: never violated
+    assert O.advection_courant(om, p, (np.full_like(seg, -1), data, adv[2]), 1e9)
+    # the cut-off's irrelevant grains do not count
+    mask = np.random.default_rng(32).integers(0, 1 << G, int(np.prod(cells))).astype(np.uint16)
+    dt_m = diam / max_speed(dim, cells, h, adv[2], seg, data, mask)
+    assert dt_m >= dt_crit
+    assert O.advection_courant(om, p, adv, dt_m * (1 - 1e-9), mask=mask)
+    assert not O.advection_courant(om, p, adv, dt_m * (1 + 1e-9), mask=mask)

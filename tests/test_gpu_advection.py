@@ -10,7 +10,7 @@ solves read the current velocities.
 import numpy as np
 import pytest
 
-from helpers import advection_data, block_rel_err, oracle_mesh, particle_state, random_state
+from helpers import advection_data, block_rel_err, max_speed, oracle_mesh, particle_state, random_state
 from oracle import oracle as O
 
 torch = pytest.importorskip("torch")
@@ -438,3 +438,36 @@ def test_time_loop_with_tracked_segments():
             assert [o[0] for o in owners] == [0, 1] and vft.shape == (2, 4)
             assert vft[0, 1] > 0 > vft[1, 1]  # the grains pull towards each other
     assert dist[False] < dist[True] - 1e-4
+
+
+@pytest.mark.parametrize("dim,cells,G", [(2, (37, 21), 4), (3, (13, 11, 9), 5)])
+def test_courant_check_matches_oracle(dim, cells, G):
+    op, p, om = make_op(dim, cells, G, True)
+    seg, data = advection_data(dim, cells, G, seed=71, scale=3.0)
+    set_adv(op, seg, data)
+    diam = np.sqrt(sum(H[d] ** 2 for d in range(dim)))
+    dt_crit = diam / max_speed(dim, cells, H, ORIGIN, seg, data)
+    for f in (1 - 1e-9, 1 + 1e-9, 0.5, 2.0):
+        dt = dt_crit * f
+        assert op.check_courant(dt) == O.advection_courant(om, p, (seg, data, ORIGIN), dt) == (f < 1)
+    # under the cut-off only the relevant grains count
+    u = particle_state(dim, cells, G, seed=72)
+    op.set_component_mask(op.to_device(u), 1e-3)
+    mask = O.grain_mask(om, p, u, 1e-3)
+    dt_m = diam / max_speed(dim, cells, H, ORIGIN, seg, data, mask)
+    for f in (1 - 1e-9, 1 + 1e-9):
+        assert op.check_courant(dt_m * f) == O.advection_courant(om, p, (seg, data, ORIGIN), dt_m * f, mask=mask)
+
+
+def test_time_loop_halves_dt_on_courant_violation():
+    import hpsint_b200 as hb
+    from hpsint_b200.time_integration import AdvectionData, TimeIntegrationData, TimeIntegrator
+    cells, G = (40, 20), 2
+    op = hb.SinteringOperatorGeneric(hb.Mesh(2, tuple(cells) + (1,)), hb.Params(G, tensorial=True))
+    # mt = mr = 50: velocities near 1, so the Courant limit sqrt(2) / |v| is near 1.5
+    adv = AdvectionData(k=2.5, cgb=0.0, ceq=0.9, mt=50.0, mr=50.0, check_courant=True)
+    ti = TimeIntegrator(op, td=TimeIntegrationData(time_step_init=4.0, time_step_min=1e-4), advection=adv)
+    ti.initialize(op.to_device(_two_particles(cells)))
+    ti.step()
+    courant = [f for f in ti.failures if f[2] == -1]
+    assert courant and ti.records[-1].dt <= 2.0
