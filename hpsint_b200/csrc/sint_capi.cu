@@ -70,8 +70,11 @@ namespace sint
             : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, cut, adv, s);
     if (e != cudaSuccess)
       return e;
-    return c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, active_tile_union(c), s)
-                            : launch_combine<2, R>(c->C, c->grid, part, dst, active_tile_union(c), s);
+    e = c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, active_tile_union(c), s)
+                         : launch_combine<2, R>(c->C, c->grid, part, dst, active_tile_union(c), s);
+    if (e != cudaSuccess)
+      return e;
+    return launch_periodic_condense<R>(c->grid, c->C, dst, src, 0, s);
   }
 
   template cudaError_t dispatch_jvp<double>(const Ctx *, const double *, const double *, double *, cudaStream_t);
@@ -92,8 +95,11 @@ namespace sint
             : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s);
     if (e != cudaSuccess)
       return e;
-    return c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s)
-                            : launch_combine<2, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s);
+    e = c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s)
+                         : launch_combine<2, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s);
+    if (e != cudaSuccess)
+      return e;
+    return launch_periodic_condense<double>(c->grid, c->C, dst, nullptr, 1, s);
   }
 
   static cudaError_t dispatch_diag(const Ctx *c, double *dst, cudaStream_t s)
@@ -108,8 +114,11 @@ namespace sint
             : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s);
     if (e != cudaSuccess)
       return e;
-    return c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s)
-                            : launch_combine<2, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s);
+    e = c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s)
+                         : launch_combine<2, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s);
+    if (e != cudaSuccess)
+      return e;
+    return launch_periodic_condense<double>(c->grid, c->G + 4, dst, nullptr, 2, s);
   }
 
   // --- preconditioner point kernels ----------------------------------------

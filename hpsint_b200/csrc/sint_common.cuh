@@ -84,6 +84,10 @@ namespace sint
     // the same for nn[0] and nn[1] (node index -> node coordinates; N < 2^31)
     unsigned long long mnode[2];
     int                snode[2];
+    // periodic directions (bit d): the nodes at coordinate n[d] are constrained
+    // to the nodes at 0 (DoFTools::make_periodicity_constraints), so the cell
+    // kernels read the master values there
+    int periodic = 0;
   };
 
   // Granlund-Montgomery division by an invariant integer d >= 1: with
@@ -224,7 +228,8 @@ namespace sint
     int       bx, by, bz;
     bool      active; // thread serves a node
     bool      inside; // node exists in the mesh
-    long long gidx;   // global node index (valid if inside)
+    long long gidx;   // global node index (valid if inside): where results go
+    long long lidx;   // node whose values are read: gidx, or its periodic master
 
     __device__ __forceinline__ BoxNode(const Grid &g, const TileCoord &tc)
     {
@@ -238,6 +243,10 @@ namespace sint
       const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
       inside       = gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2];
       gidx         = inside ? node_index(g, gi, gj, gk) : 0;
+      lidx         = gidx;
+      if (g.periodic && inside)
+        lidx = node_index(g, ((g.periodic & 1) && gi == g.n[0]) ? 0 : gi, ((g.periodic & 2) && gj == g.n[1]) ? 0 : gj,
+                          ((g.periodic & 4) && gk == g.n[2]) ? 0 : gk);
     }
   };
 
@@ -252,7 +261,7 @@ namespace sint
     using T = Tile<DIM>;
     if (!bn.active)
       return;
-    const S *p = src + bn.gidx;
+    const S *p = src + bn.lidx;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
       s[comp * T::BOX + bn.b] = bn.inside ? R(p[(mapped ? comp_of(comp, gl) : comp) * g.ld]) : R(0);
   }
@@ -288,7 +297,7 @@ namespace sint
     using T = Tile<DIM>;
     if (!bn.active)
       return;
-    const R *p = bn.inside ? src + bn.gidx : src;
+    const R *p = bn.inside ? src + bn.lidx : src;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
       cp_async_elem(s + comp * T::BOX + bn.b, bn.inside ? p + (mapped ? comp_of(comp, gl) : comp) * g.ld : src,
                     bn.inside);

@@ -776,7 +776,7 @@ namespace sint
                   R v = R(0);
                   if (comp != 1 && bn.inside)
                     {
-                      const long long off = (CUT ? comp_of(comp, gl) : comp) * g.ld + bn.gidx;
+                      const long long off = (CUT ? comp_of(comp, gl) : comp) * g.ld + bn.lidx;
                       v                   = h0[off] * ph.w_hist[0];
                       if (ph.order > 1)
                         v += h1[off] * ph.w_hist[1];

@@ -47,6 +47,15 @@ namespace sint
   cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, const uint16_t *tile_mask,
                              cudaStream_t s);
 
+  // Periodic constraints after the combine step: slave rows added to their
+  // masters, then set to src (mode 0, J v), zero (mode 1, residual) or the
+  // identity of the preconditioner's outputs (mode 2).  No-op without
+  // periodic directions.
+  template <typename R>
+  cudaError_t launch_periodic_condense(const Grid &g, int ncomp, R *dst, const R *src, int mode, cudaStream_t s);
+  // slaves <- masters (AffineConstraints::distribute)
+  cudaError_t launch_periodic_distribute(const Grid &g, int ncomp, double *u, cudaStream_t s);
+
   // Counts kernel launches issued by this library.
   void count_launches(int n);
 } // namespace sint

@@ -54,6 +54,7 @@ namespace sint
       Phys            key   = {};
       const uint16_t *mask  = nullptr; // cell masks the captured kernels read (nullptr: no cut-off)
       AdvData         adv   = {};      // advection tables the captured kernels read (none: null pointers)
+      int             periodic = 0;    // periodic directions of the captured kernels
       int             nodes = 0;
     } graphs[MAX_MULTIDOT];
     // [FP32 Krylov vectors][grain cut-off][advection]: one eager solve with
@@ -348,7 +349,7 @@ namespace sint
         {
           auto &g = ws->graphs[j];
           if (!g.exec || std::memcmp(&g.key, &c->phys, sizeof(Phys)) != 0 || g.mask != active_mask(c) ||
-              std::memcmp(&g.adv, &adv, sizeof(AdvData)) != 0)
+              std::memcmp(&g.adv, &adv, sizeof(AdvData)) != 0 || g.periodic != c->grid.periodic)
             {
               cudaGraph_t       graph = nullptr;
               const long long   n0    = sint_kernel_launch_count();
@@ -389,6 +390,7 @@ namespace sint
               g.key   = c->phys;
               g.mask  = active_mask(c);
               g.adv   = adv;
+              g.periodic = c->grid.periodic;
               g.nodes = int(nn);
             }
           const cudaError_t e = cudaGraphLaunch(g.exec, s);
@@ -756,7 +758,12 @@ int sint_newton_solve(sint_ctx *c, double *u, const double *const *hist, const s
                                       : "Newton: non-finite residual");
       return SINT_ERR_NEWTON;
     }
-  const cudaError_t e = cudaStreamSynchronize(s);
+  // periodic constraints: the slave entries of the converged step follow
+  // their masters (the updates leave them untouched: J v has identity rows
+  // and the residual zero rows there)
+  cudaError_t e = launch_periodic_distribute(c->grid, c->C, u, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
   return e == cudaSuccess ? SINT_OK : cuda_fail(e, "sint_newton_solve");
 }
 

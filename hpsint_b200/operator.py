@@ -214,6 +214,21 @@ class SinteringOperatorGeneric:
         L.check(L.lib().sint_get_component_mask(self._h, _ptr(out), _stream()), "sint_get_component_mask")
         return out
 
+    def set_periodicity(self, directions):
+        """Periodic directions (iterable of axis indices, e.g. (0, 1)); the
+        nodes at the upper face become slaves of the lower face's
+        (DoFTools::make_periodicity_constraints)."""
+        bits = 0
+        for d in directions:
+            bits |= 1 << int(d)
+        L.check(L.lib().sint_set_periodicity(self._h, bits), "sint_set_periodicity")
+        self.periodic = tuple(sorted(int(d) for d in directions))
+
+    def distribute_constraints(self, u):
+        """Slave entries of u take their masters' values."""
+        self._check_vec(u, torch.float64)
+        L.check(L.lib().sint_distribute_constraints(self._h, _ptr(u), _stream()), "sint_distribute_constraints")
+
     def set_advection(self, cell_segments, segments):
         """Rigid-body motion of the grains (AdvectionMechanism,
         sintering/advection.h:297-520): the residual and J v gain the terms

@@ -261,6 +261,25 @@ int sint_grain_segment_properties(sint_ctx *ctx, const double *eta, const int *p
                                   double *props, sint_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Periodic constraints (DoFTools::make_periodicity_constraints, driver.h:  */
+/* 629-643; OperatorBase::vmult's constrained rows, operator_base.h:        */
+/* 294-353).                                                                */
+
+/* Makes the mesh periodic in the directions whose bit is set (bit d =
+ * direction d; each needs >= 2 cells).  The nodes at coordinate n_cells[d]
+ * become slaves of the nodes at 0: the residual, J v and the preconditioner
+ * read the masters' values there, add the slave rows to the master rows,
+ * and give the slave rows zero (residual) or the identity (J v,
+ * preconditioner).  sint_newton_solve distributes the solution at the end.
+ * 0 switches periodicity off.  The grain tracker and the grain cut-off's
+ * masks read the nodal values as they are: pass distributed vectors. */
+int sint_set_periodicity(sint_ctx *ctx, unsigned directions);
+
+/* AffineConstraints::distribute: every slave entry of u (all components)
+ * takes its master's value. */
+int sint_distribute_constraints(sint_ctx *ctx, double *u, sint_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Advection: rigid-body motion of the grains (AdvectionMechanism,          */
 /* sintering/advection.h:297-520).  Replaces the AdvectionMechanism the     */
 /* operator is constructed with (operator_sintering_generic.h:347-361).     */

@@ -293,3 +293,65 @@ def advection_courant(mesh, params, advection, dt, mask=None):
     if r < 0:
         raise ValueError("advection_courant: bad arguments")
     return bool(r)
+
+
+# --- periodic constraints (DoFTools::make_periodicity_constraints) ---------
+# In a periodic direction d the nodes at coordinate n[d] are slaves of the
+# nodes at 0; chains resolve to the node with all such coordinates at 0.
+# Constrained operators (OperatorBase::vmult, operator_base.h:294-353) read
+# masters for slaves, add the slave rows to the master rows and give the
+# slave rows the identity (J v) or zero (residual).
+
+
+def periodic_pairs(mesh, dirs):
+    """(slave, master) node indices of the periodic directions `dirs`."""
+    dim = mesh.dim
+    nn = [mesh.n[d] + 1 for d in range(dim)]
+    idx = np.arange(int(np.prod(nn)))
+    co = [(idx // int(np.prod(nn[:d]))) % nn[d] for d in range(dim)]
+    slave = np.zeros(idx.size, dtype=bool)
+    mco = [c.copy() for c in co]
+    for d in dirs:
+        on = co[d] == mesh.n[d]
+        slave |= on
+        mco[d][on] = 0
+    master = sum(mco[d] * int(np.prod(nn[:d])) for d in range(dim))
+    return idx[slave], master[slave]
+
+
+def periodic_resolve(mesh, u, dirs):
+    sl, ma = periodic_pairs(mesh, dirs)
+    out = np.array(u, dtype=np.float64, copy=True)
+    out[:, sl] = out[:, ma]
+    return out
+
+
+def periodic_condense(mesh, dst, src, dirs, mode):
+    """mode 0: slave rows = src (J v); 1: zero (residual); 2: the
+    preconditioner outputs' identity (CH blocks 1, 0, 0, 1; AC diagonal 1)."""
+    sl, ma = periodic_pairs(mesh, dirs)
+    out = np.array(dst, dtype=np.float64, copy=True)
+    for c in range(out.shape[0]):
+        np.add.at(out[c], ma, dst[c, sl])
+        if mode == 0:
+            out[c, sl] = src[c, sl]
+        elif mode == 1:
+            out[c, sl] = 0.0
+        else:
+            out[c, sl] = 0.0 if c in (1, 2) else 1.0
+    return out
+
+
+def periodic_jvp(mesh, params, time, lin, src, dirs, **kw):
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    src = np.asarray(src, dtype=np.float64).reshape(C, N)
+    d = jvp(mesh, params, time, periodic_resolve(mesh, np.asarray(lin).reshape(C, N), dirs),
+            periodic_resolve(mesh, src, dirs), **kw)
+    return periodic_condense(mesh, d, src, dirs, 0)
+
+
+def periodic_residual(mesh, params, time, u, hist, with_td, dirs, **kw):
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    r = residual(mesh, params, time, periodic_resolve(mesh, np.asarray(u).reshape(C, N), dirs),
+                 [periodic_resolve(mesh, np.asarray(h).reshape(C, N), dirs) for h in hist], with_td, **kw)
+    return periodic_condense(mesh, r, None, dirs, 1)
