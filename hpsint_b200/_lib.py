@@ -78,6 +78,7 @@ SIGNATURES = {
     "sint_grain_segments": (_c_int, [_c_void, _c_void, _c_double, _c_void, P(_c_int), _c_void]),
     "sint_grain_segment_properties": (_c_int, [_c_void, _c_void, _c_void, _c_int, P(_c_double), _c_void]),
     "sint_get_component_mask": (_c_int, [_c_void, _c_void, _c_void]),
+    "sint_grain_segment_periodicity": (_c_int, [_c_void, _c_void, P(_c_int), _c_int, P(_c_int), _c_void]),
     "sint_set_periodicity": (_c_int, [_c_void, ctypes.c_uint]),
     "sint_distribute_constraints": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_set_advection": (_c_int, [_c_void, _c_void, _c_void, _c_int, _c_void]),

@@ -12,6 +12,7 @@
 // lexicographic order), which is the order a lexicographic flood fill
 // reaches them.  Properties come from integer moment sums and atomic maxima
 // on order-preserving keys, so they do not depend on the thread order either.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -306,6 +307,50 @@ namespace sint
       }
     return SINT_OK;
   }
+  // Periodicity between particles (tracker.h:1290-1336): for every pair of
+  // cells facing each other across a periodic boundary (coordinate n[d] - 1
+  // and 0 in direction d) that both belong to particles, the pair of particle
+  // ids (smaller first).  Appends to pairs[2 k ..] with a cursor (capacity =
+  // the number of such cell pairs, so it never overflows).
+  __global__ void seg_periodic_kernel(Grid g, const int *__restrict__ ids, int *__restrict__ pairs,
+                                      unsigned *__restrict__ count)
+  {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long       base = 0;
+    for (int d = 0; d < g.dim; ++d)
+      {
+        if (!((g.periodic >> d) & 1))
+          continue;
+        const long long face = (long long)g.n[0] * g.n[1] * g.n[2] / g.n[d];
+        if (t >= base + face)
+          {
+            base += face;
+            continue;
+          }
+        // face cell index f -> coordinates of the other directions
+        long long f  = t - base;
+        int       co[3];
+        for (int e = 0; e < 3; ++e)
+          {
+            if (e == d)
+              continue;
+            co[e] = int(f % g.n[e]);
+            f /= g.n[e];
+          }
+        co[d]             = 0;
+        const long long c0 = co[0] + (long long)g.n[0] * (co[1] + (long long)g.n[1] * co[2]);
+        co[d]             = g.n[d] - 1;
+        const long long c1 = co[0] + (long long)g.n[0] * (co[1] + (long long)g.n[1] * co[2]);
+        const int       p = ids[c0], q = ids[c1];
+        if (p >= 0 && q >= 0)
+          {
+            const unsigned k = atomicAdd(count, 1u);
+            pairs[2 * k]     = min(p, q);
+            pairs[2 * k + 1] = max(p, q);
+          }
+        return;
+      }
+  }
 } // namespace sint
 
 using namespace sint;
@@ -416,6 +461,70 @@ int sint_grain_segment_properties(sint_ctx *c, const double *eta, const int *par
       std::memcpy(&m, &mb, sizeof(double));
       o[1 + dim] = r;
       o[2 + dim] = m;
+    }
+  return SINT_OK;
+}
+
+int sint_grain_segment_periodicity(sint_ctx *c, const int *particle_ids, int *pairs, int max_pairs, int *n_pairs,
+                                   sint_stream_t stream)
+{
+  if (!c || !particle_ids || !n_pairs || max_pairs < 0 || (max_pairs > 0 && !pairs))
+    {
+      set_error("sint_grain_segment_periodicity: bad argument");
+      return SINT_ERR_ARG;
+    }
+  *n_pairs = 0;
+  long long cap = 0;
+  for (int d = 0; d < c->grid.dim; ++d)
+    if ((c->grid.periodic >> d) & 1)
+      cap += (long long)c->grid.n[0] * c->grid.n[1] * c->grid.n[2] / c->grid.n[d];
+  if (cap == 0)
+    return SINT_OK;
+  int         *buf   = nullptr;
+  unsigned    *count = nullptr;
+  cudaError_t  e     = cudaMalloc(&buf, sizeof(int) * 2 * (size_t)cap);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&count, sizeof(unsigned));
+  unsigned         k = 0;
+  std::vector<int> host;
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(count, 0, sizeof(unsigned), stream);
+  if (e == cudaSuccess)
+    {
+      seg_periodic_kernel<<<(unsigned)((cap + 255) / 256), 256, 0, stream>>>(c->grid, particle_ids, buf, count);
+      count_launches(1);
+      e = cudaGetLastError();
+    }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&k, count, sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(stream);
+  if (e == cudaSuccess && k > 0)
+    {
+      host.resize(2 * (size_t)k);
+      e = cudaMemcpy(host.data(), buf, sizeof(int) * host.size(), cudaMemcpyDeviceToHost);
+    }
+  cudaFree(buf);
+  cudaFree(count);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "sint_grain_segment_periodicity");
+  // the set of distinct pairs, in increasing order (std::set in the reference)
+  std::vector<std::pair<int, int>> uniq;
+  uniq.reserve(k);
+  for (unsigned i = 0; i < k; ++i)
+    uniq.emplace_back(host[2 * i], host[2 * i + 1]);
+  std::sort(uniq.begin(), uniq.end());
+  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+  *n_pairs = int(uniq.size());
+  if (int(uniq.size()) > max_pairs)
+    {
+      set_error("sint_grain_segment_periodicity: more pairs than max_pairs (n_pairs holds the count)");
+      return SINT_ERR_ARG;
+    }
+  for (size_t i = 0; i < uniq.size(); ++i)
+    {
+      pairs[2 * i]     = uniq[i].first;
+      pairs[2 * i + 1] = uniq[i].second;
     }
   return SINT_OK;
 }

@@ -84,6 +84,45 @@ def detect_particles(op, u, order_parameter, threshold_lower=0.01):
     return compute_particles_properties(op, eta, detect_local_particle_groups(op, eta, threshold_lower))
 
 
+def periodicity(op, particles, max_pairs=4096):
+    """Distinct pairs (p, q), p <= q, of particles that own cells facing each
+    other across a periodic boundary of op (tracker.h:1290-1353); sorted."""
+    pairs = (ctypes.c_int * (2 * max_pairs))()
+    n = ctypes.c_int()
+    L.check(L.lib().sint_grain_segment_periodicity(op._h, ctypes.c_void_p(particles.ids.data_ptr()), pairs,
+                                                   max_pairs, ctypes.byref(n), _stream()),
+            "sint_grain_segment_periodicity")
+    return [(pairs[2 * i], pairs[2 * i + 1]) for i in range(n.value)]
+
+
+def particle_groups(n_particles, pairs):
+    """PeriodicityGraph::build_groups (periodicity_graph.h:57-80): particles
+    connected through periodicity pairs form one grain of several segments.
+    Returns one group id per particle (-1: not periodic), groups numbered by
+    their smallest particle, and the number of groups."""
+    parent = list(range(n_particles))
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    in_graph = [False] * n_particles
+    for p, q in pairs:
+        in_graph[p] = in_graph[q] = True
+        a, b = find(p), find(q)
+        if a != b:
+            parent[max(a, b)] = min(a, b)
+    groups, ids = {}, []
+    for i in range(n_particles):
+        if not in_graph[i]:
+            ids.append(-1)
+            continue
+        ids.append(groups.setdefault(find(i), len(groups)))
+    return ids, len(groups)
+
+
 def advection_segments(op, u, threshold_lower=0.01):
     """Segments for the advection mechanism from the state u: every particle
     of every order parameter is one segment (the tracker's grain segments,

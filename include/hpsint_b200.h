@@ -260,6 +260,17 @@ int sint_grain_segments(sint_ctx *ctx, const double *eta, double threshold_lower
 int sint_grain_segment_properties(sint_ctx *ctx, const double *eta, const int *particle_ids, int n_particles,
                                   double *props, sint_stream_t stream);
 
+/* Periodicity between particles (tracker.h:1290-1353): the distinct pairs
+ * (p, q), p <= q, of particles of `particle_ids` (DEVICE, as returned by
+ * sint_grain_segments) that own cells facing each other across a periodic
+ * boundary of the context (sint_set_periodicity), in increasing order, into
+ * the HOST array pairs[2 * max_pairs].  The tracker groups connected
+ * particles into one grain of several segments (PeriodicityGraph::
+ * build_groups).  More pairs than max_pairs: SINT_ERR_ARG with the count in
+ * *n_pairs.  Synchronises `stream`. */
+int sint_grain_segment_periodicity(sint_ctx *ctx, const int *particle_ids, int *pairs, int max_pairs, int *n_pairs,
+                                   sint_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* Periodic constraints (DoFTools::make_periodicity_constraints, driver.h:  */
 /* 629-643; OperatorBase::vmult's constrained rows, operator_base.h:        */

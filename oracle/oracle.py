@@ -355,3 +355,20 @@ def periodic_residual(mesh, params, time, u, hist, with_td, dirs, **kw):
     r = residual(mesh, params, time, periodic_resolve(mesh, np.asarray(u).reshape(C, N), dirs),
                  [periodic_resolve(mesh, np.asarray(h).reshape(C, N), dirs) for h in hist], with_td, **kw)
     return periodic_condense(mesh, r, None, dirs, 1)
+
+
+def segment_periodicity(mesh, ids, dirs):
+    """Distinct pairs (p, q), p <= q, of particles owning cells that face each
+    other across the periodic boundaries `dirs` (tracker.h:1290-1336)."""
+    dim = mesh.dim
+    n = [mesh.n[d] for d in range(dim)]
+    cells = np.asarray(ids).reshape(tuple(reversed(n)))  # (.., y, x)
+    out = set()
+    for d in dirs:
+        ax = dim - 1 - d
+        lo = np.take(cells, 0, axis=ax).ravel()
+        hi = np.take(cells, n[d] - 1, axis=ax).ravel()
+        for p, q in zip(lo, hi):
+            if p >= 0 and q >= 0:
+                out.add((int(min(p, q)), int(max(p, q))))
+    return sorted(out)

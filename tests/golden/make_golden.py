@@ -23,6 +23,11 @@ Sources (paths inside the hpsint project):
       grain-tracker segments (center, radius, max value) of the spherical
       representation; the mesh, the indicator field and the threshold are
       re-typed below from the .cc (lines cited), the segments are parsed
+  tests/grain_tracker_advection_periodic.{cc,mpirun=4.output}
+      grains and their segments at t = 0 on a periodic mesh (a particle cut
+      by the periodic boundary is one grain of two segments); the mesh, the
+      particles, the interface width and the threshold are re-typed from the
+      .cc, the segments are parsed
   tests/advection_mechanism_data.{cc,output}
       advection velocities (translation, rotation, total) of three grain
       segments at the cell barycenters of a 4 x 4 mesh; mt and mr are re-typed
@@ -87,6 +92,28 @@ def parse_tracker_segments(path, section):
         if on and m:
             segs.append([float(x) for x in m.groups()])
     return segs
+
+
+def parse_tracker_grains(path, time_header):
+    """Grains printed after `time_header`: [{"op": k, "segments": [[cx, cy,
+    radius, max value], ...]}, ...] in the printed order."""
+    grains, on = [], False
+    for line in open(path).read().splitlines():
+        if line.startswith("Time t = "):
+            if on:
+                break
+            on = line.strip() == time_header
+            continue
+        if not on:
+            continue
+        m = re.match(r"^op_index_current = (\d+) \| op_index_old = \d+ \| segments = (\d+)$", line)
+        if m:
+            grains.append({"op": int(m.group(1)), "segments": []})
+            continue
+        m = re.match(r"^\s+segment: center = (\S+) (\S+) \| radius = (\S+) \| max_value = (\S+)$", line)
+        if m:
+            grains[-1]["segments"].append([float(x) for x in m.groups()])
+    return grains
 
 
 def parse_advection(path):
@@ -176,6 +203,25 @@ def main(ref):
         # [center x, center y, radius, max value], in the order printed
         "segments": parse_tracker_segments(os.path.join(t, "grain_tracker_elliptical.mpirun=4.output"),
                                            "Spherical grain representation"),
+        "digits": 6,
+    }
+    # grain_tracker_advection_periodic.cc:111-127 ([0, 60] x [0, 22.5], 26 x 10
+    # subdivisions, 3 global refinements -> 208 x 80 cells, periodic in x and
+    # y, interface width 2), :161-166 (five particles of radius 7.5 on
+    # y = 11.25; the ones at x = 0 and x = 60 are one particle across the
+    # periodic boundary), :201 (threshold_lower); profile of
+    # initial_values_spherical.h:51-75 (1 inside R - w/2, (1 + cos(pi (r - R +
+    # w/2) / w)) / 2 across the interface, 0 outside); order parameters as
+    # printed (particles at 0, 30, 60 on op 0, at 15, 45 on op 1)
+    golden["grain_tracker_periodic"] = {
+        "mesh": {"dim": 2, "cells": [208, 80], "lower": [0.0, 0.0], "upper": [60.0, 22.5]},
+        "periodic": [0, 1],
+        "particles": [[0.0, 11.25, 7.5, 0], [15.0, 11.25, 7.5, 1], [30.0, 11.25, 7.5, 0], [45.0, 11.25, 7.5, 1],
+                      [60.0, 11.25, 7.5, 0]],
+        "interface_width": 2.0,
+        "threshold_lower": 1e-15,
+        "grains": parse_tracker_grains(os.path.join(t, "grain_tracker_advection_periodic.mpirun=4.output"),
+                                       "Time t = 0"),
         "digits": 6,
     }
     # advection_mechanism_data.cc:38-46 (2D, [0, 1]^2, 2 global refinements

@@ -177,3 +177,54 @@ def max_speed(dim, cells, h, origin, seg, data, mask=None):
             if v.size:
                 vmax = max(vmax, float(np.sqrt((v ** 2).sum(axis=1)).max()))
     return vmax
+
+
+def tracker_periodic_golden_fields(g):
+    """Nodal fields of the order parameters of the grain_tracker_advection_periodic
+    golden: cosine-interface discs (1 inside R - w/2, (1 + cos(pi (r - R + w/2)
+    / w)) / 2 across the interface of width w, 0 outside), the largest over the
+    particles of each order parameter.  Returns dim, cells, h, origin, fields."""
+    mesh = g["mesh"]
+    cells = mesh["cells"]
+    h = [(mesh["upper"][d] - mesh["lower"][d]) / cells[d] for d in range(2)]
+    X, Y = np.meshgrid(mesh["lower"][0] + np.arange(cells[0] + 1) * h[0],
+                       mesh["lower"][1] + np.arange(cells[1] + 1) * h[1])
+    w = g["interface_width"]
+    n_ops = 1 + max(p[3] for p in g["particles"])
+    fields = [np.zeros_like(X) for _ in range(n_ops)]
+    for cx, cy, R, op in g["particles"]:
+        r = np.hypot(X - cx, Y - cy)
+        v = np.where(r <= R - w / 2, 1.0, np.where(r < R + w / 2, (1 + np.cos((r - R + w / 2) / w * np.pi)) / 2, 0.0))
+        fields[op] = np.maximum(fields[op], v)
+    return 2, cells, h, mesh["lower"], [f.ravel() for f in fields]
+
+
+def group_grains(op_index, props, groups, dim=2):
+    """Grains of one order parameter: periodic groups become one grain of
+    several segments, the other particles one grain each.  props rows:
+    measure, center[dim], radius, max value.  Returns [(op, sorted segments
+    [center..., radius, max])]."""
+    seg = [list(p[1:1 + dim]) + [p[1 + dim], p[2 + dim]] for p in props]
+    by_group, grains = {}, []
+    for i, gid in enumerate(groups):
+        if gid < 0:
+            grains.append((op_index, [seg[i]]))
+        else:
+            by_group.setdefault(gid, []).append(seg[i])
+    grains += [(op_index, sorted(v)) for v in by_group.values()]
+    return grains
+
+
+def grains_agree(ours, ref, digits):
+    """Same multiset of (op, segments) to `digits` significant digits."""
+    key = lambda gr: (gr[0], len(gr[1]), gr[1][0][0], gr[1][0][1])  # noqa: E731
+    ours, ref = sorted(ours, key=key), sorted(ref, key=key)
+    if len(ours) != len(ref):
+        return False
+    rtol = 0.5 * 10.0 ** (1 - digits)
+    for (oa, sa), (ob, sb) in zip(ours, ref):
+        if oa != ob or len(sa) != len(sb):
+            return False
+        if not all(np.allclose(x, y, rtol=rtol, atol=0) for x, y in zip(sa, sb)):
+            return False
+    return True

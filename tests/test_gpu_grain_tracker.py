@@ -103,3 +103,41 @@ def test_labels_are_deterministic():
     assert a.n_particles == b.n_particles
     assert torch.equal(a.ids, b.ids)
     assert np.array_equal(a.radii, b.radii) and np.array_equal(a.centers, b.centers)
+
+
+def test_periodic_golden_grains(goldens):
+    """grain_tracker_advection_periodic golden (t = 0) through the device
+    labelling and pairing: a grain of two segments across the x boundary."""
+    from hpsint_b200 import grain_tracker as GT
+    from helpers import group_grains, grains_agree, tracker_periodic_golden_fields
+    g = goldens["grain_tracker_periodic"]
+    dim, cells, h, origin, fields = tracker_periodic_golden_fields(g)
+    op = _op(dim, cells, tuple(h) + (1.0,), tuple(origin) + (0.0,))
+    op.set_periodicity(g["periodic"])
+    grains = []
+    for b, eta in enumerate(fields):
+        parts = _detect(op, eta, g["threshold_lower"])
+        props = np.column_stack([parts.measures, parts.centers, parts.radii, parts.max_values])
+        groups, _ = GT.particle_groups(parts.n_particles, GT.periodicity(op, parts))
+        grains += group_grains(b, props, groups)
+    ref = [(gr["op"], sorted(gr["segments"])) for gr in g["grains"]]
+    assert grains_agree(grains, ref, g["digits"]), (grains, ref)
+
+
+@pytest.mark.parametrize("dim,cells,dirs", [(2, (61, 47), (0, 1)), (3, (29, 23, 17), (0, 2)), (3, (20, 18, 16), (1,))])
+def test_periodicity_pairs_match_oracle(dim, cells, dirs):
+    from hpsint_b200 import grain_tracker as GT
+    # ragged noise particles, many of them cut by the periodic boundaries
+    rng = np.random.default_rng(92)
+    N = int(np.prod([c + 1 for c in cells]))
+    op = _op(dim, cells)
+    op.set_periodicity(dirs)
+    om = O.make_mesh(dim, list(cells) + [0] * (3 - len(cells)), (1.0, 1.0, 1.0))
+    n_pairs = 0
+    for b in range(3):
+        parts = _detect(op, rng.uniform(0, 1, N) ** 6, 0.6)
+        ids = parts.ids.cpu().numpy()
+        ref = O.segment_periodicity(om, ids, dirs)
+        assert GT.periodicity(op, parts) == ref
+        n_pairs += len(ref)
+    assert n_pairs > 0  # the packing reaches the periodic boundaries

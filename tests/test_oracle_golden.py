@@ -149,3 +149,24 @@ def test_grain_tracker_segments_match_hpsint_golden(goldens):
         assert np.allclose(a, b, rtol=rtol, atol=0), (a, b)
     # every cell of a particle is face-connected to it and above the threshold
     assert set(np.unique(ids)) == {-1, 0, 1}
+
+
+def test_periodic_grain_tracker_matches_hpsint_golden(goldens):
+    """grain_tracker_advection_periodic.cc at t = 0: on the periodic mesh the
+    particle cut by the x boundary is two particles (no flood across the
+    boundary), paired through periodicity (tracker.h:1290-1353) into one grain
+    of two segments; all centers, radii and maxima to the printed digits."""
+    from hpsint_b200.grain_tracker import particle_groups
+    from helpers import group_grains, grains_agree, tracker_periodic_golden_fields
+    g = goldens["grain_tracker_periodic"]
+    dim, cells, h, origin, fields = tracker_periodic_golden_fields(g)
+    mesh = O.make_mesh(dim, list(cells) + [0], list(h) + [1.0])
+    grains = []
+    for op, eta in enumerate(fields):
+        ids, n = O.grain_segments(mesh, eta, g["threshold_lower"])
+        props = O.segment_properties(mesh, eta, ids, n, list(origin) + [0.0])
+        pairs = O.segment_periodicity(mesh, ids, g["periodic"])
+        groups, _ = particle_groups(n, pairs)
+        grains += group_grains(op, props, groups)
+    ref = [(gr["op"], sorted(gr["segments"])) for gr in g["grains"]]
+    assert grains_agree(grains, ref, g["digits"]), (grains, ref)
