@@ -13,6 +13,11 @@ Sources (paths inside the hpsint project):
       from lines 64-72 and 78-98 and cited, not parsed)
   applications/sintering/include/pf-applications/sintering/initial_values_debug.h:39-65
       nodal state of the 2D debug case
+  tests/residual_generic_{scalar,tensorial}_rbm.mpirun=1.output
+      the same residuals with the advection mechanism (rigid-body motion):
+      tests/include/pf-applications/tests/sintering_model.h:74-76 (mt, mr),
+      :119 (tracker threshold_lower), :214-217 (k, cgb, ceq, smoothening)
+      are re-typed below, the residuals parsed
   tests/free_energy_sintering.{cc,output}
       known-answer values of the Wang free energy and its derivatives
   tests/power_sum.{cc,output}
@@ -171,6 +176,14 @@ def main(ref):
         "residual_tensorial": parse_residual(
             os.path.join(t, "residual_generic_tensorial_no_rbm.mpirun=1.output")),
         "residual_digits": 4,
+        "residual_scalar_rbm": parse_residual(
+            os.path.join(t, "residual_generic_scalar_rbm.mpirun=1.output")),
+        "residual_tensorial_rbm": parse_residual(
+            os.path.join(t, "residual_generic_tensorial_rbm.mpirun=1.output")),
+        # sintering_model.h:74-76, :119, :214-217; segments are the tracker's
+        # particles of each order parameter (threshold 1e-15)
+        "rbm": {"k": 25.0, "cgb": 0.0, "ceq": 1.0, "smoothening": 0.0, "mt": 1.0, "mr": 1.0,
+                "threshold_lower": 1e-15},
         # free_energy_sintering.cc: FreeEnergy(A=2, B=3), c=0.95, mu=0, etas
         "free_energy_kat": {
             "A": 2.0, "B": 3.0, "c": 0.95, "mu": 0.0,

@@ -471,3 +471,34 @@ def test_time_loop_halves_dt_on_courant_violation():
     ti.step()
     courant = [f for f in ti.failures if f[2] == -1]
     assert courant and ti.records[-1].dt <= 2.0
+
+
+def test_rbm_golden_residual_on_gpu(goldens):
+    """hpsint's residual_generic_*_rbm goldens through the device path: device
+    tracker segments, device forces and velocities, advection kernels."""
+    import hpsint_b200 as hb
+    from hpsint_b200 import grain_tracker as GT
+    from test_oracle_golden import agrees_to_digits, debug_case, rbm_segments
+    a = goldens["rbm"]
+    for tens, key in [(False, "residual_scalar_rbm"), (True, "residual_tensorial_rbm")]:
+        mesh_o, P, T, u, perm = debug_case(goldens, tens)
+        m = goldens["model"]
+        op = hb.SinteringOperatorGeneric(
+            hb.Mesh(2, (2, 1, 1)),
+            hb.Params(2, m["A"], m["B"], m["kappa_c"], m["kappa_p"], m["Mvol"], m["Mvap"], m["Msurf"], m["Mgb"],
+                      m["L"], tens))
+        w0 = 1.0 / m["bdf1_dt"]
+        op.set_time_weights(w0, [-w0], 1.0)
+        ud = op.to_device(u)
+        seg, centers, owners = GT.advection_segments(op, ud, a["threshold_lower"])
+        op.set_advection_mechanism(seg, centers, a["k"], a["cgb"], a["ceq"], a["smoothening"], a["mt"], a["mr"])
+        dst = op.initialize_dof_vector()
+        op.evaluate_nonlinear_residual(dst, ud, 2, [ud.clone()])
+        ours = op.to_host(dst)
+        seg_o, cen_o = rbm_segments(mesh_o, u, a["threshold_lower"])
+        assert np.array_equal(seg.cpu().numpy(), seg_o)
+        vft = O.advection_forces(mesh_o, P, u, seg_o, cen_o, (0, 0, 0), a["k"], a["cgb"], a["ceq"], a["smoothening"])
+        table = O.advection_velocities(2, vft, cen_o, a["mt"], a["mr"])
+        ref = O.residual(mesh_o, P, T, u, [u.copy()], 2, advection=(seg_o, table, (0, 0, 0)))
+        assert np.max(np.abs(ours - ref)) < 1e-9  # the BDF1 term cancels (w0 = 1e5): absolute bound
+        assert agrees_to_digits(ours[:, perm], np.array(goldens[key]), goldens["residual_digits"])

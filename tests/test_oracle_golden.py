@@ -170,3 +170,39 @@ def test_periodic_grain_tracker_matches_hpsint_golden(goldens):
         grains += group_grains(op, props, groups)
     ref = [(gr["op"], sorted(gr["segments"])) for gr in g["grains"]]
     assert grains_agree(grains, ref, g["digits"]), (grains, ref)
+
+
+def rbm_segments(mesh, u, thr):
+    """The tracker's particles of each order parameter as advection segments:
+    (cell_segments, centers), as the reference's sintering model sets them up
+    (sintering_model.h:119, :230)."""
+    G = u.shape[0] - 2
+    n_cells = int(np.prod([mesh.n[d] for d in range(mesh.dim)]))
+    seg = np.full((G, n_cells), -1, dtype=np.int32)
+    centers, base = [], 0
+    for b in range(G):
+        ids, n = O.grain_segments(mesh, u[2 + b], thr)
+        props = O.segment_properties(mesh, u[2 + b], ids, n, (0.0, 0.0, 0.0))
+        seg[b] = np.where(ids >= 0, ids + base, -1)
+        for p in props:
+            centers.append(list(p[1:1 + mesh.dim]) + [0.0] * (3 - mesh.dim))
+        base += n
+    return seg, np.array(centers)
+
+
+@pytest.mark.parametrize("tensorial,key", [(False, "residual_scalar_rbm"), (True, "residual_tensorial_rbm")])
+def test_rbm_residual_matches_hpsint_golden(goldens, tensorial, key):
+    """residual_generic_{scalar,tensorial}_rbm: the advection mechanism end to
+    end (tracker segments, forces, velocities, advection terms) reproduces
+    hpsint's residual to the printed digits."""
+    mesh, P, T, u, perm = debug_case(goldens, tensorial)
+    a = goldens["rbm"]
+    seg, centers = rbm_segments(mesh, u, a["threshold_lower"])
+    vft = O.advection_forces(mesh, P, u, seg, centers, (0, 0, 0), a["k"], a["cgb"], a["ceq"], a["smoothening"])
+    table = O.advection_velocities(2, vft, centers, a["mt"], a["mr"])
+    r = O.residual(mesh, P, T, u, [u.copy()], 2, advection=(seg, table, (0, 0, 0)))
+    gold = np.array(goldens[key])
+    assert agrees_to_digits(r[:, perm], gold, goldens["residual_digits"]), (r[:, perm], gold)
+    # the rigid-body motion changed the eta rows (against the no_rbm golden)
+    plain = np.array(goldens[key.replace("_rbm", "")])
+    assert not agrees_to_digits(plain, gold, goldens["residual_digits"])
