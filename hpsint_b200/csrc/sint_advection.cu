@@ -592,7 +592,7 @@ int sint_set_advection_mechanism(sint_ctx *c, const int32_t *cell_segments, cons
   if (S > 0)
     {
       long long nb = (n_items + 8191) / 8192;
-      nb           = nb < 1 ? 1 : (nb > 1024 ? 1024 : nb);
+      nb           = nb < 1 ? 1 : (nb > 4096 ? 4096 : nb);
       while (nb > 1 && nb * S > ADV_HIST)
         nb /= 2;
       const long long range = (n_items + nb - 1) / nb;

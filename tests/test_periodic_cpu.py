@@ -96,3 +96,29 @@ def test_slaves_are_ignored_on_input():
     a, b = O.periodic_jvp(om, p, T, u, src, dirs), O.periodic_jvp(om, p, T, u, src2, dirs)
     keep = np.setdiff1d(np.arange(u.shape[1]), sl)
     assert np.array_equal(a[:, keep], b[:, keep]) and np.all(b[:, sl] == 7.0)
+
+
+def test_particle_groups():
+    """PeriodicityGraph::build_groups (periodicity_graph.h:57-80): particles
+    connected through periodicity pairs form one group; particles outside
+    the graph have none."""
+    from hpsint_b200.grain_tracker import particle_groups
+    ids, n = particle_groups(6, [(0, 4), (4, 5), (2, 2)])
+    assert n == 2 and ids == [0, -1, 1, -1, 0, 0]
+    assert particle_groups(3, []) == ([-1, -1, -1], 0)
+    # order of the pairs does not matter
+    a = particle_groups(8, [(6, 7), (1, 3), (3, 6), (2, 5)])
+    b = particle_groups(8, [(2, 5), (3, 6), (6, 7), (1, 3)])
+    assert a == b == ([-1, 0, 1, 0, -1, 1, 0, 0], 2)
+
+
+def test_segment_periodicity_pairs():
+    """Pairs of particles owning cells that face each other across a periodic
+    boundary (tracker.h:1290-1336), in increasing order, without repeats."""
+    mesh = O.make_mesh(2, [4, 3, 0])
+    ids = np.array([[0, -1, -1, 1],
+                    [0, -1, 2, 2],
+                    [-1, -1, -1, 3]]).ravel()  # rows = y, x fastest
+    assert O.segment_periodicity(mesh, ids, (0,)) == [(0, 1), (0, 2)]
+    assert O.segment_periodicity(mesh, ids, (1,)) == [(1, 3)]
+    assert O.segment_periodicity(mesh, ids, (0, 1)) == [(0, 1), (0, 2), (1, 3)]
