@@ -170,13 +170,23 @@ namespace sint
       }
   }
 
+  // Nodal values of cell (i, j, k); on a periodic mesh the slaves read
+  // their masters, as the operator does (iterates of a Newton solve keep
+  // stale slave entries until the solution is distributed).
   template <int DIM>
   __device__ __forceinline__ void adv_nodes(const double *__restrict__ u, const Grid &g, int i, int j, int k,
                                             double (&out)[1 << DIM])
   {
 #pragma unroll
     for (int l = 0; l < (1 << DIM); ++l)
-      out[l] = u[node_index(g, i + (l & 1), j + ((l >> 1) & 1), DIM == 3 ? k + ((l >> 2) & 1) : 0)];
+      {
+        int n[3] = {i + (l & 1), j + ((l >> 1) & 1), DIM == 3 ? k + ((l >> 2) & 1) : 0};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          if (((g.periodic >> d) & 1) && n[d] == g.n[d])
+            n[d] = 0;
+        out[l] = u[node_index(g, n[0], n[1], n[2])];
+      }
   }
 
   struct AdvForceParams

@@ -171,3 +171,23 @@ def test_distribute_constraints():
     op.distribute_constraints(ud)
     torch.cuda.synchronize()
     assert np.array_equal(op.to_host(ud), O.periodic_resolve(om, u, dirs))
+
+
+def test_advection_forces_read_periodic_masters():
+    """The force evaluation reads the periodic masters as the operator does,
+    so stale slave entries of an iterate do not enter the velocities."""
+    from helpers import advection_data
+    dim, cells, G, dirs = 2, (37, 21), 3, (0, 1)
+    op, p, om = make_op(dim, cells, G, True, dirs)
+    u = distributed(om, particle_state(dim, cells, G, seed=87), dirs)
+    sl, ma = O.periodic_pairs(om, dirs)
+    stale = u.copy()
+    stale[:, sl] += 0.3
+    seg, data = advection_data(dim, cells, G, seed=88)
+    centers = np.ascontiguousarray(data[:, 6:9])
+    op.set_advection_mechanism(torch.from_numpy(seg).cuda(), torch.from_numpy(centers).cuda(), k=2.5, cgb=0.0,
+                               ceq=0.9, smoothening=0.0, mt=1.0, mr=1.0)
+    vft = op.advection_forces(op.to_device(stale)).cpu().numpy()
+    ref = O.advection_forces(om, p, u, seg, centers, (0.0, 0.0, 0.0), 2.5, 0.0, 0.9, 0.0)
+    scale = np.abs(ref).max(axis=0, keepdims=True)
+    assert np.all(np.abs(vft - ref) <= 1e-12 * scale + 1e-300)
