@@ -37,7 +37,13 @@ namespace sint
     const int nl = g.dim == 3 ? 8 : 4;
     long long node[8];
     for (int l = 0; l < nl; ++l)
-      node[l] = node_index(g, i + (l & 1), j + ((l >> 1) & 1), k + ((l >> 2) & 1));
+      {
+        int n[3] = {i + (l & 1), j + ((l >> 1) & 1), k + ((l >> 2) & 1)};
+        for (int d = 0; d < 3; ++d)
+          if (((g.periodic >> d) & 1) && n[d] == g.n[d])
+            n[d] = 0; // a slave reads its periodic master, as the operator does
+        node[l] = node_index(g, n[0], n[1], n[2]);
+      }
     unsigned bits = 0;
     for (int b = 0; b < G; ++b)
       {
@@ -140,13 +146,28 @@ namespace sint
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= g.N)
       return;
-    const int i = int(n % g.nn[0]), j = int((n / g.nn[0]) % g.nn[1]), k = int(n / ((long long)g.nn[0] * g.nn[1]));
-    unsigned  u = 0;
-    for (int ck = k - 1; ck <= k; ++ck)
-      for (int cj = j - 1; cj <= j; ++cj)
-        for (int ci = i - 1; ci <= i; ++ci)
-          if (ci >= 0 && ci < g.n[0] && cj >= 0 && cj < g.n[1] && ck >= 0 && ck < g.n[2])
-            u |= cell_mask[ci + (long long)g.n[0] * (cj + (long long)g.n[1] * ck)];
+    const int co[3] = {int(n % g.nn[0]), int((n / g.nn[0]) % g.nn[1]), int(n / ((long long)g.nn[0] * g.nn[1]))};
+    // the cells around the node; across a periodic boundary a master node
+    // and its slaves share the cells of both sides (the slave rows are added
+    // to the master rows), so both get the same set
+    int cells[3][2];
+    for (int d = 0; d < 3; ++d)
+      for (int o = 0; o < 2; ++o)
+        {
+          int c = co[d] - 1 + o;
+          if ((g.periodic >> d) & 1)
+            c = c < 0 ? g.n[d] - 1 : (c >= g.n[d] ? 0 : c);
+          cells[d][o] = (c >= 0 && c < g.n[d]) ? c : -1;
+        }
+    unsigned u = 0;
+    for (int ok = 0; ok < 2; ++ok)
+      for (int oj = 0; oj < 2; ++oj)
+        for (int oi = 0; oi < 2; ++oi)
+          {
+            const int ci = cells[0][oi], cj = cells[1][oj], ck = cells[2][ok];
+            if (ci >= 0 && cj >= 0 && ck >= 0)
+              u |= cell_mask[ci + (long long)g.n[0] * (cj + (long long)g.n[1] * ck)];
+          }
     node_mask[n] = (uint16_t)u;
   }
 
