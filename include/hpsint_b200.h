@@ -282,8 +282,9 @@ int sint_grain_segment_periodicity(sint_ctx *ctx, const int *particle_ids, int *
  * read the masters' values there, add the slave rows to the master rows,
  * and give the slave rows zero (residual) or the identity (J v,
  * preconditioner).  sint_newton_solve distributes the solution at the end.
- * 0 switches periodicity off.  The grain tracker and the grain cut-off's
- * masks read the nodal values as they are: pass distributed vectors. */
+ * 0 switches periodicity off.  The grain cut-off's masks and the advection
+ * forces read the masters too; the grain tracker reads the nodal values as
+ * they are (pass distributed vectors, as hpsint's tracker gets). */
 int sint_set_periodicity(sint_ctx *ctx, unsigned directions);
 
 /* AffineConstraints::distribute: every slave entry of u (all components)
