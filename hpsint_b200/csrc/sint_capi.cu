@@ -25,13 +25,14 @@ namespace sint
 
   void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
-  size_t smem_diag(int dim, int G)
+  size_t smem_diag(int dim, int G, bool adv)
   {
     const int C = G + 2;
-    // NCOEF = 2 dim^2 + dim + 1 + G coefficients per point, NOUT = G + 4 outputs
+    // NCOEF = 2 dim^2 + dim + 1 + G (+ G dim velocities) coefficients per point, NOUT = G + 4 outputs
+    const int nadv = adv ? G * dim : 0;
     if (dim == 3)
-      return (C * Tile<3>::BOX + (22 + G) * Tile<3>::THREADS + (G + 4) * Tile<3>::CS) * sizeof(double);
-    return (C * Tile<2>::BOX + (11 + G) * Tile<2>::THREADS + (G + 4) * Tile<2>::CS) * sizeof(double);
+      return (C * Tile<3>::BOX + (22 + G + nadv) * Tile<3>::THREADS + (G + 4) * Tile<3>::CS) * sizeof(double);
+    return (C * Tile<2>::BOX + (11 + G + nadv) * Tile<2>::THREADS + (G + 4) * Tile<2>::CS) * sizeof(double);
   }
 
   template <int DIM, typename R>
@@ -106,12 +107,14 @@ namespace sint
   {
     const bool t = c->params.tensorial != 0;
     cudaError_t e;
+    const uint16_t *m   = preconditioner_mask(c);
+    const AdvData  *adv = active_adv(c);
     if (c->grid.dim == 3)
-      e = t ? launch_diag<3, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s)
-            : launch_diag<3, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s);
+      e = t ? launch_diag<3, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, m, adv, s)
+            : launch_diag<3, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, m, adv, s);
     else
-      e = t ? launch_diag<2, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s)
-            : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, preconditioner_mask(c), s);
+      e = t ? launch_diag<2, true>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, m, adv, s)
+            : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, m, adv, s);
     if (e != cudaSuccess)
       return e;
     e = c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s)

@@ -4,5 +4,5 @@
 namespace sint
 {
   template cudaError_t launch_diag<2, false>(int, const Grid &, const Phys &, const double *, double *, double *,
-                                            const uint16_t *, cudaStream_t);
+                                            const uint16_t *, const AdvData *, cudaStream_t);
 } // namespace sint

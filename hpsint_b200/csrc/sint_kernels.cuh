@@ -815,23 +815,28 @@ namespace sint
   // Each thread first computes its point's coefficients (mobility matrix M,
   // dM/dc grad mu, dM/dgrad c, f_cc, f_eta_i eta_i), then, as the owner of
   // local node l, sums phi_l / grad phi_l weighted terms over the cell's points.
-  template <int DIM, int G, bool TENS>
+  template <int DIM, int G, bool TENS, bool ADV = false>
   struct DiagLayout
   {
     static constexpr int NOUT  = G + 4;
-    static constexpr int NCOEF = DIM * DIM + DIM + DIM * DIM + 1 + G;
+    static constexpr int NADV  = ADV ? G * DIM : 0; // the grains' velocities at the point
+    static constexpr int NCOEF = DIM * DIM + DIM + DIM * DIM + 1 + G + NADV;
   };
 
   // CUT: the grains absent on a cell (mask bit clear) have zero values there
   // and no Allen-Cahn diagonal contribution from it (preconditioners.h:787-817).
-  template <int DIM, int G, bool TENS, bool CUT>
+  // ADV: the advection terms of the preconditioner's operators
+  // (precondition_advection_ch / _ac, operator_sintering_generic.h:800-850):
+  // J_cc gains -(phi_l sum_i v_i, grad phi_l) and grain i's diagonal
+  // -(phi_l v_i, grad phi_l), with the velocities of the current table.
+  template <int DIM, int G, bool TENS, bool CUT, bool ADV = false>
   __global__ void __launch_bounds__(Tile<DIM>::THREADS)
     diag_kernel(const Grid g, const Phys ph, const double *__restrict__ lin, double *__restrict__ dst,
-                double *__restrict__ partial, const uint16_t *__restrict__ mask)
+                double *__restrict__ partial, const uint16_t *__restrict__ mask, const AdvData adv)
   {
     using R          = double;
     using T          = Tile<DIM>;
-    using LY         = DiagLayout<DIM, G, TENS>;
+    using LY         = DiagLayout<DIM, G, TENS, ADV>;
     constexpr int C  = G + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *s_lin  = reinterpret_cast<R *>(smem_raw);
@@ -908,6 +913,43 @@ namespace sint
           cf[2 * DIM * DIM + DIM + 1 + i] =
             p.B * (R(12) - R(12) * c + R(2) * e * (R(12) * c - R(24)) + R(24) * (e * e) + R(12) * s2);
         }
+      if constexpr (ADV)
+        {
+          // velocity of every grain at this thread's point (zero without a segment)
+          R        *vc = cf + 2 * DIM * DIM + DIM + 1 + G;
+          int       cc[3];
+          const int q  = threadIdx.x & (T::NQ - 1);
+          const bool in = cell_global<DIM>(cell, tc, g, cc);
+          const long long n_cells = (long long)g.n[0] * g.n[1] * g.n[2];
+          const long long lin_cell = cc[0] + (long long)g.n[0] * (cc[1] + (long long)g.n[1] * cc[2]);
+          const double gp0 = 0.5 - 0.5 / sqrt(3.0), gp1 = 0.5 + 0.5 / sqrt(3.0);
+#pragma unroll 1
+          for (int i = 0; i < G; ++i)
+            {
+              int s = -1;
+              if (in && (!CUT || ((gmask >> i) & 1u)))
+                {
+                  s = adv.cell_segments[i * n_cells + lin_cell];
+                  if (s >= adv.n_segments)
+                    s = -1;
+                }
+              R v[3] = {R(0), R(0), R(0)};
+              if (s >= 0)
+                {
+                  const double *d    = adv.segments + 9 * (long long)s;
+                  double        r[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                  for (int e = 0; e < DIM; ++e)
+                    r[e] = adv.origin[e] + (cc[e] + (((q >> e) & 1) ? gp1 : gp0)) * g.h[e] - d[6 + e];
+                  v[0] = d[0] + d[4] * r[2] - d[5] * r[1];
+                  v[1] = d[1] + d[5] * r[0] - d[3] * r[2];
+                  v[2] = d[2] + d[3] * r[1] - d[4] * r[0];
+                }
+#pragma unroll
+              for (int e = 0; e < DIM; ++e)
+                vc[i * DIM + e] = v[e];
+            }
+        }
     }
     __syncthreads();
 
@@ -964,6 +1006,20 @@ namespace sint
 #pragma unroll
           for (int i = 0; i < G; ++i)
             acc[4 + i] += w.JxW * ((p.w0 + p.L * cf[2 * DIM * DIM + DIM + 1 + i]) * pp + p.L * p.kp * gg);
+          if constexpr (ADV)
+            {
+              const R *vc = cf + 2 * DIM * DIM + DIM + 1 + G;
+#pragma unroll
+              for (int i = 0; i < G; ++i)
+                {
+                  R vd = R(0);
+#pragma unroll
+                  for (int e = 0; e < DIM; ++e)
+                    vd += vc[i * DIM + e] * dphi[e];
+                  acc[0] -= w.JxW * phi * vd;
+                  acc[4 + i] -= w.JxW * phi * vd;
+                }
+            }
         }
 #pragma unroll
       for (int i = 0; i < G; ++i)

@@ -12,8 +12,9 @@
 
 namespace sint
 {
-  // Dynamic shared memory of the diagonal kernel (bytes).
-  size_t smem_diag(int dim, int G);
+  // Dynamic shared memory of the diagonal kernel (bytes); adv: with the
+  // grains' velocities per point.
+  size_t smem_diag(int dim, int G, bool adv = false);
 
   // cut: the grain cut-off's tile classes, nullptr for the full operator;
   // adv: the grains' rigid-body velocities, nullptr for no advection
@@ -36,10 +37,16 @@ namespace sint
                                   const double *const *hist, double *dst, double *partial, const CutTiles *cut,
                                   const AdvData &adv, cudaStream_t s);
 
-  // mask: the cut-off's per-cell grain masks, nullptr for the full operator
+  // mask: the cut-off's per-cell grain masks, nullptr for the full operator;
+  // adv: the advection velocities, nullptr for none
   template <int DIM, bool TENS>
   cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
-                          const uint16_t *mask, cudaStream_t s);
+                          const uint16_t *mask, const AdvData *adv, cudaStream_t s);
+
+  // The same with the advection terms (instantiated in sint_inst_adv_diag_*.cu).
+  template <int DIM, bool TENS>
+  cudaError_t launch_diag_adv(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
+                              const uint16_t *mask, const AdvData &adv, cudaStream_t s);
 
   // tile_mask: per tile id, the grains whose partials the tile wrote (grain
   // cut-off); nullptr = every component of every tile

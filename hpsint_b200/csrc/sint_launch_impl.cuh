@@ -82,16 +82,16 @@ namespace sint
     return cudaGetLastError();
   }
 
-  template <int DIM, int G, bool TENS, bool CUT>
+  template <int DIM, int G, bool TENS, bool CUT, bool ADV>
   cudaError_t launch_diag_g(const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
-                            const uint16_t *mask, cudaStream_t s)
+                            const uint16_t *mask, const AdvData &adv, cudaStream_t s)
   {
-    const size_t smem = smem_diag(DIM, G);
-    auto         k    = diag_kernel<DIM, G, TENS, CUT>;
+    const size_t smem = smem_diag(DIM, G, ADV);
+    auto         k    = diag_kernel<DIM, G, TENS, CUT, ADV>;
     cudaError_t  e    = prepare_smem(k, smem);
     if (e != cudaSuccess)
       return e;
-    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, dst, partial, mask);
+    k<<<dim3((unsigned)g.n_tiles), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, dst, partial, mask, adv);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -231,18 +231,27 @@ namespace sint
     return launch_residual_impl<DIM, TENS, false>(G, wtd, g, p, src, hist, dst, partial, cut, AdvData(), s);
   }
 
-  template <int DIM, bool TENS>
-  cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
-                          const uint16_t *mask, cudaStream_t s)
+  template <int DIM, bool TENS, bool ADV>
+  cudaError_t launch_diag_impl(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
+                               const uint16_t *mask, const AdvData &adv, cudaStream_t s)
   {
     if (mask)
       {
-#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS, true>(g, p, lin, dst, partial, mask, s)
+#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS, true, ADV>(g, p, lin, dst, partial, mask, adv, s)
         SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
       }
-#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS, false>(g, p, lin, dst, partial, nullptr, s)
+#define SINT_CALL(GG) launch_diag_g<DIM, GG, TENS, false, ADV>(g, p, lin, dst, partial, nullptr, adv, s)
     SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
+  }
+
+  template <int DIM, bool TENS>
+  cudaError_t launch_diag(int G, const Grid &g, const Phys &p, const double *lin, double *dst, double *partial,
+                          const uint16_t *mask, const AdvData *adv, cudaStream_t s)
+  {
+    if (adv)
+      return launch_diag_adv<DIM, TENS>(G, g, p, lin, dst, partial, mask, *adv, s);
+    return launch_diag_impl<DIM, TENS, false>(G, g, p, lin, dst, partial, mask, AdvData(), s);
   }
 } // namespace sint

@@ -61,8 +61,10 @@ def lib():
                                       _c_int, U16, P(Advection), P(_c_double), _c_int]
         L.oracle_jvp.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), P(_c_double),
                                  U16, P(Advection), P(_c_double), _c_int]
-        L.oracle_ac_diagonal.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
-        L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(_c_double), _c_int]
+        L.oracle_ac_diagonal.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(Advection), P(_c_double),
+                                         _c_int]
+        L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(Advection), P(_c_double),
+                                       _c_int]
         L.oracle_grain_mask.argtypes = [P(Mesh), P(Params), P(_c_double), _c_double, U16]
         L.oracle_grain_segments.argtypes = [P(Mesh), P(_c_double), _c_double, P(_c_int), P(_c_int)]
         L.oracle_segment_properties.argtypes = [P(Mesh), P(_c_double), P(_c_double), P(_c_int), _c_int,
@@ -206,23 +208,25 @@ def jvp(mesh, params, time, lin, src, threads=0, mask=None, advection=None):
     return dst
 
 
-def ac_diagonal(mesh, params, time, lin, threads=0, mask=None):
+def ac_diagonal(mesh, params, time, lin, threads=0, mask=None, advection=None):
     C, N, G = params.n_grains + 2, n_nodes(mesh), params.n_grains
     lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
     d = np.zeros((G, N))
     keep, mp = _mptr(mask, mesh)
+    keep_a, ap = _adv(advection, mesh)
     _check(lib().oracle_ac_diagonal(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
-                                    mp, _dptr(d), threads or os.cpu_count()), "ac_diagonal")
+                                    mp, ap, _dptr(d), threads or os.cpu_count()), "ac_diagonal")
     return d
 
 
-def ch_blocks(mesh, params, time, lin, threads=0, mask=None):
+def ch_blocks(mesh, params, time, lin, threads=0, mask=None, advection=None):
     C, N = params.n_grains + 2, n_nodes(mesh)
     lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
     b = np.zeros((4, N))
     keep, mp = _mptr(mask, mesh)
+    keep_a, ap = _adv(advection, mesh)
     _check(lib().oracle_ch_blocks(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
-                                  mp, _dptr(b), threads or os.cpu_count()), "ch_blocks")
+                                  mp, ap, _dptr(b), threads or os.cpu_count()), "ch_blocks")
     return b
 
 

@@ -897,7 +897,7 @@ int oracle_jvp(const oracle_mesh *m, const oracle_params *p, const oracle_time *
 // coupling lands off the diagonal, so
 //   d_i(n) = sum_cells sum_q JxW [(w0 + L f_{eta_i eta_i}) phi_n^2 + L kappa_p |grad phi_n|^2].
 int oracle_ac_diagonal(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *lin,
-                       const uint16_t *mask, double *diag, int n_threads)
+                       const uint16_t *mask, const oracle_advection *adv, double *diag, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
@@ -929,7 +929,12 @@ int oracle_ac_diagonal(const oracle_mesh *m, const oracle_params *p, const oracl
               const double         phi = geo.shape[q][l];
               const V3             dphi{{geo.dshape[q][l][0], geo.dshape[q][l][1], geo.dshape[q][l][2]}};
               const double         vr  = phi * t->w0 + p->L * fe.d2f_detai2(lv[2 + ig]) * phi;
-              const V3             gr  = (p->L * p->kappa_p) * dphi;
+              V3                   gr  = (p->L * p->kappa_p) * dphi;
+              // precondition_advection_ac (operator_sintering_generic.h:826-850),
+              // each grain with its own velocity and its own trial function
+              V3 vel;
+              if (advection_velocity(adv, geo, blk[2 + ig] - 2, i, j, k, q, vel))
+                gr = gr - vel * phi;
               d += geo.JxW * (vr * phi + dot(gr, dphi));
             }
           diag[(blk[2 + ig] - 2) * N + geo.node(i, j, k, l)] += d;
@@ -943,7 +948,7 @@ int oracle_ac_diagonal(const oracle_mesh *m, const oracle_params *p, const oracl
 // restricted to (node n, node n):  blocks[0*N+n] = J_cc, [1*N+n] = J_c,mu,
 // [2*N+n] = J_mu,c, [3*N+n] = J_mu,mu  (row = tested equation, col = unknown).
 int oracle_ch_blocks(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *lin,
-                     const uint16_t *mask, double *blocks, int n_threads)
+                     const uint16_t *mask, const oracle_advection *adv, double *blocks, int n_threads)
 {
   if (int e = check_args(m, p))
     return e;
@@ -983,8 +988,15 @@ int oracle_ch_blocks(const oracle_mesh *m, const oracle_params *p, const oracle_
             {
               const double vr0 = phi * t->w0;
               const double vr1 = -fe.d2f_dc2() * phi;
-              const V3     gr0 = mul(mob.dM_dc(c, c_grad), mu_grad) * phi + mul(mob.dM_dgrad_c(c, c_grad, mu_grad), dphi);
+              V3 gr0 = mul(mob.dM_dc(c, c_grad), mu_grad) * phi + mul(mob.dM_dgrad_c(c, c_grad, mu_grad), dphi);
               const V3     gr1 = (-p->kappa_c) * dphi;
+              // precondition_advection_ch (operator_sintering_generic.h:800-824)
+              for (int ig = 0; ig < G; ++ig)
+                {
+                  V3 vel;
+                  if (advection_velocity(adv, geo, blk[2 + ig] - 2, i, j, k, q, vel))
+                    gr0 = gr0 - vel * phi;
+                }
               J[0] += geo.JxW * (vr0 * phi + dot(gr0, dphi));
               J[2] += geo.JxW * (vr1 * phi + dot(gr1, dphi));
             }

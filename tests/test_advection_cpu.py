@@ -283,3 +283,34 @@ def test_courant_check(dim, cells, G):
     assert dt_m >= dt_crit
     assert O.advection_courant(om, p, adv, dt_m * (1 - 1e-9), mask=mask)
     assert not O.advection_courant(om, p, adv, dt_m * (1 + 1e-9), mask=mask)
+
+
+@pytest.mark.parametrize("dim,cells,G", [(2, (7, 6), 3), (3, (4, 4, 3), 2)])
+def test_preconditioner_diagonals_with_advection(dim, cells, G):
+    """precondition_advection_ch / _ac (operator_sintering_generic.h:800-850):
+    the block preconditioner's diagonals gain the diagonal of the advection
+    terms, i.e. what J v with advection adds on the diagonal (probed with
+    nodes two apart, whose supports share no cell)."""
+    om, p = oracle_mesh(dim, cells), O.make_params(G, tensorial=True)
+    u = random_state(dim, cells, G, seed=41)
+    seg, data = advection_data(dim, cells, G, seed=42)
+    adv = (seg, data, (0.0, 0.0, 0.0))
+    T = O.make_time(10.0, 1.0, [-10.0])
+    C, N = G + 2, u.shape[1]
+    nn = [c + 1 for c in cells]
+    co = np.stack([(np.arange(N) // int(np.prod(nn[:d]))) % nn[d] for d in range(dim)])
+    colour = sum((co[d] % 2) << d for d in range(dim))
+    diag = np.zeros((C, N))
+    for comp in [0] + list(range(2, C)):
+        for col in range(1 << dim):
+            probe = np.zeros((C, N))
+            probe[comp, colour == col] = 1.0
+            d = O.jvp(om, p, T, u, probe, advection=adv) - O.jvp(om, p, T, u, probe)
+            diag[comp, colour == col] = d[comp, colour == col]
+    ch = O.ch_blocks(om, p, T, u, advection=adv) - O.ch_blocks(om, p, T, u)
+    ac = O.ac_diagonal(om, p, T, u, advection=adv) - O.ac_diagonal(om, p, T, u)
+    scale = np.abs(diag).max()
+    assert scale > 1e-3
+    assert np.allclose(ch[0], diag[0], atol=1e-12 * scale, rtol=0)
+    assert not ch[1:].any()  # the c-mu, mu-c and mu-mu entries do not change
+    assert np.allclose(ac, diag[2:], atol=1e-12 * scale, rtol=0)

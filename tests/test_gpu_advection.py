@@ -238,7 +238,9 @@ def test_newton_with_advection_matches_cpu_newton(prec):
 def test_graph_replayed_solve_reads_the_current_velocities(prec):
     """The second solve replays the GMRES graphs captured in the first one;
     new velocities in the same tables must give bitwise the result of a
-    fresh context."""
+    fresh context.  Both compared solves start with a cleared Newton history,
+    so both build the preconditioner (which carries the advection terms) from
+    the new velocities at their first iteration."""
     import hpsint_b200 as hb
     cells, G, dt = (40, 20), 2, 1e-2
     u_old = _two_particles(cells)
@@ -246,12 +248,15 @@ def test_graph_replayed_solve_reads_the_current_velocities(prec):
     data2 = data.copy()
     data2[0, 0], data2[1, 5] = -1.5, -0.4
 
-    def solve(op, d):
+    def solve(op, d, clear=False):
         set_adv(op, seg, d)
         old = op.to_device(u_old)
         u = old.clone()
-        st = hb.DampedNewtonSolver(op, hb.NonLinearData(nl_rel_tol=1e-9, nl_abs_tol=1e-16,
-                                                        inner_precision=prec)).solve(u, [old])
+        newton = hb.DampedNewtonSolver(op, hb.NonLinearData(nl_rel_tol=1e-9, nl_abs_tol=1e-16,
+                                                            inner_precision=prec))
+        if clear:
+            newton.clear()
+        st = newton.solve(u, [old])
         torch.cuda.synchronize()
         assert st.status == 0
         return u
@@ -264,10 +269,10 @@ def test_graph_replayed_solve_reads_the_current_velocities(prec):
     op = new_op()
     solve(op, data)
     solve(op, data)  # graphs captured by now
-    replayed = solve(op, data2)
+    replayed = solve(op, data2, clear=True)
     fresh_op = new_op()
     solve(fresh_op, data2)
-    fresh = solve(fresh_op, data2)
+    fresh = solve(fresh_op, data2, clear=True)
     assert torch.equal(replayed, fresh)
 
 
@@ -502,3 +507,36 @@ def test_rbm_golden_residual_on_gpu(goldens):
         ref = O.residual(mesh_o, P, T, u, [u.copy()], 2, advection=(seg_o, table, (0, 0, 0)))
         assert np.max(np.abs(ours - ref)) < 1e-9  # the BDF1 term cancels (w0 = 1e5): absolute bound
         assert agrees_to_digits(ours[:, perm], np.array(goldens[key]), goldens["residual_digits"])
+
+
+@pytest.mark.parametrize("case", [CASES[0], CASES[1], CASES[3], CASES[5]],
+                         ids=[ids(c) for c in (CASES[0], CASES[1], CASES[3], CASES[5])])
+def test_preconditioner_with_advection_matches_oracle(case):
+    """precondition_advection_ch / _ac: the block-Jacobi diagonals with the
+    advection terms, full operator and under the cut-off's preconditioner."""
+    import hpsint_b200 as hb
+    dim, cells, G, tens = case
+    op, p, om = make_op(dim, cells, G, tens)
+    u = particle_state(dim, cells, G, seed=93)
+    seg, data = advection_data(dim, cells, G, seed=94, scale=5.0)
+    set_adv(op, seg, data)
+    adv = (seg, data, ORIGIN)
+    ud = op.to_device(u)
+    op.set_time_weights(40.0, [-40.0], 1.0)
+    op.fill_quadrature_point_values(ud)
+    pc = hb.BlockPreconditioner2(op)
+    T = O.make_time(40.0, 1.0, [-40.0])
+    N = op.N
+    for cut in (False, True):
+        mask = None
+        if cut:
+            op.set_component_mask(ud, 1e-3)
+            op.set_preconditioner_cut_off(True)
+            mask = O.grain_mask(om, p, u, 1e-3)
+        pc.do_update()
+        ch = O.ch_blocks(om, p, T, u, mask=mask, advection=adv)
+        assert block_rel_err(pc.ch_blocks()[:, :N].cpu().numpy(), ch) <= 1e-12
+        inv = O.inverse_diagonal(O.ac_diagonal(om, p, T, u, mask=mask, advection=adv))
+        assert block_rel_err(pc.inverse_diagonal()[:, :N].cpu().numpy(), inv) <= 1e-12
+    # the terms are there: differ from the preconditioner without advection
+    assert block_rel_err(ch, O.ch_blocks(om, p, T, u, mask=mask)) > 1e-8
