@@ -140,6 +140,8 @@ int sint_set_periodicity(sint_ctx *c, unsigned directions)
         set_error("sint_set_periodicity: a periodic direction needs at least 2 cells");
         return SINT_ERR_ARG;
       }
+  if (c->grid.periodic != int(directions))
+    c->has_pc = false; // the preconditioner's diagonals change with the constraints
   c->grid.periodic = int(directions);
   return SINT_OK;
 }
