@@ -122,3 +122,32 @@ def test_segment_periodicity_pairs():
     assert O.segment_periodicity(mesh, ids, (0,)) == [(0, 1), (0, 2)]
     assert O.segment_periodicity(mesh, ids, (1,)) == [(1, 3)]
     assert O.segment_periodicity(mesh, ids, (0, 1)) == [(0, 1), (0, 2), (1, 3)]
+
+
+@pytest.mark.parametrize("dim,cells,G,dirs", [(2, (6, 5), 3, (0, 1)), (3, (4, 3, 3), 2, (0, 2))])
+def test_periodic_operator_with_translation(dim, cells, G, dirs):
+    """Periodic constraints and advection together: with translations only
+    (the velocity field is then periodic) the constrained operator with
+    advection equals the tiled operator with the same velocities."""
+    p = O.make_params(G, tensorial=True)
+    om = O.make_mesh(dim, list(cells) + [0] * (3 - dim))
+    u, uu = periodic_state(dim, cells, G, dirs, seed=11)
+    src, us = periodic_state(dim, cells, G, dirs, seed=12)
+    T = O.make_time(10.0, 1.0, [-10.0])
+    big, ub = tiled(dim, cells, dirs, uu)
+    _, sb = tiled(dim, cells, dirs, us)
+    bm = O.make_mesh(dim, list(big) + [0] * (3 - dim))
+    rng = np.random.default_rng(13)
+    data = np.zeros((G, 9))
+    data[:, :dim] = rng.normal(size=(G, dim))
+    seg = np.repeat(np.arange(G, dtype=np.int32)[:, None], int(np.prod(cells)), axis=1)
+    seg_b = np.repeat(np.arange(G, dtype=np.int32)[:, None], int(np.prod(big)), axis=1)
+    rows, orig = middle_rows(dim, cells, dirs, big)
+    jv = O.periodic_jvp(om, p, T, u, src, dirs, advection=(seg, data, (0, 0, 0)))
+    ref = O.jvp(bm, p, T, ub, sb, advection=(seg_b, data, (0, 0, 0)))
+    assert np.allclose(jv[:, orig], ref[:, rows], rtol=1e-12, atol=1e-12)
+    r = O.periodic_residual(om, p, T, u, [u], 2, dirs, advection=(seg, data, (0, 0, 0)))
+    rb = O.residual(bm, p, T, ub, [ub], 2, advection=(seg_b, data, (0, 0, 0)))
+    assert np.allclose(r[:, orig], rb[:, rows], rtol=1e-12, atol=1e-12)
+    # the translation changed the operator
+    assert not np.allclose(jv, O.periodic_jvp(om, p, T, u, src, dirs), rtol=1e-6, atol=1e-9)
