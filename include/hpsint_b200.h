@@ -156,7 +156,11 @@ int sint_jvp_f64_noalloc(const sint_mesh *mesh, const sint_params *params, doubl
  * (lac/preconditioners.h:217-315) in place of the reference's ILU.
  * Block 1 (eta): InverseDiagonalMatrix of OperatorAllenCahn
  * (preconditioners.h:342-414, lac/preconditioners.h:159-213,
- * operator_base.h:364-389).  Kept in FP64 and FP32. */
+ * operator_base.h:364-389).  Kept in FP64 and FP32.  With advection set, both
+ * blocks include the advection terms of the current velocity table
+ * (precondition_advection_ch / _ac, operator_sintering_generic.h:800-850); on a
+ * periodic mesh the slave rows are condensed into their masters and get the
+ * identity. */
 int sint_precond_setup(sint_ctx *ctx, sint_stream_t stream);
 
 /* BlockPreconditioner2::vmult (preconditioners.h:1222-1258): z = P^-1 r. */
