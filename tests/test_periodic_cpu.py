@@ -151,3 +151,20 @@ def test_periodic_operator_with_translation(dim, cells, G, dirs):
     assert np.allclose(r[:, orig], rb[:, rows], rtol=1e-12, atol=1e-12)
     # the translation changed the operator
     assert not np.allclose(jv, O.periodic_jvp(om, p, T, u, src, dirs), rtol=1e-6, atol=1e-9)
+
+
+@pytest.mark.parametrize("dim,cells,G,dirs", [(2, (6, 5), 3, (0, 1)), (3, (4, 3, 3), 2, (0, 2))])
+def test_condensed_preconditioner_diagonals_are_periodic(dim, cells, G, dirs):
+    """The preconditioner's diagonals condensed over the periodic pairs equal
+    the diagonals of the tiled (genuinely periodic) operator."""
+    p = O.make_params(G, tensorial=True)
+    om = O.make_mesh(dim, list(cells) + [0] * (3 - dim))
+    u, uu = periodic_state(dim, cells, G, dirs, seed=21)
+    T = O.make_time(10.0, 1.0, [-10.0])
+    big, ub = tiled(dim, cells, dirs, uu)
+    bm = O.make_mesh(dim, list(big) + [0] * (3 - dim))
+    rows, orig = middle_rows(dim, cells, dirs, big)
+    raw = np.concatenate([O.ch_blocks(om, p, T, u), O.ac_diagonal(om, p, T, u)])
+    ours = O.periodic_condense(om, raw, None, dirs, 2)
+    ref = np.concatenate([O.ch_blocks(bm, p, T, ub), O.ac_diagonal(bm, p, T, ub)])
+    assert np.allclose(ours[:, orig], ref[:, rows], rtol=1e-12, atol=1e-12)
