@@ -80,3 +80,22 @@ def test_bdf_weights():
     w = bdf_weights(3, [dt, dt, dt])
     assert w == pytest.approx([11 / 6 / dt, -3 / dt, 1.5 / dt, -1 / 3 / dt])
     assert sum(bdf_weights(2, [0.1, 0.3])) == pytest.approx(0.0, abs=1e-12)
+
+
+def test_new_entry_points_reject_a_null_context():
+    """Argument checks of the cut-off, tracker, periodic and advection entry
+    points run before any device work (SINT_ERR_ARG = 1)."""
+    from hpsint_b200 import _lib as L
+    lib = L.lib()
+    ok = ctypes.c_int()
+    prm = L.SintAdvectionParams(1, 0, 1, 0, 1, 1)
+    assert lib.sint_set_periodicity(None, 1) == 1
+    assert lib.sint_distribute_constraints(None, None, None) == 1
+    assert lib.sint_set_advection(None, None, None, 0, None) == 1
+    assert lib.sint_set_advection_mechanism(None, None, None, 0, ctypes.byref(prm), None) == 1
+    assert lib.sint_advection_forces(None, None, None, None) == 1
+    assert lib.sint_advection_check_courant(None, 1.0, ctypes.byref(ok), None) == 1
+    n = ctypes.c_int()
+    assert lib.sint_grain_segment_periodicity(None, None, None, 0, ctypes.byref(n), None) == 1
+    assert lib.sint_set_component_mask(None, None, 0.0, None) == 1
+    assert lib.sint_set_cut_off_skip_zero_chunks(None, 1) == 1
