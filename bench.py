@@ -149,19 +149,48 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(u, v, G, tensorial, budget_s, n):
+def fma_peaks(stream_ptr):
+    """Measured FMA throughput (TFLOP/s) of this GPU in FP64 and FP32, from the
+    bench-only probe library (hpsint_b200/libfma_probe.so, built with the
+    operator library): the denominator of the ALU roofline."""
+    import ctypes
+    probe = ctypes.CDLL(os.path.join(ROOT, "hpsint_b200", "libfma_probe.so"))
+    probe.fma_probe_tflops.restype = ctypes.c_int
+    probe.fma_probe_tflops.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    out = {}
+    for prec in (64, 32):
+        t = ctypes.c_double()
+        rc = probe.fma_probe_tflops(prec, ctypes.byref(t), stream_ptr)
+        if rc != 0:
+            raise RuntimeError(f"fma_probe_tflops({prec}) failed with CUDA error {rc}")
+        out[prec] = t.value
+    return out
+
+
+SLAB_LAYERS = 16  # z-layers of cells in the CPU baseline's sample
+
+
+def cpu_baseline(u, v, G, tensorial, budget_s, n, gpu_product=None):
     """Time the CPU restatement of the operator (oracle) on a bounded sample of
-    the same workload: a slab of z-layers, repeated until `budget_s` elapses."""
+    the same workload: a slab of z-layers, repeated until `budget_s` elapses.
+    With `gpu_product` (the GPU's J v on the full mesh, C x N), the oracle's
+    product on the slab checks it: rows of the slab's nodes below its top
+    layer (whose cells all lie inside the slab) must agree to 1e-12."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
-    nz = max(2, min(n, 16))
+    nz = max(2, min(n, SLAB_LAYERS))
     N_slab = (n + 1) * (n + 1) * (nz + 1)
     us = np.ascontiguousarray(u[:, :N_slab])
     vs = np.ascontiguousarray(v[:, :N_slab])
     mesh = O.make_mesh(3, [n, n, nz])
     prm = O.make_params(**{k: val for k, val in model_params(G, tensorial).items()})
     T = O.make_time(1.0 / DT, 1.0, [-1.0 / DT])
-    O.jvp(mesh, prm, T, us, vs, threads)  # warm-up
+    ref = O.jvp(mesh, prm, T, us, vs, threads)  # warm-up, and the parity reference
+    parity = None
+    if gpu_product is not None:
+        inner = (n + 1) * (n + 1) * nz  # nodes with z < nz
+        ours, want = gpu_product[:, :inner], ref[:, :inner]
+        parity = max(float(np.linalg.norm(ours[b] - want[b]) / np.linalg.norm(want[b])) for b in range(want.shape[0]))
     reps, t0 = 0, time.perf_counter()
     while True:
         O.jvp(mesh, prm, T, us, vs, threads)
@@ -170,9 +199,12 @@ def cpu_baseline(u, v, G, tensorial, budget_s, n):
         if el >= budget_s or reps >= 1000:
             break
     dofs = (G + 2) * N_slab * reps
-    return {"value": dofs / el / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"FP64 Jacobian-vector product, CPU restatement (OpenMP, {threads} threads), "
-                      f"{n}x{n}x{nz}-cell z-slab of the same state, {reps} reps in {el:.1f} s"}
+    out = {"value": dofs / el / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"FP64 Jacobian-vector product, CPU restatement (OpenMP, {threads} threads), "
+                     f"{n}x{n}x{nz}-cell z-slab of the same state, {reps} reps in {el:.1f} s"}
+    if parity is not None:
+        out["parity_rel_err"] = parity
+    return out
 
 
 def run_reference(args):
@@ -819,6 +851,9 @@ def main():
     ms_jvp64 = time_loop(lambda: op.vmult(dst, vd), args.steps, 0)
     clocks = sampler.stop()
     launches = hb.kernel_launch_count() - launches0
+    # the headline product on the oracle slab's nodes, for the parity check
+    slab_nodes = (n + 1) * (n + 1) * (min(n, SLAB_LAYERS) + 1)
+    gpu_slab = dst[:, :slab_nodes].cpu().numpy()
 
     # --- the other kernels of the path ----------------------------------------
     v32, dst32 = vd.float(), op.initialize_dof_vector(torch.float32)
@@ -875,11 +910,7 @@ def main():
     assert torch.equal(h_dsts[0], h_dst)  # same product, bitwise
 
     # --- measured FMA throughput: denominator of the ALU roofline ---------------
-    fma = {}
-    for prec in (64, 32):
-        t = ctypes.c_double()
-        L.check(lib.sint_device_fma_peak(prec, ctypes.byref(t), sp), "sint_device_fma_peak")
-        fma[prec] = t.value
+    fma = fma_peaks(sp)
 
     # --- roofline of the dominant kernel (algorithmic bytes) ------------------
     peaks = {}
@@ -940,7 +971,7 @@ def main():
                      "note": f"FP64 J v: algorithmic bytes 24*C*N = {alg_bytes/1e6:.1f} MB per launch; "
                              f"peak {peak_src}; kernel is FP64-ALU bound (on-the-fly linearisation)"},
         "roofline_alu": {"bound": "fp64", "peak_fp64_tflops": fma[64], "peak_fp32_tflops": fma[32],
-                         "peak_note": "measured FMA-chain throughput on this GPU (sint_device_fma_peak)",
+                         "peak_note": "measured FMA-chain throughput on this GPU (bench-only libfma_probe.so)",
                          "achieved_fp64_tflops": (flops / (ms_jvp64 * 1e-3) / 1e12) if flops else None,
                          "frac": (flops / (ms_jvp64 * 1e-3) / 1e12 / fma[64]) if flops else None,
                          "flops_source": "executed FP64 add/mul/fma (fma = 2) of one ncu capture" if flops else None},
@@ -957,7 +988,11 @@ def main():
         torch.cuda.empty_cache()
         line["solve"] = solve_comparison(args.solve_compare_steps)
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(u, v, G, tensorial, args.cpu_seconds, n)
+        cb = cpu_baseline(u, v, G, tensorial, args.cpu_seconds, n, gpu_product=gpu_slab)
+        # per-block relative l2 error of the headline product against the oracle
+        # on the slab's interior rows (16 z-layers of cells, 4.4 M DoFs)
+        line["parity_rel_err"] = cb.pop("parity_rel_err", None)
+        line["cpu_baseline"] = cb
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -129,7 +129,6 @@ SIGNATURES = {
                                               ctypes.c_float, _c_void, _c_void, _c_void, _c_void, _c_void]),
     "sint_nn_apply_guess_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,
                                          _c_void, _c_void, _c_void, _c_void]),
-    "sint_device_fma_peak": (_c_int, [_c_int, P(_c_double), _c_void]),
     "sint_last_error": (ctypes.c_char_p, []),
     "sint_kernel_launch_count": (_c_int64, []),
 }

@@ -1,12 +1,12 @@
-// Measured FMA throughput of the device (FP64 and FP32), the denominator of
-// the ALU roofline of the cell kernels: every thread runs 8 independent FMA
-// chains; the rate is timed with CUDA events.
-#include <string>
+// Measured FMA throughput of the device (FP64 and FP32): the denominator of
+// the ALU roofline that bench.py reports for the cell kernels.  Every thread
+// runs 8 independent FMA chains; the rate is timed with CUDA events.
+//
+// This is a measurement aid of the benchmark, built as its own library
+// (libfma_probe.so); it is not part of the operator's C ABI.
+#include <cuda_runtime.h>
 
-#include "sint_internal.h"
-#include "sint_launch.h"
-
-namespace sint
+namespace
 {
   template <typename R>
   __global__ void __launch_bounds__(256) fma_probe_kernel(int iters, R a, R b, R *out)
@@ -30,26 +30,25 @@ namespace sint
   }
 
   template <typename R>
-  static int probe(double *tflops, cudaStream_t s)
+  cudaError_t probe(double *tflops, cudaStream_t s)
   {
-    int dev = 0, sms = 0;
+    int         dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess)
       e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess)
-      return cuda_fail(e, "fma probe: device query");
+      return e;
     R *out = nullptr;
     if ((e = cudaMalloc(&out, sizeof(R))) != cudaSuccess)
-      return cuda_fail(e, "fma probe: alloc");
-    const int    blocks = sms * 8, threads = 256, iters = 1 << 14;
-    cudaEvent_t  e0, e1;
+      return e;
+    const int   blocks = sms * 8, threads = 256, iters = 1 << 14;
+    cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     fma_probe_kernel<R><<<blocks, threads, 0, s>>>(iters / 8, R(0.999999), R(1e-7), out); // warm-up
     cudaEventRecord(e0, s);
     fma_probe_kernel<R><<<blocks, threads, 0, s>>>(iters, R(0.999999), R(1e-7), out);
     cudaEventRecord(e1, s);
-    count_launches(2);
     e = cudaEventSynchronize(e1);
     float ms = 0.f;
     if (e == cudaSuccess)
@@ -58,19 +57,19 @@ namespace sint
     cudaEventDestroy(e1);
     cudaFree(out);
     if (e != cudaSuccess)
-      return cuda_fail(e, "fma probe: timing");
+      return e;
     const double flops = 2.0 * 8.0 * double(iters) * double(blocks) * threads;
     *tflops            = flops / (double(ms) * 1e-3) / 1e12;
-    return SINT_OK;
+    return cudaSuccess;
   }
-} // namespace sint
+} // namespace
 
-extern "C" int sint_device_fma_peak(int precision, double *tflops, sint_stream_t stream)
+// FMA throughput of the current device in TFLOP/s (precision 64 or 32).
+// Synchronous.  Returns a cudaError_t code (0 = success).
+extern "C" int fma_probe_tflops(int precision, double *tflops, void *stream)
 {
   if (!tflops || (precision != 32 && precision != 64))
-    {
-      sint::set_error("sint_device_fma_peak: precision must be 32 or 64 and tflops non-null");
-      return SINT_ERR_ARG;
-    }
-  return precision == 64 ? sint::probe<double>(tflops, stream) : sint::probe<float>(tflops, stream);
+    return int(cudaErrorInvalidValue);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return int(precision == 64 ? probe<double>(tflops, s) : probe<float>(tflops, s));
 }

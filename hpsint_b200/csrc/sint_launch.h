@@ -6,12 +6,42 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "sint_common.cuh"
 
 namespace sint
 {
+  // Launch set-up that belongs to one device: function attributes live in the
+  // device's context, persistent grids follow its SM count.  A kernel keeps
+  // one value per device ordinal (0 = not set up yet); `setup(dev, value)`
+  // runs once per ordinal, with that device current.  Concurrent first calls
+  // may both run the (idempotent) set-up.  A process that resets a device
+  // (cudaDeviceReset) must not call this library on it again.
+  constexpr int MAX_DEVICES = 64;
+  using DeviceCache         = std::atomic<int>[MAX_DEVICES];
+
+  template <typename Setup>
+  inline cudaError_t per_device(DeviceCache &cache, int &value, Setup setup)
+  {
+    int         dev = 0;
+    cudaError_t e   = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+      return e;
+    if (dev < 0 || dev >= MAX_DEVICES)
+      return cudaErrorInvalidDevice;
+    int v = cache[dev].load(std::memory_order_acquire);
+    if (v == 0)
+      {
+        if ((e = setup(dev, v)) != cudaSuccess)
+          return e;
+        cache[dev].store(v, std::memory_order_release);
+      }
+    value = v;
+    return cudaSuccess;
+  }
+
   // Dynamic shared memory of the diagonal kernel (bytes); adv: with the
   // grains' velocities per point.
   size_t smem_diag(int dim, int G, bool adv = false);

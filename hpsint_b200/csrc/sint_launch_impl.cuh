@@ -27,26 +27,34 @@ namespace sint
     return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
   }
 
+  // Persistent grid of kernel k on the current device: its shared-memory
+  // attributes set, as many blocks as are resident at once (once per device).
+  template <typename Kernel>
+  inline cudaError_t persistent_grid(DeviceCache &cache, Kernel k, size_t smem, int blocks_per_sm, int threads,
+                                     int &grid_cap)
+  {
+    return per_device(cache, grid_cap, [&](int dev, int &cap) {
+      cudaError_t e = prepare_smem(k, smem, blocks_per_sm);
+      int         sms = 0, per_sm = 0;
+      if (e != cudaSuccess || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+          (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem)) != cudaSuccess)
+        return e;
+      cap = sms * (per_sm > 0 ? per_sm : 1);
+      return cudaSuccess;
+    });
+  }
+
   template <int DIM, int G, bool TENS, typename R, bool CUT, bool ADV>
   cudaError_t launch_jvp_g(const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
                            const CutTiles &ct, const AdvData &adv, cudaStream_t s)
   {
     const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false, ADV>::TOTAL * sizeof(R);
     auto         k    = jvp_kernel<DIM, G, TENS, R, CUT, ADV>;
-    // persistent grid: as many blocks as are resident at once
-    static int   grid_cap = 0;
-    cudaError_t  e        = cudaSuccess;
-    if (grid_cap == 0)
-      {
-        if ((e = prepare_smem(k, smem, jvp_blocks_per_sm<DIM, G, R>())) != cudaSuccess)
-          return e;
-        int dev = 0, sms = 0, per_sm = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
-            (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Tile<DIM>::THREADS, smem)) != cudaSuccess)
-          return e;
-        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
-      }
+    static DeviceCache cache;
+    int                grid_cap = 0;
+    if (const cudaError_t e =
+          persistent_grid(cache, k, smem, jvp_blocks_per_sm<DIM, G, R>(), Tile<DIM>::THREADS, grid_cap))
+      return e;
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
     k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, ct, adv);
     count_launches(1);
@@ -60,19 +68,11 @@ namespace sint
   {
     const size_t  smem     = ThreePhaseSmem<DIM, G, TENS, false, WTD == 2, ADV>::TOTAL * sizeof(double);
     auto          k        = residual_kernel<DIM, G, TENS, WTD, CUT, ADV>;
-    static int    grid_cap = 0;
-    cudaError_t   e        = cudaSuccess;
-    if (grid_cap == 0)
-      {
-        if ((e = prepare_smem(k, smem, residual_blocks_per_sm<DIM, G>())) != cudaSuccess)
-          return e;
-        int dev = 0, sms = 0, per_sm = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
-            (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Tile<DIM>::THREADS, smem)) != cudaSuccess)
-          return e;
-        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
-      }
+    static DeviceCache cache;
+    int                grid_cap = 0;
+    if (const cudaError_t e =
+          persistent_grid(cache, k, smem, residual_blocks_per_sm<DIM, G>(), Tile<DIM>::THREADS, grid_cap))
+      return e;
     const double *h0     = WTD == 2 ? hist[0] : nullptr;
     const double *h1     = (WTD == 2 && p.order > 1) ? hist[1] : nullptr;
     const double *h2     = (WTD == 2 && p.order > 2) ? hist[2] : nullptr;

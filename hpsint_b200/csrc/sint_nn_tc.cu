@@ -394,25 +394,24 @@ namespace
                 int accumulate, const float *addend, int add_group, int act, float slope, int *status,
                 cudaStream_t s)
   {
-    static int grid_cap = 0;
-    auto       k        = tc::conv3x3_tc_kernel<N>;
-    if (grid_cap == 0)
-      {
-        int         dev = 0, sms = 0;
-        const int   smax = int(tc::ws_smem_bytes(tc::chunks_of(tc::CIN_MAX), N));
-        cudaError_t e    = cudaGetDevice(&dev);
-        if (e == cudaSuccess)
-          e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess)
-          e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
-        if (e == cudaSuccess) // all of the unified L1 / shared storage as shared memory
-          e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess)
-          return cuda_fail(e, "sint_nn_conv3x3_tc_f32: setup");
-        // two CTAs per SM: the launch bound caps registers at 128 and the largest
-        // configuration takes 83 KB of shared memory, so both fit on every SM
-        grid_cap = sms * tc::CTAS_PER_SM;
-      }
+    static DeviceCache cache; // per device: attributes set, grid size
+    auto               k        = tc::conv3x3_tc_kernel<N>;
+    int                grid_cap = 0;
+    const cudaError_t  es       = per_device(cache, grid_cap, [&](int dev, int &cap) {
+      int         sms  = 0;
+      const int   smax = int(tc::ws_smem_bytes(tc::chunks_of(tc::CIN_MAX), N));
+      cudaError_t e    = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+      if (e == cudaSuccess) // all of the unified L1 / shared storage as shared memory
+        e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      // two CTAs per SM: the launch bound caps registers at 128 and the largest
+      // configuration takes 83 KB of shared memory, so both fit on every SM
+      cap = sms * tc::CTAS_PER_SM;
+      return e;
+    });
+    if (es != cudaSuccess)
+      return cuda_fail(es, "sint_nn_conv3x3_tc_f32: setup");
     const int       KC    = tc::chunks_of(Cin);
     const long long tiles = (long long)B * ((H + tc::TY - 1) / tc::TY) * ((W + tc::TX - 1) / tc::TX);
     const int       grid  = int(tiles < grid_cap ? tiles : grid_cap);

@@ -520,10 +520,6 @@ int sint_nn_increment_scales_f64(const double *u_n, const double *u_nm1, int64_t
                                  float ratio, float dt, const float *base, unsigned *work, float *scale,
                                  float *oscale, sint_stream_t stream);
 
-/* Measured FMA throughput of the current device in TFLOP/s (precision 64 or
- * 32): the denominator of the cell kernels' ALU roofline.  Synchronous. */
-int sint_device_fma_peak(int precision, double *tflops, sint_stream_t stream);
-
 /* Text of the last error recorded on this thread (never NULL). */
 const char *sint_last_error(void);
 

@@ -1,9 +1,9 @@
 """Extract hpsint's golden test vectors for the sintering operator into JSON.
 
-Run once in a checkout that has the reference sources (default location
-/root/reference, or pass the path as the first argument); the JSON fixtures
-it writes next to this script are committed, so nothing at test time reads
-the reference tree.
+Run once with the path of an hpsint checkout as the only argument
+(`python tests/golden/make_golden.py <path-to-hpsint>`); the JSON fixtures it
+writes next to this script are committed, so nothing at test time reads the
+reference tree.
 
 Sources (paths inside the hpsint project):
   tests/residual_generic_{scalar,tensorial}_no_rbm.mpirun=1.output
@@ -251,4 +251,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the hpsint checkout>")
+    main(sys.argv[1])

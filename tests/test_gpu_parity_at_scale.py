@@ -1,0 +1,200 @@
+"""CUDA operator vs the CPU oracle on packing states with many more tiles than
+the persistent grid has resident blocks (needs a B200).
+
+The other parity tests use meshes of at most a few dozen tiles, so every
+block of the persistent cell kernels computes one tile.  Here each block
+walks many tiles, with the next tile's node boxes prefetched while the
+current one is computed -- the loop every benchmark and solve runs:
+
+  * 3D: a 42 x 41 x 40-cell crop of the operator-bench packing (128^3 mesh,
+    8 spheres with radii U[12, 18], 4 order parameters, tanh width 2 plus
+    U(-1e-3, 1e-3) noise, tensorial mobility) around two sphere contacts;
+  * 2D: a 256 x 256-cell crop of the learned-guess packing of seed 0 (512^2
+    mesh, 100 circles with radii U[6, 12], 8 order parameters, scalar
+    mobility).
+
+Both crops hold vapour regions where the surface-mobility and |grad c|
+thresholds switch, grain boundaries and triple junctions.  Tolerances are
+those of the other parity tests: per-block relative l2 error <= 1e-12 in
+FP64, <= 2e-5 for the FP32 product against the oracle at FP32-rounded
+inputs.
+"""
+import numpy as np
+import pytest
+
+from helpers import advection_data, block_rel_err, oracle_mesh, random_state
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+C2_CELLS = (42, 41, 40)
+C2_ORIGIN = (52.0, 50.0, 34.0)  # contacts of spheres 0-1 and 0-3 of the packing
+C4_CELLS = (256, 256)
+C4_ORIGIN = (128.0, 128.0)
+
+
+def c2_crop(noise_seed=1, noise=1e-3):
+    from hpsint_b200 import packings as P
+    centers, radii, colours = P.operator_bench_packing(n=128)
+    u = P.initial_state(3, C2_CELLS, (1.0, 1.0, 1.0), C2_ORIGIN, centers, radii, colours, width=2.0,
+                        noise=noise, seed=noise_seed)
+    return u, int(colours.max()) + 1
+
+
+def c4_crop():
+    from hpsint_b200 import learned_guess as LG
+    from hpsint_b200 import packings as P
+    centers, radii, colours = LG.packing_2d(0)
+    u = P.initial_state(2, C4_CELLS, (1.0, 1.0), C4_ORIGIN, centers, radii, colours, width=2.0)
+    # a smooth chemical potential, so the mobility flux of the residual is not zero
+    rng = np.random.default_rng(5)
+    x = np.arange(C4_CELLS[0] + 1) / C4_CELLS[0]
+    X, Y = np.meshgrid(x, x)
+    u[1] = (0.3 * np.cos(3 * np.pi * X + rng.uniform(0, 6)) * np.cos(2 * np.pi * Y)).ravel()
+    return u, int(colours.max()) + 1
+
+
+STATES = {"3d-c2-crop": (3, C2_CELLS, True, c2_crop), "2d-c4-crop": (2, C4_CELLS, False, c4_crop)}
+
+
+@pytest.fixture(scope="module", params=list(STATES))
+def state(request):
+    import hpsint_b200 as hb
+    dim, cells, tens, make = STATES[request.param]
+    u, G = make()
+    op = hb.SinteringOperatorGeneric(hb.Mesh(dim, tuple(cells) + (1,) * (3 - dim)), hb.Params(G, tensorial=tens))
+    # the crop really is many tiles per resident block
+    tiles = np.prod([-(-cells[d] // t) for d, t in enumerate((4, 4, 2) if dim == 3 else (8, 8))])
+    assert tiles >= 1000
+    return dict(dim=dim, cells=cells, G=G, tens=tens, u=u, op=op, om=oracle_mesh(dim, cells),
+                p=O.make_params(G, tensorial=tens))
+
+
+def _perturbed(u, seed, scale=0.02):
+    rng = np.random.default_rng(seed)
+    return u + scale * rng.uniform(-1.0, 1.0, u.shape)
+
+
+@pytest.mark.parametrize("wtd,order", [(0, 1), (1, 1), (2, 1), (2, 2)])
+def test_residual_at_scale(state, wtd, order):
+    op, u = state["op"], state["u"]
+    hist = [_perturbed(u, 11), _perturbed(u, 12)][:order] if wtd == 2 else []
+    w = {1: [50.0, -50.0], 2: [75.0, -100.0, 25.0]}[order]
+    op.set_time_weights(w[0], w[1:], 1.0)
+    dst = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(dst, op.to_device(u), wtd, [op.to_device(x) for x in hist])
+    torch.cuda.synchronize()
+    ref = O.residual(state["om"], state["p"], O.make_time(w[0], 1.0, w[1:]), u, hist, wtd)
+    assert block_rel_err(op.to_host(dst), ref) <= 1e-12
+
+
+def test_jvp_f64_at_scale(state):
+    op, u = state["op"], state["u"]
+    src = random_state(state["dim"], state["cells"], state["G"], seed=13, smooth=False) - 0.5
+    op.set_time_weights(1e3, [-1e3], 1.0)
+    op.fill_quadrature_point_values(op.to_device(u))
+    dst = op.initialize_dof_vector()
+    op.vmult(dst, op.to_device(src))
+    torch.cuda.synchronize()
+    ref = O.jvp(state["om"], state["p"], O.make_time(1e3, 1.0, [-1e3]), u, src)
+    assert block_rel_err(op.to_host(dst), ref) <= 1e-12
+
+
+def test_jvp_f32_at_scale(state):
+    op = state["op"]
+    u = state["u"].astype(np.float32).astype(np.float64)
+    src = (random_state(state["dim"], state["cells"], state["G"], seed=14, smooth=False) - 0.5)
+    src = src.astype(np.float32).astype(np.float64)
+    op.set_time_weights(1e3, [-1e3], 1.0)
+    op.fill_quadrature_point_values(op.to_device(u))
+    dst = op.initialize_dof_vector(torch.float32)
+    op.vmult(dst, op.to_device(src, torch.float32))
+    torch.cuda.synchronize()
+    ref = O.jvp(state["om"], state["p"], O.make_time(1e3, 1.0, [-1e3]), u, src)
+    assert block_rel_err(op.to_host(dst), ref) <= 2e-5
+
+
+def test_preconditioner_at_scale(state):
+    import hpsint_b200 as hb
+    op, u = state["op"], state["u"]
+    op.set_time_weights(1e3, [-1e3], 1.0)
+    op.fill_quadrature_point_values(op.to_device(u))
+    pc = hb.BlockPreconditioner2(op)
+    pc.do_update()
+    T = O.make_time(1e3, 1.0, [-1e3])
+    ch_ref = O.ch_blocks(state["om"], state["p"], T, u)
+    ac_ref = O.ac_diagonal(state["om"], state["p"], T, u)
+    N = op.N
+    assert block_rel_err(pc.ch_blocks()[:, :N].cpu().numpy(), ch_ref) <= 1e-12
+    inv_ref = O.inverse_diagonal(ac_ref)
+    assert block_rel_err(pc.inverse_diagonal()[:, :N].cpu().numpy(), inv_ref) <= 1e-12
+    r = random_state(state["dim"], state["cells"], state["G"], seed=15, smooth=False) - 0.5
+    z = op.initialize_dof_vector()
+    pc.vmult(z, op.to_device(r))
+    det = ch_ref[0] * ch_ref[3] - ch_ref[1] * ch_ref[2]
+    zref = np.vstack([(ch_ref[3] * r[0] - ch_ref[1] * r[1]) / det, (-ch_ref[2] * r[0] + ch_ref[0] * r[1]) / det,
+                      inv_ref * r[2:]])
+    assert block_rel_err(op.to_host(z), zref) <= 1e-12
+
+
+@pytest.mark.parametrize("tol", [1e-5, 1e-2])
+def test_cut_off_at_scale(state, tol):
+    op, u, om, p = state["op"], state["u"], state["om"], state["p"]
+    ud = op.to_device(u)
+    op.set_component_mask(ud, tol)
+    mask = O.grain_mask(om, p, u, tol)
+    assert np.array_equal(op.get_component_mask().cpu().numpy().view(np.uint16), mask)
+    # several tile classes are populated: vapour, one grain, grain boundaries
+    counts = np.bincount([bin(int(x)).count("1") for x in mask], minlength=state["G"] + 1)
+    assert np.count_nonzero(counts) >= 3
+    old = _perturbed(u, 16)
+    op.set_time_weights(1e3, [-1e3], 1.0)
+    T = O.make_time(1e3, 1.0, [-1e3])
+    r = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(r, ud, 2, [op.to_device(old)])
+    src = random_state(state["dim"], state["cells"], state["G"], seed=17, smooth=False) - 0.5
+    op.fill_quadrature_point_values(ud)
+    j = op.initialize_dof_vector()
+    op.vmult(j, op.to_device(src))
+    j32 = op.initialize_dof_vector(torch.float32)
+    op.vmult(j32, op.to_device(src, torch.float32))
+    torch.cuda.synchronize()
+    assert block_rel_err(op.to_host(r), O.residual(om, p, T, u, [old], 2, mask=mask)) <= 1e-12
+    j_ref = O.jvp(om, p, T, u, src, mask=mask)
+    assert block_rel_err(op.to_host(j), j_ref) <= 1e-12
+    # FP32 product: the linearisation point is the FP32 shadow of u
+    u32 = u.astype(np.float32).astype(np.float64)
+    src32 = src.astype(np.float32).astype(np.float64)
+    assert block_rel_err(op.to_host(j32), O.jvp(om, p, T, u32, src32, mask=mask)) <= 2e-5
+    op.set_component_mask(None, 0.0)
+
+
+def test_advection_at_scale(state):
+    dim, cells, G = state["dim"], state["cells"], state["G"]
+    op, u, om, p = state["op"], state["u"], state["om"], state["p"]
+    seg, data = advection_data(dim, cells, G, seed=18, n_seg_per_grain=3, scale=0.5)
+    op.set_advection(torch.from_numpy(seg).cuda().contiguous(), torch.from_numpy(data).cuda().contiguous())
+    adv = (seg, data, (0.0, 0.0, 0.0))
+    ud = op.to_device(u)
+    old = _perturbed(u, 19)
+    op.set_time_weights(1e3, [-1e3], 1.0)
+    T = O.make_time(1e3, 1.0, [-1e3])
+    r = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(r, ud, 2, [op.to_device(old)])
+    src = random_state(dim, cells, G, seed=20, smooth=False) - 0.5
+    op.fill_quadrature_point_values(ud)
+    j = op.initialize_dof_vector()
+    op.vmult(j, op.to_device(src))
+    torch.cuda.synchronize()
+    assert block_rel_err(op.to_host(r), O.residual(om, p, T, u, [old], 2, advection=adv)) <= 1e-12
+    assert block_rel_err(op.to_host(j), O.jvp(om, p, T, u, src, advection=adv)) <= 1e-12
+    # the same under the grain cut-off
+    op.set_component_mask(ud, 1e-5)
+    mask = O.grain_mask(om, p, u, 1e-5)
+    op.vmult(j, op.to_device(src))
+    torch.cuda.synchronize()
+    assert block_rel_err(op.to_host(j), O.jvp(om, p, T, u, src, mask=mask, advection=adv)) <= 1e-12
+    op.set_component_mask(None, 0.0)
+    op.set_advection(None, None)
