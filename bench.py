@@ -74,6 +74,9 @@ def parse_args():
     ap.add_argument("--solve-steps", type=int, default=100)
     ap.add_argument("--arms", default=None,
                     help="solve3d: comma-separated subset of the arms to run (default: all)")
+    ap.add_argument("--preconditioners", action="store_true",
+                    help="solve3d: also run right-preconditioned GMRES with block-Jacobi and with the Gauss-Seidel "
+                         "Cahn-Hilliard block")
     ap.add_argument("--cut-off", type=float, default=0.0,
                     help="solve3d: also run both solves with this GrainCutOffTolerance and time the cut-off J v")
     return ap.parse_args()
@@ -295,7 +298,51 @@ def two_particle_solve(args):
         "speedup_accepted_attempts": sum(x.accepted_wall_s for x in ref["rec"]) /
                                      sum(x.accepted_wall_s for x in mp["rec"]),
     }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_solve_baseline(u0, h, schedule, args.cpu_seconds)
     print(json.dumps(line), flush=True)
+
+
+def cpu_solve_baseline(u0, h, schedule, budget_s):
+    """The same solve on the host cores: the CPU restatement of the damped
+    Newton-GMRES step (oracle/newton_cpu.py: FP64 GMRES(30), block-Jacobi,
+    the oracle's residual and J v with OpenMP) on the first steps of the
+    FP64 run's time grid, as many as fit in about `budget_s` seconds; plus
+    the CPU residual and J v of the initial state."""
+    from oracle import newton_cpu as NC
+    from oracle import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    nx, ny = 256, 128
+    mesh = O.make_mesh(2, [nx, ny, 0], (h[0], h[1], 1.0))
+    prm = O.make_params(**model_params(2, True))
+    solver = NC.NewtonCPU(mesh, prm, threads, nl_rel_tol=1e-8)
+    u = u0.copy()
+    recs, t0 = [], time.perf_counter()
+    for dt in schedule:
+        T = O.make_time(1.0 / dt, 1.0, [-1.0 / dt])
+        old = u.copy()
+        recs.append(solver.solve(T, u, [old]))
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    el = time.perf_counter() - t0
+    T = O.make_time(1.0 / schedule[0], 1.0, [-1.0 / schedule[0]])
+    reps = 5
+    t1 = time.perf_counter()
+    for _ in range(reps):
+        O.residual(mesh, prm, T, u0, [u0], 2, threads)
+    t_res = (time.perf_counter() - t1) / reps
+    t1 = time.perf_counter()
+    for _ in range(reps):
+        O.jvp(mesh, prm, T, u0, u0, threads)
+    t_jvp = (time.perf_counter() - t1) / reps
+    dofs = u0.size
+    return {"value": el / len(recs), "unit": "s/step", "cores": threads, "kind": "port",
+            "sample": f"first {len(recs)} steps of the FP64 run's time grid, FP64 Newton-GMRES(30) with "
+                      f"block-Jacobi on the CPU restatement (oracle/newton_cpu.py, OpenMP, {threads} threads)",
+            "newton_iterations": sum(r["newton_iterations"] for r in recs),
+            "linear_iterations": sum(r["linear_iterations"] for r in recs),
+            "residual_gdofs": dofs / t_res / 1e9, "jvp_gdofs": dofs / t_jvp / 1e9}
 
 
 def operator_2d(args):
@@ -441,21 +488,30 @@ def mixed_precision_solve_3d(args):
     c0 = float(np.einsum("k,j,i,kji->", w, w, w, u0[0].reshape(n + 1, n + 1, n + 1)))
     del u0
     operator_rates = cut_off_operator_rates(op, u0d, args.cut_off) if args.cut_off > 0 else None
-    # (label, Krylov precision, cut-off tolerance, preconditioner with the cut-off too)
-    arms = [("fp64_inner", 64, 0.0, False), ("fp32_inner", 32, 0.0, False)]
+    # (label, Krylov precision, cut-off tolerance, preconditioner with the cut-off too,
+    #  block-0 preconditioner, right-preconditioned GMRES)
+    BJ, GS = "block_jacobi", "ch_gauss_seidel"
+    arms = [("fp64_inner", 64, 0.0, False, BJ, False), ("fp32_inner", 32, 0.0, False, BJ, False)]
     if args.cut_off > 0:
-        arms += [("fp64_inner_cut_off", 64, args.cut_off, False), ("fp32_inner_cut_off", 32, args.cut_off, False),
-                 ("fp32_inner_cut_off_cut_preconditioner", 32, args.cut_off, True)]
+        arms += [("fp64_inner_cut_off", 64, args.cut_off, False, BJ, False),
+                 ("fp32_inner_cut_off", 32, args.cut_off, False, BJ, False),
+                 ("fp32_inner_cut_off_cut_preconditioner", 32, args.cut_off, True, BJ, False)]
+    if args.preconditioners:
+        arms += [("fp32_inner_right", 32, 0.0, False, BJ, True), ("fp32_inner_ch_gs_right", 32, 0.0, False, GS, True),
+                 ("fp64_inner_ch_gs_right", 64, 0.0, False, GS, True)]
+        if args.cut_off > 0:
+            arms += [("fp32_inner_cut_off_ch_gs_right", 32, args.cut_off, False, GS, True)]
     if args.arms:
         keep = args.arms.split(",")
         arms = [a for a in arms if a[0] in keep]
         if not arms:
             raise SystemExit(f"--arms {args.arms}: no such arm")
     runs, schedule = {}, None
-    for label, prec, tol, cut_pc in arms:
+    for label, prec, tol, cut_pc, block0, right in arms:
         op.set_component_mask(u0d, tol)  # 0 switches a previous arm's cut-off off
         op.set_preconditioner_cut_off(cut_pc)
-        ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec),
+        op.set_preconditioner_type(block0)
+        ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec, right_preconditioning=right),
                             TimeIntegrationData(time_step_init=1e-4), grain_cut_off_tolerance=tol)
         ti.initialize(u0d)
         ti.run(2, dt_schedule=[1e-4, 1e-4])  # warm-up: workspaces, first launches (discarded)
@@ -495,6 +551,17 @@ def mixed_precision_solve_3d(args):
             "speedup_accepted_attempts": sum(x.accepted_wall_s for x in ref["recs"]) /
                                          sum(x.accepted_wall_s for x in mp["recs"]),
         }
+    if ref:
+        for label in ("fp32_inner_right", "fp32_inner_ch_gs_right", "fp64_inner_ch_gs_right",
+                      "fp32_inner_cut_off_ch_gs_right"):
+            if label in runs:
+                r = runs[label]
+                line[label].update({
+                    "max_abs_diff_c_vs_fp64_inner": float(np.abs(r["u"][0] - ref["u"][0]).max()),
+                    "max_abs_diff_eta_vs_fp64_inner": float(np.abs(r["u"][2:] - ref["u"][2:]).max()),
+                    "speedup_s_per_step_vs_fp64_inner": (ref["wall"] / len(ref["recs"])) / (r["wall"] / len(r["recs"])),
+                    "linear_iterations_per_newton": sum(x.linear_iterations for x in r["recs"]) /
+                                                    max(1, sum(x.newton_iterations for x in r["recs"]))})
     if args.cut_off > 0 and ref:
         line["cut_off"] = {"tolerance": args.cut_off, "operator_at_initial_state": operator_rates}
         for label in ("fp64_inner_cut_off", "fp32_inner_cut_off", "fp32_inner_cut_off_cut_preconditioner"):

@@ -41,7 +41,8 @@ class SintNewtonParams(ctypes.Structure):
                 ("l_max_iter", _c_int), ("l_abs_tol", _c_double), ("l_rel_tol", _c_double),
                 ("gmres_restart", _c_int), ("threshold_newton_iter", _c_int),
                 ("threshold_linear_iter", _c_int), ("use_damping", _c_int),
-                ("reuse_preconditioner", _c_int), ("inner_precision", _c_int)]
+                ("reuse_preconditioner", _c_int), ("inner_precision", _c_int),
+                ("right_preconditioning", _c_int)]
 
 
 class SintNewtonStats(ctypes.Structure):
@@ -69,6 +70,8 @@ SIGNATURES = {
     "sint_precond_apply_f64": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_precond_apply_f32": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_ac_inverse_diagonal_f64": (_c_int, [_c_void, _c_void, _c_void]),
+    "sint_set_preconditioner_type": (_c_int, [_c_void, _c_int]),
+    "sint_ch_matrix_f64": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_ch_blocks_f64": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_set_component_mask": (_c_int, [_c_void, _c_void, _c_double, _c_void]),
     "sint_component_mask_statistics": (_c_int, [_c_void, P(_c_int64), _c_void]),

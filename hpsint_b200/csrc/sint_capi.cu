@@ -404,6 +404,10 @@ int sint_destroy(sint_ctx *c)
   cudaFree(c->adv_off);
   cudaFree(c->adv_items);
   cudaFree(c->adv_slots);
+  cudaFree(c->ch_A64);
+  cudaFree(c->ch_A32);
+  cudaFree(c->ch_dinv64);
+  cudaFree(c->ch_dinv32);
   cudaFree(c->pc_raw);
   cudaFree(c->pc_inv64);
   cudaFree(c->pc_inv32);
@@ -564,8 +568,48 @@ int sint_precond_setup(sint_ctx *c, sint_stream_t stream)
   count_launches(1);
   if ((e = cudaGetLastError()) != cudaSuccess)
     return cuda_fail(e, "sint_precond_setup: invert");
+  c->has_ch = false;
+  if (c->pc_kind == 1)
+    {
+      if (int rc = ch_sgs_setup(c, stream))
+        return rc;
+      c->has_ch = true;
+    }
   c->has_pc = true;
   return SINT_OK;
+}
+
+int sint_set_preconditioner_type(sint_ctx *c, int type)
+{
+  if (int e = check_ctx(c))
+    return e;
+  if (type != 0 && type != 1)
+    {
+      set_error("sint_set_preconditioner_type: type must be 0 (block-Jacobi) or 1 (Cahn-Hilliard Gauss-Seidel)");
+      return SINT_ERR_ARG;
+    }
+  if (type != c->pc_kind)
+    c->has_pc = false; // takes effect at the next set-up
+  c->pc_kind = type;
+  return SINT_OK;
+}
+
+int sint_ch_matrix_f64(sint_ctx *c, double *A, sint_stream_t stream)
+{
+  if (int e = check_ctx(c))
+    return e;
+  if (!c->has_ch)
+    {
+      set_error("sint_ch_matrix_f64: the Cahn-Hilliard matrix is not set up (preconditioner type 1 and "
+                "sint_precond_setup first)");
+      return SINT_ERR_NOT_READY;
+    }
+  if (int e = check_vec(A, "A"))
+    return e;
+  const size_t nk = c->grid.dim == 3 ? 27 : 9;
+  const cudaError_t e =
+    cudaMemcpyAsync(A, c->ch_A64, sizeof(double) * nk * 4 * c->ld, cudaMemcpyDeviceToDevice, stream);
+  return e == cudaSuccess ? SINT_OK : cuda_fail(e, "sint_ch_matrix_f64");
 }
 
 int sint_precond_apply_f64(sint_ctx *c, double *z, const double *r, sint_stream_t stream)
@@ -584,7 +628,9 @@ int sint_precond_apply_f64(sint_ctx *c, double *z, const double *r, sint_stream_
   const long long nb = (c->N + 255) / 256;
   precond_apply_kernel<double><<<dim3((unsigned)nb), 256, 0, stream>>>(c->N, c->ld, c->G, c->pc_inv64, r, z);
   count_launches(1);
-  const cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && c->has_ch) // Cahn-Hilliard block by the Gauss-Seidel sweeps
+    e = ch_sgs_apply<double>(c, r, z, stream);
   return e == cudaSuccess ? SINT_OK : cuda_fail(e, "sint_precond_apply_f64");
 }
 
@@ -604,7 +650,9 @@ int sint_precond_apply_f32(sint_ctx *c, float *z, const float *r, sint_stream_t 
   const long long nb = (c->N + 255) / 256;
   precond_apply_kernel<float><<<dim3((unsigned)nb), 256, 0, stream>>>(c->N, c->ld, c->G, c->pc_inv32, r, z);
   count_launches(1);
-  const cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && c->has_ch) // Cahn-Hilliard block by the Gauss-Seidel sweeps
+    e = ch_sgs_apply<float>(c, r, z, stream);
   return e == cudaSuccess ? SINT_OK : cuda_fail(e, "sint_precond_apply_f32");
 }
 

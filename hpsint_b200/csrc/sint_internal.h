@@ -90,6 +90,15 @@ namespace sint
     long long             adv_n_valid   = 0;       // items with a segment
     long long adv_cen_cap = 0, adv_vft_cap = 0, adv_off_cap = 0, adv_items_cap = 0, adv_slots_cap = 0;
 
+    // preconditioner of the Cahn-Hilliard block: 0 = 2x2 node-block Jacobi,
+    // 1 = symmetric Gauss-Seidel on the assembled block (sint_chsgs.cu)
+    int     pc_kind   = 0;
+    bool    has_ch    = false;   // the assembled block belongs to the current set-up
+    double *ch_A64    = nullptr; // 3^dim x 4 blocks of ld: 2x2 blocks per node row and neighbour
+    float  *ch_A32    = nullptr;
+    double *ch_dinv64 = nullptr; // 4 blocks of ld: inverted centre blocks
+    float  *ch_dinv32 = nullptr;
+
     double *pc_raw   = nullptr; // (G+4) blocks: CH 2x2 entries, AC diagonal
     double *pc_inv64 = nullptr; // (G+4) blocks: CH 2x2 inverse, AC inverse diagonal
     float  *pc_inv32 = nullptr;
@@ -158,6 +167,12 @@ namespace sint
   // The advection mechanism's update before a residual evaluation: forces of
   // u, then the velocity table (sint_advection.cu).
   int advection_update(Ctx *c, const double *u, cudaStream_t s);
+  // The assembled Cahn-Hilliard block and its Gauss-Seidel sweeps
+  // (sint_chsgs.cu): set-up at the linearisation point, and z_(c,mu) =
+  // SGS(r_(c,mu)) on the first two blocks of z (the others untouched).
+  int ch_sgs_setup(Ctx *c, cudaStream_t s);
+  template <typename R>
+  cudaError_t ch_sgs_apply(const Ctx *c, const R *r, R *z, cudaStream_t s);
   // J v through the cell kernel + combine, with c->partial as scratch.
   template <typename R>
   cudaError_t dispatch_jvp(const Ctx *c, const R *lin, const R *src, R *dst, cudaStream_t s);

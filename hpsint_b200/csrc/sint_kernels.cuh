@@ -220,6 +220,17 @@ namespace sint
     const R omc = R(1) - c;
     const R fcc = R(2) * p.A * (c * c) + R(4) * p.A * c * (R(2) * c - R(2)) + R(2) * p.A * (omc * omc) + R(2) * p.B;
     const R B12 = p.B * R(12);
+    // f_{c eta_i} = 12 B eta_i (eta_i - 1) (free_energy.h:150-152), shared by the mu
+    // and eta rows; f_{eta_i eta_i} = B (12 - 12 c + 2 eta_i (12 c - 24) + 24 eta_i^2
+    // + 12 sum eta^2) (:154-158) in Horner form: f0 + eta_i (f1 + f2 eta_i)
+    R fce[gdim(G)];
+#pragma unroll
+    for (int i = 0; i < G; ++i)
+      {
+        const R be = B12 * eta[i];
+        fce[i]     = be * eta[i] - be;
+      }
+    const R fee0 = B12 * ((R(1) - c) + s2), fee1 = p.B * (R(24) * c - R(48)), fee2 = p.B * R(24);
 
     // 1) c row (generic.h:120-134)
     {
@@ -235,7 +246,7 @@ namespace sint
       R v = p.walg * dmu - fcc * dc;
 #pragma unroll
       for (int i = 0; i < G; ++i)
-        v -= B12 * eta[i] * (eta[i] - R(1)) * deta[i];
+        v -= fce[i] * deta[i];
       pstore<DIM>(P, DIM + 1, q, cell, v);
     }
     // 3) eta row values (generic.h:150-163, free_energy.h:233-252)
@@ -249,11 +260,10 @@ namespace sint
       for (int i = 0; i < G; ++i)
         {
           const R e   = eta[i];
-          const R fce = B12 * e * (e - R(1));
-          const R fee = p.B * (R(12) - R(12) * c + R(2) * e * (R(12) * c - R(24)) + R(24) * (e * e) + R(12) * s2);
-          R       v   = deta[i] * p.w0 + p.L * (fce * dc + fee * deta[i]);
+          const R fee = fee0 + e * (fee1 + fee2 * e);
+          R       v   = deta[i] * p.w0 + p.L * (fce[i] * dc + fee * deta[i]);
           if constexpr (G > 1)
-            v += cL24B * e * (S - e * deta[i]);
+            v += (cL24B * e) * (S - e * deta[i]);
           pstore<DIM>(P, DIM + 2 + i, q, cell, v);
         }
     }

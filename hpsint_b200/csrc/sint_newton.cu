@@ -5,7 +5,7 @@
 //   NewtonSolverSolverControl      solvers_nonlinear.h:37-156 (convergence test)
 //   TimeMarchingImplicit lambdas   time_integration/time_marching.h:129-241
 //   SolverGMRESWrapper             lac/solvers_linear.h:57-117 -> deal.II SolverGMRES
-//                                  (left preconditioning, classical Gram-Schmidt,
+//                                  (left preconditioning -- right as an option --, classical Gram-Schmidt,
 //                                  ReductionControl(l_max_iter, l_abs_tol, l_rel_tol))
 //
 // Mixed precision (inner_precision == 32): the Newton residual, update and
@@ -55,11 +55,13 @@ namespace sint
       const uint16_t *mask  = nullptr; // cell masks the captured kernels read (nullptr: no cut-off)
       AdvData         adv   = {};      // advection tables the captured kernels read (none: null pointers)
       int             periodic = 0;    // periodic directions of the captured kernels
+      int             variant  = 0;    // bit 0: right preconditioning, bit 1: Gauss-Seidel CH block
       int             nodes = 0;
     } graphs[MAX_MULTIDOT];
-    // [FP32 Krylov vectors][grain cut-off][advection]: one eager solve with
-    // this kernel set has run (lazy kernel set-up is done outside any capture)
-    bool warm[2][2][2] = {};
+    // [FP32 Krylov vectors][grain cut-off][advection][variant]: one eager
+    // solve with this kernel set has run (lazy kernel set-up is done outside
+    // any capture)
+    bool warm[2][2][2][4] = {};
   };
 
   int free_workspace(Ctx *c)
@@ -291,6 +293,13 @@ namespace sint
   // converges.  An iteration enqueued past convergence only writes basis
   // vector j + 2 and Hessenberg column j + 1, which the solution update
   // (columns 0..j) never reads.
+  // Kernel-sequence variant of an Arnoldi iteration: bit 0 = right
+  // preconditioning, bit 1 = the Gauss-Seidel Cahn-Hilliard block.
+  static int gmres_variant(const Ctx *c, const sint_newton_params &prm)
+  {
+    return (prm.right_preconditioning ? 1 : 0) | (c->has_ch ? 2 : 0);
+  }
+
   template <typename R>
   static int gmres_body(Ctx *c, const sint_newton_params &prm, cudaStream_t s, int *its_out)
   {
@@ -316,10 +325,14 @@ namespace sint
         return cuda_fail(e, "GMRES: reset");
     }
 
+    const bool right   = prm.right_preconditioning != 0;
+    const int  variant = gmres_variant(c, prm);
     auto enqueue_kernels = [&](int j) -> int {
       R  *vj = V + (long long)j * n;
       int r;
-      if ((r = jvp<R>(c, t, vj, s)) || (r = prec<R>(c, w, t, s)) ||
+      // left: w = P^-1 J v_j; right: w = J P^-1 v_j
+      if ((right ? ((r = prec<R>(c, t, vj, s)) || (r = jvp<R>(c, w, t, s)))
+                 : ((r = jvp<R>(c, t, vj, s)) || (r = prec<R>(c, w, t, s)))) ||
           (r = multidot<R>(c, n, w, V, n, j + 1, ws->d_s, s, live)) ||
           (r = multiaxpy_norm2<R>(c, n, w, V, n, j + 1, ws->d_s, ws->d_s + MAX_MULTIDOT, s, live)))
         return r;
@@ -343,13 +356,14 @@ namespace sint
     auto enqueue = [&](int j) -> int {
       int r = SINT_OK;
       const AdvData adv = c->adv ? c->adv_view : AdvData();
-      if (!ws->warm[sizeof(R) == 4][c->cut][c->adv])
+      if (!ws->warm[sizeof(R) == 4][c->cut][c->adv][variant])
         r = enqueue_kernels(j);
       else
         {
           auto &g = ws->graphs[j];
           if (!g.exec || std::memcmp(&g.key, &c->phys, sizeof(Phys)) != 0 || g.mask != active_mask(c) ||
-              std::memcmp(&g.adv, &adv, sizeof(AdvData)) != 0 || g.periodic != c->grid.periodic)
+              std::memcmp(&g.adv, &adv, sizeof(AdvData)) != 0 || g.periodic != c->grid.periodic ||
+              g.variant != variant)
             {
               cudaGraph_t       graph = nullptr;
               const long long   n0    = sint_kernel_launch_count();
@@ -391,6 +405,7 @@ namespace sint
               g.mask  = active_mask(c);
               g.adv   = adv;
               g.periodic = c->grid.periodic;
+              g.variant  = variant;
               g.nodes = int(nn);
             }
           const cudaError_t e = cudaGraphLaunch(g.exec, s);
@@ -408,15 +423,16 @@ namespace sint
       return rc;
     for (;;)
       {
-        // w = P^-1 (b - J x)
+        // left: w = P^-1 (b - J x); right: w = b - J x
         if (first)
           {
-            if ((rc = prec<R>(c, w, b, s)))
+            if ((rc = right ? axpby<R>(n, 1.0, b, 0.0, w, s, live) : prec<R>(c, w, b, s)))
               return rc;
           }
         else
           {
-            if ((rc = jvp<R>(c, t, x, s)) || (rc = axpby<R>(n, 1.0, b, -1.0, t, s, live)) || (rc = prec<R>(c, w, t, s)))
+            if ((rc = jvp<R>(c, t, x, s)) || (rc = axpby<R>(n, 1.0, b, -1.0, t, s, live)) ||
+                (rc = right ? axpby<R>(n, 1.0, t, 0.0, w, s, live) : prec<R>(c, w, t, s)))
               return rc;
           }
         if ((rc = multidot<R>(c, n, w, w, 0, 1, ws->d_s, s, live)) || (rc = fetch(ws, 1, s)))
@@ -515,7 +531,14 @@ namespace sint
           cudaError_t e = cudaMemcpyAsync(ws->d_y, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s);
           if (e != cudaSuccess)
             return cuda_fail(e, "GMRES: upload y");
-          if ((rc = lincomb<R>(n, x, V, n, k, ws->d_y, s, live)))
+          if (right)
+            {
+              // x += P^-1 (V y)
+              if ((rc = axpby<R>(n, 0.0, b, 0.0, t, s, live)) || (rc = lincomb<R>(n, t, V, n, k, ws->d_y, s, live)) ||
+                  (rc = prec<R>(c, w, t, s)) || (rc = axpby<R>(n, 1.0, w, 1.0, x, s, live)))
+                return rc;
+            }
+          else if ((rc = lincomb<R>(n, x, V, n, k, ws->d_y, s, live)))
             return rc;
           // y lives in a host vector that the next cycle overwrites
           if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
@@ -552,7 +575,7 @@ namespace sint
     if (e != cudaSuccess)
       return cuda_fail(e, "GMRES: join back");
     if (rc == SINT_OK)
-      ws->warm[sizeof(R) == 4][c->cut][c->adv] = true;
+      ws->warm[sizeof(R) == 4][c->cut][c->adv][gmres_variant(c, prm)] = true;
     return rc;
   }
 
@@ -587,6 +610,7 @@ void sint_newton_default_params(sint_newton_params *p)
   p->use_damping           = 1;
   p->reuse_preconditioner  = 1;
   p->inner_precision       = 64;
+  p->right_preconditioning = 0;
 }
 
 int sint_newton_clear(sint_ctx *c)

@@ -235,10 +235,12 @@ namespace sint
         const R k3       = -fs3 * inrm3;
         const R a2       = (fvv2 + dfs * R(1.001)) * dc;
         const R b2       = dfs * nc_gmu * dc;
+        // (fvv + fsurf) grad dmu - nc (fsurf nc.grad dmu) + a2 grad mu - nc b2
+        //   + k3 (nc.grad mu temp + nc grad mu.temp), the nc terms collected
+        const R al = fvv + fsurf, be = fsurf * nc_gdmu + b2 - k3 * gmu_temp, ga = k3 * nc_gmu;
 #pragma unroll
         for (int d = 0; d < DIM; ++d)
-          out[d] = (fvv + fsurf) * gdmu[d] - nc[d] * (fsurf * nc_gdmu) + a2 * gmu[d] - nc[d] * b2 +
-                   k3 * (nc_gmu * temp[d] + nc[d] * gmu_temp);
+          out[d] = al * gdmu[d] + a2 * gmu[d] - nc[d] * be + ga * temp[d];
         if constexpr (G > 1)
           {
             // 4) sum_{i>j} [ eta_i eta_j P_ij grad dmu + (eta_j deta_i + eta_i deta_j) P_ij grad mu ]
@@ -247,6 +249,18 @@ namespace sint
 #pragma unroll
             for (int d = 0; d < DIM; ++d)
               acc[d] = R(0);
+            // with many grains, d_ij . v = grad eta_i . v - grad eta_j . v from per-grain dots
+            constexpr bool PER_GRAIN = G >= 5;
+            R              ag[PER_GRAIN ? G : 1], bg[PER_GRAIN ? G : 1];
+            if constexpr (PER_GRAIN)
+              {
+#pragma unroll
+                for (int i = 0; i < G; ++i)
+                  {
+                    ag[i] = dotv<DIM>(geta[i], gdmu);
+                    bg[i] = dotv<DIM>(geta[i], gmu);
+                  }
+              }
 #pragma unroll
             for (int i = 0; i < G; ++i)
 #pragma unroll
@@ -263,7 +277,18 @@ namespace sint
                   const R p2 = eta[j] * deta[i] + eta[i] * deta[j];
                   s1 += p1;
                   s2 += p2;
-                  const R t = f * (p1 * dotv<DIM>(dd, gdmu) + p2 * dotv<DIM>(dd, gmu));
+                  R da, db;
+                  if constexpr (PER_GRAIN)
+                    {
+                      da = ag[i] - ag[j];
+                      db = bg[i] - bg[j];
+                    }
+                  else
+                    {
+                      da = dotv<DIM>(dd, gdmu);
+                      db = dotv<DIM>(dd, gmu);
+                    }
+                  const R t = f * (p1 * da + p2 * db);
 #pragma unroll
                   for (int d = 0; d < DIM; ++d)
                     acc[d] -= t * dd[d];

@@ -179,6 +179,15 @@ class SinteringOperatorGeneric:
                 "sint_set_component_mask")
         self.cut_off_tolerance = tol
 
+    def set_preconditioner_type(self, block_0):
+        """Block 0 of the block preconditioner: "block_jacobi" (2x2 node
+        blocks, default) or "ch_gauss_seidel" (the assembled Cahn-Hilliard
+        block by multicolour symmetric Gauss-Seidel); takes effect at the next
+        preconditioner set-up."""
+        kind = BlockPreconditioner2.BLOCK0[block_0]
+        L.check(L.lib().sint_set_preconditioner_type(self._h, kind), "sint_set_preconditioner_type")
+        self.preconditioner_type = block_0
+
     def set_preconditioner_cut_off(self, on):
         """Build the block preconditioner with the grain cut-off too (the
         reference's assembly, preconditioners.h:787-817) instead of from the
@@ -349,10 +358,19 @@ class SinteringOperatorGeneric:
 
 
 class BlockPreconditioner2:
-    """z = P^-1 r with CH 2x2 node-block Jacobi and AC point Jacobi (FP64 and FP32)."""
+    """z = P^-1 r: the Cahn-Hilliard block by 2x2 node-block Jacobi
+    (block_0="block_jacobi") or by a multicolour symmetric Gauss-Seidel sweep
+    pair on the assembled Cahn-Hilliard matrix (block_0="ch_gauss_seidel",
+    in place of the reference's ILU); the grains by their inverse diagonal.
+    FP64 and FP32.  The block-0 type is a property of the operator context
+    (the device Newton solver uses the same)."""
 
-    def __init__(self, op: SinteringOperatorGeneric):
+    BLOCK0 = {"block_jacobi": 0, "ch_gauss_seidel": 1}
+
+    def __init__(self, op: SinteringOperatorGeneric, block_0=None):
         self.op = op
+        if block_0 is not None:
+            op.set_preconditioner_type(block_0)
 
     def do_update(self):
         L.check(L.lib().sint_precond_setup(self.op._h, _stream()), "sint_precond_setup")
@@ -375,6 +393,14 @@ class BlockPreconditioner2:
         L.check(L.lib().sint_ch_blocks_f64(self.op._h, _ptr(out), _stream()), "sint_ch_blocks_f64")
         return out
 
+    def ch_matrix(self):
+        """The assembled Cahn-Hilliard block (block_0="ch_gauss_seidel"):
+        (3^dim, 4, ld) = 2x2 blocks per node row and neighbour."""
+        nk = 27 if self.op.mesh.dim == 3 else 9
+        out = torch.zeros((nk, 4, self.op.ld), dtype=torch.float64, device="cuda")
+        L.check(L.lib().sint_ch_matrix_f64(self.op._h, _ptr(out), _stream()), "sint_ch_matrix_f64")
+        return out
+
     def clear(self):
         pass
 
@@ -394,12 +420,13 @@ class NonLinearData:
     use_damping: bool = True
     reuse_preconditioner: bool = True
     inner_precision: int = 64
+    right_preconditioning: bool = False
 
     def to_c(self):
         return L.SintNewtonParams(self.nl_max_iter, self.nl_abs_tol, self.nl_rel_tol, self.l_max_iter,
                                   self.l_abs_tol, self.l_rel_tol, self.gmres_restart, self.threshold_newton_iter,
                                   self.threshold_linear_iter, int(self.use_damping), int(self.reuse_preconditioner),
-                                  self.inner_precision)
+                                  self.inner_precision, int(self.right_preconditioning))
 
 
 @dataclass

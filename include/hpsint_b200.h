@@ -163,6 +163,29 @@ int sint_jvp_f64_noalloc(const sint_mesh *mesh, const sint_params *params, doubl
  * identity. */
 int sint_precond_setup(sint_ctx *ctx, sint_stream_t stream);
 
+/* Block 0 of the preconditioner (BlockPreconditioner2Data::block_0,
+ * preconditioner_parameters.h; default "ILU" in the reference):
+ *   0  the 2x2 node-block Jacobi above (this library's default);
+ *   1  the assembled Cahn-Hilliard block (OperatorCahnHilliard through
+ *      MyMatrixFreeTools::compute_matrix, matrix_free/tools.h:29-175: 2x2
+ *      blocks of every node row for its 3^dim neighbours) applied by one
+ *      symmetric Gauss-Seidel sweep pair in multicolour order (nodes coloured
+ *      by index parity), the GPU-parallel stand-in for the reference's ILU(0)
+ *      (lac/preconditioners.h:607-1088).  The grain block keeps the inverse
+ *      diagonal.  Not available with periodic constraints (set-up returns
+ *      SINT_ERR_ARG).  Pairs best with right-preconditioned GMRES
+ *      (sint_newton_params.right_preconditioning): with left preconditioning
+ *      GMRES stops on a residual dominated by the Cahn-Hilliard rows.
+ * Takes effect at the next sint_precond_setup; type 1 allocates the matrix
+ * (3^dim x 4 FP64 + FP32 values per node) at its first set-up. */
+int sint_set_preconditioner_type(sint_ctx *ctx, int type);
+
+/* The assembled Cahn-Hilliard block of preconditioner type 1: 3^dim x 4
+ * blocks of block_stride (device), A[(k * 4 + e) * block_stride + n] = entry e
+ * (J_cc, J_c,mu, J_mu,c, J_mu,mu) of node n's row for its neighbour k =
+ * (dx + 1) + 3 (dy + 1) (+ 9 (dz + 1)).  Requires sint_precond_setup first. */
+int sint_ch_matrix_f64(sint_ctx *ctx, double *A, sint_stream_t stream);
+
 /* BlockPreconditioner2::vmult (preconditioners.h:1222-1258): z = P^-1 r. */
 int sint_precond_apply_f64(sint_ctx *ctx, double *z, const double *r, sint_stream_t stream);
 int sint_precond_apply_f32(sint_ctx *ctx, float *z, const float *r, sint_stream_t stream);
@@ -404,6 +427,10 @@ typedef struct
   int    inner_precision;      /* 64: FP64 GMRES/Jacobian/preconditioner,
                                   32: FP32 Arnoldi vectors, Jacobian and
                                   preconditioner with FP64 dots and norms */
+  int    right_preconditioning;/* 0: left preconditioning (deal.II SolverGMRES's
+                                  default, as the reference); 1: right
+                                  preconditioning, J P^-1 y = b, x = P^-1 y:
+                                  GMRES stops on the true residual */
 } sint_newton_params;
 
 typedef struct

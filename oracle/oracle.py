@@ -65,6 +65,9 @@ def lib():
                                          _c_int]
         L.oracle_ch_blocks.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(Advection), P(_c_double),
                                        _c_int]
+        L.oracle_ch_matrix.argtypes = [P(Mesh), P(Params), P(Time), P(_c_double), U16, P(Advection), P(_c_double),
+                                       _c_int]
+        L.oracle_ch_sgs.argtypes = [P(Mesh), P(_c_double), P(_c_double), P(_c_double)]
         L.oracle_grain_mask.argtypes = [P(Mesh), P(Params), P(_c_double), _c_double, U16]
         L.oracle_grain_segments.argtypes = [P(Mesh), P(_c_double), _c_double, P(_c_int), P(_c_int)]
         L.oracle_segment_properties.argtypes = [P(Mesh), P(_c_double), P(_c_double), P(_c_int), _c_int,
@@ -228,6 +231,29 @@ def ch_blocks(mesh, params, time, lin, threads=0, mask=None, advection=None):
     _check(lib().oracle_ch_blocks(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
                                   mp, ap, _dptr(b), threads or os.cpu_count()), "ch_blocks")
     return b
+
+
+def ch_matrix(mesh, params, time, lin, threads=0, mask=None, advection=None):
+    """Assembled CH block, (3^dim, 4, N): 2x2 blocks per node row and neighbour."""
+    C, N = params.n_grains + 2, n_nodes(mesh)
+    NK = 27 if mesh.dim == 3 else 9
+    lin = np.ascontiguousarray(lin, dtype=np.float64).reshape(C, N)
+    A = np.zeros((NK, 4, N))
+    keep, mp = _mptr(mask, mesh)
+    keep_a, ap = _adv(advection, mesh)
+    _check(lib().oracle_ch_matrix(ctypes.byref(mesh), ctypes.byref(params), ctypes.byref(time), _dptr(lin),
+                                  mp, ap, _dptr(A), threads or os.cpu_count()), "ch_matrix")
+    return A
+
+
+def ch_sgs(mesh, A, r):
+    """Multicolour symmetric Gauss-Seidel of the assembled CH block applied to r (2, N)."""
+    N = n_nodes(mesh)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    r = np.ascontiguousarray(r, dtype=np.float64).reshape(2, N)
+    z = np.zeros((2, N))
+    _check(lib().oracle_ch_sgs(ctypes.byref(mesh), _dptr(A), _dptr(r), _dptr(z)), "ch_sgs")
+    return z
 
 
 def inverse_diagonal(d):

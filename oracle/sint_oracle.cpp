@@ -1016,6 +1016,181 @@ int oracle_ch_blocks(const oracle_mesh *m, const oracle_params *p, const oracle_
   return 0;
 }
 
+// Assembled Cahn-Hilliard block of the tangent, the matrix hpsint builds for
+// its matrix-based CH preconditioner (MyMatrixFreeTools::compute_matrix,
+// matrix_free/tools.h:29-175, on OperatorCahnHilliard::do_vmult_kernel,
+// sintering/preconditioners.h:85-169, set up by BlockPreconditioner2::
+// do_update, preconditioners.h:1260-1283).  Stored by node row as 2x2 blocks
+// for each of the 3^dim neighbours: A[(k * 4 + e) * N + n] with neighbour
+// k = (dx + 1) + 3 (dy + 1) (+ 9 (dz + 1)) of node n and entry e = 0 J_cc,
+// 1 J_c,mu, 2 J_mu,c, 3 J_mu,mu (row = tested equation, column = unknown).
+// The trial functions of the columns enter exactly as in oracle_ch_blocks,
+// whose values are the k = centre blocks.
+int oracle_ch_matrix(const oracle_mesh *m, const oracle_params *p, const oracle_time *t, const double *lin,
+                     const uint16_t *mask, const oracle_advection *adv, double *A, int n_threads)
+{
+  if (int e = check_args(m, p))
+    return e;
+  const Geometry geo(*m);
+  const Mobility mob = make_mobility(m, p);
+  const int      nq  = geo.nq, NK = geo.dim == 3 ? 27 : 9;
+  const int64_t  N   = geo.n_nodes;
+  std::memset(A, 0, sizeof(double) * NK * 4 * N);
+  coloured_cell_loop(geo, n_threads, [&](int i, int j, int k) {
+    int       blk[MAXC];
+    const int G = cell_blocks(geo, mask, p->n_grains, i, j, k, blk), C = G + 2;
+    double    ll[MAXC][8], lval[MAXC][8];
+    V3        lgrad[MAXC][8];
+    for (int l = 0; l < nq; ++l)
+      for (int b = 0; b < C; ++b)
+        ll[b][l] = lin[blk[b] * N + geo.node(i, j, k, l)];
+    for (int b = 0; b < C; ++b)
+      evaluate(geo, ll[b], lval[b], lgrad[b]);
+    for (int l = 0; l < nq; ++l)
+      for (int mm = 0; mm < nq; ++mm)
+        {
+          double J[4] = {0, 0, 0, 0};
+          for (int q = 0; q < nq; ++q)
+            {
+              double lv[MAXC];
+              V3     lg[MAXC];
+              for (int b = 0; b < C; ++b)
+                {
+                  lv[b] = lval[b][q];
+                  lg[b] = lgrad[b][q];
+                }
+              const double         c = lv[0];
+              const V3            &c_grad = lg[0], &mu_grad = lg[1];
+              const FreeEnergyEval fe(p->A, p->B, lv, G);
+              const double         phi = geo.shape[q][l], psi = geo.shape[q][mm];
+              const V3 dphi{{geo.dshape[q][l][0], geo.dshape[q][l][1], geo.dshape[q][l][2]}};
+              const V3 dpsi{{geo.dshape[q][mm][0], geo.dshape[q][mm][1], geo.dshape[q][mm][2]}};
+              // unknown c: value = psi, gradient = dpsi (mu = 0)
+              {
+                const double vr0 = psi * t->w0;
+                const double vr1 = -fe.d2f_dc2() * psi;
+                V3 gr0 = mul(mob.dM_dc(c, c_grad), mu_grad) * psi + mul(mob.dM_dgrad_c(c, c_grad, mu_grad), dpsi);
+                const V3 gr1 = (-p->kappa_c) * dpsi;
+                for (int ig = 0; ig < G; ++ig)
+                  {
+                    V3 vel;
+                    if (advection_velocity(adv, geo, blk[2 + ig] - 2, i, j, k, q, vel))
+                      gr0 = gr0 - vel * psi;
+                  }
+                J[0] += geo.JxW * (vr0 * phi + dot(gr0, dphi));
+                J[2] += geo.JxW * (vr1 * phi + dot(gr1, dphi));
+              }
+              // unknown mu: value = psi, gradient = dpsi (c = 0)
+              {
+                const double vr1 = psi * t->w_alg;
+                const V3     gr0 = mob.apply_M(c, lv + 2, G, c_grad, lg + 2, dpsi);
+                J[1] += geo.JxW * dot(gr0, dphi);
+                J[3] += geo.JxW * (vr1 * phi);
+              }
+            }
+          const int dx = (mm & 1) - (l & 1), dy = ((mm >> 1) & 1) - ((l >> 1) & 1),
+                    dz = geo.dim == 3 ? ((mm >> 2) & 1) - ((l >> 2) & 1) : 0;
+          const int     kk = (dx + 1) + 3 * (dy + 1) + (geo.dim == 3 ? 9 * (dz + 1) : 0);
+          const int64_t gi = geo.node(i, j, k, l);
+          for (int e = 0; e < 4; ++e)
+            A[(int64_t(kk) * 4 + e) * N + gi] += J[e];
+        }
+  });
+  return 0;
+}
+
+namespace
+{
+  // 2x2 inverse of a node's centre block, guarded as the block-Jacobi
+  // preconditioner's: a singular block falls back to the guarded point
+  // inverse of its diagonal (operator_base.h:386-388).
+  inline void invert_2x2(double a, double b, double c, double d, double inv[4])
+  {
+    const double det   = a * d - b * c;
+    const double scale = std::fabs(a * d) + std::fabs(b * c);
+    if (det != 0.0 && std::isfinite(det) && std::fabs(det) > 1e-14 * scale)
+      {
+        inv[0] = d / det;
+        inv[1] = -b / det;
+        inv[2] = -c / det;
+        inv[3] = a / det;
+      }
+    else
+      {
+        inv[0] = std::fabs(a) > 1.0e-10 ? 1.0 / a : 1.0;
+        inv[3] = std::fabs(d) > 1.0e-10 ? 1.0 / d : 1.0;
+        inv[1] = inv[2] = 0.0;
+      }
+  }
+} // namespace
+
+// Symmetric Gauss-Seidel preconditioner of the assembled CH block in
+// multicolour order: z = M^-1 r with M = (D + L) D^-1 (D + U), where nodes are
+// ordered by colour (parity of the node index in each direction: 2^dim
+// colours, no two nodes of one colour share a cell) and D holds the 2x2
+// centre blocks.  Forward sweep, colours ascending:
+//   y_n = D_n^-1 (r_n - sum_{j, colour(j) < colour(n)} A_nj y_j),
+// backward sweep, colours descending from the second-last:
+//   z_n = y_n - D_n^-1 sum_{j, colour(j) > colour(n)} A_nj z_j.
+// Neighbours are summed in the order k = 0 .. 3^dim - 1.  r and z: 2 x N.
+int oracle_ch_sgs(const oracle_mesh *m, const double *A, const double *r, double *z)
+{
+  if (!m || !A || !r || !z)
+    return 1;
+  const Geometry geo(*m);
+  const int      NK = geo.dim == 3 ? 27 : 9, n_col = 1 << geo.dim;
+  const int64_t  N  = geo.n_nodes;
+  std::vector<double> y(2 * N);
+  auto colour = [&](int x, int yy, int zz) { return (x & 1) | ((yy & 1) << 1) | ((zz & 1) << 2); };
+  auto sweep  = [&](int col, bool forward) {
+    for (int kz = 0; kz < geo.nn[2]; ++kz)
+      for (int ky = 0; ky < geo.nn[1]; ++ky)
+        for (int kx = 0; kx < geo.nn[0]; ++kx)
+          {
+            if (colour(kx, ky, kz) != col)
+              continue;
+            const int64_t n = kx + int64_t(geo.nn[0]) * (ky + int64_t(geo.nn[1]) * kz);
+            double        s0 = 0.0, s1 = 0.0;
+            for (int k = 0; k < NK; ++k)
+              {
+                const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = geo.dim == 3 ? k / 9 - 1 : 0;
+                const int x = kx + dx, yy = ky + dy, zz = kz + dz;
+                if (x < 0 || yy < 0 || zz < 0 || x >= geo.nn[0] || yy >= geo.nn[1] || zz >= geo.nn[2])
+                  continue;
+                const int cj = colour(x, yy, zz);
+                if (forward ? !(cj < col) : !(cj > col))
+                  continue;
+                const int64_t j  = x + int64_t(geo.nn[0]) * (yy + int64_t(geo.nn[1]) * zz);
+                const double *v  = forward ? y.data() : z;
+                const double  v0 = v[j], v1 = v[N + j];
+                s0 += A[(int64_t(k) * 4 + 0) * N + n] * v0 + A[(int64_t(k) * 4 + 1) * N + n] * v1;
+                s1 += A[(int64_t(k) * 4 + 2) * N + n] * v0 + A[(int64_t(k) * 4 + 3) * N + n] * v1;
+              }
+            const int ctr = NK / 2;
+            double    inv[4];
+            invert_2x2(A[(int64_t(ctr) * 4 + 0) * N + n], A[(int64_t(ctr) * 4 + 1) * N + n],
+                       A[(int64_t(ctr) * 4 + 2) * N + n], A[(int64_t(ctr) * 4 + 3) * N + n], inv);
+            if (forward)
+              {
+                const double a0 = r[n] - s0, a1 = r[N + n] - s1;
+                y[n]            = inv[0] * a0 + inv[1] * a1;
+                y[N + n]        = inv[2] * a0 + inv[3] * a1;
+              }
+            else
+              {
+                z[n]     = y[n] - (inv[0] * s0 + inv[1] * s1);
+                z[N + n] = y[N + n] - (inv[2] * s0 + inv[3] * s1);
+              }
+          }
+  };
+  for (int col = 0; col < n_col; ++col)
+    sweep(col, true);
+  std::memcpy(z, y.data(), sizeof(double) * 2 * N);
+  for (int col = n_col - 2; col >= 0; --col)
+    sweep(col, false);
+  return 0;
+}
+
 // GrainTracker particle detection for one order parameter on one process:
 // run_flooding / detect_local_particle_groups
 // (grain_tracker/distributed_stitching.h:41-100, :441-480).  A cell belongs

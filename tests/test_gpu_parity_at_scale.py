@@ -57,6 +57,10 @@ def c4_crop():
 
 
 STATES = {"3d-c2-crop": (3, C2_CELLS, True, c2_crop), "2d-c4-crop": (2, C4_CELLS, False, c4_crop)}
+# grain cut-off tolerances: the 3D state carries U(-1e-3, 1e-3) noise on every
+# nodal value, so its tolerances sit above the noise (below it every cell keeps
+# every grain); the 2D state has no noise
+CUT_TOLS = {3: (5e-3, 5e-2), 2: (1e-5, 1e-2)}
 
 
 @pytest.fixture(scope="module", params=list(STATES))
@@ -139,9 +143,10 @@ def test_preconditioner_at_scale(state):
     assert block_rel_err(op.to_host(z), zref) <= 1e-12
 
 
-@pytest.mark.parametrize("tol", [1e-5, 1e-2])
-def test_cut_off_at_scale(state, tol):
+@pytest.mark.parametrize("which", [0, 1])
+def test_cut_off_at_scale(state, which):
     op, u, om, p = state["op"], state["u"], state["om"], state["p"]
+    tol = CUT_TOLS[state["dim"]][which]
     ud = op.to_device(u)
     op.set_component_mask(ud, tol)
     mask = O.grain_mask(om, p, u, tol)
@@ -191,8 +196,9 @@ def test_advection_at_scale(state):
     assert block_rel_err(op.to_host(r), O.residual(om, p, T, u, [old], 2, advection=adv)) <= 1e-12
     assert block_rel_err(op.to_host(j), O.jvp(om, p, T, u, src, advection=adv)) <= 1e-12
     # the same under the grain cut-off
-    op.set_component_mask(ud, 1e-5)
-    mask = O.grain_mask(om, p, u, 1e-5)
+    tol = CUT_TOLS[dim][0]
+    op.set_component_mask(ud, tol)
+    mask = O.grain_mask(om, p, u, tol)
     op.vmult(j, op.to_device(src))
     torch.cuda.synchronize()
     assert block_rel_err(op.to_host(j), O.jvp(om, p, T, u, src, mask=mask, advection=adv)) <= 1e-12
