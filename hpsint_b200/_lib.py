@@ -36,6 +36,10 @@ class SintAdvectionParams(ctypes.Structure):
                 ("mt", _c_double), ("mr", _c_double)]
 
 
+class SintResidualHooks(ctypes.Structure):
+    _fields_ = [("perturb", _c_void), ("perturb_scale", _c_double), ("subtract", _c_void), ("scale", _c_double)]
+
+
 class SintNewtonParams(ctypes.Structure):
     _fields_ = [("nl_max_iter", _c_int), ("nl_abs_tol", _c_double), ("nl_rel_tol", _c_double),
                 ("l_max_iter", _c_int), ("l_abs_tol", _c_double), ("l_rel_tol", _c_double),
@@ -62,6 +66,8 @@ SIGNATURES = {
     "sint_set_mobility": (_c_int, [_c_void, _c_double, _c_double, _c_double, _c_double, _c_double]),
     "sint_set_linearization_point": (_c_int, [_c_void, _c_void, _c_void]),
     "sint_residual_f64": (_c_int, [_c_void, _c_void, _c_void, P(_c_void), _c_int, _c_void]),
+    "sint_residual_f64_hooks": (_c_int, [_c_void, _c_void, _c_void, P(_c_void), _c_int, P(SintResidualHooks),
+                                         _c_void]),
     "sint_jvp_f64": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_jvp_f32": (_c_int, [_c_void, _c_void, _c_void, _c_void]),
     "sint_jvp_f64_noalloc": (_c_int, [P(SintMesh), P(SintParams), _c_double, _c_double, _c_void, _c_void, _c_void,

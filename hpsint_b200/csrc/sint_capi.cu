@@ -37,22 +37,35 @@ namespace sint
 
   template <int DIM, typename R>
   cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, const uint16_t *tile_mask,
-                             cudaStream_t s)
+                             cudaStream_t s, const ResidualHooks *epi)
   {
-    const long long nb = (g.N + 255) / 256;
-    combine_kernel<DIM, R>
-      <<<dim3((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u), 256, 0, s>>>(g, ncomp, partial, dst, tile_mask);
+    const long long nb   = (g.N + 255) / 256;
+    const bool      fin  = epi && epi->epilogue;
+    combine_kernel<DIM, R><<<dim3((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u), 256, 0, s>>>(
+      g, ncomp, partial, dst, tile_mask, fin ? epi->subtract : nullptr, fin ? epi->scale : 1.0, fin ? 1 : 0);
     count_launches(1);
     return cudaGetLastError();
   }
+
+  // dst = (dst - sub) * scale over the C blocks (the residual's epilogue hook
+  // on periodic meshes, after the slave rows are condensed)
+  __global__ void residual_epilogue_kernel(long long N, long long ld, int C, const double *__restrict__ sub,
+                                           double scale, double *__restrict__ dst)
+  {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N)
+      return;
+    for (int b = 0; b < C; ++b)
+      dst[b * ld + n] = (dst[b * ld + n] - (sub ? sub[b * ld + n] : 0.0)) * scale;
+  }
   template cudaError_t launch_combine<2, double>(int, const Grid &, const double *, double *, const uint16_t *,
-                                                 cudaStream_t);
+                                                cudaStream_t, const ResidualHooks *);
   template cudaError_t launch_combine<3, double>(int, const Grid &, const double *, double *, const uint16_t *,
-                                                 cudaStream_t);
+                                                cudaStream_t, const ResidualHooks *);
   template cudaError_t launch_combine<2, float>(int, const Grid &, const float *, float *, const uint16_t *,
-                                                cudaStream_t);
+                                                cudaStream_t, const ResidualHooks *);
   template cudaError_t launch_combine<3, float>(int, const Grid &, const float *, float *, const uint16_t *,
-                                                cudaStream_t);
+                                                cudaStream_t, const ResidualHooks *);
 
   // --- dispatch over (dim, mobility) ---------------------------------------
   template <typename R>
@@ -71,8 +84,8 @@ namespace sint
             : launch_jvp<2, false, R>(c->G, c->grid, c->phys, lin, src, dst, part, cut, adv, s);
     if (e != cudaSuccess)
       return e;
-    e = c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, active_tile_union(c), s)
-                         : launch_combine<2, R>(c->C, c->grid, part, dst, active_tile_union(c), s);
+    e = c->grid.dim == 3 ? launch_combine<3, R>(c->C, c->grid, part, dst, active_tile_union(c), s, nullptr)
+                         : launch_combine<2, R>(c->C, c->grid, part, dst, active_tile_union(c), s, nullptr);
     if (e != cudaSuccess)
       return e;
     return launch_periodic_condense<R>(c->grid, c->C, dst, src, 0, s);
@@ -81,26 +94,43 @@ namespace sint
   template cudaError_t dispatch_jvp<double>(const Ctx *, const double *, const double *, double *, cudaStream_t);
   template cudaError_t dispatch_jvp<float>(const Ctx *, const float *, const float *, float *, cudaStream_t);
 
+  // hooks: the residual's pre/post range operations in device form (nullptr
+  // for none).  The epilogue is fused into the stores and the combine step,
+  // except on periodic meshes, where it follows the condensation of the slave
+  // rows as one extra pass.
   static cudaError_t dispatch_residual(const Ctx *c, int wtd, const double *src, const double *const *hist,
-                                       double *dst, cudaStream_t s)
+                                       double *dst, cudaStream_t s, const ResidualHooks *hooks = nullptr)
   {
     const bool      t   = c->params.tensorial != 0;
     const CutTiles *cut = active_cut(c);
     const AdvData  *adv = active_adv(c);
+    Phys            ph  = c->phys;
+    const bool      epi_after = hooks && hooks->epilogue && c->grid.periodic;
+    if (hooks)
+      {
+        ph.hooks = *hooks;
+        if (epi_after)
+          ph.hooks.epilogue = 0;
+      }
     cudaError_t e;
     if (c->grid.dim == 3)
-      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s)
-            : launch_residual<3, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s);
+      e = t ? launch_residual<3, true>(c->G, wtd, c->grid, ph, src, hist, dst, c->partial, cut, adv, s)
+            : launch_residual<3, false>(c->G, wtd, c->grid, ph, src, hist, dst, c->partial, cut, adv, s);
     else
-      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s)
-            : launch_residual<2, false>(c->G, wtd, c->grid, c->phys, src, hist, dst, c->partial, cut, adv, s);
+      e = t ? launch_residual<2, true>(c->G, wtd, c->grid, ph, src, hist, dst, c->partial, cut, adv, s)
+            : launch_residual<2, false>(c->G, wtd, c->grid, ph, src, hist, dst, c->partial, cut, adv, s);
     if (e != cudaSuccess)
       return e;
-    e = c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s)
-                         : launch_combine<2, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s);
+    e = c->grid.dim == 3 ? launch_combine<3, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s, &ph.hooks)
+                         : launch_combine<2, double>(c->C, c->grid, c->partial, dst, active_tile_union(c), s, &ph.hooks);
     if (e != cudaSuccess)
       return e;
-    return launch_periodic_condense<double>(c->grid, c->C, dst, nullptr, 1, s);
+    if ((e = launch_periodic_condense<double>(c->grid, c->C, dst, nullptr, 1, s)) != cudaSuccess || !epi_after)
+      return e;
+    residual_epilogue_kernel<<<dim3((unsigned)((c->N + 255) / 256)), 256, 0, s>>>(c->N, c->ld, c->C, hooks->subtract,
+                                                                                   hooks->scale, dst);
+    count_launches(1);
+    return cudaGetLastError();
   }
 
   static cudaError_t dispatch_diag(const Ctx *c, double *dst, cudaStream_t s)
@@ -117,8 +147,8 @@ namespace sint
             : launch_diag<2, false>(c->G, c->grid, c->phys, c->lin64, dst, c->partial, m, adv, s);
     if (e != cudaSuccess)
       return e;
-    e = c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s)
-                         : launch_combine<2, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s);
+    e = c->grid.dim == 3 ? launch_combine<3, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s, nullptr)
+                         : launch_combine<2, double>(c->G + 4, c->grid, c->partial, dst, nullptr, s, nullptr);
     if (e != cudaSuccess)
       return e;
     return launch_periodic_condense<double>(c->grid, c->G + 4, dst, nullptr, 2, s);
@@ -509,6 +539,62 @@ int sint_residual_f64(sint_ctx *c, double *dst, const double *src, const double 
   const cudaError_t e = dispatch_residual(c, with_time_derivative, src, hist, dst, stream);
   if (e != cudaSuccess)
     return cuda_fail(e, "sint_residual_f64");
+  return SINT_OK;
+}
+
+int sint_residual_f64_hooks(sint_ctx *c, double *dst, const double *src, const double *const *hist,
+                            int with_time_derivative, const sint_residual_hooks *hooks, sint_stream_t stream)
+{
+  if (!hooks)
+    return sint_residual_f64(c, dst, src, hist, with_time_derivative, stream);
+  if (int e = check_ctx(c))
+    return e;
+  if (int e = check_vec(dst, "dst"))
+    return e;
+  if (int e = check_vec(src, "src"))
+    return e;
+  if ((hooks->perturb && check_vec(hooks->perturb, "hooks->perturb")) ||
+      (hooks->subtract && check_vec(hooks->subtract, "hooks->subtract")))
+    return SINT_ERR_ARG;
+  if (hooks->perturb == dst || (hooks->subtract == dst && hooks->subtract))
+    {
+      set_error("sint_residual_f64_hooks: dst must not alias the hook vectors");
+      return SINT_ERR_ARG;
+    }
+  if (hooks->perturb && c->adv_mech)
+    {
+      set_error("sint_residual_f64_hooks: a perturbed evaluation with the advection mechanism is not supported "
+                "(its forces would need the perturbed state); evaluate src + a x into a vector first");
+      return SINT_ERR_ARG;
+    }
+  if (with_time_derivative < 0 || with_time_derivative > 2)
+    {
+      set_error("sint_residual_f64_hooks: with_time_derivative must be 0, 1 or 2");
+      return SINT_ERR_ARG;
+    }
+  if (with_time_derivative == 2)
+    {
+      if (c->phys.order < 1 || !hist)
+        {
+          set_error("sint_residual_f64_hooks: with_time_derivative == 2 needs time weights of order >= 1 and hist");
+          return SINT_ERR_ARG;
+        }
+      for (int i = 0; i < c->phys.order; ++i)
+        if (int e = check_vec(hist[i], "hist[i]"))
+          return e;
+    }
+  if (c->adv_mech)
+    if (int rc = advection_update(c, src, stream))
+      return rc;
+  ResidualHooks h;
+  h.perturb       = hooks->perturb;
+  h.perturb_scale = hooks->perturb ? hooks->perturb_scale : 0.0;
+  h.subtract      = hooks->subtract;
+  h.scale         = hooks->scale;
+  h.epilogue      = (hooks->subtract || hooks->scale != 1.0) ? 1 : 0;
+  const cudaError_t e = dispatch_residual(c, with_time_derivative, src, hist, dst, stream, &h);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "sint_residual_f64_hooks");
   return SINT_OK;
 }
 

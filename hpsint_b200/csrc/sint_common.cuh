@@ -120,7 +120,24 @@ namespace sint
     return g.kxf[x];
   }
 
-  // Point-wise model parameters (FP64 on the host, cast per kernel).
+  // Device form of the residual's range hooks (pre_operation /
+  // post_operation of evaluate_nonlinear_residual,
+  // operator_sintering_generic.h:393-401), as the Jacobian-free operator uses
+  // them (lac/jacobian_operator.h:160-232): the residual is evaluated at
+  // src + perturb_scale * perturb (formed while the node boxes are staged, src
+  // is never modified), and with `epilogue` the result is stored as
+  // (R - subtract) * scale (fused into the stores and the combine step).
+  struct ResidualHooks
+  {
+    const double *perturb       = nullptr;
+    double        perturb_scale = 0.0;
+    const double *subtract      = nullptr; // may be null: (R - 0) * scale
+    double        scale         = 1.0;
+    int           epilogue      = 0;
+  };
+
+  // Point-wise model parameters (FP64 on the host, cast per kernel), and the
+  // residual hooks of one evaluation (left empty everywhere else).
   struct Phys
   {
     double A, B, kappa_c, kappa_p;
@@ -128,6 +145,7 @@ namespace sint
     double w0, w_alg;
     double w_hist[4];
     int    order;
+    ResidualHooks hooks;
   };
 
   template <typename R>
@@ -256,14 +274,25 @@ namespace sint
   // With `mapped`, box component b is component comp_of(b, gl) of src.
   template <int DIM, typename R, typename S>
   __device__ __forceinline__ void load_box(R *s, const S *__restrict__ src, int ncomp, const Grid &g,
-                                           const BoxNode<DIM> &bn, unsigned long long gl = 0, bool mapped = false)
+                                           const BoxNode<DIM> &bn, unsigned long long gl = 0, bool mapped = false,
+                                           const S *__restrict__ perturb = nullptr, S perturb_scale = S(0))
   {
     using T = Tile<DIM>;
     if (!bn.active)
       return;
     const S *p = src + bn.lidx;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
-      s[comp * T::BOX + bn.b] = bn.inside ? R(p[(mapped ? comp_of(comp, gl) : comp) * g.ld]) : R(0);
+      {
+        R v = R(0);
+        if (bn.inside)
+          {
+            const long long off = (mapped ? comp_of(comp, gl) : comp) * g.ld;
+            v                   = R(p[off]);
+            if (perturb) // the residual's perturbation hook: src + a x
+              v = R(p[off] + perturb_scale * perturb[bn.lidx + off]);
+          }
+        s[comp * T::BOX + bn.b] = v;
+      }
   }
 
   // Asynchronous global->shared copies (cp.async, sm_80+): the node box of the
@@ -533,11 +562,13 @@ namespace sint
   // c_all components; the owned nodes of the grains absent from the tile
   // (bit clear in tmask) are written as zero, their partial slots are left
   // alone (the combine step skips them).
+  // With `epi` (the residual's epilogue hook) the owned nodes are stored as
+  // (sum - sub) * scale; the partials stay raw (the combine step applies it).
   template <int DIM, typename R>
   __device__ __forceinline__ void sum_and_store(const R *s_con, int ncomp, const Grid &g, const TileCoord &tc,
                                                 const BoxNode<DIM> &bn, R *__restrict__ dst, R *__restrict__ partial,
                                                 unsigned long long gl = 0, bool mapped = false, int c_all = 0,
-                                                unsigned tmask = 0)
+                                                unsigned tmask = 0, const ResidualHooks *epi = nullptr)
   {
     using T = Tile<DIM>;
     if (!bn.active || !bn.inside)
@@ -559,6 +590,14 @@ namespace sint
       owned = owned && (bn.bz > 0 || gk == 0) && (bn.bz < T::TZ || gk == g.n[2]);
     R *out = owned ? dst + bn.gidx : partial + tc.linear * (mapped ? c_all : ncomp) * (long long)T::BOX + bn.b;
     const long long ost = owned ? g.ld : (long long)T::BOX;
+    const bool      fin = owned && epi && epi->epilogue;
+    // (v - sub) * scale for the owned entry of component cc
+    auto finish = [&](R v, int cc) -> R {
+      if (!fin)
+        return v;
+      const R sub = epi->subtract ? R(epi->subtract[cc * g.ld + bn.gidx]) : R(0);
+      return (v - sub) * R(epi->scale);
+    };
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
       {
         const R *sc  = s_con + comp * T::CS;
@@ -567,12 +606,13 @@ namespace sint
         for (int l = 0; l < T::NQ; ++l)
           if (ok[l])
             sum += sc[src_off[l]];
-        out[(mapped ? comp_of(comp, gl) : comp) * ost] = sum;
+        const int cc = mapped ? comp_of(comp, gl) : comp;
+        out[cc * ost] = finish(sum, cc);
       }
     if (mapped && owned)
       for (int comp = 2 + bn.grp; comp < c_all; comp += T::NG)
         if (((tmask >> (comp - 2)) & 1u) == 0u)
-          out[comp * ost] = R(0);
+          out[comp * ost] = finish(R(0), comp);
   }
 
   // Second pass of the scatter: nodes on an interior tile face sum the
@@ -581,9 +621,13 @@ namespace sint
   // partial loads of different components are independent.
   // tile_mask (grain cut-off): a tile's partial of grain component 2 + b
   // exists only when bit b of tile_mask[tile] is set; nullptr = all exist.
+  // epi (the residual's epilogue hook, nullptr for none): the combined sums
+  // are stored as (sum - sub) * scale.
   template <int DIM, typename R>
   __global__ void __launch_bounds__(256) combine_kernel(const Grid g, int ncomp, const R *__restrict__ partial,
-                                                        R *__restrict__ dst, const uint16_t *__restrict__ tile_mask)
+                                                        R *__restrict__ dst, const uint16_t *__restrict__ tile_mask,
+                                                        const double *__restrict__ epi_sub = nullptr,
+                                                        double epi_scale = 1.0, int epi = 0)
   {
     using T              = Tile<DIM>;
     const long long idx  = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -658,6 +702,8 @@ namespace sint
         for (int k = 0; k < 8; ++k)
           if (has[k] && (cp < 2 || ((tm[k] >> (cp - 2)) & 1u) != 0u))
             sum += partial[slot[k] + cp * (long long)T::BOX];
+        if (epi)
+          sum = (sum - (epi_sub ? R(epi_sub[cp * g.ld + idx]) : R(0))) * R(epi_scale);
         dst[cp * g.ld + idx] = sum;
       }
   }

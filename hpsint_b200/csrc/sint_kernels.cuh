@@ -776,7 +776,7 @@ namespace sint
         const TileCoord          tc   = tile_coord_of<DIM>(g, tile);
         const BoxNode<DIM>       bn(g, tc);
         const unsigned m = CUT ? local_mask<G>(cell_mask<DIM>(ct.cell_mask, g, tc, threadIdx.x % T::CELLS), gl) : ~0u;
-        load_box<DIM>(s_u, src, C, g, bn, gl, CUT);
+        load_box<DIM>(s_u, src, C, g, bn, gl, CUT, ph.hooks.perturb, ph.hooks.perturb_scale);
         if constexpr (WTD == 2)
           {
             // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966); mu has no history
@@ -811,7 +811,7 @@ namespace sint
         __syncthreads();
         phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, s_u, K, m, A_vel, A_has);
         __syncthreads();
-        sum_and_store<DIM>(K, C, g, tc, bn, dst, partial, gl, CUT, ct.c_all, tm);
+        sum_and_store<DIM>(K, C, g, tc, bn, dst, partial, gl, CUT, ct.c_all, tm, &ph.hooks);
         __syncthreads();
       }
   }

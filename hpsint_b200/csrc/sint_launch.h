@@ -80,9 +80,10 @@ namespace sint
 
   // tile_mask: per tile id, the grains whose partials the tile wrote (grain
   // cut-off); nullptr = every component of every tile
+  // epi: the residual's epilogue hook ((sum - sub) * scale), nullptr for none
   template <int DIM, typename R>
   cudaError_t launch_combine(int ncomp, const Grid &g, const R *partial, R *dst, const uint16_t *tile_mask,
-                             cudaStream_t s);
+                             cudaStream_t s, const ResidualHooks *epi = nullptr);
 
   // Periodic constraints after the combine step: slave rows added to their
   // masters, then set to src (mode 0, J v), zero (mode 1, residual) or the

@@ -309,15 +309,32 @@ class SinteringOperatorGeneric:
             raise ValueError(f"cell_segments must be a contiguous int32 CUDA tensor of {self.params.n_grains} x "
                              f"{n_cells} ids")
 
-    def evaluate_nonlinear_residual(self, dst, src, with_time_derivative=2, history=()):
+    def evaluate_nonlinear_residual(self, dst, src, with_time_derivative=2, history=(), perturb=None,
+                                    perturb_scale=0.0, subtract=None, scale=1.0):
+        """dst = R(src) (operator_sintering_generic.h:393-448).  The range
+        hooks of the reference's signature in device form: with `perturb`
+        the residual is evaluated at src + perturb_scale * perturb (src is
+        not modified), with `subtract` / `scale` it is stored as
+        scale * (R - subtract) -- the pre/post operations of the
+        Jacobian-free operator (lac/jacobian_operator.h:160-232), fused
+        into the cell loop and its stores."""
         self._check_vec(dst, torch.float64)
         self._check_vec(src, torch.float64)
         hist = list(history)
         for h in hist:
             self._check_vec(h, torch.float64)
         arr = (ctypes.c_void_p * max(1, len(hist)))(*[h.data_ptr() for h in hist])
-        L.check(L.lib().sint_residual_f64(self._h, _ptr(dst), _ptr(src), arr, int(with_time_derivative), _stream()),
-                "sint_residual_f64")
+        if perturb is None and subtract is None and scale == 1.0:
+            L.check(L.lib().sint_residual_f64(self._h, _ptr(dst), _ptr(src), arr, int(with_time_derivative),
+                                              _stream()), "sint_residual_f64")
+            return
+        for v in (perturb, subtract):
+            if v is not None:
+                self._check_vec(v, torch.float64)
+        hooks = L.SintResidualHooks(_ptr(perturb) if perturb is not None else None, float(perturb_scale),
+                                    _ptr(subtract) if subtract is not None else None, float(scale))
+        L.check(L.lib().sint_residual_f64_hooks(self._h, _ptr(dst), _ptr(src), arr, int(with_time_derivative),
+                                                ctypes.byref(hooks), _stream()), "sint_residual_f64_hooks")
 
     def vmult(self, dst, src):
         if src.dtype == torch.float32:

@@ -117,6 +117,34 @@ int sint_set_linearization_point(sint_ctx *ctx, const double *u, sint_stream_t s
 int sint_residual_f64(sint_ctx *ctx, double *dst, const double *src, const double *const *hist,
                       int with_time_derivative, sint_stream_t stream);
 
+/* The residual's range hooks in device form.  evaluate_nonlinear_residual
+ * (operator_sintering_generic.h:393-401) takes pre_operation and
+ * post_operation callbacks that the cell loop calls on ranges of dst before
+ * and after writing them; the reference's Jacobian-free operator uses them to
+ * perturb the state and form a finite-difference quotient in the same pass
+ * (lac/jacobian_operator.h:160-232).  Host callbacks cannot run inside the
+ * device cell loop, so this entry point offers that use as data:
+ *   dst = scale * (R(src + perturb_scale * perturb) - subtract)
+ * with the perturbation formed while the node boxes are staged (src is not
+ * modified and no perturbed vector is stored) and the epilogue fused into
+ * the stores and the combine step (on periodic meshes it follows the
+ * condensation of the slave rows as one extra pass).  perturb and subtract
+ * may be NULL (no perturbation; subtract zero); perturb_scale = 0 and scale
+ * = 1 leave the plain residual.  The pre_operation's zeroing of dst is
+ * implied: every entry of dst is written.  Not with the advection mechanism
+ * and a perturbation (SINT_ERR_ARG: the forces would need the perturbed
+ * state).  dst must not alias perturb or subtract. */
+typedef struct
+{
+  const double *perturb;
+  double        perturb_scale;
+  const double *subtract;
+  double        scale;
+} sint_residual_hooks;
+
+int sint_residual_f64_hooks(sint_ctx *ctx, double *dst, const double *src, const double *const *hist,
+                            int with_time_derivative, const sint_residual_hooks *hooks, sint_stream_t stream);
+
 /* OperatorBase::vmult -> SinteringOperatorGeneric::vmult_internal
  * (operator_base.h:294-353, operator_sintering_generic.h:539-606):
  * dst = J(u_lin) src in FP64.  dst is overwritten. */
