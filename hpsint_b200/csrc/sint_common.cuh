@@ -268,6 +268,58 @@ namespace sint
     }
   };
 
+  // The same node-major view, fixed for a whole launch: computed once per
+  // thread, it serves every tile.  For an interior tile (one that touches no
+  // mesh boundary: o[d] > 0 and o[d] + T[d] < n[d]) every box node exists,
+  // none is a periodic slave, and a node is owned by the tile exactly when it
+  // lies on no face of the box, so the load and the store need only the
+  // tile's first node plus the thread's fixed offset.
+  template <int DIM>
+  struct NodePlan
+  {
+    int      b, grp; // box node, first component served
+    bool     active;
+    bool     inner;  // on no face of the box (owned in an interior tile)
+    int      off;    // node offset from the tile's first node: bx + nn0 (by + nn1 bz)
+    unsigned ok;     // bit l: the cell whose local node l this is lies in the tile
+    int      cbase;  // contribution offset of local node 0: bx + TX (by + TY bz)
+
+    __device__ __forceinline__ explicit NodePlan(const Grid &g)
+    {
+      using T = Tile<DIM>;
+      b       = threadIdx.x % T::BOX;
+      grp     = threadIdx.x / T::BOX;
+      active  = grp < T::NG;
+      const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
+      inner        = bx > 0 && bx < T::TX && by > 0 && by < T::TY && (DIM == 2 || (bz > 0 && bz < T::TZ));
+      off          = bx + g.nn[0] * (by + g.nn[1] * bz);
+      cbase        = bx + T::TX * (by + T::TY * bz);
+      ok           = 0u;
+#pragma unroll
+      for (int l = 0; l < T::NQ; ++l)
+        {
+          const int cx = bx - (l & 1), cy = by - ((l >> 1) & 1), cz = (DIM == 3) ? bz - ((l >> 2) & 1) : 0;
+          if (cx >= 0 && cx < T::TX && cy >= 0 && cy < T::TY && cz >= 0 && cz < T::TZ)
+            ok |= 1u << l;
+        }
+    }
+  };
+
+  // Whether tile tc touches no mesh boundary (the fast path of NodePlan).
+  template <int DIM>
+  __device__ __forceinline__ bool tile_interior(const Grid &g, const TileCoord &tc)
+  {
+    using T = Tile<DIM>;
+    return tc.o[0] > 0 && tc.o[0] + T::TX < g.n[0] && tc.o[1] > 0 && tc.o[1] + T::TY < g.n[1] &&
+           (DIM == 2 || (tc.o[2] > 0 && tc.o[2] + T::TZ < g.n[2]));
+  }
+
+  // Global index of the first node of tile tc.
+  __device__ __forceinline__ long long tile_node0(const Grid &g, const TileCoord &tc)
+  {
+    return node_index(g, tc.o[0], tc.o[1], tc.o[2]);
+  }
+
   // Stage the node box of `ncomp` components of `src` (block stride g.ld) in
   // shared memory, layout s[comp * BOX + box_node]; nodes outside the mesh
   // read as zero.
@@ -330,6 +382,21 @@ namespace sint
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
       cp_async_elem(s + comp * T::BOX + bn.b, bn.inside ? p + (mapped ? comp_of(comp, gl) : comp) * g.ld : src,
                     bn.inside);
+  }
+
+  // Interior-tile form of load_box_async: every box node exists and is read
+  // at node0 + the thread's fixed offset.
+  template <int DIM, typename R>
+  __device__ __forceinline__ void load_box_async_interior(R *s, const R *__restrict__ src, int ncomp, const Grid &g,
+                                                          const NodePlan<DIM> &np, long long node0,
+                                                          unsigned long long gl = 0, bool mapped = false)
+  {
+    using T = Tile<DIM>;
+    if (!np.active)
+      return;
+    const R *p = src + node0 + np.off;
+    for (int comp = np.grp; comp < ncomp; comp += T::NG)
+      cp_async_elem(s + comp * T::BOX + np.b, p + (mapped ? comp_of(comp, gl) : comp) * g.ld, true);
   }
 
   template <int DIM>
@@ -611,6 +678,48 @@ namespace sint
       }
     if (mapped && owned)
       for (int comp = 2 + bn.grp; comp < c_all; comp += T::NG)
+        if (((tmask >> (comp - 2)) & 1u) == 0u)
+          out[comp * ost] = finish(R(0), comp);
+  }
+
+  // Interior-tile form of sum_and_store: the owned nodes are the ones on no
+  // face of the box (np.inner), written at node0 + the fixed offset; the
+  // others go to the tile's partial slot.
+  template <int DIM, typename R>
+  __device__ __forceinline__ void sum_and_store_interior(const R *s_con, int ncomp, const Grid &g,
+                                                         long long tile_linear, const NodePlan<DIM> &np,
+                                                         long long node0, R *__restrict__ dst,
+                                                         R *__restrict__ partial, unsigned long long gl = 0,
+                                                         bool mapped = false, int c_all = 0, unsigned tmask = 0,
+                                                         const ResidualHooks *epi = nullptr)
+  {
+    using T = Tile<DIM>;
+    if (!np.active)
+      return;
+    const bool      owned = np.inner;
+    R              *out   = owned ? dst + node0 + np.off
+                                  : partial + tile_linear * (mapped ? c_all : ncomp) * (long long)T::BOX + np.b;
+    const long long ost   = owned ? g.ld : (long long)T::BOX;
+    const bool      fin   = owned && epi && epi->epilogue;
+    auto finish = [&](R v, int cc) -> R {
+      if (!fin)
+        return v;
+      const R sub = epi->subtract ? R(epi->subtract[cc * g.ld + node0 + np.off]) : R(0);
+      return (v - sub) * R(epi->scale);
+    };
+    for (int comp = np.grp; comp < ncomp; comp += T::NG)
+      {
+        const R *sc  = s_con + comp * T::CS + np.cbase;
+        R        sum = R(0);
+#pragma unroll
+        for (int l = 0; l < T::NQ; ++l)
+          if ((np.ok >> l) & 1u)
+            sum += sc[l * T::CP - ((l & 1) + T::TX * ((l >> 1) & 1) + T::TX * T::TY * ((l >> 2) & 1))];
+        const int cc  = mapped ? comp_of(comp, gl) : comp;
+        out[cc * ost] = finish(sum, cc);
+      }
+    if (mapped && owned)
+      for (int comp = 2 + np.grp; comp < c_all; comp += T::NG)
         if (((tmask >> (comp - 2)) & 1u) == 0u)
           out[comp * ost] = finish(R(0), comp);
   }

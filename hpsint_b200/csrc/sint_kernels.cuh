@@ -538,9 +538,20 @@ namespace sint
             cell_nodes<DIM>(stiff + (row == 1 ? 0 : row) * T::BOX, b0, u);
             cell_stiffness_add<DIM>(row == 1 ? -p.kc : p.L * p.kp, u, g, r);
           }
+        // a branch, not a select per value: in tiles inside the mesh every
+        // cell keeps its row
+        if (keep)
+          {
 #pragma unroll
-        for (int l = 0; l < NQ; ++l)
-          K[(row * NQ + l) * T::CP + cell] = keep ? r[l] : R(0);
+            for (int l = 0; l < NQ; ++l)
+              K[(row * NQ + l) * T::CP + cell] = r[l];
+          }
+        else
+          {
+#pragma unroll
+            for (int l = 0; l < NQ; ++l)
+              K[(row * NQ + l) * T::CP + cell] = R(0);
+          }
       }
   }
 
@@ -639,10 +650,26 @@ namespace sint
 
     const PhysR<R>           p(ph);
     const CellConsts<DIM, R> k(g);
+    const NodePlan<DIM>      np(g);
     const int                cell = threadIdx.x % T::CELLS;
     const long long          i0   = CUT ? (long long)ct.range[G] : 0;
     const long long          i1   = CUT ? (long long)ct.range[G + 1] : g.n_tiles;
     long long                idx  = i0 + blockIdx.x;
+    // node boxes of both inputs of tile tcx into buffer bb
+    auto prefetch = [&](R *bb, const TileCoord &tcx, unsigned long long glx) {
+      if (tile_interior<DIM>(g, tcx))
+        {
+          const long long n0 = tile_node0(g, tcx);
+          load_box_async_interior<DIM>(bb, lin, C, g, np, n0, glx, CUT);
+          load_box_async_interior<DIM>(bb + C * T::BOX, src, C, g, np, n0, glx, CUT);
+        }
+      else
+        {
+          const BoxNode<DIM> bn(g, tcx);
+          load_box_async<DIM>(bb, lin, C, g, bn, glx, CUT);
+          load_box_async<DIM>(bb + C * T::BOX, src, C, g, bn, glx, CUT);
+        }
+    };
     // current and next tile: id, grain list, union mask, this thread's cell mask
     long long          tile = 0, t_next = 0;
     unsigned long long gl = 0, gl_next = 0;
@@ -666,10 +693,8 @@ namespace sint
       tile = idx;
     if (idx < i1)
       {
-        const TileCoord    tc0 = tile_coord_of<DIM>(g, tile);
-        const BoxNode<DIM> bn(g, tc0);
-        load_box_async<DIM>(s_buf, lin, C, g, bn, gl, CUT);
-        load_box_async<DIM>(s_buf + C * T::BOX, src, C, g, bn, gl, CUT);
+        const TileCoord tc0 = tile_coord_of<DIM>(g, tile);
+        prefetch(s_buf, tc0, gl);
         if constexpr (CUT)
           m_glob = cell_mask<DIM>(ct.cell_mask, g, tc0, cell);
       }
@@ -683,11 +708,9 @@ namespace sint
         unsigned           tm_nn = 0;
         if (nidx < i1)
           {
-            const long long    next = CUT ? t_next : nidx;
-            const TileCoord    tcn  = tile_coord_of<DIM>(g, next);
-            const BoxNode<DIM> bnn(g, tcn);
-            load_box_async<DIM>(nb, lin, C, g, bnn, gl_next, CUT);
-            load_box_async<DIM>(nb + C * T::BOX, src, C, g, bnn, gl_next, CUT);
+            const long long next = CUT ? t_next : nidx;
+            const TileCoord tcn  = tile_coord_of<DIM>(g, next);
+            prefetch(nb, tcn, gl_next);
             if constexpr (CUT)
               {
                 m_glob_next = cell_mask<DIM>(ct.cell_mask, g, tcn, cell);
@@ -719,8 +742,14 @@ namespace sint
         __syncthreads();
         phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, cb + C * T::BOX, K, m, A_vel, A_has);
         __syncthreads();
-        sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
-        __syncthreads(); // K and this buffer are reused by the next iterations
+        if (tile_interior<DIM>(g, tc))
+          sum_and_store_interior<DIM>(K, C, g, tc.linear, np, tile_node0(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
+        else
+          sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
+        // No barrier here: the next tile's prefetch writes the other box
+        // buffer, whose last readers (this tile's phases 1 and 3) passed the
+        // barrier above, and K (aliasing F) is next written in phase 1, after
+        // the barrier that follows the next cp.async wait.
         if constexpr (CUT)
           {
             tile    = t_next;
@@ -766,6 +795,7 @@ namespace sint
 
     const PhysR<R>           p(ph);
     const CellConsts<DIM, R> k(g);
+    const NodePlan<DIM>      np(g);
     const long long          i0 = CUT ? (long long)ct.range[G] : 0;
     const long long          i1 = CUT ? (long long)ct.range[G + 1] : g.n_tiles;
     for (long long idx = i0 + blockIdx.x; idx < i1; idx += gridDim.x)
@@ -774,28 +804,42 @@ namespace sint
         const unsigned long long gl   = CUT ? ct.tile_grains[idx] : 0ull;
         const unsigned           tm   = CUT ? ct.tile_mask[idx] : 0u;
         const TileCoord          tc   = tile_coord_of<DIM>(g, tile);
-        const BoxNode<DIM>       bn(g, tc);
+        const bool               interior = tile_interior<DIM>(g, tc);
+        const long long          node0    = tile_node0(g, tc);
         const unsigned m = CUT ? local_mask<G>(cell_mask<DIM>(ct.cell_mask, g, tc, threadIdx.x % T::CELLS), gl) : ~0u;
-        load_box<DIM>(s_u, src, C, g, bn, gl, CUT, ph.hooks.perturb, ph.hooks.perturb_scale);
-        if constexpr (WTD == 2)
+        // this thread's box node: in an interior tile it exists and reads itself
+        bool      inside = true;
+        long long lidx   = node0 + np.off;
+        if (!interior)
           {
-            // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966); mu has no history
-            if (bn.active)
-              for (int comp = bn.grp; comp < C; comp += T::NG)
-                {
-                  R v = R(0);
-                  if (comp != 1 && bn.inside)
-                    {
-                      const long long off = (CUT ? comp_of(comp, gl) : comp) * g.ld + bn.lidx;
-                      v                   = h0[off] * ph.w_hist[0];
-                      if (ph.order > 1)
-                        v += h1[off] * ph.w_hist[1];
-                      if (ph.order > 2)
-                        v += h2[off] * ph.w_hist[2];
-                    }
-                  s_h[comp * T::BOX + bn.b] = v;
-                }
+            const BoxNode<DIM> bn(g, tc);
+            inside = bn.inside;
+            lidx   = bn.lidx;
           }
+        if (np.active)
+          for (int comp = np.grp; comp < C; comp += T::NG)
+            {
+              R v = R(0), hv = R(0);
+              if (inside)
+                {
+                  const long long off = (CUT ? comp_of(comp, gl) : comp) * g.ld + lidx;
+                  v                   = src[off];
+                  if (ph.hooks.perturb) // the residual's perturbation hook: src + a x
+                    v = src[off] + ph.hooks.perturb_scale * ph.hooks.perturb[off];
+                  // sum_i w_{i+1} u_old_i at the nodes (generic.h:947-966); mu has no history
+                  if (WTD == 2 && comp != 1)
+                    {
+                      hv = h0[off] * ph.w_hist[0];
+                      if (ph.order > 1)
+                        hv += h1[off] * ph.w_hist[1];
+                      if (ph.order > 2)
+                        hv += h2[off] * ph.w_hist[2];
+                    }
+                }
+              s_u[comp * T::BOX + np.b] = v;
+              if constexpr (WTD == 2)
+                s_h[comp * T::BOX + np.b] = hv;
+            }
         if constexpr (ADV)
           adv_stage<DIM, G, R, CUT>(adv, g, tc, gl, A_vel, A_has);
         __syncthreads();
@@ -811,8 +855,13 @@ namespace sint
         __syncthreads();
         phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, s_u, K, m, A_vel, A_has);
         __syncthreads();
-        sum_and_store<DIM>(K, C, g, tc, bn, dst, partial, gl, CUT, ct.c_all, tm, &ph.hooks);
-        __syncthreads();
+        if (interior)
+          sum_and_store_interior<DIM>(K, C, g, tc.linear, np, node0, dst, partial, gl, CUT, ct.c_all, tm, &ph.hooks);
+        else
+          sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, gl, CUT, ct.c_all, tm, &ph.hooks);
+        // no barrier: the next tile's staging writes the boxes, read last in
+        // phase 3 before the barrier above; K (aliasing F) is next written in
+        // phase 1, after the barrier that follows the staging
       }
   }
 

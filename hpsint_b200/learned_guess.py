@@ -387,6 +387,49 @@ class LinearPredictor:
         return self.guess
 
 
+class EulerPredictor:
+    """hpsint's "Euler" predictor (driver.h:2005-2011): the residual without
+    time terms R0(u_n) (evaluate_nonlinear_residual<0>), then
+    extrap = u_n - dt R0(u_n) (VectorType::sadd).  As in the reference it
+    acts from the second step on (t > 0)."""
+
+    def __init__(self, op: SinteringOperatorGeneric):
+        self.op = op
+        self.guess = None
+
+    def _euler(self, out, u, dt):
+        self.op.evaluate_nonlinear_residual(out, u, 0)
+        L.check(L.lib().sint_vec_sadd_f64(out.numel(), -dt, 1.0, _p(u), _p(out), _s()), "sint_vec_sadd_f64")
+
+    def __call__(self, history, dts, dt):
+        if len(history) < 2 or not dts:
+            return None
+        if self.guess is None:
+            self.guess = self.op.initialize_dof_vector()
+        self._euler(self.guess, history[0], dt)
+        return self.guess
+
+
+class MidpointPredictor(EulerPredictor):
+    """hpsint's "Midpoint" predictor (driver.h:2012-2023): midpoint =
+    u_n - dt/2 R0(u_n), extrap = u_n - dt R0(midpoint)."""
+
+    def __init__(self, op: SinteringOperatorGeneric):
+        super().__init__(op)
+        self.mid = None
+
+    def __call__(self, history, dts, dt):
+        if len(history) < 2 or not dts:
+            return None
+        if self.guess is None:
+            self.guess, self.mid = self.op.initialize_dof_vector(), self.op.initialize_dof_vector()
+        self._euler(self.mid, history[0], dt / 2.0)
+        self.op.evaluate_nonlinear_residual(self.guess, self.mid, 0)
+        L.check(L.lib().sint_vec_sadd_f64(self.guess.numel(), -dt, 1.0, _p(history[0]), _p(self.guess), _s()),
+                "sint_vec_sadd_f64")
+        return self.guess
+
+
 class LearnedPredictor:
     """Whole-mesh inference: features of (u_{n-1}, u_n, r) -> net -> guess
     u_n + r (u_n - u_{n-1}) + output / oscale.  FP32 network, FP64 guess.
@@ -454,6 +497,10 @@ ARMS = {
     "fp64_learned_safeguarded": (64, "learned_safeguarded", 0.0),
     "fp32_inner_plain": (32, None, 0.0),
     "fp32_inner_linear": (32, "linear", 0.0),
+    "fp64_euler": (64, "euler", 0.0),
+    "fp64_midpoint": (64, "midpoint", 0.0),
+    "fp32_inner_euler": (32, "euler", 0.0),
+    "fp32_inner_midpoint": (32, "midpoint", 0.0),
     "fp32_inner_learned": (32, "learned", 0.0),
     "fp32_inner_learned_safeguarded": (32, "learned_safeguarded", 0.0),
     "fp32_inner_linear_cut_off": (32, "linear", GRAIN_CUT_OFF),
@@ -496,7 +543,8 @@ def compare_arms(case, n_steps, net=None, norm=None, arms=None, warmup_steps=2):
     arms = list(arms or ARMS)
     if arms[0] != "fp64_plain":
         arms = ["fp64_plain"] + [a for a in arms if a != "fp64_plain"]
-    preds = {"linear": LinearPredictor(case.op)}
+    preds = {"linear": LinearPredictor(case.op), "euler": EulerPredictor(case.op),
+             "midpoint": MidpointPredictor(case.op)}
     if net is not None:
         preds["learned"] = LearnedPredictor(case.op, net, norm)
         preds["learned_safeguarded"] = LearnedPredictor(case.op, net, norm, safeguard=True)
