@@ -430,16 +430,17 @@ def solve_comparison(n_steps):
     """s/step of the metric's solve arms on a held-out 2D many-grain packing
     (512^2 cells, 100 circles, seed 1000, scalar mobility, Newton 1e-8): the
     plain FP64 solve (hpsint's method) fixes the time grid, the FP32-inner
-    arms replay it with the previous-solution, linear and safeguarded
-    learned guesses (the net trained by --workload learned2d on seeds 0..9,
-    hpsint_b200/weights/learned_guess_c4.npz), the last two also with the
+    arms replay it with the previous-solution guess, hpsint's Linear and
+    Euler predictors, and the learned guess raw and safeguarded (the net
+    trained by --workload learned2d on seeds 0..9,
+    hpsint_b200/weights/learned_guess_c4.npz); the last two arms add the
     grain cut-off (GrainCutOffTolerance 1e-5)."""
     from hpsint_b200 import learned_guess as LG
     wpath = os.path.join(ROOT, "hpsint_b200", "weights", "learned_guess_c4.npz")
     net, norm = LG.load_predictor(wpath)
     case = LG.make_case(1000)
-    arms = ["fp64_plain", "fp32_inner_plain", "fp32_inner_linear", "fp32_inner_learned_safeguarded",
-            "fp32_inner_linear_cut_off", "fp32_inner_learned_safeguarded_cut_off"]
+    arms = ["fp64_plain", "fp32_inner_plain", "fp32_inner_linear", "fp32_inner_euler", "fp32_inner_learned",
+            "fp32_inner_learned_safeguarded", "fp32_inner_linear_cut_off", "fp32_inner_learned_safeguarded_cut_off"]
     res = LG.compare_arms(case, n_steps, net, norm, arms=arms)
     plain = res["fp64_plain"]["s_per_step"]
     pick = lambda key: {a: res[a].get(key) for a in arms if a in res}

@@ -31,8 +31,8 @@ namespace sint
     // NCOEF = 2 dim^2 + dim + 1 + G (+ G dim velocities) coefficients per point, NOUT = G + 4 outputs
     const int nadv = adv ? G * dim : 0;
     if (dim == 3)
-      return (C * Tile<3>::BOX + (22 + G + nadv) * Tile<3>::THREADS + (G + 4) * Tile<3>::CS) * sizeof(double);
-    return (C * Tile<2>::BOX + (11 + G + nadv) * Tile<2>::THREADS + (G + 4) * Tile<2>::CS) * sizeof(double);
+      return (C * Tile<3>::BOXS + (22 + G + nadv) * Tile<3>::THREADS + (G + 4) * Tile<3>::CS) * sizeof(double);
+    return (C * Tile<2>::BOXS + (11 + G + nadv) * Tile<2>::THREADS + (G + 4) * Tile<2>::CS) * sizeof(double);
   }
 
   template <int DIM, typename R>

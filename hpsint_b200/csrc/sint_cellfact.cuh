@@ -71,7 +71,7 @@ namespace sint
     using T = Tile<DIM>;
 #pragma unroll
     for (int l = 0; l < (1 << DIM); ++l)
-      u[l] = s[b0 + (l & 1) + T::BX * ((l >> 1) & 1) + (DIM == 3 ? T::BX * T::BY * ((l >> 2) & 1) : 0)];
+      u[l] = s[b0 + (l & 1) + T::SY * ((l >> 1) & 1) + (DIM == 3 ? T::SZ * ((l >> 2) & 1) : 0)];
   }
 
   // Phase 1, value + gradient: writes F[(base + slot) * CELLS + cell] for the

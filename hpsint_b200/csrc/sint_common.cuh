@@ -39,6 +39,12 @@ namespace sint
     static constexpr int CELLS   = TX * TY * TZ;
     static constexpr int BX      = TX + 1, BY = TY + 1, BZ = TZ + 1;
     static constexpr int BOX     = BX * BY * BZ;
+    // storage of a node box in shared memory: node (bx, by, bz) at
+    // bx + SY by + SZ bz.  With these pitches the base nodes of a warp's 32
+    // cells (4 x 4 x 2) fall on every 8-byte bank pair exactly twice (FP64:
+    // two wavefronts, the minimum) and on 32 distinct 4-byte banks (FP32)
+    static constexpr int SY = 8, SZ = 44;
+    static constexpr int BOXS    = (BX - 1) + SY * (BY - 1) + SZ * (BZ - 1) + 1;
     static constexpr int THREADS = CELLS * NQ;
     // node contributions are parked as [comp][l][cell] with row pitch CP: the
     // +2 makes both the write (lane = cell * 8 + l) and the per-node read
@@ -56,6 +62,8 @@ namespace sint
     static constexpr int CELLS   = TX * TY;
     static constexpr int BX      = TX + 1, BY = TY + 1, BZ = 1;
     static constexpr int BOX     = BX * BY;
+    static constexpr int SY = BX, SZ = BOX; // dense storage
+    static constexpr int BOXS    = BOX;
     static constexpr int THREADS = CELLS * NQ;
     static constexpr int CP      = CELLS + 4;
     static constexpr int CS      = NQ * CP;
@@ -242,6 +250,7 @@ namespace sint
   struct BoxNode
   {
     int       b;      // box node index
+    int       sb;     // its place in the shared-memory box (pitches SY, SZ)
     int       grp;    // first component served
     int       bx, by, bz;
     bool      active; // thread serves a node
@@ -258,6 +267,7 @@ namespace sint
       bx      = b % T::BX;
       by      = (b / T::BX) % T::BY;
       bz      = b / (T::BX * T::BY);
+      sb      = bx + T::SY * by + T::SZ * bz;
       const int gi = tc.o[0] + bx, gj = tc.o[1] + by, gk = (DIM == 3) ? tc.o[2] + bz : 0;
       inside       = gi < g.nn[0] && gj < g.nn[1] && gk < g.nn[2];
       gidx         = inside ? node_index(g, gi, gj, gk) : 0;
@@ -278,6 +288,7 @@ namespace sint
   struct NodePlan
   {
     int      b, grp; // box node, first component served
+    int      sb;     // its place in the shared-memory box
     bool     active;
     bool     inner;  // on no face of the box (owned in an interior tile)
     int      off;    // node offset from the tile's first node: bx + nn0 (by + nn1 bz)
@@ -291,6 +302,7 @@ namespace sint
       grp     = threadIdx.x / T::BOX;
       active  = grp < T::NG;
       const int bx = b % T::BX, by = (b / T::BX) % T::BY, bz = b / (T::BX * T::BY);
+      sb           = bx + T::SY * by + T::SZ * bz;
       inner        = bx > 0 && bx < T::TX && by > 0 && by < T::TY && (DIM == 2 || (bz > 0 && bz < T::TZ));
       off          = bx + g.nn[0] * (by + g.nn[1] * bz);
       cbase        = bx + T::TX * (by + T::TY * bz);
@@ -321,7 +333,7 @@ namespace sint
   }
 
   // Stage the node box of `ncomp` components of `src` (block stride g.ld) in
-  // shared memory, layout s[comp * BOX + box_node]; nodes outside the mesh
+  // shared memory, layout s[comp * BOXS + sb]; nodes outside the mesh
   // read as zero.
   // With `mapped`, box component b is component comp_of(b, gl) of src.
   template <int DIM, typename R, typename S>
@@ -343,7 +355,7 @@ namespace sint
             if (perturb) // the residual's perturbation hook: src + a x
               v = R(p[off] + perturb_scale * perturb[bn.lidx + off]);
           }
-        s[comp * T::BOX + bn.b] = v;
+        s[comp * T::BOXS + bn.sb] = v;
       }
   }
 
@@ -369,7 +381,7 @@ namespace sint
   }
 
   // Issue the asynchronous load of `ncomp` components of `src` into the box
-  // buffer s (layout s[comp * BOX + box_node]).
+  // buffer s (layout s[comp * BOXS + sb]).
   template <int DIM, typename R>
   __device__ __forceinline__ void load_box_async(R *s, const R *__restrict__ src, int ncomp, const Grid &g,
                                                  const BoxNode<DIM> &bn, unsigned long long gl = 0,
@@ -380,7 +392,7 @@ namespace sint
       return;
     const R *p = bn.inside ? src + bn.lidx : src;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
-      cp_async_elem(s + comp * T::BOX + bn.b, bn.inside ? p + (mapped ? comp_of(comp, gl) : comp) * g.ld : src,
+      cp_async_elem(s + comp * T::BOXS + bn.sb, bn.inside ? p + (mapped ? comp_of(comp, gl) : comp) * g.ld : src,
                     bn.inside);
   }
 
@@ -396,7 +408,7 @@ namespace sint
       return;
     const R *p = src + node0 + np.off;
     for (int comp = np.grp; comp < ncomp; comp += T::NG)
-      cp_async_elem(s + comp * T::BOX + np.b, p + (mapped ? comp_of(comp, gl) : comp) * g.ld, true);
+      cp_async_elem(s + comp * T::BOXS + np.sb, p + (mapped ? comp_of(comp, gl) : comp) * g.ld, true);
   }
 
   template <int DIM>
@@ -452,7 +464,7 @@ namespace sint
         }
       JxW = R(jxw);
       using T = Tile<DIM>;
-      const int stride[3] = {1, T::BX, T::BX * T::BY};
+      const int stride[3] = {1, T::SY, T::SZ};
 #pragma unroll
       for (int x = 0; x < (1 << DIM); ++x)
         {
@@ -471,7 +483,7 @@ namespace sint
   {
     using T      = Tile<DIM>;
     const int cx = cell % T::TX, cy = (cell / T::TX) % T::TY, cz = cell / (T::TX * T::TY);
-    return cx + T::BX * (cy + T::BY * cz);
+    return cx + T::SY * cy + T::SZ * cz;
   }
 
   template <int DIM>
@@ -490,7 +502,7 @@ namespace sint
     using T = Tile<DIM>;
     if constexpr (DIM == 3)
       {
-        constexpr int SY = T::BX, SZ = T::BX * T::BY;
+        constexpr int SY = T::SY, SZ = T::SZ;
         R vx[2][2], dx[2][2];
 #pragma unroll
         for (int lz = 0; lz < 2; ++lz)
@@ -516,7 +528,7 @@ namespace sint
       }
     else
       {
-        constexpr int SY = T::BX;
+        constexpr int SY = T::SY;
         R vx[2], dx[2];
 #pragma unroll
         for (int ly = 0; ly < 2; ++ly)
@@ -538,7 +550,7 @@ namespace sint
     using T = Tile<DIM>;
     if constexpr (DIM == 3)
       {
-        constexpr int SY = T::BX, SZ = T::BX * T::BY;
+        constexpr int SY = T::SY, SZ = T::SZ;
         R vxy[2];
 #pragma unroll
         for (int lz = 0; lz < 2; ++lz)
@@ -551,7 +563,7 @@ namespace sint
       }
     else
       {
-        constexpr int SY = T::BX;
+        constexpr int SY = T::SY;
         const R a = w.wA[0] * s[b0] + w.wB[0] * s[b0 + 1];
         const R b = w.wA[0] * s[b0 + SY] + w.wB[0] * s[b0 + 1 + SY];
         return w.wA[1] * a + w.wB[1] * b;

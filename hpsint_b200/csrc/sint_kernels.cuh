@@ -146,7 +146,7 @@ namespace sint
         int buf = 0, comp = 0;
         FM::source(it, buf, comp);
         R u[1 << DIM];
-        cell_nodes<DIM>((buf == 0 ? box0 : box1) + comp * T::BOX, b0, u);
+        cell_nodes<DIM>((buf == 0 ? box0 : box1) + comp * T::BOXS, b0, u);
         if constexpr (CUT)
           if (absent)
 #pragma unroll
@@ -506,7 +506,7 @@ namespace sint
                 for (int d = 0; d < DIM; ++d)
                   gg[d][q] = R(0);
               }
-            cell_nodes<DIM>(stiff + row * T::BOX, b0, u);
+            cell_nodes<DIM>(stiff + row * T::BOXS, b0, u);
             const int it = (row - 2) * T::CELLS + cell;
             if (has[it])
               {
@@ -535,7 +535,7 @@ namespace sint
               v[q] = P[(res * NQ + q) * T::CELLS + cell];
             cell_integrate_v<DIM>(v, k, r);
             R u[NQ];
-            cell_nodes<DIM>(stiff + (row == 1 ? 0 : row) * T::BOX, b0, u);
+            cell_nodes<DIM>(stiff + (row == 1 ? 0 : row) * T::BOXS, b0, u);
             cell_stiffness_add<DIM>(row == 1 ? -p.kc : p.L * p.kp, u, g, r);
           }
         // a branch, not a select per value: in tiles inside the mesh every
@@ -589,7 +589,7 @@ namespace sint
     using FM                    = FieldMap<DIM, G, TENS, JVP, HIST>;
     static constexpr int C      = G + 2;
     static constexpr int NQ     = 1 << DIM;
-    static constexpr int BOXES  = 2 * C * T::BOX;                  // both inputs of one tile
+    static constexpr int BOXES  = 2 * C * T::BOXS;                 // both inputs of one tile
     static constexpr int F_SIZE = FM::NSLOT * T::CELLS;            // point fields (K aliases it)
     static constexpr int P_SIZE = (DIM + 2 + G) * NQ * T::CELLS;   // point results
     static constexpr int K_SIZE = C * NQ * T::CP;
@@ -661,13 +661,13 @@ namespace sint
         {
           const long long n0 = tile_node0(g, tcx);
           load_box_async_interior<DIM>(bb, lin, C, g, np, n0, glx, CUT);
-          load_box_async_interior<DIM>(bb + C * T::BOX, src, C, g, np, n0, glx, CUT);
+          load_box_async_interior<DIM>(bb + C * T::BOXS, src, C, g, np, n0, glx, CUT);
         }
       else
         {
           const BoxNode<DIM> bn(g, tcx);
           load_box_async<DIM>(bb, lin, C, g, bn, glx, CUT);
-          load_box_async<DIM>(bb + C * T::BOX, src, C, g, bn, glx, CUT);
+          load_box_async<DIM>(bb + C * T::BOXS, src, C, g, bn, glx, CUT);
         }
     };
     // current and next tile: id, grain list, union mask, this thread's cell mask
@@ -730,7 +730,7 @@ namespace sint
         const unsigned  m  = CUT ? local_mask<G>(m_glob, gl) : ~0u;
         if constexpr (ADV)
           adv_stage<DIM, G, R, CUT>(adv, g, tc, gl, A_vel, A_has);
-        phase_evaluate<DIM, G, TENS, true, false, R, CUT>(cb, cb + C * T::BOX, F, k, m);
+        phase_evaluate<DIM, G, TENS, true, false, R, CUT>(cb, cb + C * T::BOXS, F, k, m);
         __syncthreads();
         jvp_point<DIM, G, TENS, R>(p, F, P, threadIdx.x / T::CELLS, cell, m);
         if constexpr (ADV)
@@ -740,7 +740,7 @@ namespace sint
                                            A_has);
           }
         __syncthreads();
-        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, cb + C * T::BOX, K, m, A_vel, A_has);
+        phase_integrate<DIM, G, R, CUT, ADV>(p, g, k, tc, P, cb + C * T::BOXS, K, m, A_vel, A_has);
         __syncthreads();
         if (tile_interior<DIM>(g, tc))
           sum_and_store_interior<DIM>(K, C, g, tc.linear, np, tile_node0(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
@@ -786,7 +786,7 @@ namespace sint
     constexpr int C = G + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *s_u = reinterpret_cast<R *>(smem_raw);
-    R *s_h = s_u + C * T::BOX;
+    R *s_h = s_u + C * T::BOXS;
     R *F   = s_u + SM::BOXES;
     R *P   = F + SM::F_SIZE;
     R *K   = F;
@@ -836,9 +836,9 @@ namespace sint
                         hv += h2[off] * ph.w_hist[2];
                     }
                 }
-              s_u[comp * T::BOX + np.b] = v;
+              s_u[comp * T::BOXS + np.sb] = v;
               if constexpr (WTD == 2)
-                s_h[comp * T::BOX + np.b] = hv;
+                s_h[comp * T::BOXS + np.sb] = hv;
             }
         if constexpr (ADV)
           adv_stage<DIM, G, R, CUT>(adv, g, tc, gl, A_vel, A_has);
@@ -899,7 +899,7 @@ namespace sint
     constexpr int C  = G + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *s_lin  = reinterpret_cast<R *>(smem_raw);
-    R *s_coef = s_lin + C * T::BOX;
+    R *s_coef = s_lin + C * T::BOXS;
     R *s_con  = s_coef + LY::NCOEF * T::THREADS; // NOUT * CS
 
     const TileCoord    tc = tile_coord<DIM>(g);
@@ -917,13 +917,13 @@ namespace sint
     {
       R c, gc[DIM], mu_unused, gmu[DIM];
       eval_vg<DIM>(s_lin, b0, w, c, gc);
-      eval_vg<DIM>(s_lin + T::BOX, b0, w, mu_unused, gmu);
+      eval_vg<DIM>(s_lin + T::BOXS, b0, w, mu_unused, gmu);
       R eta[G];
       R geta[G][DIM];
 #pragma unroll
       for (int i = 0; i < G; ++i)
         {
-          eval_vg<DIM>(s_lin + (2 + i) * T::BOX, b0, w, eta[i], geta[i]);
+          eval_vg<DIM>(s_lin + (2 + i) * T::BOXS, b0, w, eta[i], geta[i]);
           if (CUT && ((gmask >> i) & 1u) == 0u)
             {
               eta[i] = R(0);

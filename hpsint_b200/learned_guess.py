@@ -554,11 +554,16 @@ def compare_arms(case, n_steps, net=None, norm=None, arms=None, warmup_steps=2):
     mass = lumped_mass_2d(case.nodes)
     u0 = case.op.to_host(case.u0)
     c0 = float(mass @ u0[0])
-    out, ref, schedule = {}, None, None
+    out, ref, schedule, prev_prec = {}, None, None, None
     for a in arms:
         prec, kind, cut = ARMS[a]
         if kind is not None and kind not in preds:
             continue
+        # the Newton workspace is rebuilt when the Krylov precision changes:
+        # warm the new one up (GMRES graphs, first launches) outside the timing
+        if prev_prec is not None and prec != prev_prec:
+            run_arm(case, warmup_steps, prec, None, cut_off=cut)
+        prev_prec = prec
         try:
             u, recs, wall = run_arm(case, n_steps, prec, preds.get(kind), schedule, cut_off=cut)
         except L.SintError as e:

@@ -168,8 +168,11 @@ int sint_jvp_f32(sint_ctx *ctx, float *dst, const float *src, sint_stream_t stre
  * bytes per 8 x 8 cells in 2D: with G = 4, up to 64 x 64 x 36 cells in 3D or
  * 520 x 520 cells in 2D.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current, so make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * (different streams, or different host threads) race and give wrong results. */
+ * stream capture.  That address is kept per device ordinal for the life of
+ * the process: after a device reset (cudaDeviceReset) the process must not
+ * call this entry point on that device again.  All calls share the array:
+ * calls that overlap on the GPU (different streams, or different host
+ * threads) race and give wrong results. */
 #define SINT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 int sint_jvp_f64_noalloc(const sint_mesh *mesh, const sint_params *params, double w0, double w_alg,
                          const double *lin, const double *src, double *dst, sint_stream_t stream);
