@@ -71,9 +71,12 @@ def parse_args():
     ap.add_argument("--cells", type=int, default=512)
     ap.add_argument("--circles", type=int, default=100)
     ap.add_argument("--save-net", default=None, help="write the trained predictor (.npz) here")
+    ap.add_argument("--net-width", type=int, default=32, help="learned2d: channels of the hidden layers")
     ap.add_argument("--solve-steps", type=int, default=100)
     ap.add_argument("--arms", default=None,
                     help="solve3d: comma-separated subset of the arms to run (default: all)")
+    ap.add_argument("--predictor", choices=["none", "linear", "euler"], default="none",
+                    help="solve3d: initial guess of every arm but the FP64 reference (hpsint's predictors)")
     ap.add_argument("--preconditioners", action="store_true",
                     help="solve3d: also run right-preconditioned GMRES with block-Jacobi and with the Gauss-Seidel "
                          "Cahn-Hilliard block")
@@ -508,12 +511,18 @@ def mixed_precision_solve_3d(args):
         if not arms:
             raise SystemExit(f"--arms {args.arms}: no such arm")
     runs, schedule = {}, None
+    from hpsint_b200 import learned_guess as LG
+    make_pred = {"none": None, "linear": LG.LinearPredictor, "euler": LG.EulerPredictor}[args.predictor]
     for label, prec, tol, cut_pc, block0, right in arms:
         op.set_component_mask(u0d, tol)  # 0 switches a previous arm's cut-off off
         op.set_preconditioner_cut_off(cut_pc)
         op.set_preconditioner_type(block0)
+        # the FP64-inner reference arm keeps hpsint's default (no predictor);
+        # predicted arms stop at the same absolute tolerance (old-solution base)
+        pred = make_pred(op) if (make_pred and label != "fp64_inner") else None
         ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec, right_preconditioning=right),
-                            TimeIntegrationData(time_step_init=1e-4), grain_cut_off_tolerance=tol)
+                            TimeIntegrationData(time_step_init=1e-4), grain_cut_off_tolerance=tol, predictor=pred,
+                            tolerance_base="old_solution" if pred else "initial_guess")
         ti.initialize(u0d)
         ti.run(2, dt_schedule=[1e-4, 1e-4])  # warm-up: workspaces, first launches (discarded)
         ti.initialize(u0d)
@@ -796,7 +805,7 @@ def learned_guess_solve(args):
     train = list(range(args.train_seeds))
     held = list(range(1000, 1000 + args.eval_seeds))
     net, norm, trainer, info = LG.train_learned_guess(
-        train, n=args.cells, n_circles=args.circles, n_steps=args.train_steps, net_cfg=NetConfig(),
+        train, n=args.cells, n_circles=args.circles, n_steps=args.train_steps, net_cfg=NetConfig(width=args.net_width),
         train_cfg=LG.TrainConfig(iterations=args.train_iters, smooth=args.smooth), verbose=False)
     if args.save_net:
         LG.save_predictor(args.save_net, net, norm)

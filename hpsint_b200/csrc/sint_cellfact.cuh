@@ -400,7 +400,7 @@ namespace sint
 
   // r_l += coef (K u)_l with the exact element Laplacian K_lm = kx[l xor m].
   template <int DIM, typename R>
-  __device__ __forceinline__ void cell_stiffness_add(const R coef, const R (&u)[1 << DIM], const Grid &g,
+  __device__ __forceinline__ void cell_stiffness_add(const nd<R> coef, const R (&u)[1 << DIM], const Grid &g,
                                                      R (&r)[1 << DIM])
   {
     R cu[1 << DIM];

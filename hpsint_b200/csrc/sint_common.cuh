@@ -23,6 +23,7 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "sint_f2.cuh"
 
 namespace sint
 {
@@ -126,6 +127,11 @@ namespace sint
   __device__ __forceinline__ float kx<float>(const Grid &g, int x)
   {
     return g.kxf[x];
+  }
+  template <>
+  __device__ __forceinline__ F2 kx<F2>(const Grid &g, int x)
+  {
+    return F2(g.kxf[x]);
   }
 
   // Device form of the residual's range hooks (pre_operation /
@@ -381,8 +387,9 @@ namespace sint
   }
 
   // Issue the asynchronous load of `ncomp` components of `src` into the box
-  // buffer s (layout s[comp * BOXS + sb]).
-  template <int DIM, typename R>
+  // buffer s (layout s[(comp * BOXS + sb) * LS]: LS = 2 fills one lane of a
+  // box of packed pairs, s pointing at that lane).
+  template <int DIM, typename R, int LS = 1>
   __device__ __forceinline__ void load_box_async(R *s, const R *__restrict__ src, int ncomp, const Grid &g,
                                                  const BoxNode<DIM> &bn, unsigned long long gl = 0,
                                                  bool mapped = false)
@@ -392,13 +399,13 @@ namespace sint
       return;
     const R *p = bn.inside ? src + bn.lidx : src;
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
-      cp_async_elem(s + comp * T::BOXS + bn.sb, bn.inside ? p + (mapped ? comp_of(comp, gl) : comp) * g.ld : src,
-                    bn.inside);
+      cp_async_elem(s + (comp * T::BOXS + bn.sb) * LS,
+                    bn.inside ? p + (mapped ? comp_of(comp, gl) : comp) * g.ld : src, bn.inside);
   }
 
   // Interior-tile form of load_box_async: every box node exists and is read
   // at node0 + the thread's fixed offset.
-  template <int DIM, typename R>
+  template <int DIM, typename R, int LS = 1>
   __device__ __forceinline__ void load_box_async_interior(R *s, const R *__restrict__ src, int ncomp, const Grid &g,
                                                           const NodePlan<DIM> &np, long long node0,
                                                           unsigned long long gl = 0, bool mapped = false)
@@ -408,7 +415,7 @@ namespace sint
       return;
     const R *p = src + node0 + np.off;
     for (int comp = np.grp; comp < ncomp; comp += T::NG)
-      cp_async_elem(s + comp * T::BOXS + np.sb, p + (mapped ? comp_of(comp, gl) : comp) * g.ld, true);
+      cp_async_elem(s + (comp * T::BOXS + np.sb) * LS, p + (mapped ? comp_of(comp, gl) : comp) * g.ld, true);
   }
 
   template <int DIM>
@@ -643,7 +650,8 @@ namespace sint
   // alone (the combine step skips them).
   // With `epi` (the residual's epilogue hook) the owned nodes are stored as
   // (sum - sub) * scale; the partials stay raw (the combine step applies it).
-  template <int DIM, typename R>
+  // LS = 2: s_con points at one lane of contributions held as packed pairs.
+  template <int DIM, typename R, int LS = 1>
   __device__ __forceinline__ void sum_and_store(const R *s_con, int ncomp, const Grid &g, const TileCoord &tc,
                                                 const BoxNode<DIM> &bn, R *__restrict__ dst, R *__restrict__ partial,
                                                 unsigned long long gl = 0, bool mapped = false, int c_all = 0,
@@ -660,7 +668,7 @@ namespace sint
       {
         const int cx = bn.bx - (l & 1), cy = bn.by - ((l >> 1) & 1), cz = (DIM == 3) ? bn.bz - ((l >> 2) & 1) : 0;
         ok[l]      = cx >= 0 && cx < T::TX && cy >= 0 && cy < T::TY && cz >= 0 && cz < T::TZ;
-        src_off[l] = l * T::CP + (ok[l] ? cx + T::TX * (cy + T::TY * cz) : 0);
+        src_off[l] = (l * T::CP + (ok[l] ? cx + T::TX * (cy + T::TY * cz) : 0)) * LS;
       }
     const int gi = tc.o[0] + bn.bx, gj = tc.o[1] + bn.by, gk = (DIM == 3) ? tc.o[2] + bn.bz : 0;
     bool owned   = (bn.bx > 0 || gi == 0) && (bn.bx < T::TX || gi == g.n[0]) && (bn.by > 0 || gj == 0) &&
@@ -679,7 +687,7 @@ namespace sint
     };
     for (int comp = bn.grp; comp < ncomp; comp += T::NG)
       {
-        const R *sc  = s_con + comp * T::CS;
+        const R *sc  = s_con + comp * T::CS * LS;
         R        sum = R(0);
 #pragma unroll
         for (int l = 0; l < T::NQ; ++l)
@@ -697,7 +705,7 @@ namespace sint
   // Interior-tile form of sum_and_store: the owned nodes are the ones on no
   // face of the box (np.inner), written at node0 + the fixed offset; the
   // others go to the tile's partial slot.
-  template <int DIM, typename R>
+  template <int DIM, typename R, int LS = 1>
   __device__ __forceinline__ void sum_and_store_interior(const R *s_con, int ncomp, const Grid &g,
                                                          long long tile_linear, const NodePlan<DIM> &np,
                                                          long long node0, R *__restrict__ dst,
@@ -721,12 +729,12 @@ namespace sint
     };
     for (int comp = np.grp; comp < ncomp; comp += T::NG)
       {
-        const R *sc  = s_con + comp * T::CS + np.cbase;
+        const R *sc  = s_con + (comp * T::CS + np.cbase) * LS;
         R        sum = R(0);
 #pragma unroll
         for (int l = 0; l < T::NQ; ++l)
           if ((np.ok >> l) & 1u)
-            sum += sc[l * T::CP - ((l & 1) + T::TX * ((l >> 1) & 1) + T::TX * T::TY * ((l >> 2) & 1))];
+            sum += sc[(l * T::CP - ((l & 1) + T::TX * ((l >> 1) & 1) + T::TX * T::TY * ((l >> 2) & 1))) * LS];
         const int cc  = mapped ? comp_of(comp, gl) : comp;
         out[cc * ost] = finish(sum, cc);
       }

@@ -176,7 +176,7 @@ namespace sint
   // point results: P[(res * NQ + q) * CELLS + cell]; res 0 = c row value,
   // 1..DIM = c row flux, DIM + 1 = mu row value, DIM + 2 + i = eta_i row value
   template <int DIM, typename R>
-  __device__ __forceinline__ void pstore(R *P, int res, int q, int cell, R v)
+  __device__ __forceinline__ void pstore(R *P, int res, int q, int cell, nd<R> v)
   {
     P[(res * Slots<DIM>::NQ + q) * Tile<DIM>::CELLS + cell] = v;
   }
@@ -453,11 +453,14 @@ namespace sint
   // cell gains the flux -v_i eta_i (operator_sintering_generic.h:1015-1036,
   // :167-177), eta_i interpolated from the same nodal values `stiff` holds;
   // warps in which no cell of the row moves keep the value-only integration.
+  // tc_b (packed pairs only): the tile of lane y, whose cells outside the
+  // mesh are zeroed lane by lane.
   template <int DIM, int G, typename R, bool CUT = false, bool ADV = false>
   __device__ __forceinline__ void phase_integrate(const PhysR<R> &p, const Grid &g, const CellConsts<DIM, R> &k,
                                                   const TileCoord &tc, const R *P, const R *stiff, R *K,
                                                   unsigned m = ~0u, const R *vel = nullptr,
-                                                  const unsigned char *has = nullptr)
+                                                  const unsigned char *has = nullptr,
+                                                  const TileCoord *tc_b = nullptr)
   {
     using T            = Tile<DIM>;
     constexpr int NQ   = 1 << DIM;
@@ -466,6 +469,7 @@ namespace sint
     const int     cell = threadIdx.x % T::CELLS;
     const int     b0   = cell_box_base<DIM>(cell);
     const bool    in   = cell_in_mesh<DIM>(cell, tc, g);
+    const bool    in_b = tc_b ? cell_in_mesh<DIM>(cell, *tc_b, g) : in;
     for (int row = threadIdx.x / T::CELLS; row < C; row += NGRP)
       {
         bool keep = in;
@@ -540,7 +544,7 @@ namespace sint
           }
         // a branch, not a select per value: in tiles inside the mesh every
         // cell keeps its row
-        if (keep)
+        if (keep && in_b)
           {
 #pragma unroll
             for (int l = 0; l < NQ; ++l)
@@ -550,7 +554,7 @@ namespace sint
           {
 #pragma unroll
             for (int l = 0; l < NQ; ++l)
-              K[(row * NQ + l) * T::CP + cell] = R(0);
+              K[(row * NQ + l) * T::CP + cell] = lane_keep(r[l], keep, in_b);
           }
       }
   }
@@ -746,10 +750,10 @@ namespace sint
           sum_and_store_interior<DIM>(K, C, g, tc.linear, np, tile_node0(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
         else
           sum_and_store<DIM>(K, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, gl, CUT, ct.c_all, tm);
-        // No barrier here: the next tile's prefetch writes the other box
+        // No further barrier: the next tile's prefetch writes the other box
         // buffer, whose last readers (this tile's phases 1 and 3) passed the
-        // barrier above, and K (aliasing F) is next written in phase 1, after
-        // the barrier that follows the next cp.async wait.
+        // barrier after phase 3, and K (aliasing F) is next written in phase
+        // 1, after the barrier that follows the next cp.async wait.
         if constexpr (CUT)
           {
             tile    = t_next;
@@ -762,6 +766,101 @@ namespace sint
           }
         else
           tile = nidx;
+      }
+    cp_async_wait<0>();
+  }
+
+  // -------------------------------------------------------------------------
+  // FP32 Jacobian-vector product on tile pairs.  sm_100 executes FP32 add,
+  // multiply and fused multiply-add on two values held in a 64-bit register
+  // pair with one instruction (FADD2 / FMUL2 / FFMA2); the FP32 product is
+  // bound by instruction issue, so the block computes tiles 2j and 2j + 1
+  // together: every shared-memory value is a pair (lane x of tile 2j, lane y
+  // of tile 2j + 1), phases 1-3 run once on F2 for both tiles, and the node
+  // sums are stored per lane.  Each lane rounds exactly as the scalar FP32
+  // arithmetic of the same expression does.  Full operator only (no grain
+  // cut-off, no advection: those keep jvp_kernel); shared memory and
+  // registers as the FP64 product.
+  template <int DIM, int G, bool TENS>
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, jvp_blocks_per_sm<DIM, G, double>())
+    jvp_pair_kernel(const Grid g, const Phys ph, const float *__restrict__ lin, const float *__restrict__ src,
+                    float *__restrict__ dst, float *__restrict__ partial)
+  {
+    using T  = Tile<DIM>;
+    using SM = ThreePhaseSmem<DIM, G, TENS, true, false, false>;
+    constexpr int C = G + 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    F2 *s_buf = reinterpret_cast<F2 *>(smem_raw); // 2 x BOXES pairs
+    F2 *F     = s_buf + 2 * SM::BOXES;
+    F2 *P     = F + SM::F_SIZE;
+    F2 *K     = F; // aliases the point fields, dead after phase 2
+
+    const PhysR<F2>           p(ph);
+    const CellConsts<DIM, F2> k(g);
+    const NodePlan<DIM>       np(g);
+    const int                 cell   = threadIdx.x % T::CELLS;
+    const long long           npairs = (g.n_tiles + 1) / 2;
+    long long                 idx    = blockIdx.x;
+    // node boxes of both inputs of the tiles of pair j into buffer bb (a
+    // missing second tile leaves its lane stale: computed, never stored)
+    auto prefetch = [&](F2 *bb, long long j) {
+#pragma unroll
+      for (int lane = 0; lane < 2; ++lane)
+        {
+          const long long tile = 2 * j + lane;
+          if (tile >= g.n_tiles)
+            break;
+          const TileCoord tcx = tile_coord_of<DIM>(g, tile);
+          float          *fb  = reinterpret_cast<float *>(bb) + lane;
+          if (tile_interior<DIM>(g, tcx))
+            {
+              const long long n0 = tile_node0(g, tcx);
+              load_box_async_interior<DIM, float, 2>(fb, lin, C, g, np, n0);
+              load_box_async_interior<DIM, float, 2>(fb + 2 * C * T::BOXS, src, C, g, np, n0);
+            }
+          else
+            {
+              const BoxNode<DIM> bn(g, tcx);
+              load_box_async<DIM, float, 2>(fb, lin, C, g, bn);
+              load_box_async<DIM, float, 2>(fb + 2 * C * T::BOXS, src, C, g, bn);
+            }
+        }
+    };
+    if (idx < npairs)
+      prefetch(s_buf, idx);
+    cp_async_commit();
+    for (int it = 0; idx < npairs; ++it, idx += gridDim.x)
+      {
+        const long long nidx = idx + gridDim.x;
+        if (nidx < npairs)
+          prefetch(s_buf + ((it + 1) & 1) * SM::BOXES, nidx);
+        cp_async_commit();
+        cp_async_wait<1>(); // this pair's group has landed (only the prefetch may be pending)
+        __syncthreads();
+        const long long tile_a = 2 * idx, tile_b = tile_a + 1;
+        const bool      has_b  = tile_b < g.n_tiles;
+        const TileCoord tca    = tile_coord_of<DIM>(g, tile_a);
+        const TileCoord tcb    = tile_coord_of<DIM>(g, has_b ? tile_b : tile_a);
+        const F2       *cb     = s_buf + (it & 1) * SM::BOXES;
+        phase_evaluate<DIM, G, TENS, true, false, F2, false>(cb, cb + C * T::BOXS, F, k);
+        __syncthreads();
+        jvp_point<DIM, G, TENS, F2>(p, F, P, threadIdx.x / T::CELLS, cell);
+        __syncthreads();
+        phase_integrate<DIM, G, F2, false, false>(p, g, k, tca, P, cb + C * T::BOXS, K, ~0u, nullptr, nullptr,
+                                                  &tcb);
+        __syncthreads();
+#pragma unroll
+        for (int lane = 0; lane < 2; ++lane)
+          {
+            if (lane == 1 && !has_b)
+              break;
+            const TileCoord &tc = lane ? tcb : tca;
+            const float     *kf = reinterpret_cast<const float *>(K) + lane;
+            if (tile_interior<DIM>(g, tc))
+              sum_and_store_interior<DIM, float, 2>(kf, C, g, tc.linear, np, tile_node0(g, tc), dst, partial);
+            else
+              sum_and_store<DIM, float, 2>(kf, C, g, tc, BoxNode<DIM>(g, tc), dst, partial);
+          }
       }
     cp_async_wait<0>();
   }

@@ -2,6 +2,7 @@
 // sint_inst_*.cu translation units, each of which instantiates one
 // (dimension, mobility) combination for all grain counts.
 #pragma once
+#include <type_traits>
 
 #include "sint_kernels.cuh"
 #include "sint_launch.h"
@@ -18,11 +19,14 @@ namespace sint
     if (bytes > 48 * 1024 && (e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))) !=
                                cudaSuccess)
       return e;
-    int dev = 0, per_sm = 0;
+    int                dev = 0, per_sm = 0;
+    cudaFuncAttributes fa{};
     if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
-        (e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+        (e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess ||
+        (e = cudaFuncGetAttributes(&fa, k)) != cudaSuccess)
       return e;
-    const size_t need = size_t(blocks) * (bytes + 1024); // + the per-block reservation
+    // dynamic + static shared memory + the per-block reservation
+    const size_t need = size_t(blocks) * (bytes + fa.sharedSizeBytes + 1024);
     const int    pct  = need >= size_t(per_sm) ? 100 : int((need * 100 + per_sm - 1) / per_sm);
     return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
   }
@@ -57,6 +61,24 @@ namespace sint
       return e;
     const long long blocks = g.n_tiles < grid_cap ? g.n_tiles : grid_cap;
     k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, ct, adv);
+    count_launches(1);
+    return cudaGetLastError();
+  }
+
+  template <int DIM, int G, bool TENS>
+  cudaError_t launch_jvp_pair_g(const Grid &g, const Phys &p, const float *lin, const float *src, float *dst,
+                                float *partial, cudaStream_t s)
+  {
+    const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false, false>::TOTAL * sizeof(F2);
+    auto         k    = jvp_pair_kernel<DIM, G, TENS>;
+    static DeviceCache cache;
+    int                grid_cap = 0;
+    if (const cudaError_t e =
+          persistent_grid(cache, k, smem, jvp_blocks_per_sm<DIM, G, double>(), Tile<DIM>::THREADS, grid_cap))
+      return e;
+    const long long pairs  = (g.n_tiles + 1) / 2;
+    const long long blocks = pairs < grid_cap ? pairs : grid_cap;
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -158,10 +180,20 @@ namespace sint
             return e;
         return cudaSuccess;
       }
-    const CutTiles none;
-#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, false, ADV>(g, p, lin, src, dst, partial, none, adv, s)
-    SINT_G_SWITCH(SINT_CALL)
+    if constexpr (std::is_same_v<R, float> && !ADV)
+      {
+        // the full FP32 operator runs on tile pairs (packed FP32)
+#define SINT_CALL(GG) launch_jvp_pair_g<DIM, GG, TENS>(g, p, lin, src, dst, partial, s)
+        SINT_G_SWITCH(SINT_CALL)
 #undef SINT_CALL
+      }
+    else
+      {
+        const CutTiles none;
+#define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, false, ADV>(g, p, lin, src, dst, partial, none, adv, s)
+        SINT_G_SWITCH(SINT_CALL)
+#undef SINT_CALL
+      }
   }
 
   // The advection kernels are instantiated in their own translation units

@@ -11,9 +11,18 @@
 #pragma once
 
 #include "sint_common.cuh"
+#include <type_traits>
 
 namespace sint
 {
+  // c ? a : b, written as a call so that the packed FP32 pairs (F2, whose
+  // comparisons give one flag per lane) select lane by lane
+  template <typename R>
+  __device__ __forceinline__ R sel(bool c, R a, R b)
+  {
+    return c ? a : b;
+  }
+
   template <int D, typename R>
   __device__ __forceinline__ R dotv(const R (&a)[D], const R (&b)[D])
   {
@@ -31,9 +40,12 @@ namespace sint
   //   reciprocal:          y <- y + y (1 - x y)
   //   inverse square root: y <- y + (y / 2) (1 - x y^2)
   // One step squares the relative error: ~3e-14 in double (far inside the
-  // operator's 1e-12 parity bound), float rounding level in float.  Valid for
-  // arguments in [FLT_MIN, FLT_MAX]; the squared gradient norms this is used
-  // for are filtered below 1e-20 by the callers.
+  // operator's 1e-12 parity bound), float rounding level in float.  The seeds
+  // need the argument and the result inside the normal float range: the
+  // callers filter squared norms below 1e-20, and in double an argument above
+  // 2^126 for the reciprocal (whose seed 1/x would flush to zero) or above
+  // FLT_MAX for the inverse square root (a gradient steeper than ~1e19 per
+  // unit length) takes the exact division instead.
   __device__ __forceinline__ float rcp_seed(float x)
   {
     float y;
@@ -48,16 +60,46 @@ namespace sint
   }
 
   template <typename R>
+  __device__ __forceinline__ R seed_rcp(R x)
+  {
+    return R(rcp_seed(float(x)));
+  }
+  template <>
+  __device__ __forceinline__ F2 seed_rcp<F2>(F2 x)
+  {
+    return F2(rcp_seed(x.v.x), rcp_seed(x.v.y));
+  }
+  template <typename R>
+  __device__ __forceinline__ R seed_rsqrt(R x)
+  {
+    return R(rsqrt_seed(float(x)));
+  }
+  template <>
+  __device__ __forceinline__ F2 seed_rsqrt<F2>(F2 x)
+  {
+    return F2(rsqrt_seed(x.v.x), rsqrt_seed(x.v.y));
+  }
+
+  constexpr double RCP_SEED_MAX   = 8.507059173023462e37;  // 2^126: 1/x stays a normal float
+  constexpr double RSQRT_SEED_MAX = 3.4028234663852886e38; // FLT_MAX
+
+  template <typename R>
   __device__ __forceinline__ R rcp_pos(R x)
   {
-    const R y = R(rcp_seed(float(x)));
+    if constexpr (std::is_same_v<R, double>)
+      if (x > RCP_SEED_MAX)
+        return 1.0 / x;
+    const R y = seed_rcp(x);
     return y + y * (R(1) - x * y);
   }
 
   template <typename R>
   __device__ __forceinline__ R rsqrt_pos(R x)
   {
-    const R y = R(rsqrt_seed(float(x)));
+    if constexpr (std::is_same_v<R, double>)
+      if (x > RSQRT_SEED_MAX)
+        return 1.0 / sqrt(x);
+    const R y = seed_rsqrt(x);
     return y + (R(0.5) * y) * (R(1) - (x * y) * y);
   }
 
@@ -66,6 +108,7 @@ namespace sint
   {
     return fmin(fmax(x, R(0)), R(1));
   }
+  __device__ __forceinline__ F2 clamp01(const P2 &x) { return clamp01(F2(x)); }
 
   // tensor.h:137-154 unit_vector(v, 1e-10): v / |v| if |v| > 1e-10, else 0.
   // Also returns n2 = |v|^2 and rs = 1 / |v| (0 below the threshold), which
@@ -75,7 +118,7 @@ namespace sint
   {
     n2 = dotv<D>(v, v);
     // |v| > 1e-10  <=>  |v|^2 > 1e-20
-    rs = n2 > R(1e-20) ? rsqrt_pos<R>(n2) : R(0);
+    rs = sel(n2 > R(1e-20), rsqrt_pos<R>(n2), R(0));
 #pragma unroll
     for (int d = 0; d < D; ++d)
       n[d] = v[d] * rs;
@@ -86,7 +129,7 @@ namespace sint
   __device__ __forceinline__ R unit_vector_filter_2(const R (&v)[D])
   {
     const R n2 = dotv<D>(v, v);
-    return n2 > R(1e-20) ? rcp_pos<R>(n2) : R(0);
+    return sel(n2 > R(1e-20), rcp_pos<R>(n2), R(0));
   }
 
   // Grain cut-off (operator_sintering_data.h:149-203): bit i of the cell mask m
@@ -222,10 +265,10 @@ namespace sint
         // 2) dM/dc (hpsint uses dphidc = 30 * 4 c^2 (1-c)^2 here, mobility.h:852-854)
         const R fvv2  = (p.Mvol - p.Mvap) * (R(30) * c2);
         R       dfs   = p.Msurf * R(8) * c * omc * (R(1) - R(2) * c);
-        dfs           = fsurf < R(1e-6) ? R(0) : dfs;
+        dfs           = sel(fsurf < R(1e-6), R(0), dfs);
         // 3) dM/dgrad c; |grad c| < 1e-4 (|grad c|^2 < 1e-8) counts as 1
-        const R fs3   = fsurf < R(1e-6) ? R(0) : fsurf;
-        const R inrm3 = n2 < R(1e-8) ? R(1) : rs;
+        const R fs3   = sel(fsurf < R(1e-6), R(0), fsurf);
+        const R inrm3 = sel(n2 < R(1e-8), R(1), rs);
         const R nc_gdc = dotv<DIM>(nc, gdc);
         R       temp[DIM];
 #pragma unroll

@@ -82,7 +82,19 @@ def test_jvp_f64_matches_oracle(case):
     assert block_rel_err(op.to_host(dst), ref) <= 1e-12
 
 
-@pytest.mark.parametrize("case", CASES[:6], ids=[ids(c) for c in CASES[:6]])
+# The full FP32 product runs two tiles per block in packed pairs: odd tile
+# counts (a lone last tile), partial tiles at the mesh's high faces in
+# either lane, and the large-G one-block-per-SM instances.
+F32_CASES = CASES[:6] + [
+    (3, (9, 4, 2), 2, True, (1.0, 1.0, 1.0)),     # 3 tiles
+    (3, (13, 5, 3), 5, False, (0.9, 1.0, 1.2)),   # 4 x 2 x 2 tiles, partial in x, y and z
+    (3, (6, 5, 5), 12, True, (1.0, 1.0, 1.0)),
+    (2, (25, 9), 3, True, (1.0, 1.0, 1.0)),       # 4 x 2 tiles, the last column partial
+    (2, (9, 10), 12, False, (1.0, 1.0, 1.0)),
+]
+
+
+@pytest.mark.parametrize("case", F32_CASES, ids=[ids(c) for c in F32_CASES])
 def test_jvp_f32_close_to_oracle(case):
     dim, cells, G, tens, h = case
     op, p = make_op(dim, cells, G, tens, h)
@@ -205,3 +217,44 @@ def test_errors_are_reported():
     with pytest.raises(hb.SintError) as e:
         op.vmult(op.initialize_dof_vector(), op.initialize_dof_vector())
     assert e.value.status_name == "SINT_ERR_NOT_READY"
+
+
+def _residual_and_jvp_errors(dim, cells, G, tens, h, u, lin, src):
+    op, p = make_op(dim, cells, G, tens, h)
+    op.set_time_weights(10.0, [-10.0], 1.0)
+    T = O.make_time(10.0, 1.0, [-10.0])
+    M = oracle_mesh(dim, cells, h)
+    dst = op.initialize_dof_vector()
+    op.evaluate_nonlinear_residual(dst, op.to_device(u), 1, [])
+    e_res = block_rel_err(op.to_host(dst), O.residual(M, oracle_params(p), T, u, [], 1))
+    op.fill_quadrature_point_values(op.to_device(lin))
+    op.vmult(dst, op.to_device(src))
+    torch.cuda.synchronize()
+    e_jvp = block_rel_err(op.to_host(dst), O.jvp(M, oracle_params(p), T, lin, src))
+    return e_res, e_jvp
+
+
+def test_grain_boundary_filter_near_its_threshold():
+    """unit_vector_filter_2 (tensor.h:156-174) switches at |grad(eta_i - eta_j)|^2
+    = 1e-20.  Grains 1 and 2 are faint (nodal values ~1e-9, exact to full
+    relative precision), so the squared norms of their gradient difference
+    spread over 5e-22 .. 5e-20 (64 % of the nodes above the threshold) and
+    both branches are taken at many points."""
+    dim, cells, G = 3, (8, 7, 6), 3
+    mk = lambda seed: random_state(dim, cells, G, seed=seed)
+    u, lin, src = mk(21), mk(22), mk(23) - 0.5
+    for x in (u, lin):
+        x[3] *= 1e-9
+        x[4] *= 7e-10
+    assert max(_residual_and_jvp_errors(dim, cells, G, True, (1.0, 1.0, 1.0), u, lin, src)) <= 1e-12
+
+
+def test_steep_gradients_beyond_the_float_seed_range():
+    """With cells of 1e-20 the squared gradient norms reach ~1e40: above
+    2^126 the float reciprocal seed of the grain-boundary filter would flush
+    to zero, above FLT_MAX the inverse square root seed overflows; the double
+    path must take the exact division there and still match the oracle."""
+    dim, cells, G = 3, (5, 4, 3), 3
+    mk = lambda seed: random_state(dim, cells, G, seed=seed)
+    u, lin, src = mk(24), mk(25), mk(26) - 0.5
+    assert max(_residual_and_jvp_errors(dim, cells, G, True, (1e-20, 1e-20, 1e-20), u, lin, src)) <= 1e-12
