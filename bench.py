@@ -50,7 +50,8 @@ def parse_args():
     ap.add_argument("--scalar", action="store_true", help="scalar instead of tensorial mobility")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "nnconv",
+    ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "learned3d",
+                                           "nnconv",
                                            "cutoff", "tracker", "advection"],
                     default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
@@ -75,8 +76,12 @@ def parse_args():
     ap.add_argument("--solve-steps", type=int, default=100)
     ap.add_argument("--arms", default=None,
                     help="solve3d: comma-separated subset of the arms to run (default: all)")
-    ap.add_argument("--predictor", choices=["none", "linear", "euler"], default="none",
-                    help="solve3d: initial guess of every arm but the FP64 reference (hpsint's predictors)")
+    ap.add_argument("--predictor", default="none",
+                    help="solve3d: comma-separated initial guesses (none, linear, euler, learned) each arm but the "
+                         "FP64 reference runs with (hpsint's predictors; learned: the 3D network of --net3d or the "
+                         "one learned3d trains)")
+    ap.add_argument("--net3d", default=None, help="solve3d: trained 3D predictor (.npz of learned_guess.save_predictor)")
+    ap.add_argument("--train-n3", type=int, default=64, help="learned3d: cells per direction of the training packings")
     ap.add_argument("--preconditioners", action="store_true",
                     help="solve3d: also run right-preconditioned GMRES with block-Jacobi and with the Gauss-Seidel "
                          "Cahn-Hilliard block")
@@ -459,7 +464,7 @@ def solve_comparison(n_steps):
             "weights": "hpsint_b200/weights/learned_guess_c4.npz"}
 
 
-def mixed_precision_solve_3d(args):
+def mixed_precision_solve_3d(args, learned=None, train_info=None):
     """3D mixed-precision solve: 192^3 Q1 cells at unit spacing, 51 spheres
     with lognormal radii (median 10, sigma 0.2) in a random sequential packing
     with 2-cell overlaps, coloured to <= 10 order parameters, width-2 tanh
@@ -512,14 +517,32 @@ def mixed_precision_solve_3d(args):
             raise SystemExit(f"--arms {args.arms}: no such arm")
     runs, schedule = {}, None
     from hpsint_b200 import learned_guess as LG
-    make_pred = {"none": None, "linear": LG.LinearPredictor, "euler": LG.EulerPredictor}[args.predictor]
-    for label, prec, tol, cut_pc, block0, right in arms:
+    from hpsint_b200 import learned_guess3d as LG3
+    kinds = [k.strip() for k in args.predictor.split(",") if k.strip()]
+    if "learned" in kinds and learned is None:
+        if not args.net3d:
+            raise SystemExit("--predictor learned needs --net3d (or the learned3d workload)")
+        learned = LG.load_predictor(args.net3d)
+    factories = {"none": None, "linear": LG.LinearPredictor, "euler": LG.EulerPredictor,
+                 "learned": (lambda o: LG3.LearnedPredictor3D(o, *learned)) if learned else None}
+    for k in kinds:
+        if k not in factories:
+            raise SystemExit(f"--predictor {k}: not one of {sorted(factories)}")
+    # the FP64-inner reference arm keeps hpsint's default (no predictor); every
+    # other arm runs once per predictor kind
+    expanded = []
+    for a in arms:
+        if a[0] == "fp64_inner":
+            expanded.append((a, "none"))
+        else:
+            expanded += [(a, k) for k in kinds]
+    for (label, prec, tol, cut_pc, block0, right), kind in expanded:
+        label = label if kind == "none" else f"{label}_{kind}"
         op.set_component_mask(u0d, tol)  # 0 switches a previous arm's cut-off off
         op.set_preconditioner_cut_off(cut_pc)
         op.set_preconditioner_type(block0)
-        # the FP64-inner reference arm keeps hpsint's default (no predictor);
         # predicted arms stop at the same absolute tolerance (old-solution base)
-        pred = make_pred(op) if (make_pred and label != "fp64_inner") else None
+        pred = factories[kind](op) if factories[kind] else None
         ti = TimeIntegrator(op, hb.NonLinearData(nl_rel_tol=1e-8, inner_precision=prec, right_preconditioning=right),
                             TimeIntegrationData(time_step_init=1e-4), grain_cut_off_tolerance=tol, predictor=pred,
                             tolerance_base="old_solution" if pred else "initial_guess")
@@ -562,8 +585,10 @@ def mixed_precision_solve_3d(args):
                                          sum(x.accepted_wall_s for x in mp["recs"]),
         }
     if ref:
-        for label in ("fp32_inner_right", "fp32_inner_ch_gs_right", "fp64_inner_ch_gs_right",
-                      "fp32_inner_cut_off_ch_gs_right"):
+        for label in runs:
+            if label in ("fp64_inner", "fp32_inner") or label in ("fp64_inner_cut_off", "fp32_inner_cut_off",
+                                                                  "fp32_inner_cut_off_cut_preconditioner"):
+                continue
             if label in runs:
                 r = runs[label]
                 line[label].update({
@@ -584,7 +609,36 @@ def mixed_precision_solve_3d(args):
                 "max_abs_diff_c_vs_fp64_inner": float(np.abs(r["u"][0] - ref["u"][0]).max()),
                 "max_abs_diff_eta_vs_fp64_inner": float(np.abs(r["u"][2:] - ref["u"][2:]).max()),
                 "speedup_s_per_step_vs_fp64_inner": (ref["wall"] / len(ref["recs"])) / (r["wall"] / len(r["recs"]))}
+    if train_info is not None:
+        line["learned_training"] = train_info
     print(json.dumps(line), flush=True)
+
+
+def learned_guess_3d(args):
+    """Trains the 3D learned guess (FP64 trajectories of --train-seeds
+    lognormal packings of --train-n3 cells, --train-steps steps each; 3x3x3
+    equivariant net of --net-width channels; --train-iters Adam steps on
+    24^3 windows), optionally saves it (--save-net), then runs the 3D solve
+    workload with the --predictor kinds (learned among them)."""
+    import torch
+
+    from hpsint_b200 import learned_guess as LG
+    from hpsint_b200 import learned_guess3d as LG3
+    from hpsint_b200.predictor import NetConfig
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    net, norm, tr, info = LG3.train_learned_guess3d(
+        list(range(100, 100 + args.train_seeds)), n=args.train_n3, n_spheres=max(4, args.train_n3 ** 3 // 20000),
+        n_steps=args.train_steps, net_cfg=NetConfig(dim=3, width=args.net_width, layers=3),
+        train_cfg=LG.TrainConfig(window=24, batch=2, iterations=args.train_iters, smooth=args.smooth),
+        median=args.median, sigma=args.sigma, max_grains=args.max_grains)
+    info = {k: v for k, v in info.items() if k != "loss_history"} | {
+        "loss_first_last": [info["loss_history"][0], info["loss_history"][-1]] if info["loss_history"] else None}
+    if args.save_net:
+        LG.save_predictor(args.save_net, net, norm)
+    if "learned" not in args.predictor:
+        args.predictor = args.predictor + ",learned"
+    mixed_precision_solve_3d(args, learned=(net, norm), train_info=info)
 
 
 def cut_off_operator(args):
@@ -855,6 +909,9 @@ def main():
         return
     if args.workload == "nnconv":
         nn_conv(args)
+        return
+    if args.workload == "learned3d":
+        learned_guess_3d(args)
         return
     if args.workload == "solve3d":
         mixed_precision_solve_3d(args)

@@ -138,6 +138,13 @@ SIGNATURES = {
                                               ctypes.c_float, _c_void, _c_void, _c_void, _c_void, _c_void]),
     "sint_nn_apply_guess_f64": (_c_int, [_c_void, _c_void, _c_int64, _c_int64, _c_int, ctypes.c_float, _c_void,
                                          _c_void, _c_void, _c_void, _c_void]),
+    "sint_nn_features3d_f64": (_c_int, [_c_void, _c_void, _c_int64] + [_c_int] * 10 +
+                               [ctypes.c_float, _c_void, _c_void, _c_void, _c_int, _c_void]),
+    "sint_nn_targets3d_f64": (_c_int, [_c_void, _c_void, _c_void, _c_int64] + [_c_int] * 10 +
+                              [ctypes.c_float, _c_void, _c_void, _c_void, _c_int, _c_void]),
+    "sint_nn_apply_guess3d_f64": (_c_int, [_c_void, _c_void, _c_int64] + [_c_int] * 7 +
+                                  [ctypes.c_float, _c_void, _c_void, _c_void, _c_void, _c_void]),
+    "sint_nn_zero_pad_slices_f32": (_c_int, [_c_void, _c_int, _c_int, _c_int64, _c_void]),
     "sint_last_error": (ctypes.c_char_p, []),
     "sint_kernel_launch_count": (_c_int64, []),
 }

@@ -406,6 +406,120 @@ namespace sint
       }
   }
 
+  // --- 3D windows ------------------------------------------------------------
+  // A 3D window of D x H x W nodes is held depth-major with one zero slice
+  // before and after: [sample][D + 2][channels][H][W].  Every depth slice of
+  // every sample is then one contiguous [channels][H][W] image, so a 3x3x3
+  // convolution is three 3x3 convolutions of the slice batch shifted by one
+  // slice (the zero slices are the padding in depth).
+  __device__ __forceinline__ bool window_node3(int nx, int ny, int nz, int x0, int y0, int z0, int H, int W,
+                                               long long i, int &z, long long &node, long long &pix)
+  {
+    const long long hw = (long long)H * W;
+    z                  = int(i / hw);
+    pix                = i % hw;
+    const int yy = y0 + int(pix / W), xx = x0 + int(pix % W), zz = z0 + z;
+    const bool ok = xx >= 0 && xx < nx && yy >= 0 && yy < ny && zz >= 0 && zz < nz;
+    node          = ok ? ((long long)zz * ny + yy) * nx + xx : 0;
+    return ok;
+  }
+
+  __global__ void features3d_kernel(const double *__restrict__ u_n, const double *__restrict__ u_nm1, long long ld,
+                                    int nx, int ny, int nz, int G, int x0, int y0, int z0, int D, int H, int W,
+                                    float ratio, const float *__restrict__ scale, float *__restrict__ grain_in,
+                                    float *__restrict__ shared_in, int b)
+  {
+    const long long hw = (long long)H * W, n = hw * D;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      {
+        int       z;
+        long long node, pix;
+        const bool ok = window_node3(nx, ny, nz, x0, y0, z0, H, W, i, z, node, pix);
+        for (int k = 0; k < 2; ++k)
+          {
+            const double a = ok ? u_n[k * ld + node] : 0.0;
+            const double d = ok ? (u_n[k * ld + node] - u_nm1[k * ld + node]) * ratio : 0.0;
+            float *o       = shared_in + (((long long)b * (D + 2) + z + 1) * 4 + 2 * k) * hw + pix;
+            o[0]           = float(a) * scale[2 * k];
+            o[hw]          = float(d) * scale[2 * k + 1];
+          }
+        for (int g = 0; g < G; ++g)
+          {
+            const double a = ok ? u_n[(2 + g) * ld + node] : 0.0;
+            const double d = ok ? (u_n[(2 + g) * ld + node] - u_nm1[(2 + g) * ld + node]) * ratio : 0.0;
+            float *o       = grain_in + ((((long long)b * G + g) * (D + 2) + z + 1) * 2) * hw + pix;
+            o[0]           = float(a) * scale[4];
+            o[hw]          = float(d) * scale[5];
+          }
+      }
+  }
+
+  __global__ void targets3d_kernel(const double *__restrict__ u_np1, const double *__restrict__ u_n,
+                                   const double *__restrict__ u_nm1, long long ld, int nx, int ny, int nz, int G,
+                                   int x0, int y0, int z0, int D, int H, int W, float ratio,
+                                   const float *__restrict__ oscale, float *__restrict__ grain_t,
+                                   float *__restrict__ shared_t, int b)
+  {
+    const long long hw = (long long)H * W, n = hw * D;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      {
+        int       z;
+        long long node, pix;
+        const bool ok = window_node3(nx, ny, nz, x0, y0, z0, H, W, i, z, node, pix);
+        for (int k = 0; k < 2 + G; ++k)
+          {
+            double t = 0.0;
+            if (ok)
+              {
+                const long long o = k * ld + node;
+                t = (u_np1[o] - u_n[o]) - double(ratio) * (u_n[o] - u_nm1[o]);
+              }
+            const float v = float(t) * oscale[k < 2 ? k : 2];
+            if (k < 2)
+              shared_t[(((long long)b * (D + 2) + z + 1) * 2 + k) * hw + pix] = v;
+            else
+              grain_t[(((long long)b * G + (k - 2)) * (D + 2) + z + 1) * hw + pix] = v;
+          }
+      }
+  }
+
+  // Guess at the nodes of depth slices z0 .. z0 + D - 1 of the mesh from the
+  // outputs of a whole-plane window (H = ny, W = nx) whose slice 1 + off + j
+  // holds mesh slice z0 + j (off: the window's halo in depth).
+  __global__ void apply_guess3d_kernel(const double *__restrict__ u_n, const double *__restrict__ u_nm1, long long ld,
+                                       int nx, int ny, int G, int z0, int D, int off, int Dw, float ratio,
+                                       const float *__restrict__ oscale, const float *__restrict__ grain_out,
+                                       const float *__restrict__ shared_out, double *__restrict__ guess)
+  {
+    const long long hw = (long long)nx * ny, n = hw * D;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      {
+        const int       z    = int(i / hw);
+        const long long pix  = i % hw;
+        const long long node = (long long)(z0 + z) * hw + pix;
+        const long long ws   = 1 + off + z; // window slice
+        for (int k = 0; k < 2 + G; ++k)
+          {
+            const long long o = k * ld + node;
+            const float out = k < 2 ? shared_out[(ws * 2 + k) * hw + pix]
+                                    : grain_out[((long long)(k - 2) * (Dw + 2) + ws) * hw + pix];
+            guess[o] = u_n[o] + double(ratio) * (u_n[o] - u_nm1[o]) + double(out / oscale[k < 2 ? k : 2]);
+          }
+      }
+  }
+
+  // zero slices 0 and D2 - 1 of each of S samples of slice_elems floats
+  __global__ void zero_pad_slices_kernel(float *__restrict__ x, int S, int D2, long long slice_elems)
+  {
+    const long long n = 2ll * S * slice_elems;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      {
+        const long long s = i / (2 * slice_elems), r = i % (2 * slice_elems);
+        const long long sl = r < slice_elems ? 0 : D2 - 1;
+        x[(s * D2 + sl) * slice_elems + r % slice_elems] = 0.f;
+      }
+  }
+
   static int launch_err(const char *what)
   {
     count_launches(1);
@@ -623,6 +737,60 @@ int sint_nn_increment_scales_f64(const double *u_n, const double *u_nm1, int64_t
     return rc;
   increment_scales_kernel<<<1, 32, 0, s>>>(work, base, dt, scale, oscale);
   return launch_err("sint_nn_increment_scales_f64: scales");
+}
+
+int sint_nn_features3d_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int nx, int ny, int nz,
+                           int G, int x0, int y0, int z0, int D, int H, int W, float ratio, const float *scale,
+                           float *grain_in, float *shared_in, int b, sint_stream_t s)
+{
+  if (!u_n || !u_nm1 || !scale || !grain_in || !shared_in || G < 1 || D < 1 || H < 1 || W < 1 || b < 0)
+    {
+      set_error("sint_nn_features3d_f64: bad argument");
+      return SINT_ERR_ARG;
+    }
+  features3d_kernel<<<1184, 256, 0, s>>>(u_n, u_nm1, block_stride, nx, ny, nz, G, x0, y0, z0, D, H, W, ratio, scale,
+                                         grain_in, shared_in, b);
+  return launch_err("sint_nn_features3d_f64");
+}
+
+int sint_nn_targets3d_f64(const double *u_np1, const double *u_n, const double *u_nm1, int64_t block_stride, int nx,
+                          int ny, int nz, int G, int x0, int y0, int z0, int D, int H, int W, float ratio,
+                          const float *oscale, float *grain_t, float *shared_t, int b, sint_stream_t s)
+{
+  if (!u_np1 || !u_n || !u_nm1 || !oscale || !grain_t || !shared_t || G < 1 || D < 1 || H < 1 || W < 1 || b < 0)
+    {
+      set_error("sint_nn_targets3d_f64: bad argument");
+      return SINT_ERR_ARG;
+    }
+  targets3d_kernel<<<1184, 256, 0, s>>>(u_np1, u_n, u_nm1, block_stride, nx, ny, nz, G, x0, y0, z0, D, H, W, ratio,
+                                        oscale, grain_t, shared_t, b);
+  return launch_err("sint_nn_targets3d_f64");
+}
+
+int sint_nn_apply_guess3d_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int nx, int ny, int G,
+                              int z0, int D, int halo, int Dw, float ratio, const float *oscale, const float *grain_out,
+                              const float *shared_out, double *guess, sint_stream_t s)
+{
+  if (!u_n || !u_nm1 || !oscale || !grain_out || !shared_out || !guess || G < 1 || D < 1 || halo < 0 ||
+      halo + D > Dw || nx < 1 || ny < 1 || z0 < 0)
+    {
+      set_error("sint_nn_apply_guess3d_f64: bad argument");
+      return SINT_ERR_ARG;
+    }
+  apply_guess3d_kernel<<<1184, 256, 0, s>>>(u_n, u_nm1, block_stride, nx, ny, G, z0, D, halo, Dw, ratio, oscale,
+                                            grain_out, shared_out, guess);
+  return launch_err("sint_nn_apply_guess3d_f64");
+}
+
+int sint_nn_zero_pad_slices_f32(float *x, int S, int D2, int64_t slice_elems, sint_stream_t s)
+{
+  if (!x || S < 1 || D2 < 2 || slice_elems < 1)
+    {
+      set_error("sint_nn_zero_pad_slices_f32: bad argument");
+      return SINT_ERR_ARG;
+    }
+  zero_pad_slices_kernel<<<592, 256, 0, s>>>(x, S, D2, slice_elems);
+  return launch_err("sint_nn_zero_pad_slices_f32");
 }
 
 } // extern "C"

@@ -596,15 +596,16 @@ def save_predictor(path, net: EquivariantNet, norm: Normaliser):
     cfg = net.cfg
     np.savez(path, params=net.params.detach().cpu().numpy(), base=np.asarray(norm.base, np.float64),
              cfg=np.asarray([cfg.width, cfg.layers, cfg.grain_in, cfg.shared_in, cfg.shared_out, cfg.seed],
-                            np.int64), slope=np.float64(cfg.slope))
+                            np.int64), slope=np.float64(cfg.slope), dim=np.int64(cfg.dim))
 
 
 def load_predictor(path):
     """(net, normaliser) from save_predictor's file."""
     with np.load(path) as f:
         w, layers, gi, si, so, seed = (int(x) for x in f["cfg"])
+        dim = int(f["dim"]) if "dim" in f.files else 2
         net = EquivariantNet(NetConfig(width=w, layers=layers, grain_in=gi, shared_in=si, shared_out=so,
-                                       slope=float(f["slope"]), seed=seed))
+                                       slope=float(f["slope"]), seed=seed, dim=dim))
         params = torch.as_tensor(f["params"], dtype=torch.float32)
         if params.numel() != net.n_params:
             raise ValueError(f"{path}: {params.numel()} parameters, the architecture needs {net.n_params}")

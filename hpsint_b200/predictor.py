@@ -95,6 +95,56 @@ def conv3x3_weight_grad(x, dout, dw, db, ws, accumulate=True):
                                               _p(work), _s()), "sint_nn_conv3x3_wgrad_f32")
 
 
+# --- 3D: depth-padded windows [sample][D + 2][channels][H][W] ----------------------
+# Every depth slice of every sample is one contiguous [C][H][W] image; a 3x3x3
+# convolution is three 3x3 convolutions of the slice batch shifted by -1, 0,
+# +1 slices (weights w3 [3][Cout][Cin][3][3], index 0 = the slice below), the
+# zero slices around each sample being the depth padding.  Shifted batches
+# also write the padding slices of the output (across sample boundaries);
+# they are zeroed after every convolution.
+
+def _slices(t):
+    S, D2, C, H, W = t.shape
+    return t.view(S * D2, C, H, W)
+
+
+def zero_pads(t):
+    L.check(L.lib().sint_nn_zero_pad_slices_f32(_p(t), t.shape[0], t.shape[1], t[0, 0].numel(), _s()),
+            "sint_nn_zero_pad_slices_f32")
+
+
+def conv3x3x3(x, w3, bias, out, accumulate=False, tc_status=None):
+    """out (+)= conv(x, w3) + bias on depth-padded windows; tc_status: run on the
+    tensor cores (TF32 products) and report timed-out waits there."""
+    xs, os_ = _slices(x), _slices(out)
+    n = xs.shape[0]
+    for j, dz in enumerate((-1, 0, 1)):
+        src, dst = xs[1 + dz:n - 1 + dz], os_[1:n - 1]
+        acc, b = accumulate or j > 0, (bias if j == 0 else None)
+        if tc_status is not None:
+            conv3x3_tc(src, w3[j], b, dst, tc_status, acc)
+        else:
+            conv3x3(src, w3[j], b, dst, acc)
+    zero_pads(out)
+
+
+def conv3x3x3_input_grad(dout, w3, din, accumulate=False):
+    """din (+)= d(conv(x, w3))/dx applied to dout: din[z] = sum_dz W_dz^T * dout[z - dz]."""
+    ds, dis = _slices(dout), _slices(din)
+    n = ds.shape[0]
+    for j, dz in enumerate((-1, 0, 1)):
+        conv3x3_input_grad(ds[1 - dz:n - 1 - dz], w3[j], dis[1:n - 1], accumulate or j > 0)
+    zero_pads(din)
+
+
+def conv3x3x3_weight_grad(x, dout, dw3, db, ws):
+    """dw3[dz] += sum over slices of x[z + dz] correlated with dout[z]; db += sum of dout."""
+    xs, ds = _slices(x), _slices(dout)
+    n = xs.shape[0]
+    for j, dz in enumerate((-1, 0, 1)):
+        conv3x3_weight_grad(xs[1 + dz:n - 1 + dz], ds[1:n - 1], dw3[j], db if j == 1 else None, ws)
+
+
 def leaky(x, y, slope):
     L.check(L.lib().sint_nn_leaky_relu_f32(x.numel(), slope, _p(x), _p(y), _s()), "sint_nn_leaky_relu_f32")
 
@@ -118,6 +168,7 @@ def grain_bcast_add(Q, B, G, Z):
 class NetConfig:
     width: int = 32
     layers: int = 4
+    dim: int = 2          # 3: 3x3x3 convolutions on depth-padded windows
     grain_in: int = 2     # eta_i, extrapolated eta_i increment
     shared_in: int = 4    # c, c increment, mu, mu increment
     shared_out: int = 2   # corrections of c and mu (one grain channel per eta_i)
@@ -141,9 +192,11 @@ class EquivariantNet:
             self.dims.append((cg, cs, go, so))
             cg, cs = go, so
         self.shapes = []
+        cw = (lambda co, ci: (co, ci, 3, 3)) if cfg.dim == 2 else (lambda co, ci: (3, co, ci, 3, 3))
         for (cg, cs, go, so) in self.dims:
-            self.shapes.append({"A": (go, cg, 3, 3), "B": (go, cg, 3, 3), "C": (go, cs, 3, 3), "D": (so, cs, 3, 3),
-                                "E": (so, cg, 3, 3), "a": (go,), "d": (so,)})
+            self.shapes.append({"A": cw(go, cg), "B": cw(go, cg), "C": cw(go, cs), "D": cw(so, cs),
+                                "E": cw(so, cg), "a": (go,), "d": (so,)})
+        self.taps = 9 if cfg.dim == 2 else 27
         n = sum(math.prod(s) for sh in self.shapes for s in sh.values())
         self.n_params = n
         self.params = torch.zeros(n, dtype=torch.float32, device="cuda")
@@ -174,11 +227,11 @@ class EquivariantNet:
         for l, (cg, cs, go, so) in enumerate(self.dims):
             last = l == len(self.dims) - 1
             for k in ("A", "B", "C"):
-                fan = 9 * (2 * cg + cs)
+                fan = self.taps * (2 * cg + cs)
                 std = math.sqrt(2.0 / fan) * (0.1 if last else 1.0)
                 self.w[l][k].copy_(torch.randn(self.shapes[l][k], generator=gen) * std)
             for k in ("D", "E"):
-                fan = 9 * (cs + cg)
+                fan = self.taps * (cs + cg)
                 std = math.sqrt(2.0 / fan) * (0.1 if last else 1.0)
                 self.w[l][k].copy_(torch.randn(self.shapes[l][k], generator=gen) * std)
 
@@ -187,29 +240,34 @@ class EquivariantNet:
         """xg [B*G][grain_in][H][W], xs [B][shared_in][H][W] -> (yg [B*G][1], ys [B][2]).
         tensor_cores: run the convolutions on the tensor cores (TF32 products,
         FP32 accumulation; inference) instead of the FP32 kernel."""
-        H, W = xs.shape[2], xs.shape[3]
-        if tensor_cores and not keep and max(max(d) for d in self.dims) <= 32:
+        H, W = xs.shape[-2], xs.shape[-1]
+        if self.cfg.dim == 2 and tensor_cores and not keep and max(max(d) for d in self.dims) <= 32:
             return self._forward_fused(xg, xs, B, G, H, W)
         cache = []
         hg, hs = xg, xs
+        # 2D: [n][C][H][W]; 3D: [n][D + 2][C][H][W]
+        shape = (lambda n, c: (n, c, H, W)) if self.cfg.dim == 2 else (lambda n, c: (n, xs.shape[1], c, H, W))
 
         def conv(x, wt, bias, out, accumulate=False):
-            if tensor_cores and wt.shape[0] <= 32 and wt.shape[1] <= 32:
+            tc = tensor_cores and wt.shape[-4] <= 32 and wt.shape[-3] <= 32
+            if self.cfg.dim == 3:
+                conv3x3x3(x, wt, bias, out, accumulate, self.tc_status if tc else None)
+            elif tc:
                 conv3x3_tc(x, wt, bias, out, self.tc_status, accumulate)
             else:
                 conv3x3(x, wt, bias, out, accumulate)
 
         for l, (cg, cs, go, so) in enumerate(self.dims):
             w = self.w[l]
-            P = torch.empty((B, cg, H, W), dtype=torch.float32, device="cuda")
+            P = torch.empty(shape(B, cg), dtype=torch.float32, device="cuda")
             grain_sum(hg, B, G, P)
-            Zg = torch.empty((B * G, go, H, W), dtype=torch.float32, device="cuda")
+            Zg = torch.empty(shape(B * G, go), dtype=torch.float32, device="cuda")
             conv(hg, w["A"], w["a"], Zg)
-            Q = torch.empty((B, go, H, W), dtype=torch.float32, device="cuda")
+            Q = torch.empty(shape(B, go), dtype=torch.float32, device="cuda")
             conv(P, w["B"], None, Q)
             conv(hs, w["C"], None, Q, accumulate=True)
             grain_bcast_add(Q, B, G, Zg)
-            Zs = torch.empty((B, so, H, W), dtype=torch.float32, device="cuda")
+            Zs = torch.empty(shape(B, so), dtype=torch.float32, device="cuda")
             conv(hs, w["D"], w["d"], Zs)
             conv(P, w["E"], None, Zs, accumulate=True)
             if keep:
@@ -257,25 +315,31 @@ class EquivariantNet:
                 leaky_bwd(Zs, dZs, dZs, self.cfg.slope)
             w, g = self.w[l], self.g[l]
             cg, cs, go, so = self.dims[l]
-            H, W = hs.shape[2], hs.shape[3]
-            dQ = torch.empty((B, go, H, W), dtype=torch.float32, device="cuda")
+            H, W = hs.shape[-2], hs.shape[-1]
+            if self.cfg.dim == 2:
+                shape = lambda n, c: (n, c, H, W)
+                wgrad, igrad = conv3x3_weight_grad, conv3x3_input_grad
+            else:
+                shape = lambda n, c: (n, hs.shape[1], c, H, W)
+                wgrad, igrad = conv3x3x3_weight_grad, conv3x3x3_input_grad
+            dQ = torch.empty(shape(B, go), dtype=torch.float32, device="cuda")
             grain_sum(dZg, B, G, dQ)
-            conv3x3_weight_grad(hg, dZg, g["A"], g["a"], self.ws)
-            conv3x3_weight_grad(P, dQ, g["B"], None, self.ws)
-            conv3x3_weight_grad(hs, dQ, g["C"], None, self.ws)
-            conv3x3_weight_grad(hs, dZs, g["D"], g["d"], self.ws)
-            conv3x3_weight_grad(P, dZs, g["E"], None, self.ws)
+            wgrad(hg, dZg, g["A"], g["a"], self.ws)
+            wgrad(P, dQ, g["B"], None, self.ws)
+            wgrad(hs, dQ, g["C"], None, self.ws)
+            wgrad(hs, dZs, g["D"], g["d"], self.ws)
+            wgrad(P, dZs, g["E"], None, self.ws)
             if l == 0:
                 break
-            dhg = torch.empty((B * G, cg, H, W), dtype=torch.float32, device="cuda")
-            conv3x3_input_grad(dZg, w["A"], dhg)
-            dP = torch.empty((B, cg, H, W), dtype=torch.float32, device="cuda")
-            conv3x3_input_grad(dQ, w["B"], dP)
-            conv3x3_input_grad(dZs, w["E"], dP, accumulate=True)
+            dhg = torch.empty(shape(B * G, cg), dtype=torch.float32, device="cuda")
+            igrad(dZg, w["A"], dhg)
+            dP = torch.empty(shape(B, cg), dtype=torch.float32, device="cuda")
+            igrad(dQ, w["B"], dP)
+            igrad(dZs, w["E"], dP, accumulate=True)
             grain_bcast_add(dP, B, G, dhg)
-            dhs = torch.empty((B, cs, H, W), dtype=torch.float32, device="cuda")
-            conv3x3_input_grad(dQ, w["C"], dhs)
-            conv3x3_input_grad(dZs, w["D"], dhs, accumulate=True)
+            dhs = torch.empty(shape(B, cs), dtype=torch.float32, device="cuda")
+            igrad(dQ, w["C"], dhs)
+            igrad(dZs, w["D"], dhs, accumulate=True)
             dZg, dZs = dhg, dhs
 
     def check_tensor_cores(self):

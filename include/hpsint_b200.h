@@ -568,6 +568,31 @@ int sint_nn_apply_guess_f64(const double *u_n, const double *u_nm1, int64_t bloc
                             float ratio, const float *oscale, const float *grain_out, const float *shared_out,
                             double *guess, sint_stream_t stream);
 
+/* 3D windows of D x H x W nodes at (x0, y0, z0) of an nx x ny x nz node mesh
+ * (x fastest), held depth-major with a zero slice before and after:
+ * grain_in [(b G + g)][D + 2][2][H][W], shared_in [b][D + 2][4][H][W];
+ * the features of sint_nn_features_f64, written to slices 1 .. D (the zero
+ * slices are left alone).  A 3x3x3 convolution of such a tensor is three 3x3
+ * convolutions of its slice batch shifted by -1, 0, +1 slices. */
+int sint_nn_features3d_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int nx, int ny, int nz,
+                           int G, int x0, int y0, int z0, int D, int H, int W, float ratio, const float *scale,
+                           float *grain_in, float *shared_in, int b, sint_stream_t stream);
+/* Training targets of a 3D window (layout grain_t [(b G + g)][D + 2][1][H][W],
+ * shared_t [b][D + 2][2][H][W]), as sint_nn_targets_f64. */
+int sint_nn_targets3d_f64(const double *u_np1, const double *u_n, const double *u_nm1, int64_t block_stride, int nx,
+                          int ny, int nz, int G, int x0, int y0, int z0, int D, int H, int W, float ratio,
+                          const float *oscale, float *grain_t, float *shared_t, int b, sint_stream_t stream);
+/* guess = u_n + ratio (u_n - u_{n-1}) + out / oscale at the nodes of mesh
+ * depth slices z0 .. z0 + D - 1, from the outputs of a whole-plane 3D window
+ * (H = ny, W = nx) of Dw depth slices starting at mesh slice z0 - halo (its
+ * padded slice 1 + halo + j holds mesh slice z0 + j). */
+int sint_nn_apply_guess3d_f64(const double *u_n, const double *u_nm1, int64_t block_stride, int nx, int ny, int G,
+                              int z0, int D, int halo, int Dw, float ratio, const float *oscale, const float *grain_out,
+                              const float *shared_out, double *guess, sint_stream_t stream);
+/* Zero depth slices 0 and D2 - 1 of each of S samples (slice_elems floats per
+ * slice): the padding of a 3D window after a convolution wrote into it. */
+int sint_nn_zero_pad_slices_f32(float *x, int S, int D2, int64_t slice_elems, sint_stream_t stream);
+
 /* Per-state scales of the network inputs and outputs: with m_c, m_mu, m_eta
  * the largest |ratio (u_n - u_{n-1})| of c, mu and any eta_i over the mesh and
  * dt the step being predicted, scale = (base[0], 1/m_c, base[1], 1/m_mu,

@@ -164,3 +164,130 @@ def test_curvature_loss_term_and_gradient_match_autograd():
     ref.backward()
     assert abs(float(loss.item()) - float(ref.item())) <= 1e-5 * float(ref.item())
     assert rel((grad - g0).cpu().numpy(), pp.grad.cpu().numpy()) < 1e-5
+
+
+# --- 3D: depth-padded windows [n][D + 2][C][H][W] -------------------------------------
+
+def dev_padded(x):
+    """[N][D][C][H][W] -> device [N][D + 2][C][H][W] with zero depth padding."""
+    x = np.asarray(x, np.float32)
+    out = np.zeros((x.shape[0], x.shape[1] + 2) + x.shape[2:], np.float32)
+    out[:, 1:-1] = x
+    return torch.tensor(out, device="cuda")
+
+
+def inner(t):
+    a = t.cpu().numpy()
+    assert not a[:, 0].any() and not a[:, -1].any(), "depth padding must stay zero"
+    return a[:, 1:-1]
+
+
+@pytest.mark.parametrize("N,D,Cin,Cout,H,W", [(2, 5, 3, 4, 11, 13), (1, 3, 32, 32, 17, 9)])
+def test_conv3x3x3_forward_and_gradients(N, D, Cin, Cout, H, W):
+    from hpsint_b200 import predictor as P
+    rng = np.random.default_rng(D * 10 + Cin)
+    x, w3, b = rng.normal(size=(N, D, Cin, H, W)), rng.normal(size=(3, Cout, Cin, 3, 3)), rng.normal(size=Cout)
+    dout = rng.normal(size=(N, D, Cout, H, W))
+    out = torch.zeros((N, D + 2, Cout, H, W), device="cuda")
+    P.conv3x3x3(dev_padded(x), dev(w3), dev(b), out)
+    assert rel(inner(out), R.conv3x3x3(x, w3, b)) < 2e-5
+    din = torch.zeros((N, D + 2, Cin, H, W), device="cuda")
+    P.conv3x3x3_input_grad(dev_padded(dout), dev(w3), din)
+    assert rel(inner(din), R.conv3x3x3_input_grad(dout, w3)) < 2e-5
+    dw, db = torch.zeros((3, Cout, Cin, 3, 3), device="cuda"), torch.zeros(Cout, device="cuda")
+    P.conv3x3x3_weight_grad(dev_padded(x), dev_padded(dout), dw, db, P._Workspace())
+    rw, rb = R.conv3x3x3_weight_grad(x, dout)
+    assert rel(dw.cpu().numpy(), rw) < 2e-5 and rel(db.cpu().numpy(), rb) < 2e-5
+    # tensor cores (TF32 products)
+    out_tc = torch.zeros_like(out)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    P.conv3x3x3(dev_padded(x), dev(w3), dev(b), out_tc, tc_status=status)
+    assert int(status.item()) == 0
+    assert rel(inner(out_tc), R.conv3x3x3(x, w3, b)) < 3e-3
+
+
+def test_network3d_forward_backward_match_reference():
+    from hpsint_b200 import predictor as P
+    net = P.EquivariantNet(P.NetConfig(width=6, layers=3, seed=3, dim=3))
+    B, G, D, H, W = 2, 3, 4, 9, 10
+    rng = np.random.default_rng(6)
+    xg, xs = rng.normal(size=(B * G, D, 2, H, W)), rng.normal(size=(B, D, 4, H, W))
+    tg, ts = rng.normal(size=(B * G, D, 1, H, W)), rng.normal(size=(B, D, 2, H, W))
+    yg, ys, cache = net.forward(dev_padded(xg), dev_padded(xs), B, G, keep=True)
+    params = to_ref(net)
+    ryg, rys, rcache = R.forward(params, xg, xs, B, G, net.cfg.slope)
+    assert rel(inner(yg), ryg) < 2e-5 and rel(inner(ys), rys) < 2e-5
+    net.zero_grad()
+    net.backward(cache, dev_padded(ryg - tg), dev_padded(rys - ts), B, G)
+    rgrads = R.backward(params, rcache, ryg - tg, rys - ts, B, G, net.cfg.slope)
+    for l, layer in enumerate(net.g):
+        for k, g in layer.items():
+            assert rel(g.cpu().numpy(), rgrads[l][k]) < 1e-4, (l, k)
+    # inference on the tensor cores
+    tyg, tys, _ = net.forward(dev_padded(xg), dev_padded(xs), B, G, tensor_cores=True)
+    net.check_tensor_cores()
+    assert rel(inner(tyg), ryg) < 5e-3 and rel(inner(tys), rys) < 5e-3
+
+
+def test_window3d_features_targets_and_guess():
+    """sint_nn_features3d / targets3d / apply_guess3d against NumPy on a random
+    3D state, with a window that reaches past the mesh (zeros there)."""
+    import ctypes
+    from hpsint_b200 import _lib as L
+    nx, ny, nz, G = 7, 6, 5, 2
+    N = nx * ny * nz
+    ld = (N + 31) // 32 * 32
+    rng = np.random.default_rng(11)
+    u = [rng.normal(size=(2 + G, ld)) for _ in range(3)]  # u_{n-1}, u_n, u_{n+1}
+    um, un, up = (torch.tensor(a, device="cuda") for a in u)
+    scale = torch.tensor([1.5, 2.0, 0.5, 3.0, 1.25, 0.75], dtype=torch.float32, device="cuda")
+    oscale = torch.tensor([2.0, 0.5, 4.0], dtype=torch.float32, device="cuda")
+    x0, y0, z0, D, H, W, r = -1, 2, 1, 5, 5, 8, 0.8
+    xg = torch.zeros((G, D + 2, 2, H, W), device="cuda")
+    xs = torch.zeros((1, D + 2, 4, H, W), device="cuda")
+    tg = torch.zeros((G, D + 2, 1, H, W), device="cuda")
+    ts = torch.zeros((1, D + 2, 2, H, W), device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    lib = L.lib()
+    L.check(lib.sint_nn_features3d_f64(p(un), p(um), ld, nx, ny, nz, G, x0, y0, z0, D, H, W, r, p(scale), p(xg),
+                                       p(xs), 0, s), "features3d")
+    L.check(lib.sint_nn_targets3d_f64(p(up), p(un), p(um), ld, nx, ny, nz, G, x0, y0, z0, D, H, W, r, p(oscale),
+                                      p(tg), p(ts), 0, s), "targets3d")
+    sc, osc = scale.cpu().numpy(), oscale.cpu().numpy()
+    exg, exs = np.zeros((G, D, 2, H, W)), np.zeros((1, D, 4, H, W))
+    etg, ets = np.zeros((G, D, 1, H, W)), np.zeros((1, D, 2, H, W))
+    for z in range(D):
+        for y in range(H):
+            for x in range(W):
+                zz, yy, xx = z0 + z, y0 + y, x0 + x
+                if not (0 <= zz < nz and 0 <= yy < ny and 0 <= xx < nx):
+                    continue
+                n = (zz * ny + yy) * nx + xx
+                for k in range(2 + G):
+                    a, d = u[1][k, n], (u[1][k, n] - u[0][k, n]) * r
+                    t = (u[2][k, n] - u[1][k, n]) - r * (u[1][k, n] - u[0][k, n])
+                    if k < 2:
+                        exs[0, z, 2 * k:2 * k + 2, y, x] = a * sc[2 * k], d * sc[2 * k + 1]
+                        ets[0, z, k, y, x] = t * osc[k]
+                    else:
+                        exg[k - 2, z, :, y, x] = a * sc[4], d * sc[5]
+                        etg[k - 2, z, 0, y, x] = t * osc[2]
+    for got, ref in ((xg, exg), (xs, exs), (tg, etg), (ts, ets)):
+        assert np.allclose(inner(got), ref, rtol=1e-6, atol=1e-6)
+    # whole-plane window of mesh slices 1..4 with a halo of 1; guess for slices 2..3
+    Dw, halo, zs, Dg = 4, 1, 2, 2
+    yg = torch.tensor(rng.normal(size=(G, Dw + 2, 1, ny, nx)), dtype=torch.float32, device="cuda")
+    ys = torch.tensor(rng.normal(size=(1, Dw + 2, 2, ny, nx)), dtype=torch.float32, device="cuda")
+    guess = torch.zeros_like(un)
+    L.check(lib.sint_nn_apply_guess3d_f64(p(un), p(um), ld, nx, ny, G, zs, Dg, halo, Dw, r, p(oscale), p(yg), p(ys),
+                                          p(guess), s), "apply_guess3d")
+    gy, sy, gs = yg.cpu().numpy(), ys.cpu().numpy(), guess.cpu().numpy()
+    for z in range(zs, zs + Dg):
+        wsl = 1 + halo + (z - zs)
+        for k in range(2 + G):
+            out = sy[0, wsl, k] if k < 2 else gy[k - 2, wsl, 0]
+            sl = slice(z * nx * ny, (z + 1) * nx * ny)
+            ref = u[1][k, sl] + r * (u[1][k, sl] - u[0][k, sl]) + out.ravel() / osc[min(k, 2)]
+            assert np.allclose(gs[k, sl], ref, rtol=1e-6, atol=1e-6)
+    assert not gs[:, :zs * nx * ny].any() and not gs[:, (zs + Dg) * nx * ny:N].any()
