@@ -182,7 +182,7 @@ class LearnedPredictor3D:
     network on the tensor cores, FP64 guess.  safeguard: keep the smaller
     residual of this guess and hpsint's linear one (device only)."""
 
-    def __init__(self, op: SinteringOperatorGeneric, net: EquivariantNet, norm: Normaliser, slab=32,
+    def __init__(self, op: SinteringOperatorGeneric, net: EquivariantNet, norm: Normaliser, slab=64,
                  tensor_cores=True, safeguard=False):
         if op.mesh.dim != 3 or net.cfg.dim != 3:
             raise ValueError("LearnedPredictor3D needs a 3D mesh and a NetConfig(dim=3) network")
