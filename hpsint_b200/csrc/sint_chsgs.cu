@@ -366,19 +366,62 @@ namespace sint
       }
   }
 
-  // Centre-block inverses (guarded as precond_invert_kernel) in both
-  // precisions and the FP32 copy of the matrix.
+  // The nodes of colour c (bit d = parity of the index in direction d) form
+  // the lattice x = 2 a + p0, y = 2 b + p1 (, z = 2 c + p2) of m[c][d] nodes
+  // per direction, t = a + m0 (b + m1 c) their index in it.  The FP32 copy of
+  // the matrix and of the centre-block inverses, which the FP32 Krylov solve
+  // sweeps, is stored colour by colour, each colour's rows entry-major over
+  // t: one colour's sweep then reads them contiguously (in node order a
+  // colour's rows are every other element in x, and half of every sector read
+  // would be another colour's).
+  struct ColourLattice
+  {
+    long long cnt[8]; // nodes of the colour
+    long long off[8]; // nodes of the colours before it
+    int       m[8][3];
+  };
+
   template <int DIM>
-  __global__ void ch_matrix_finish_kernel(long long N, long long ld, const double *__restrict__ A,
+  ColourLattice colour_lattice(const Grid &g)
+  {
+    ColourLattice L{};
+    long long     off = 0;
+    for (int col = 0; col < 8; ++col)
+      {
+        long long cnt = col < (1 << DIM) ? 1 : 0;
+        for (int d = 0; d < 3; ++d)
+          {
+            L.m[col][d] = d < DIM ? (g.nn[d] - ((col >> d) & 1) + 1) / 2 : 1;
+            cnt *= L.m[col][d];
+          }
+        L.cnt[col] = cnt;
+        L.off[col] = off;
+        off += cnt;
+      }
+    return L;
+  }
+
+  // Centre-block inverses (guarded as precond_invert_kernel) in both
+  // precisions and the FP32 copies of the matrix and of the inverses in the
+  // colour-major layout.
+  template <int DIM>
+  __global__ void ch_matrix_finish_kernel(const Grid g, const ColourLattice cl, const double *__restrict__ A,
                                           float *__restrict__ A32, double *__restrict__ dinv64,
                                           float *__restrict__ dinv32)
   {
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N)
+    if (n >= g.N)
       return;
-    constexpr int NK = ChStencil<DIM>::NK, CTR = ChStencil<DIM>::CTR;
+    constexpr int   NK = ChStencil<DIM>::NK, CTR = ChStencil<DIM>::CTR;
+    const long long ld = g.ld;
+    const int       x = int(n % g.nn[0]), y = int((n / g.nn[0]) % g.nn[1]);
+    const int       z = DIM == 3 ? int(n / ((long long)g.nn[0] * g.nn[1])) : 0;
+    const int       col = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+    const long long t   = (x >> 1) + (long long)cl.m[col][0] * ((y >> 1) + (long long)cl.m[col][1] * (z >> 1));
+    const long long cnt = cl.cnt[col];
+    float          *a32 = A32 + cl.off[col] * (NK * 4) + t;
     for (int i = 0; i < NK * 4; ++i)
-      A32[i * ld + n] = float(A[i * ld + n]);
+      a32[i * cnt] = float(A[i * ld + n]);
     const double a = A[(CTR * 4 + 0) * ld + n], b = A[(CTR * 4 + 1) * ld + n], c = A[(CTR * 4 + 2) * ld + n],
                  d = A[(CTR * 4 + 3) * ld + n];
     const double det   = a * d - b * c;
@@ -400,30 +443,36 @@ namespace sint
     const double inv[4] = {i00, i01, i10, i11};
     for (int e = 0; e < 4; ++e)
       {
-        dinv64[e * ld + n] = inv[e];
-        dinv32[e * ld + n] = float(inv[e]);
+        dinv64[e * ld + n]                   = inv[e];
+        dinv32[cl.off[col] * 4 + e * cnt + t] = float(inv[e]);
       }
   }
 
   // One colour of the forward (FWD) or backward sweep; z holds the c and mu
   // blocks of the result (y of the forward sweep, overwritten by the
   // backward one).  Neighbours are summed in the order k = 0 .. NK - 1.
+  // The matrix and the inverses: node-major rows (FP64, stride ld) or the
+  // colour-major FP32 copies (entry stride = the colour's node count).
   template <int DIM, typename R, bool FWD>
   __global__ void __launch_bounds__(256)
-    ch_sgs_kernel(const Grid g, int colour, const R *__restrict__ A, const R *__restrict__ dinv,
-                  const R *__restrict__ r, R *__restrict__ z)
+    ch_sgs_kernel(const Grid g, int colour, const ColourLattice cl, const R *__restrict__ A,
+                  const R *__restrict__ dinv, const R *__restrict__ r, R *__restrict__ z)
   {
-    constexpr int NK = ChStencil<DIM>::NK;
-    const int     p[3] = {colour & 1, (colour >> 1) & 1, (colour >> 2) & 1};
-    const int     m0 = (g.nn[0] - p[0] + 1) / 2, m1 = (g.nn[1] - p[1] + 1) / 2;
-    const int     m2 = DIM == 3 ? (g.nn[2] - p[2] + 1) / 2 : 1;
+    constexpr int  NK = ChStencil<DIM>::NK;
+    constexpr bool CM = sizeof(R) == 4; // colour-major matrix
+    const int      p[3] = {colour & 1, (colour >> 1) & 1, (colour >> 2) & 1};
+    const int      m0 = cl.m[colour][0], m1 = cl.m[colour][1];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)m0 * m1 * m2)
+    if (t >= cl.cnt[colour])
       return;
     const int a = int(t % m0), b = int((t / m0) % m1), c = int(t / ((long long)m0 * m1));
     const int x = 2 * a + p[0], y = 2 * b + p[1], zz = DIM == 3 ? 2 * c + p[2] : 0;
     const long long n  = node_index(g, x, y, zz);
     const long long ld = g.ld;
+    // row entries of this node: A_row[i * as]
+    const long long as    = CM ? cl.cnt[colour] : ld;
+    const R        *A_row = CM ? A + cl.off[colour] * (NK * 4) + t : A + n;
+    const R        *d_row = CM ? dinv + cl.off[colour] * 4 + t : dinv + n;
     R               s0 = R(0), s1 = R(0);
 #pragma unroll
     for (int k = 0; k < NK; ++k)
@@ -438,10 +487,10 @@ namespace sint
           continue;
         const long long j  = node_index(g, xx, yy, zn);
         const R         v0 = z[j], v1 = z[ld + j];
-        s0 += A[(k * 4 + 0) * ld + n] * v0 + A[(k * 4 + 1) * ld + n] * v1;
-        s1 += A[(k * 4 + 2) * ld + n] * v0 + A[(k * 4 + 3) * ld + n] * v1;
+        s0 += A_row[(k * 4 + 0) * as] * v0 + A_row[(k * 4 + 1) * as] * v1;
+        s1 += A_row[(k * 4 + 2) * as] * v0 + A_row[(k * 4 + 3) * as] * v1;
       }
-    const R i00 = dinv[n], i01 = dinv[ld + n], i10 = dinv[2 * ld + n], i11 = dinv[3 * ld + n];
+    const R i00 = d_row[0], i01 = d_row[as], i10 = d_row[2 * as], i11 = d_row[3 * as];
     if (FWD)
       {
         const R a0 = r[n] - s0, a1 = r[ld + n] - s1;
@@ -506,8 +555,8 @@ namespace sint
           return e;
       }
     const long long nb = (c->N + 255) / 256;
-    ch_matrix_finish_kernel<DIM><<<dim3((unsigned)nb), 256, 0, s>>>(c->N, c->ld, c->ch_A64, c->ch_A32, c->ch_dinv64,
-                                                                   c->ch_dinv32);
+    ch_matrix_finish_kernel<DIM><<<dim3((unsigned)nb), 256, 0, s>>>(g, colour_lattice<DIM>(g), c->ch_A64, c->ch_A32,
+                                                                   c->ch_dinv64, c->ch_dinv32);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -560,18 +609,17 @@ namespace sint
   template <int DIM, typename R>
   static cudaError_t sweeps(const Grid &g, const R *A, const R *dinv, const R *r, R *z, cudaStream_t s)
   {
-    constexpr int NCOL = 1 << DIM;
-    auto          launch = [&](int colour, bool fwd) -> cudaError_t {
-      long long cnt = 1;
-      for (int d = 0; d < DIM; ++d)
-        cnt *= (g.nn[d] - ((colour >> d) & 1) + 1) / 2;
+    constexpr int       NCOL = 1 << DIM;
+    const ColourLattice cl   = colour_lattice<DIM>(g);
+    auto                launch = [&](int colour, bool fwd) -> cudaError_t {
+      const long long cnt = cl.cnt[colour];
       if (cnt == 0)
         return cudaSuccess;
       const unsigned nb = (unsigned)((cnt + 255) / 256);
       if (fwd)
-        ch_sgs_kernel<DIM, R, true><<<nb, 256, 0, s>>>(g, colour, A, dinv, r, z);
+        ch_sgs_kernel<DIM, R, true><<<nb, 256, 0, s>>>(g, colour, cl, A, dinv, r, z);
       else
-        ch_sgs_kernel<DIM, R, false><<<nb, 256, 0, s>>>(g, colour, A, dinv, r, z);
+        ch_sgs_kernel<DIM, R, false><<<nb, 256, 0, s>>>(g, colour, cl, A, dinv, r, z);
       count_launches(1);
       return cudaGetLastError();
     };

@@ -781,11 +781,24 @@ namespace sint
   // arithmetic of the same expression does.  Full operator only (no grain
   // cut-off, no advection: those keep jvp_kernel); shared memory and
   // registers as the FP64 product.
-  template <int DIM, int G, bool TENS>
-  __global__ void __launch_bounds__(Tile<DIM>::THREADS, jvp_blocks_per_sm<DIM, G, double>())
-    jvp_pair_kernel(const Grid g, const Phys ph, const float *__restrict__ lin, const float *__restrict__ src,
-                    float *__restrict__ dst, float *__restrict__ partial)
+  // CUT (G = 0 only): the grain cut-off's class of tiles without a relevant
+  // grain, ct.tiles[ct.range[0] .. ct.range[1]), on c and mu; their owned
+  // nodes get zero grain rows, as jvp_kernel's class-0 instance writes them.
+  // Resident blocks per SM: as the FP64 product (pairs take the FP64 product's
+  // registers), but three for the class without grains, whose pairs need
+  // ~70 registers (four blocks would cap them at 64 and spill).
+  template <int DIM, int G>
+  constexpr int jvp_pair_blocks_per_sm()
   {
+    return G == 0 ? 3 : jvp_blocks_per_sm<DIM, G, double>();
+  }
+
+  template <int DIM, int G, bool TENS, bool CUT = false>
+  __global__ void __launch_bounds__(Tile<DIM>::THREADS, jvp_pair_blocks_per_sm<DIM, G>())
+    jvp_pair_kernel(const Grid g, const Phys ph, const float *__restrict__ lin, const float *__restrict__ src,
+                    float *__restrict__ dst, float *__restrict__ partial, const CutTiles ct)
+  {
+    static_assert(!CUT || G == 0, "the cut-off pair kernel serves the class without grains");
     using T  = Tile<DIM>;
     using SM = ThreePhaseSmem<DIM, G, TENS, true, false, false>;
     constexpr int C = G + 2;
@@ -799,7 +812,11 @@ namespace sint
     const CellConsts<DIM, F2> k(g);
     const NodePlan<DIM>       np(g);
     const int                 cell   = threadIdx.x % T::CELLS;
-    const long long           npairs = (g.n_tiles + 1) / 2;
+    // the tiles served: all of them, or the class-0 list of the cut-off
+    const long long           i0     = CUT ? (long long)ct.range[0] : 0;
+    const long long           nt     = CUT ? (long long)ct.range[1] - i0 : g.n_tiles;
+    const long long           npairs = (nt + 1) / 2;
+    auto tile_id = [&](long long i) -> long long { return CUT ? (long long)ct.tiles[i0 + i] : i; };
     long long                 idx    = blockIdx.x;
     // node boxes of both inputs of the tiles of pair j into buffer bb (a
     // missing second tile leaves its lane stale: computed, never stored)
@@ -807,10 +824,10 @@ namespace sint
 #pragma unroll
       for (int lane = 0; lane < 2; ++lane)
         {
-          const long long tile = 2 * j + lane;
-          if (tile >= g.n_tiles)
+          if (2 * j + lane >= nt)
             break;
-          const TileCoord tcx = tile_coord_of<DIM>(g, tile);
+          const long long tile = tile_id(2 * j + lane);
+          const TileCoord tcx  = tile_coord_of<DIM>(g, tile);
           float          *fb  = reinterpret_cast<float *>(bb) + lane;
           if (tile_interior<DIM>(g, tcx))
             {
@@ -837,10 +854,10 @@ namespace sint
         cp_async_commit();
         cp_async_wait<1>(); // this pair's group has landed (only the prefetch may be pending)
         __syncthreads();
-        const long long tile_a = 2 * idx, tile_b = tile_a + 1;
-        const bool      has_b  = tile_b < g.n_tiles;
+        const bool      has_b  = 2 * idx + 1 < nt;
+        const long long tile_a = tile_id(2 * idx), tile_b = has_b ? tile_id(2 * idx + 1) : tile_a;
         const TileCoord tca    = tile_coord_of<DIM>(g, tile_a);
-        const TileCoord tcb    = tile_coord_of<DIM>(g, has_b ? tile_b : tile_a);
+        const TileCoord tcb    = tile_coord_of<DIM>(g, tile_b);
         const F2       *cb     = s_buf + (it & 1) * SM::BOXES;
         phase_evaluate<DIM, G, TENS, true, false, F2, false>(cb, cb + C * T::BOXS, F, k);
         __syncthreads();
@@ -856,10 +873,13 @@ namespace sint
               break;
             const TileCoord &tc = lane ? tcb : tca;
             const float     *kf = reinterpret_cast<const float *>(K) + lane;
+            // CUT: c and mu are components 0 and 1 of the c_all-component
+            // layout; no grain is relevant on the tile (union mask 0)
             if (tile_interior<DIM>(g, tc))
-              sum_and_store_interior<DIM, float, 2>(kf, C, g, tc.linear, np, tile_node0(g, tc), dst, partial);
+              sum_and_store_interior<DIM, float, 2>(kf, C, g, tc.linear, np, tile_node0(g, tc), dst, partial, 0, CUT,
+                                                    ct.c_all, 0u);
             else
-              sum_and_store<DIM, float, 2>(kf, C, g, tc, BoxNode<DIM>(g, tc), dst, partial);
+              sum_and_store<DIM, float, 2>(kf, C, g, tc, BoxNode<DIM>(g, tc), dst, partial, 0, CUT, ct.c_all, 0u);
           }
       }
     cp_async_wait<0>();

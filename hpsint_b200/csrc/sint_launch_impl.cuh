@@ -65,20 +65,21 @@ namespace sint
     return cudaGetLastError();
   }
 
-  template <int DIM, int G, bool TENS>
+  template <int DIM, int G, bool TENS, bool CUT = false>
   cudaError_t launch_jvp_pair_g(const Grid &g, const Phys &p, const float *lin, const float *src, float *dst,
-                                float *partial, cudaStream_t s)
+                                float *partial, cudaStream_t s, const CutTiles &ct = CutTiles())
   {
     const size_t smem = ThreePhaseSmem<DIM, G, TENS, true, false, false>::TOTAL * sizeof(F2);
-    auto         k    = jvp_pair_kernel<DIM, G, TENS>;
+    auto         k    = jvp_pair_kernel<DIM, G, TENS, CUT>;
     static DeviceCache cache;
     int                grid_cap = 0;
     if (const cudaError_t e =
-          persistent_grid(cache, k, smem, jvp_blocks_per_sm<DIM, G, double>(), Tile<DIM>::THREADS, grid_cap))
+          persistent_grid(cache, k, smem, jvp_pair_blocks_per_sm<DIM, G>(), Tile<DIM>::THREADS, grid_cap))
       return e;
-    const long long pairs  = (g.n_tiles + 1) / 2;
+    // the class size of the cut-off lives on the device: a full persistent grid
+    const long long pairs  = CUT ? (long long)grid_cap : (g.n_tiles + 1) / 2;
     const long long blocks = pairs < grid_cap ? pairs : grid_cap;
-    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial);
+    k<<<dim3((unsigned)blocks), Tile<DIM>::THREADS, smem, s>>>(g, p, lin, src, dst, partial, ct);
     count_launches(1);
     return cudaGetLastError();
   }
@@ -160,6 +161,11 @@ namespace sint
   cudaError_t launch_jvp_class(int K, const Grid &g, const Phys &p, const R *lin, const R *src, R *dst, R *partial,
                                const CutTiles &ct, const AdvData &adv, cudaStream_t s)
   {
+    // FP32: the class without grains (c and mu only, the bulk of a packing's
+    // vapour) runs on tile pairs
+    if constexpr (std::is_same_v<R, float> && !ADV)
+      if (K == 0)
+        return launch_jvp_pair_g<DIM, 0, TENS, true>(g, p, lin, src, dst, partial, s, ct);
 #define SINT_CALL(GG) launch_jvp_g<DIM, GG, TENS, R, true, ADV>(g, p, lin, src, dst, partial, ct, adv, s)
     SINT_CLASS_SWITCH(K, SINT_CALL)
 #undef SINT_CALL
