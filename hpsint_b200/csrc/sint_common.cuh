@@ -822,15 +822,26 @@ namespace sint
             slot[k] = tile * ncomp * (long long)T::BOX + bx + T::BX * (by + T::BY * bz);
             tm[k]   = (has[k] && tile_mask) ? unsigned(tile_mask[tile]) : ~0u;
           }
+    // grains written by any of the sharing tiles: the others sum to zero
+    // without a look at the candidates (most shared nodes of a packing lie
+    // between tiles without a relevant grain)
+    unsigned any = 0u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (has[k])
+        any |= tm[k];
     // 2D: one component per thread (blockIdx.y); 3D: one thread loops over all components
     const int c_end = DIM == 2 ? comp + 1 : ncomp;
     for (int cp = DIM == 2 ? comp : 0; cp < c_end; ++cp)
       {
         R sum = R(0);
+        if (cp < 2 || ((any >> (cp - 2)) & 1u) != 0u)
+          {
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-          if (has[k] && (cp < 2 || ((tm[k] >> (cp - 2)) & 1u) != 0u))
-            sum += partial[slot[k] + cp * (long long)T::BOX];
+            for (int k = 0; k < 8; ++k)
+              if (has[k] && (cp < 2 || ((tm[k] >> (cp - 2)) & 1u) != 0u))
+                sum += partial[slot[k] + cp * (long long)T::BOX];
+          }
         if (epi)
           sum = (sum - (epi_sub ? R(epi_sub[cp * g.ld + idx]) : R(0))) * R(epi_scale);
         dst[cp * g.ld + idx] = sum;
