@@ -319,6 +319,7 @@ namespace sint
     p.Msurf   = params->Msurf;
     p.Mgb     = params->Mgb;
     p.L       = params->L;
+    set_row_stiffness(g, p.kappa_c, p.kappa_p, p.L);
     p.w0      = 0.0;
     p.w_alg   = 1.0;
     p.order   = 0;
@@ -485,6 +486,7 @@ int sint_set_mobility(sint_ctx *c, double Mvol, double Mvap, double Msurf, doubl
   c->phys.Msurf = c->params.Msurf = Msurf;
   c->phys.Mgb   = c->params.Mgb = Mgb;
   c->phys.L     = c->params.L = L;
+  sint::set_row_stiffness(c->grid, c->phys.kappa_c, c->phys.kappa_p, L);
   return SINT_OK;
 }
 

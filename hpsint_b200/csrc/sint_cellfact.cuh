@@ -23,6 +23,7 @@ namespace sint
   struct CellConsts
   {
     R x0, x1;   // Gauss point coordinates
+    R nx1;      // -x1
     R ih[DIM];  // 1 / h
     R dih[DIM]; // (+1) / h: derivative of phi_1 (phi_0 has the negative)
     R JxW;
@@ -32,6 +33,7 @@ namespace sint
       const double s3 = 0.5 / 1.7320508075688772935274463415058723669428;
       x0              = R(0.5 - s3);
       x1              = R(0.5 + s3);
+      nx1             = R(-(0.5 + s3));
       double jxw      = 1.0;
 #pragma unroll
       for (int d = 0; d < DIM; ++d)
@@ -267,12 +269,25 @@ namespace sint
   }
 
   // 1D contraction of a point pair (a at x_0, b at x_1) with phi_l:
-  // l = 0 -> x_1 a + x_0 b, l = 1 -> x_0 a + x_1 b
+  // l = 0 -> x_1 a + x_0 b, l = 1 -> x_0 a + x_1 b.  With x_0 + x_1 = 1 both
+  // share the difference: r_0 = b + x_1 (a - b), r_1 = a - x_1 (a - b) (three
+  // operations instead of four).
   template <typename R>
-  __device__ __forceinline__ void contract(const R a, const R b, const R x0, const R x1, R &r0, R &r1)
+  __device__ __forceinline__ void contract(const R a, const R b, const R x1, const R nx1, R &r0, R &r1)
   {
-    r0 = x1 * a + x0 * b;
-    r1 = x0 * a + x1 * b;
+    const R d = a - b;
+    r0        = b + x1 * d;
+    r1        = a + nx1 * d;
+  }
+  // one output of the contraction: l = HZ
+  template <int HZ, typename R>
+  __device__ __forceinline__ R contract1(const R a, const R b, const R x1, const R nx1)
+  {
+    const R d = a - b;
+    if constexpr (HZ == 0)
+      return b + x1 * d;
+    else
+      return a + nx1 * d;
   }
 
   // Phase 3, full row: r_l = JxW sum_q (v_q phi_l(x_q) + g_q . grad phi_l(x_q)).
@@ -292,11 +307,11 @@ namespace sint
               const int q0 = qx + 2 * qy, q1 = q0 + 4;
               const R   sz = (g[2][q0] + g[2][q1]) * k.dih[2];
               R         a0, a1;
-              contract(v[q0], v[q1], k.x0, k.x1, a0, a1);
+              contract(v[q0], v[q1], k.x1, k.nx1, a0, a1);
               A[0][qy][qx] = a0 - sz;
               A[1][qy][qx] = a1 + sz;
-              contract(g[0][q0], g[0][q1], k.x0, k.x1, BX[0][qy][qx], BX[1][qy][qx]);
-              contract(g[1][q0], g[1][q1], k.x0, k.x1, BY[0][qy][qx], BY[1][qy][qx]);
+              contract(g[0][q0], g[0][q1], k.x1, k.nx1, BX[0][qy][qx], BX[1][qy][qx]);
+              contract(g[1][q0], g[1][q1], k.x1, k.nx1, BY[0][qy][qx], BY[1][qy][qx]);
             }
         // contract y
         R A2[2][2][2], BX2[2][2][2];
@@ -307,10 +322,10 @@ namespace sint
             {
               const R sy = (BY[lz][0][qx] + BY[lz][1][qx]) * k.dih[1];
               R       a0, a1;
-              contract(A[lz][0][qx], A[lz][1][qx], k.x0, k.x1, a0, a1);
+              contract(A[lz][0][qx], A[lz][1][qx], k.x1, k.nx1, a0, a1);
               A2[lz][0][qx] = a0 - sy;
               A2[lz][1][qx] = a1 + sy;
-              contract(BX[lz][0][qx], BX[lz][1][qx], k.x0, k.x1, BX2[lz][0][qx], BX2[lz][1][qx]);
+              contract(BX[lz][0][qx], BX[lz][1][qx], k.x1, k.nx1, BX2[lz][0][qx], BX2[lz][1][qx]);
             }
         // contract x
 #pragma unroll
@@ -320,7 +335,7 @@ namespace sint
             {
               const R sx = (BX2[lz][ly][0] + BX2[lz][ly][1]) * k.dih[0];
               R       a0, a1;
-              contract(A2[lz][ly][0], A2[lz][ly][1], k.x0, k.x1, a0, a1);
+              contract(A2[lz][ly][0], A2[lz][ly][1], k.x1, k.nx1, a0, a1);
               r[2 * ly + 4 * lz]     = (a0 - sx) * k.JxW;
               r[1 + 2 * ly + 4 * lz] = (a1 + sx) * k.JxW;
             }
@@ -334,20 +349,62 @@ namespace sint
             const int q0 = qx, q1 = qx + 2;
             const R   sy = (g[1][q0] + g[1][q1]) * k.dih[1];
             R         a0, a1;
-            contract(v[q0], v[q1], k.x0, k.x1, a0, a1);
+            contract(v[q0], v[q1], k.x1, k.nx1, a0, a1);
             A[0][qx] = a0 - sy;
             A[1][qx] = a1 + sy;
-            contract(g[0][q0], g[0][q1], k.x0, k.x1, BX[0][qx], BX[1][qx]);
+            contract(g[0][q0], g[0][q1], k.x1, k.nx1, BX[0][qx], BX[1][qx]);
           }
 #pragma unroll
         for (int ly = 0; ly < 2; ++ly)
           {
             const R sx = (BX[ly][0] + BX[ly][1]) * k.dih[0];
             R       a0, a1;
-            contract(A[ly][0], A[ly][1], k.x0, k.x1, a0, a1);
+            contract(A[ly][0], A[ly][1], k.x1, k.nx1, a0, a1);
             r[2 * ly]     = (a0 - sx) * k.JxW;
             r[1 + 2 * ly] = (a1 + sx) * k.JxW;
           }
+      }
+  }
+
+  // Phase 3, full row in 3D, the half of the local nodes with z bit HZ: writes
+  // r[l] for l = lx + 2 ly + 4 HZ only.  Two threads of a cell share a row
+  // this way, each contracting z to its own node layer first.
+  template <int HZ, typename R>
+  __device__ __forceinline__ void cell_integrate_vg_half(const R (&v)[8], const R (&g)[3][8],
+                                                         const CellConsts<3, R> &k, R (&r)[8])
+  {
+    R A[2][2], BX[2][2], BY[2][2];
+#pragma unroll
+    for (int qy = 0; qy < 2; ++qy)
+#pragma unroll
+      for (int qx = 0; qx < 2; ++qx)
+        {
+          const int q0 = qx + 2 * qy, q1 = q0 + 4;
+          const R   sz = (g[2][q0] + g[2][q1]) * k.dih[2];
+          const R   a  = contract1<HZ>(v[q0], v[q1], k.x1, k.nx1);
+          A[qy][qx]    = HZ ? a + sz : a - sz;
+          BX[qy][qx]   = contract1<HZ>(g[0][q0], g[0][q1], k.x1, k.nx1);
+          BY[qy][qx]   = contract1<HZ>(g[1][q0], g[1][q1], k.x1, k.nx1);
+        }
+    R A2[2][2], BX2[2][2];
+#pragma unroll
+    for (int qx = 0; qx < 2; ++qx)
+      {
+        const R sy = (BY[0][qx] + BY[1][qx]) * k.dih[1];
+        R       a0, a1;
+        contract(A[0][qx], A[1][qx], k.x1, k.nx1, a0, a1);
+        A2[0][qx] = a0 - sy;
+        A2[1][qx] = a1 + sy;
+        contract(BX[0][qx], BX[1][qx], k.x1, k.nx1, BX2[0][qx], BX2[1][qx]);
+      }
+#pragma unroll
+    for (int ly = 0; ly < 2; ++ly)
+      {
+        const R sx = (BX2[ly][0] + BX2[ly][1]) * k.dih[0];
+        R       a0, a1;
+        contract(A2[ly][0], A2[ly][1], k.x1, k.nx1, a0, a1);
+        r[2 * ly + 4 * HZ]     = (a0 - sx) * k.JxW;
+        r[1 + 2 * ly + 4 * HZ] = (a1 + sx) * k.JxW;
       }
   }
 
@@ -363,20 +420,20 @@ namespace sint
         for (int qy = 0; qy < 2; ++qy)
 #pragma unroll
           for (int qx = 0; qx < 2; ++qx)
-            contract(v[qx + 2 * qy], v[qx + 2 * qy + 4], k.x0, k.x1, A[0][qy][qx], A[1][qy][qx]);
+            contract(v[qx + 2 * qy], v[qx + 2 * qy + 4], k.x1, k.nx1, A[0][qy][qx], A[1][qy][qx]);
         R A2[2][2][2];
 #pragma unroll
         for (int lz = 0; lz < 2; ++lz)
 #pragma unroll
           for (int qx = 0; qx < 2; ++qx)
-            contract(A[lz][0][qx], A[lz][1][qx], k.x0, k.x1, A2[lz][0][qx], A2[lz][1][qx]);
+            contract(A[lz][0][qx], A[lz][1][qx], k.x1, k.nx1, A2[lz][0][qx], A2[lz][1][qx]);
 #pragma unroll
         for (int lz = 0; lz < 2; ++lz)
 #pragma unroll
           for (int ly = 0; ly < 2; ++ly)
             {
               R a0, a1;
-              contract(A2[lz][ly][0], A2[lz][ly][1], k.x0, k.x1, a0, a1);
+              contract(A2[lz][ly][0], A2[lz][ly][1], k.x1, k.nx1, a0, a1);
               r[2 * ly + 4 * lz]     = a0 * k.JxW;
               r[1 + 2 * ly + 4 * lz] = a1 * k.JxW;
             }
@@ -386,34 +443,32 @@ namespace sint
         R A[2][2];
 #pragma unroll
         for (int qx = 0; qx < 2; ++qx)
-          contract(v[qx], v[qx + 2], k.x0, k.x1, A[0][qx], A[1][qx]);
+          contract(v[qx], v[qx + 2], k.x1, k.nx1, A[0][qx], A[1][qx]);
 #pragma unroll
         for (int ly = 0; ly < 2; ++ly)
           {
             R a0, a1;
-            contract(A[ly][0], A[ly][1], k.x0, k.x1, a0, a1);
+            contract(A[ly][0], A[ly][1], k.x1, k.nx1, a0, a1);
             r[2 * ly]     = a0 * k.JxW;
             r[1 + 2 * ly] = a1 * k.JxW;
           }
       }
   }
 
-  // r_l += coef (K u)_l with the exact element Laplacian K_lm = kx[l xor m].
-  template <int DIM, typename R>
-  __device__ __forceinline__ void cell_stiffness_add(const nd<R> coef, const R (&u)[1 << DIM], const Grid &g,
-                                                     R (&r)[1 << DIM])
+  // r_l += coef (K u)_l with the exact element Laplacian K_lm = kx[l xor m],
+  // coef kx taken from the grid's row coefficients (ROW 0: -kappa_c for the
+  // mu row, 1: L kappa_p for the eta rows), so every term is one fused
+  // multiply-add with a launch constant.
+  template <int DIM, int ROW, typename R>
+  __device__ __forceinline__ void cell_stiffness_add(const R (&u)[1 << DIM], const Grid &g, R (&r)[1 << DIM])
   {
-    R cu[1 << DIM];
-#pragma unroll
-    for (int x = 0; x < (1 << DIM); ++x)
-      cu[x] = coef * kx<R>(g, x);
 #pragma unroll
     for (int l = 0; l < (1 << DIM); ++l)
       {
         R acc = r[l];
 #pragma unroll
         for (int x = 0; x < (1 << DIM); ++x)
-          acc += cu[x] * u[l ^ x];
+          acc += kst<R>(g, ROW, x) * u[l ^ x];
         r[l] = acc;
       }
   }

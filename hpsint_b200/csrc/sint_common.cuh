@@ -86,6 +86,12 @@ namespace sint
     // (kx[x] = int grad phi_l . grad phi_(l xor x)), in both precisions.
     double kxd[8];
     float  kxf[8];
+    // The same stencil times the coefficient of each constant-coefficient
+    // gradient row: kst[0] = -kappa_c kx (mu row, acting on c), kst[1] =
+    // L kappa_p kx (eta rows); refreshed by set_row_stiffness whenever
+    // kappa_c, kappa_p or L change.
+    double kstd[2][8];
+    float  kstf[2][8];
     // division by nt[0] and nt[1] as multiply-shift (exact for n < 2^31):
     // n / nt[d] = (n * mdiv[d]) >> (32 + sdiv[d])
     unsigned long long mdiv[2];
@@ -114,6 +120,36 @@ namespace sint
   __device__ __forceinline__ unsigned fast_div(unsigned n, unsigned long long m, int s)
   {
     return (unsigned)(((unsigned long long)n * m) >> (32 + s));
+  }
+
+  // Row coefficients of the element Laplacian (Grid::kstd / kstf).
+  inline void set_row_stiffness(Grid &g, double kappa_c, double kappa_p, double L)
+  {
+    for (int x = 0; x < 8; ++x)
+      {
+        g.kstd[0][x] = -kappa_c * g.kxd[x];
+        g.kstd[1][x] = L * kappa_p * g.kxd[x];
+        g.kstf[0][x] = float(g.kstd[0][x]);
+        g.kstf[1][x] = float(g.kstd[1][x]);
+      }
+  }
+
+  template <typename R>
+  __device__ __forceinline__ R kst(const Grid &g, int row, int x);
+  template <>
+  __device__ __forceinline__ double kst<double>(const Grid &g, int row, int x)
+  {
+    return g.kstd[row][x];
+  }
+  template <>
+  __device__ __forceinline__ float kst<float>(const Grid &g, int row, int x)
+  {
+    return g.kstf[row][x];
+  }
+  template <>
+  __device__ __forceinline__ F2 kst<F2>(const Grid &g, int row, int x)
+  {
+    return F2(g.kstf[row][x]);
   }
 
   template <typename R>

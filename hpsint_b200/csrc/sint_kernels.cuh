@@ -442,6 +442,29 @@ namespace sint
       P[((1 + d) * Slots<DIM>::NQ + q) * T::CELLS + cell] = flux[d];
   }
 
+  // Phase 3, 3D: the c row's contributions to the local nodes with z bit HZ
+  // (K rows l = lx + 2 ly + 4 HZ) from the point values and fluxes in P.
+  template <int HZ, typename R>
+  __device__ __forceinline__ void integrate_c_row_half(const R *P, const CellConsts<3, R> &k, int cell, bool in,
+                                                       bool in_b, R *K)
+  {
+    using T          = Tile<3>;
+    constexpr int NQ = 8;
+    R v[NQ], gg[3][NQ], r[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      {
+        v[q] = P[(0 * NQ + q) * T::CELLS + cell];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          gg[d][q] = P[((1 + d) * NQ + q) * T::CELLS + cell];
+      }
+    cell_integrate_vg_half<HZ>(v, gg, k, r);
+#pragma unroll
+    for (int l = 4 * HZ; l < 4 * HZ + 4; ++l)
+      K[l * T::CP + cell] = (in && in_b) ? r[l] : lane_keep(r[l], in, in_b);
+  }
+
   // Phase 3: integrate every row of every cell into K[(row * NQ + l) * CP + cell];
   // contributions of cells outside the mesh (partial tiles) are zero.  `stiff`
   // holds the nodal values the constant-coefficient gradient terms act on
@@ -466,12 +489,27 @@ namespace sint
     constexpr int NQ   = 1 << DIM;
     constexpr int C    = G + 2;
     constexpr int NGRP = T::THREADS / T::CELLS;
+    // In 3D with fewer rows than thread groups, the c row (the only one with
+    // a point-dependent flux, the longest) is shared by two groups, one per
+    // layer of local nodes (z bit 0 / 1): C + 1 tasks instead of C rows.
+    constexpr bool SPLIT0 = DIM == 3 && C + 1 <= NGRP;
+    constexpr int  NTASK  = C + (SPLIT0 ? 1 : 0);
     const int     cell = threadIdx.x % T::CELLS;
     const int     b0   = cell_box_base<DIM>(cell);
     const bool    in   = cell_in_mesh<DIM>(cell, tc, g);
     const bool    in_b = tc_b ? cell_in_mesh<DIM>(cell, *tc_b, g) : in;
-    for (int row = threadIdx.x / T::CELLS; row < C; row += NGRP)
+    for (int task = threadIdx.x / T::CELLS; task < NTASK; task += NGRP)
       {
+        const int row = SPLIT0 ? (task < 2 ? 0 : task - 1) : task;
+        if constexpr (SPLIT0)
+          if (task < 2)
+            {
+              if (task == 0)
+                integrate_c_row_half<0>(P, k, cell, in, in_b, K);
+              else
+                integrate_c_row_half<1>(P, k, cell, in, in_b, K);
+              continue;
+            }
         bool keep = in;
         if constexpr (CUT)
           if (row >= 2)
@@ -528,7 +566,7 @@ namespace sint
                   }
               }
             cell_integrate_vg<DIM>(v, gg, k, r);
-            cell_stiffness_add<DIM>(p.L * p.kp, u, g, r);
+            cell_stiffness_add<DIM, 1>(u, g, r);
           }
         else
           {
@@ -540,7 +578,10 @@ namespace sint
             cell_integrate_v<DIM>(v, k, r);
             R u[NQ];
             cell_nodes<DIM>(stiff + (row == 1 ? 0 : row) * T::BOXS, b0, u);
-            cell_stiffness_add<DIM>(row == 1 ? -p.kc : p.L * p.kp, u, g, r);
+            if (row == 1)
+              cell_stiffness_add<DIM, 0>(u, g, r);
+            else
+              cell_stiffness_add<DIM, 1>(u, g, r);
           }
         // a branch, not a select per value: in tiles inside the mesh every
         // cell keeps its row
