@@ -145,6 +145,8 @@ SIGNATURES = {
     "sint_nn_apply_guess3d_f64": (_c_int, [_c_void, _c_void, _c_int64] + [_c_int] * 7 +
                                   [ctypes.c_float, _c_void, _c_void, _c_void, _c_void, _c_void]),
     "sint_nn_zero_pad_slices_f32": (_c_int, [_c_void, _c_int, _c_int, _c_int64, _c_void]),
+    "sint_nn_conv3d_f32": (_c_int, [_c_int] * 4 + [_c_void, _c_int, _c_void, _c_void, _c_int, _c_void, _c_void, _c_void,
+                                                    _c_int, _c_int, ctypes.c_float, _c_void, _c_int, _c_int, _c_void]),
     "sint_last_error": (ctypes.c_char_p, []),
     "sint_kernel_launch_count": (_c_int64, []),
 }

@@ -179,20 +179,26 @@ class LearnedPredictor3D:
     """Whole-mesh inference in slabs of `slab` depth slices (each with a halo
     of `layers` slices, the network's receptive field in depth):
     features -> net -> guess u_n + r (u_n - u_{n-1}) + output / oscale.  FP32
-    network on the tensor cores, FP64 guess.  safeguard: keep the smaller
+    network (one-pass FP32 3x3x3 convolutions with the layer's sums and
+    activations fused; fused=False: slice-shifted 3x3 convolutions, on the
+    tensor cores with tensor_cores), FP64 guess.  safeguard: keep the smaller
     residual of this guess and hpsint's linear one (device only)."""
 
     def __init__(self, op: SinteringOperatorGeneric, net: EquivariantNet, norm: Normaliser, slab=64,
-                 tensor_cores=True, safeguard=False):
+                 tensor_cores=True, safeguard=False, fused=True):
         if op.mesh.dim != 3 or net.cfg.dim != 3:
             raise ValueError("LearnedPredictor3D needs a 3D mesh and a NetConfig(dim=3) network")
         self.op, self.net, self.tensor_cores, self.safeguard = op, net, tensor_cores, safeguard
+        self.fused = fused
         self.base, self.inc = norm.device(), IncrementScales()
         self.scale = torch.ones(6, dtype=torch.float32, device="cuda")
         self.oscale = torch.ones(3, dtype=torch.float32, device="cuda")
         self.nx, self.ny, self.nz = (op.mesh.n_cells[d] + 1 for d in range(3))
         self.halo = net.cfg.layers
-        self.slab = min(slab, self.nz)
+        # slabs of at most `slab` slices, split evenly (no short last slab
+        # computed over a full window)
+        n_slabs = -(-self.nz // max(1, slab))
+        self.slab = -(-self.nz // n_slabs)
         G = op.params.n_grains
         Dw = self.slab + 2 * self.halo
         f = lambda n, c: torch.zeros((n, Dw + 2, c, self.ny, self.nx), dtype=torch.float32, device="cuda")
@@ -219,7 +225,7 @@ class LearnedPredictor3D:
             L.check(lib.sint_nn_features3d_f64(_p(history[0]), _p(history[1]), op.ld, self.nx, self.ny, self.nz, G,
                                                0, 0, z0 - h, Dw, self.ny, self.nx, r, _p(self.scale), _p(self.xg),
                                                _p(self.xs), 0, _s()), "sint_nn_features3d_f64")
-            yg, ys, _ = self.net.forward(self.xg, self.xs, 1, G, tensor_cores=self.tensor_cores)
+            yg, ys, _ = self.net.forward(self.xg, self.xs, 1, G, tensor_cores=self.tensor_cores, fused3d=self.fused)
             L.check(lib.sint_nn_apply_guess3d_f64(_p(history[0]), _p(history[1]), op.ld, self.nx, self.ny, G, z0, D,
                                                   h, Dw, r, _p(self.oscale), _p(yg), _p(ys), _p(self.guess), _s()),
                     "sint_nn_apply_guess3d_f64")

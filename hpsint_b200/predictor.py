@@ -128,6 +128,20 @@ def conv3x3x3(x, w3, bias, out, accumulate=False, tc_status=None):
     zero_pads(out)
 
 
+def conv3d_fused(x1, w1, out, x2=None, w2=None, bias=None, addend=None, addend_group=1, slope=None,
+                 accumulate=False):
+    """Inference form of the 3x3x3 convolution on depth-padded windows, one
+    pass: out = act(conv(x1, w1) (+ conv(x2, w2)) + bias (+ addend broadcast
+    over groups of addend_group samples) (+ out)), act = leaky ReLU with
+    `slope` (None: identity); the output's padding slices are written as zero."""
+    S, D2, c1, H, W = x1.shape
+    c2 = x2.shape[2] if x2 is not None else 0
+    L.check(L.lib().sint_nn_conv3d_f32(S, D2 - 2, H, W, _p(x1), c1, _p(w1), _p(x2), c2, _p(w2), _p(bias), _p(addend),
+                                       addend_group, 1 if slope is not None else 0,
+                                       float(slope) if slope is not None else 0.0, _p(out), out.shape[2],
+                                       int(accumulate), _s()), "sint_nn_conv3d_f32")
+
+
 def conv3x3x3_input_grad(dout, w3, din, accumulate=False):
     """din (+)= d(conv(x, w3))/dx applied to dout: din[z] = sum_dz W_dz^T * dout[z - dz]."""
     ds, dis = _slices(dout), _slices(din)
@@ -236,13 +250,18 @@ class EquivariantNet:
                 self.w[l][k].copy_(torch.randn(self.shapes[l][k], generator=gen) * std)
 
     # -- forward -------------------------------------------------------------
-    def forward(self, xg, xs, B, G, keep=False, tensor_cores=False):
+    def forward(self, xg, xs, B, G, keep=False, tensor_cores=False, fused3d=True):
         """xg [B*G][grain_in][H][W], xs [B][shared_in][H][W] -> (yg [B*G][1], ys [B][2]).
         tensor_cores: run the convolutions on the tensor cores (TF32 products,
-        FP32 accumulation; inference) instead of the FP32 kernel."""
+        FP32 accumulation; inference) instead of the FP32 kernel.
+        3D inference (keep False) with fused3d: one-pass FP32 3x3x3
+        convolutions with the layer's sums, bias and activation fused
+        (conv3d_fused; tensor_cores does not apply)."""
         H, W = xs.shape[-2], xs.shape[-1]
         if self.cfg.dim == 2 and tensor_cores and not keep and max(max(d) for d in self.dims) <= 32:
             return self._forward_fused(xg, xs, B, G, H, W)
+        if self.cfg.dim == 3 and fused3d and not keep and max(max(d) for d in self.dims) <= 32:
+            return self._forward_fused3d(xg, xs, B, G, H, W)
         cache = []
         hg, hs = xg, xs
         # 2D: [n][C][H][W]; 3D: [n][D + 2][C][H][W]
@@ -301,6 +320,26 @@ class EquivariantNet:
             Zs = torch.empty((B, so, H, W), dtype=torch.float32, device="cuda")
             conv3x3_tc(hs, w["D"], w["d"], Zs, st)
             conv3x3_tc_ex(P, w["E"], None, Zs, st, accumulate=True, slope=slope)
+            hg, hs = Zg, Zs
+        return hg, hs, []
+
+    def _forward_fused3d(self, xg, xs, B, G, H, W):
+        """3D inference, three one-pass convolutions per layer:
+        P = sum_i h_i;  Q = B*P + C*s;  h_i <- act(A*h_i + a + Q);
+        s <- act(D*s + d + E*P)."""
+        hg, hs = xg, xs
+        n, D2 = len(self.dims), xs.shape[1]
+        for l, (cg, cs, go, so) in enumerate(self.dims):
+            w = self.w[l]
+            slope = self.cfg.slope if l < n - 1 else None
+            P = torch.empty((B, D2, cg, H, W), dtype=torch.float32, device="cuda")
+            grain_sum(hg, B, G, P)
+            Q = torch.empty((B, D2, go, H, W), dtype=torch.float32, device="cuda")
+            conv3d_fused(P, w["B"], Q, x2=hs, w2=w["C"])
+            Zg = torch.empty((B * G, D2, go, H, W), dtype=torch.float32, device="cuda")
+            conv3d_fused(hg, w["A"], Zg, bias=w["a"], addend=Q, addend_group=G, slope=slope)
+            Zs = torch.empty((B, D2, so, H, W), dtype=torch.float32, device="cuda")
+            conv3d_fused(hs, w["D"], Zs, x2=P, w2=w["E"], bias=w["d"], slope=slope)
             hg, hs = Zg, Zs
         return hg, hs, []
 

@@ -592,6 +592,19 @@ int sint_nn_apply_guess3d_f64(const double *u_n, const double *u_nm1, int64_t bl
 /* Zero depth slices 0 and D2 - 1 of each of S samples (slice_elems floats per
  * slice): the padding of a 3D window after a convolution wrote into it. */
 int sint_nn_zero_pad_slices_f32(float *x, int S, int D2, int64_t slice_elems, sint_stream_t stream);
+/* One-pass 3x3x3 convolution for inference on depth-padded windows
+ * [S][D + 2][C][H][W] (slices 0 and D + 1 zero):
+ *   out[s][z][co] = act(bias[co] + sum_{dz,dy,dx,ci} w1[dz][co][ci][dy][dx]
+ *                   x1[s][z + dz - 1][ci][y + dy - 1][x + dx - 1] (+ the same for
+ *                   x2, w2 with c2 channels) (+ addend[s / addend_group][z][co])
+ *                   (+ out if accumulate)),
+ * zero outside the window, for slices z = 1 .. D; slices 0 and D + 1 of out
+ * are set to zero.  act = leaky ReLU with `slope` if leaky != 0.  FP32
+ * products and sums; 1 <= cout <= 32; x2/w2 may be NULL (c2 = 0), so may
+ * bias and addend (addend_group divides S). */
+int sint_nn_conv3d_f32(int S, int D, int H, int W, const float *x1, int c1, const float *w1, const float *x2, int c2,
+                       const float *w2, const float *bias, const float *addend, int addend_group, int leaky,
+                       float slope, float *out, int cout, int accumulate, sint_stream_t stream);
 
 /* Per-state scales of the network inputs and outputs: with m_c, m_mu, m_eta
  * the largest |ratio (u_n - u_{n-1})| of c, mu and any eta_i over the mesh and

@@ -223,10 +223,49 @@ def test_network3d_forward_backward_match_reference():
     for l, layer in enumerate(net.g):
         for k, g in layer.items():
             assert rel(g.cpu().numpy(), rgrads[l][k]) < 1e-4, (l, k)
-    # inference on the tensor cores
-    tyg, tys, _ = net.forward(dev_padded(xg), dev_padded(xs), B, G, tensor_cores=True)
+    # inference on the tensor cores (slice-shifted 3x3 convolutions)
+    tyg, tys, _ = net.forward(dev_padded(xg), dev_padded(xs), B, G, tensor_cores=True, fused3d=False)
     net.check_tensor_cores()
     assert rel(inner(tyg), ryg) < 5e-3 and rel(inner(tys), rys) < 5e-3
+    # one-pass FP32 inference (conv3d_fused): FP32 tolerance, zero padding written
+    fyg, fys, _ = net.forward(dev_padded(xg), dev_padded(xs), B, G)
+    assert rel(inner(fyg), ryg) < 2e-5 and rel(inner(fys), rys) < 2e-5
+
+
+@pytest.mark.parametrize("S,D,c1,c2,cout,H,W,group", [(3, 5, 2, 0, 8, 11, 37, 3), (1, 11, 8, 8, 8, 9, 33, 1),
+                                                        (2, 3, 4, 8, 2, 17, 13, 2), (2, 4, 8, 0, 1, 8, 32, 1),
+                                                        (1, 9, 3, 5, 5, 10, 40, 1), (1, 6, 16, 16, 16, 12, 20, 1),
+                                                        (1, 5, 32, 0, 32, 7, 35, 1)])
+def test_conv3d_fused_matches_reference(S, D, c1, c2, cout, H, W, group):
+    """The one-pass 3x3x3 convolution (two inputs, bias, addend broadcast over
+    sample groups, leaky ReLU, accumulation) against the NumPy reference, over
+    every output-channel instance (1, 2, 4, 8, 16, 32 and a padded 5), depths
+    that are and are not multiples of the kernel's slice blocking, widths not
+    a multiple of 32 and heights not a multiple of 8."""
+    from hpsint_b200 import predictor as P
+    rng = np.random.default_rng(S * 100 + D * 10 + cout)
+    x1, w1 = rng.normal(size=(S, D, c1, H, W)), rng.normal(size=(3, cout, c1, 3, 3))
+    b = rng.normal(size=cout)
+    ref = R.conv3x3x3(x1, w1, b)
+    x2 = w2 = None
+    if c2:
+        x2, w2 = rng.normal(size=(S, D, c2, H, W)), rng.normal(size=(3, cout, c2, 3, 3))
+        ref = ref + R.conv3x3x3(x2, w2)
+    add = rng.normal(size=(S // group, D, cout, H, W))
+    ref = ref + np.repeat(add, group, axis=0)
+    prev = rng.normal(size=(S, D, cout, H, W))
+    out = dev_padded(prev)
+    out[:, 0] = 7.0  # padding slices are overwritten with zero
+    out[:, -1] = -3.0
+    P.conv3d_fused(dev_padded(x1), dev(w1), out, x2=dev_padded(x2) if c2 else None, w2=dev(w2) if c2 else None,
+                   bias=dev(b), addend=dev_padded(add), addend_group=group, slope=0.1, accumulate=True)
+    expect = ref + prev
+    expect = np.where(expect < 0, 0.1 * expect, expect)
+    assert rel(inner(out), expect) < 2e-5
+    # no bias, addend, activation or accumulation
+    out2 = torch.full((S, D + 2, cout, H, W), 5.0, device="cuda")
+    P.conv3d_fused(dev_padded(x1), dev(w1), out2)
+    assert rel(inner(out2), R.conv3x3x3(x1, w1)) < 2e-5
 
 
 def test_window3d_features_targets_and_guess():
