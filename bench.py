@@ -294,6 +294,8 @@ def two_particle_solve(args):
                        "s_per_accepted_attempt": sum(x.accepted_wall_s for x in recs) / len(recs),
                        "newton_iterations": sum(x.newton_iterations for x in recs),
                        "linear_iterations": sum(x.linear_iterations for x in recs),
+                       "preconditioner_setups": sum(x.preconditioner_setups for x in recs),
+                       "predict_s_per_step": sum(x.predict_s for x in recs) / len(recs),
                        "failed_tries": sum(x.failed_tries for x in recs), "final_dt": recs[-1].dt}
     same_t = abs(ref["t"] - mp["t"]) <= 1e-12 * max(1.0, ref["t"])
     line["fp32_inner_vs_fp64"] = {

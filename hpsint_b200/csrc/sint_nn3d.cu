@@ -15,7 +15,8 @@
 // in shared memory with cp.async, double-buffered: the next channel's copies
 // are in flight while this one is computed.  A thread reads, per (dy, dx)
 // tap column, ZB + 2 input values and per dz the COUT weights (one broadcast
-// read serves the warp), and issues 3 ZB COUT fused multiply-adds.
+// read serves the warp), and issues 3 ZB COUT fused multiply-adds, as packed
+// FP32 pairs of output channels (FFMA2) when COUT is a multiple of 4.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -122,12 +123,20 @@ namespace sint
           }
       };
 
-      float acc[ZB][COUT];
+      // accumulators: scalar, or channel pairs when COUT is a multiple of 4
+      constexpr bool PAIRS = COUT % 4 == 0;
+      float          acc[PAIRS ? 1 : ZB][PAIRS ? 1 : COUT];
+      float2         acc2[PAIRS ? ZB : 1][PAIRS ? COUT / 2 : 1];
 #pragma unroll
       for (int z = 0; z < ZB; ++z)
 #pragma unroll
         for (int co = 0; co < COUT; ++co)
-          acc[z][co] = 0.f;
+          {
+            if constexpr (PAIRS)
+              (co & 1 ? acc2[z][co / 2].y : acc2[z][co / 2].x) = 0.f;
+            else
+              acc[z][co] = 0.f;
+          }
 
       stage(0, 0);
       cp_async_commit_group();
@@ -148,31 +157,48 @@ namespace sint
 #pragma unroll
                 for (int z = 0; z < BZ; ++z)
                   col[z] = s_in[b][z][ty + dy][tx + dx];
-#pragma unroll
-                for (int dz = 0; dz < 3; ++dz)
+                if constexpr (COUT % 4 == 0)
                   {
-                    float        wv[COUT];
-                    const float *wr = s_w[b][(dz * 3 + dy) * 3 + dx];
-                    if constexpr (COUT % 4 == 0)
+                    // packed FP32 pairs: two output channels per FFMA2 (each
+                    // lane rounds as fmaf does), the input value in both lanes
+                    float2 cc[BZ];
+#pragma unroll
+                    for (int z = 0; z < BZ; ++z)
+                      cc[z] = make_float2(col[z], col[z]);
+#pragma unroll
+                    for (int dz = 0; dz < 3; ++dz)
                       {
+                        const float *wr = s_w[b][(dz * 3 + dy) * 3 + dx];
 #pragma unroll
                         for (int co = 0; co < COUT; co += 4)
                           {
-                            const float4 q = *reinterpret_cast<const float4 *>(wr + co);
-                            wv[co] = q.x, wv[co + 1] = q.y, wv[co + 2] = q.z, wv[co + 3] = q.w;
+                            const float4 q  = *reinterpret_cast<const float4 *>(wr + co);
+                            const float2 w0 = make_float2(q.x, q.y), w1 = make_float2(q.z, q.w);
+#pragma unroll
+                            for (int z = 0; z < ZB; ++z)
+                              {
+                                acc2[z][co / 2]     = __ffma2_rn(w0, cc[z + dz], acc2[z][co / 2]);
+                                acc2[z][co / 2 + 1] = __ffma2_rn(w1, cc[z + dz], acc2[z][co / 2 + 1]);
+                              }
                           }
                       }
-                    else
+                  }
+                else
+                  {
+#pragma unroll
+                    for (int dz = 0; dz < 3; ++dz)
                       {
+                        const float *wr = s_w[b][(dz * 3 + dy) * 3 + dx];
+                        float        wv[COUT];
 #pragma unroll
                         for (int co = 0; co < COUT; ++co)
                           wv[co] = wr[co];
+#pragma unroll
+                        for (int z = 0; z < ZB; ++z)
+#pragma unroll
+                          for (int co = 0; co < COUT; ++co)
+                            acc[z][co] = fmaf(wv[co], col[z + dz], acc[z][co]);
                       }
-#pragma unroll
-                    for (int z = 0; z < ZB; ++z)
-#pragma unroll
-                      for (int co = 0; co < COUT; ++co)
-                        acc[z][co] = fmaf(wv[co], col[z + dz], acc[z][co]);
                   }
               }
           // the next iteration's copies overwrite the buffer read here
@@ -184,28 +210,35 @@ namespace sint
       if (x >= a.W || y >= a.H)
         return;
       const long long pix = (long long)y * a.W + x;
+      // slice z0, channel 0 of this thread's output and addend columns
+      const long long zs = (long long)a.cout * hw;
+      float          *op = a.out + ((long long)s * D2 + z0) * zs + pix;
+      const float    *ap = a.addend ? a.addend + ((long long)(s / a.addend_group) * D2 + z0) * zs + pix : nullptr;
 #pragma unroll
       for (int z = 0; z < ZB; ++z)
         {
-          const int zz = z0 + z;
-          if (zz > a.D)
+          if (z0 + z > a.D)
             break;
 #pragma unroll
           for (int co = 0; co < COUT; ++co)
             {
               if (co >= a.cout)
                 break;
-              const long long o = (((long long)s * D2 + zz) * a.cout + co) * hw + pix;
-              float           v = acc[z][co];
+              const long long o = z * zs + co * hw;
+              float           v;
+              if constexpr (PAIRS)
+                v = co & 1 ? acc2[z][co / 2].y : acc2[z][co / 2].x;
+              else
+                v = acc[z][co];
               if (a.bias)
                 v += a.bias[co];
-              if (a.addend)
-                v += a.addend[(((long long)(s / a.addend_group) * D2 + zz) * a.cout + co) * hw + pix];
+              if (ap)
+                v += ap[o];
               if (a.accumulate)
-                v += a.out[o];
+                v += op[o];
               if (a.leaky && v < 0.f)
                 v *= a.slope;
-              a.out[o] = v;
+              op[o] = v;
             }
         }
       // the depth padding of the output: slice 0 by the first z tile, D + 1 by the last

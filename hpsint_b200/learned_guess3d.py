@@ -190,6 +190,7 @@ class LearnedPredictor3D:
             raise ValueError("LearnedPredictor3D needs a 3D mesh and a NetConfig(dim=3) network")
         self.op, self.net, self.tensor_cores, self.safeguard = op, net, tensor_cores, safeguard
         self.fused = fused
+        self.ws = {}  # activation buffers of the fused network, kept between calls
         self.base, self.inc = norm.device(), IncrementScales()
         self.scale = torch.ones(6, dtype=torch.float32, device="cuda")
         self.oscale = torch.ones(3, dtype=torch.float32, device="cuda")
@@ -225,7 +226,8 @@ class LearnedPredictor3D:
             L.check(lib.sint_nn_features3d_f64(_p(history[0]), _p(history[1]), op.ld, self.nx, self.ny, self.nz, G,
                                                0, 0, z0 - h, Dw, self.ny, self.nx, r, _p(self.scale), _p(self.xg),
                                                _p(self.xs), 0, _s()), "sint_nn_features3d_f64")
-            yg, ys, _ = self.net.forward(self.xg, self.xs, 1, G, tensor_cores=self.tensor_cores, fused3d=self.fused)
+            yg, ys, _ = self.net.forward(self.xg, self.xs, 1, G, tensor_cores=self.tensor_cores, fused3d=self.fused,
+                                         ws=self.ws)
             L.check(lib.sint_nn_apply_guess3d_f64(_p(history[0]), _p(history[1]), op.ld, self.nx, self.ny, G, z0, D,
                                                   h, Dw, r, _p(self.oscale), _p(yg), _p(ys), _p(self.guess), _s()),
                     "sint_nn_apply_guess3d_f64")

@@ -250,18 +250,20 @@ class EquivariantNet:
                 self.w[l][k].copy_(torch.randn(self.shapes[l][k], generator=gen) * std)
 
     # -- forward -------------------------------------------------------------
-    def forward(self, xg, xs, B, G, keep=False, tensor_cores=False, fused3d=True):
+    def forward(self, xg, xs, B, G, keep=False, tensor_cores=False, fused3d=True, ws=None):
         """xg [B*G][grain_in][H][W], xs [B][shared_in][H][W] -> (yg [B*G][1], ys [B][2]).
         tensor_cores: run the convolutions on the tensor cores (TF32 products,
         FP32 accumulation; inference) instead of the FP32 kernel.
         3D inference (keep False) with fused3d: one-pass FP32 3x3x3
         convolutions with the layer's sums, bias and activation fused
-        (conv3d_fused; tensor_cores does not apply)."""
+        (conv3d_fused; tensor_cores does not apply); ws: a dict that keeps
+        the activation buffers of that path between calls (the caller owns
+        it and must not run two calls with one ws at the same time)."""
         H, W = xs.shape[-2], xs.shape[-1]
         if self.cfg.dim == 2 and tensor_cores and not keep and max(max(d) for d in self.dims) <= 32:
             return self._forward_fused(xg, xs, B, G, H, W)
         if self.cfg.dim == 3 and fused3d and not keep and max(max(d) for d in self.dims) <= 32:
-            return self._forward_fused3d(xg, xs, B, G, H, W)
+            return self._forward_fused3d(xg, xs, B, G, H, W, ws)
         cache = []
         hg, hs = xg, xs
         # 2D: [n][C][H][W]; 3D: [n][D + 2][C][H][W]
@@ -323,22 +325,30 @@ class EquivariantNet:
             hg, hs = Zg, Zs
         return hg, hs, []
 
-    def _forward_fused3d(self, xg, xs, B, G, H, W):
+    def _forward_fused3d(self, xg, xs, B, G, H, W, ws=None):
         """3D inference, three one-pass convolutions per layer:
         P = sum_i h_i;  Q = B*P + C*s;  h_i <- act(A*h_i + a + Q);
-        s <- act(D*s + d + E*P)."""
+        s <- act(D*s + d + E*P).  Buffers per layer and role, kept in ws."""
+        def buf(key, shape):
+            t = ws.get(key) if ws is not None else None
+            if t is None or tuple(t.shape) != shape:
+                t = torch.empty(shape, dtype=torch.float32, device="cuda")
+                if ws is not None:
+                    ws[key] = t
+            return t
+
         hg, hs = xg, xs
         n, D2 = len(self.dims), xs.shape[1]
         for l, (cg, cs, go, so) in enumerate(self.dims):
             w = self.w[l]
             slope = self.cfg.slope if l < n - 1 else None
-            P = torch.empty((B, D2, cg, H, W), dtype=torch.float32, device="cuda")
+            P = buf(("P", l), (B, D2, cg, H, W))
             grain_sum(hg, B, G, P)
-            Q = torch.empty((B, D2, go, H, W), dtype=torch.float32, device="cuda")
+            Q = buf(("Q", l), (B, D2, go, H, W))
             conv3d_fused(P, w["B"], Q, x2=hs, w2=w["C"])
-            Zg = torch.empty((B * G, D2, go, H, W), dtype=torch.float32, device="cuda")
+            Zg = buf(("Zg", l), (B * G, D2, go, H, W))
             conv3d_fused(hg, w["A"], Zg, bias=w["a"], addend=Q, addend_group=G, slope=slope)
-            Zs = torch.empty((B, D2, so, H, W), dtype=torch.float32, device="cuda")
+            Zs = buf(("Zs", l), (B, D2, so, H, W))
             conv3d_fused(hs, w["D"], Zs, x2=P, w2=w["E"], bias=w["d"], slope=slope)
             hg, hs = Zg, Zs
         return hg, hs, []

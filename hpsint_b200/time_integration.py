@@ -62,6 +62,8 @@ class StepRecord:
     final_residual: float = 0.0
     accepted_wall_s: float = 0.0   # the successful attempt alone (wall_s includes failed tries)
     reference_residual: float = 0.0  # |R(u_n)| of the step when a predicted guess was measured against it
+    preconditioner_setups: int = 0   # of the successful attempt
+    predict_s: float = 0.0           # predictor call and its reference residual, successful attempt
 
 
 class TimeIntegrator:
@@ -182,12 +184,14 @@ class TimeIntegrator:
                                       "velocity is too high.", 0, 0, 0.0, 0.0))
                 self._halve_or_raise()
                 continue
+            t_pred = time.perf_counter()
             guess = self.predictor(self.history, self.dts, self.dt) if self.predictor else None
             if guess is not None and self.grain_cut_off_tolerance != 0.0:
                 # DoFs outside the cut-off's reach have no equation this step: keep their old values
                 self.op.cut_off_freeze(guess, self.history[0])
             self._reference_residual = 0.0
-            data = self._stop_rule(wh) if guess is not None else None
+            data = self._stop_rule(wh) if guess is not None else None  # its norm waits for the guess
+            t_pred = time.perf_counter() - t_pred if guess is not None else 0.0
             u = (guess if guess is not None else self.history[0]).clone()
             st = self.newton.solve(u, self.history[:len(wh)], raise_on_failure=False, data=data)
             if st.status == L.SINT_OK:
@@ -203,7 +207,8 @@ class TimeIntegrator:
         t1 = time.perf_counter()
         self.records.append(StepRecord(self.t, self.dt, st.newton_iterations, st.linear_iterations,
                                        st.residual_evaluations, tries, t1 - t0, st.initial_residual,
-                                       st.final_residual, t1 - t_try, self._reference_residual))
+                                       st.final_residual, t1 - t_try, self._reference_residual,
+                                       st.preconditioner_setups, t_pred))
         if self.grain_cut_off_tolerance != 0.0:
             self.cut_off_statistics.append(self.op.component_mask_statistics())
         if self.advection is not None:

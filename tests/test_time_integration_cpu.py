@@ -22,6 +22,7 @@ class FakeStats:
         self.newton_iterations = 2
         self.linear_iterations = 10
         self.residual_evaluations = 3
+        self.preconditioner_setups = 1
         self.initial_residual = 1.0
         self.final_residual = 1e-9
 
