@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     ap.add_argument("--workload", choices=["operator", "operator2d", "solve2d", "solve3d", "learned2d", "learned3d",
-                                           "nnconv",
+                                           "nnconv", "nn3d",
                                            "cutoff", "tracker", "advection"],
                     default="operator",
                     help="operator: J v throughput (headline); solve2d: s/step of the 2D two-particle solve; "
@@ -574,6 +574,8 @@ def mixed_precision_solve_3d(args, learned=None, train_info=None):
                        "s_per_accepted_attempt": sum(x.accepted_wall_s for x in recs) / len(recs),
                        "newton_iterations": sum(x.newton_iterations for x in recs),
                        "linear_iterations": sum(x.linear_iterations for x in recs),
+                       "preconditioner_setups": sum(x.preconditioner_setups for x in recs),
+                       "predict_s_per_step": sum(x.predict_s for x in recs) / len(recs),
                        "failed_tries": sum(x.failed_tries for x in recs),
                        "max_final_residual": max(x.final_residual for x in recs),
                        "int_c_rel_change": abs(r["c_int"] - c0) / abs(c0)}
@@ -613,6 +615,49 @@ def mixed_precision_solve_3d(args, learned=None, train_info=None):
                 "speedup_s_per_step_vs_fp64_inner": (ref["wall"] / len(ref["recs"])) / (r["wall"] / len(r["recs"]))}
     if train_info is not None:
         line["learned_training"] = train_info
+    print(json.dumps(line), flush=True)
+
+
+def nn_inference_3d(args):
+    """One whole-mesh inference of the 3D learned guess at the 3D solve size
+    (--n3 cells per direction, --max-grains order parameters, the committed
+    C5 net or --net3d): the one-pass convolutions against the slice-shifted
+    tensor-core path, on the same seeded states, wall time per call (best of
+    --steps after --warmup calls) and the largest difference of the guesses."""
+    import torch
+
+    import hpsint_b200 as hb
+    from hpsint_b200 import learned_guess as LG
+    from hpsint_b200 import learned_guess3d as LG3
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, G = args.n3, args.max_grains
+    net, norm = LG.load_predictor(args.net3d or os.path.join(ROOT, "hpsint_b200", "weights",
+                                                             "learned_guess_c5_3d_w8.npz"))
+    op = hb.SinteringOperatorGeneric(hb.Mesh(3, (n, n, n)), hb.Params(**model_params(G, not args.scalar)))
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    un, um = op.initialize_dof_vector(), op.initialize_dof_vector()
+    un[:, :op.N] = torch.rand((op.C, op.N), device="cuda", dtype=torch.float64, generator=gen)
+    um[:, :op.N] = un[:, :op.N] - 1e-3 * torch.rand((op.C, op.N), device="cuda", dtype=torch.float64, generator=gen)
+    line = {"workload": f"nn3d-inference-{n}^3-G{G}-width{net.cfg.width}-layers{net.cfg.layers}", "unit": "ms"}
+    guesses = {}
+    for name, kw in (("fused_fp32", dict(fused=True)), ("sliced_tcgen05", dict(fused=False, tensor_cores=True))):
+        p = LG3.LearnedPredictor3D(op, net, norm, **kw)
+        for _ in range(max(1, args.warmup)):
+            p([un, um], [1e-4], 1e-4)
+        times = []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p([un, um], [1e-4], 1e-4)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        net.check_tensor_cores()
+        guesses[name] = p.guess.clone()
+        line[name] = {"ms": 1e3 * min(times)}
+        del p
+        torch.cuda.empty_cache()
+    line["max_abs_diff"] = float((guesses["fused_fp32"] - guesses["sliced_tcgen05"]).abs().max())
     print(json.dumps(line), flush=True)
 
 
@@ -914,6 +959,9 @@ def main():
         return
     if args.workload == "learned3d":
         learned_guess_3d(args)
+        return
+    if args.workload == "nn3d":
+        nn_inference_3d(args)
         return
     if args.workload == "solve3d":
         mixed_precision_solve_3d(args)
