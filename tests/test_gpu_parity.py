@@ -82,6 +82,29 @@ def test_jvp_f64_matches_oracle(case):
     assert block_rel_err(op.to_host(dst), ref) <= 1e-12
 
 
+@pytest.mark.skipif(not torch.cuda.is_available() or torch.cuda.device_count() < 2,
+                    reason="needs two visible GPUs")
+def test_jvp_on_two_devices_matches_oracle():
+    """The launch set-up (shared-memory attributes, persistent grid size) is
+    kept per device: a process that uses a second GPU first and then the
+    first one gets correct products on both (3D, G = 4: more than 48 KB of
+    dynamic shared memory per block)."""
+    dim, cells, G, tens, h = 3, (5, 7, 3), 4, True, (1.0, 1.0, 1.0)
+    lin = random_state(dim, cells, G, seed=4)
+    src = random_state(dim, cells, G, seed=5, smooth=False) - 0.5
+    for dev in (1, 0, 1):
+        with torch.cuda.device(dev):
+            op, p = make_op(dim, cells, G, tens, h)
+            op.set_time_weights(25.0, [-25.0], 1.0)
+            op.fill_quadrature_point_values(op.to_device(lin))
+            dst = op.initialize_dof_vector()
+            op.vmult(dst, op.to_device(src))
+            torch.cuda.synchronize()
+            ref = O.jvp(oracle_mesh(dim, cells, h), oracle_params(p), O.make_time(25.0, 1.0, [-25.0]), lin, src)
+            assert dst.device.index == dev
+            assert block_rel_err(op.to_host(dst), ref) <= 1e-12, dev
+
+
 # The full FP32 product runs two tiles per block in packed pairs: odd tile
 # counts (a lone last tile), partial tiles at the mesh's high faces in
 # either lane, and the large-G one-block-per-SM instances.
