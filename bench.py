@@ -63,6 +63,8 @@ def parse_args():
     ap.add_argument("--max-grains", type=int, default=10, help="3D solve: order-parameter budget")
     ap.add_argument("--no-solve", action="store_true", help="skip the s/step comparison of the operator run")
     ap.add_argument("--solve-compare-steps", type=int, default=40)
+    ap.add_argument("--solve3d-steps", type=int, default=4,
+                    help="steps of the C5 s/step comparison in the default line (0: skip)")
     ap.add_argument("--train-seeds", type=int, default=10)
     ap.add_argument("--train-steps", type=int, default=200, help="FP64 steps per training trajectory")
     ap.add_argument("--train-iters", type=int, default=4000)
@@ -467,6 +469,38 @@ def solve_comparison(n_steps):
 
 
 def mixed_precision_solve_3d(args, learned=None, train_info=None):
+    print(json.dumps(solve3d_line(args, learned, train_info)), flush=True)
+
+
+def solve_comparison_3d(n_steps):
+    """The metric's s/step on the north-star configuration C5, a few steps:
+    256^3 cells, 200 lognormal spheres (median 8, sigma 0.25), G = 10
+    (203.7 M DoFs), tensorial mobility, Newton 1e-8.  The plain FP64 solve
+    (hpsint's method) fixes the time grid; FP32-inner with the grain cut-off
+    1e-7 and the matrix-based CH preconditioner replays it without a guess
+    and with the committed 3D learned guess
+    (hpsint_b200/weights/learned_guess_c5_3d_w8.npz)."""
+    a = argparse.Namespace(n3=256, spheres=200, median=8.0, sigma=0.25, max_grains=12, scalar=False,
+                           cut_off=1e-7, preconditioners=True, solve_steps=n_steps, predictor="none,learned",
+                           net3d=os.path.join(ROOT, "hpsint_b200", "weights", "learned_guess_c5_3d_w8.npz"),
+                           arms="fp64_inner,fp32_inner_cut_off_ch_gs_right", operator_rates=False)
+    full = solve3d_line(a)
+    arms = {"fp64_plain": "fp64_inner", "fp32_inner_cut_off_ch_gs": "fp32_inner_cut_off_ch_gs_right",
+            "fp32_inner_cut_off_ch_gs_learned": "fp32_inner_cut_off_ch_gs_right_learned"}
+    out = {"workload": full["workload"], "dofs": full["dofs"], "steps": n_steps, "unit": "s/step",
+           "newton_tol": 1e-8, "weights": "hpsint_b200/weights/learned_guess_c5_3d_w8.npz"}
+    plain = full["fp64_inner"]["s_per_step"]
+    for name, key in (("s_per_step", "s_per_step"), ("newton_iterations", "newton_iterations"),
+                      ("linear_iterations", "linear_iterations"), ("int_c_rel_change", "int_c_rel_change")):
+        out[name] = {k: full[v][key] for k, v in arms.items() if v in full}
+    out["speedup_vs_fp64_plain"] = {k: plain / full[v]["s_per_step"] for k, v in arms.items() if v in full}
+    out["max_abs_diff_vs_fp64_plain"] = {
+        k: max(full[v]["max_abs_diff_c_vs_fp64_inner"], full[v]["max_abs_diff_eta_vs_fp64_inner"])
+        for k, v in arms.items() if v in full and "max_abs_diff_c_vs_fp64_inner" in full[v]}
+    return out
+
+
+def solve3d_line(args, learned=None, train_info=None):
     """3D mixed-precision solve: 192^3 Q1 cells at unit spacing, 51 spheres
     with lognormal radii (median 10, sigma 0.2) in a random sequential packing
     with 2-cell overlaps, coloured to <= 10 order parameters, width-2 tanh
@@ -498,7 +532,8 @@ def mixed_precision_solve_3d(args, learned=None, train_info=None):
     u0d = op.to_device(u0)
     c0 = float(np.einsum("k,j,i,kji->", w, w, w, u0[0].reshape(n + 1, n + 1, n + 1)))
     del u0
-    operator_rates = cut_off_operator_rates(op, u0d, args.cut_off) if args.cut_off > 0 else None
+    operator_rates = (cut_off_operator_rates(op, u0d, args.cut_off)
+                      if args.cut_off > 0 and getattr(args, "operator_rates", True) else None)
     # (label, Krylov precision, cut-off tolerance, preconditioner with the cut-off too,
     #  block-0 preconditioner, right-preconditioned GMRES)
     BJ, GS = "block_jacobi", "ch_gauss_seidel"
@@ -615,7 +650,7 @@ def mixed_precision_solve_3d(args, learned=None, train_info=None):
                 "speedup_s_per_step_vs_fp64_inner": (ref["wall"] / len(ref["recs"])) / (r["wall"] / len(r["recs"]))}
     if train_info is not None:
         line["learned_training"] = train_info
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def nn_inference_3d(args):
@@ -1171,6 +1206,9 @@ def main():
         del ud, vd, dst, v32, dst32, hist, res, z32, d_src, pc
         torch.cuda.empty_cache()
         line["solve"] = solve_comparison(args.solve_compare_steps)
+        torch.cuda.empty_cache()
+        if args.solve3d_steps > 0:
+            line["solve3d"] = solve_comparison_3d(args.solve3d_steps)
     if world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(u, v, G, tensorial, args.cpu_seconds, n, gpu_product=gpu_slab)
         # per-block relative l2 error of the headline product against the oracle
