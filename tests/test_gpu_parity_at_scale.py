@@ -143,6 +143,41 @@ def test_preconditioner_at_scale(state):
     assert block_rel_err(op.to_host(z), zref) <= 1e-12
 
 
+def test_preconditioner_on_noise_free_packing():
+    """Preconditioner set-up on the noise-free 3D crop, where the tanh tails
+    leave grain pairs with eta_i eta_j far below 1e-16 over whole vapour
+    regions (the noisy crop has none): the 2x2 node blocks, the Allen-Cahn
+    diagonal and the assembled Cahn-Hilliard matrix match the oracle to the
+    1e-12 bound."""
+    import hpsint_b200 as hb
+    u, G = c2_crop(noise=0.0)
+    cells = C2_CELLS
+    om, p = oracle_mesh(3, cells), O.make_params(G, tensorial=True)
+    # such pairs exist: at a fifth of the nodes every grain product is below 1e-16
+    eta = u[2:]
+    pmax = np.zeros(eta.shape[1])
+    for i in range(G):
+        for j in range(i):
+            pmax = np.maximum(pmax, np.abs(eta[i] * eta[j]))
+    assert (pmax < 1e-16).mean() > 0.05
+    op = hb.SinteringOperatorGeneric(hb.Mesh(3, cells), hb.Params(G, tensorial=True))
+    op.set_time_weights(1e3, [-1e3], 1.0)
+    op.fill_quadrature_point_values(op.to_device(u))
+    T = O.make_time(1e3, 1.0, [-1e3])
+    N = op.N
+    pc = hb.BlockPreconditioner2(op)
+    pc.do_update()
+    assert block_rel_err(pc.ch_blocks()[:, :N].cpu().numpy(), O.ch_blocks(om, p, T, u)) <= 1e-12
+    inv_ref = O.inverse_diagonal(O.ac_diagonal(om, p, T, u))
+    assert block_rel_err(pc.inverse_diagonal()[:, :N].cpu().numpy(), inv_ref) <= 1e-12
+    gs = hb.BlockPreconditioner2(op, block_0="ch_gauss_seidel")
+    gs.do_update()
+    A_ref = O.ch_matrix(om, p, T, u)
+    nk = A_ref.shape[0]
+    A = gs.ch_matrix()[:, :, :N].cpu().numpy()
+    assert block_rel_err(A.reshape(nk * 4, -1), A_ref.reshape(nk * 4, -1)) <= 1e-12
+
+
 @pytest.mark.parametrize("which", [0, 1])
 def test_cut_off_at_scale(state, which):
     op, u, om, p = state["op"], state["u"], state["om"], state["p"]
