@@ -473,7 +473,7 @@ def mixed_precision_solve_3d(args, learned=None, train_info=None):
 
 
 def solve_comparison_3d(n_steps):
-    """The metric's s/step on the north-star configuration C5, a few steps:
+    """The metric's s/step on the 3D combined configuration, a few steps:
     256^3 cells, 200 lognormal spheres (median 8, sigma 0.25), G = 10
     (203.7 M DoFs), tensorial mobility, Newton 1e-8.  The plain FP64 solve
     (hpsint's method) fixes the time grid; FP32-inner with the grain cut-off
