@@ -97,79 +97,6 @@ namespace sint
       }
   }
 
-  // The mobility as a DIM x DIM matrix, M grad mu = apply_M(grad mu) for
-  // every grad mu (mobility.h:439-472 scalar, :756-804 tensorial): one pass
-  // over the grain pairs instead of one apply_M per unit vector.
-  template <int DIM, int G, bool TENS, typename R>
-  __device__ __forceinline__ void mobility_matrix(const PhysR<R> &p, R c, const R (&eta)[gdim(G)],
-                                                  const R (&gc)[DIM], const R (*geta)[DIM], R (&Mm)[DIM][DIM])
-  {
-    const R phi = phi_clamped(c);
-    if constexpr (!TENS)
-      {
-        R etaij = R(0);
-#pragma unroll
-        for (int i = 0; i < G; ++i)
-#pragma unroll
-          for (int j = 0; j < i; ++j)
-            etaij += eta[i] * eta[j];
-        const R M = p.Mvol * phi + p.Mvap * (R(1) - phi) + p.Msurf * R(4) * c * c * (R(1) - c) * (R(1) - c) +
-                    (R(2) * p.Mgb) * etaij;
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int b = 0; b < DIM; ++b)
-            Mm[a][b] = a == b ? M : R(0);
-      }
-    else
-      {
-        const R fvv   = p.Mvol * phi + p.Mvap * (R(1) - phi);
-        const R fsurf = p.Msurf * R(4) * (c * c) * ((R(1) - c) * (R(1) - c));
-        R       nc[DIM], n2, rs;
-        unit_vector<DIM>(gc, nc, n2, rs);
-        const R diag = fvv + fsurf * R(1.001);
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-#pragma unroll
-          for (int b = 0; b < DIM; ++b)
-            Mm[a][b] = (a == b ? diag : R(0)) - fsurf * nc[a] * nc[b];
-        if constexpr (G > 1)
-          {
-            const R m2 = R(2) * p.Mgb;
-            R       s1 = R(0), acc[DIM][DIM];
-#pragma unroll
-            for (int a = 0; a < DIM; ++a)
-#pragma unroll
-              for (int b = 0; b < DIM; ++b)
-                acc[a][b] = R(0);
-#pragma unroll 1
-            for (int i = 0; i < G; ++i)
-#pragma unroll 1
-              for (int j = 0; j < i; ++j)
-                {
-                  R dd[DIM];
-#pragma unroll
-                  for (int d = 0; d < DIM; ++d)
-                    dd[d] = geta[i][d] - geta[j][d];
-                  const R f  = unit_vector_filter_2<DIM>(dd);
-                  const R pe = eta[i] * eta[j];
-                  s1 += pe;
-                  const R t = pe * f;
-#pragma unroll
-                  for (int a = 0; a < DIM; ++a)
-#pragma unroll
-                    for (int b = 0; b < DIM; ++b)
-                      acc[a][b] -= t * dd[a] * dd[b];
-                }
-#pragma unroll
-            for (int a = 0; a < DIM; ++a)
-#pragma unroll
-              for (int b = 0; b < DIM; ++b)
-                Mm[a][b] += m2 * ((a == b ? s1 : R(0)) + acc[a][b]);
-          }
-      }
-  }
-
   // Cells of colour `colour` (bit d = parity in direction d) taken in bricks
   // of Tile<DIM> cells of the colour's coarse lattice; one thread per (cell,
   // point).  Adds each cell's element matrix of the CH block into the rows of

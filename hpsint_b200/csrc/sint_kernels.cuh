@@ -1093,19 +1093,17 @@ namespace sint
             }
         }
       R *cf = s_coef + threadIdx.x * LY::NCOEF;
-      // mobility matrix: column e = apply_M(..., unit vector e)
+      // mobility matrix (M grad mu = apply_M(grad mu)) in one pass over the
+      // grain pairs; absent grains (CUT) enter with zero values
+      {
+        R Mm[DIM][DIM];
+        mobility_matrix<DIM, G, TENS>(p, c, eta, gc, geta, Mm);
 #pragma unroll
-      for (int e = 0; e < DIM; ++e)
-        {
-          R unit[DIM], col[DIM];
+        for (int a = 0; a < DIM; ++a)
 #pragma unroll
-          for (int d = 0; d < DIM; ++d)
-            unit[d] = d == e ? R(1) : R(0);
-          apply_M<DIM, G, TENS>(p, c, eta, gc, geta, unit, col, gmask);
-#pragma unroll
-          for (int d = 0; d < DIM; ++d)
-            cf[d * DIM + e] = col[d];
-        }
+          for (int b = 0; b < DIM; ++b)
+            cf[a * DIM + b] = Mm[a][b];
+      }
       R m[DIM];
       dM_dc_times<DIM, TENS>(p, c, gc, gmu, m);
 #pragma unroll
