@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "sint_internal.h"
 #include "sint_kernels.cuh"
@@ -41,8 +42,25 @@ namespace sint
   {
     const long long nb   = (g.N + 255) / 256;
     const bool      fin  = epi && epi->epilogue;
-    combine_kernel<DIM, R><<<dim3((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u), 256, 0, s>>>(
-      g, ncomp, partial, dst, tile_mask, fin ? epi->subtract : nullptr, fin ? epi->scale : 1.0, fin ? 1 : 0);
+    const dim3      grid((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u);
+    const double   *sub  = fin ? epi->subtract : nullptr;
+    const double    sc   = fin ? epi->scale : 1.0;
+    // 3D: the instance for this component count (C = G + 2 <= 14, the
+    // preconditioner's G + 4 <= 16)
+    auto go = [&](auto nc) {
+      constexpr int NC = decltype(nc)::value;
+      combine_kernel<DIM, R, DIM == 3 ? NC : 0><<<grid, 256, 0, s>>>(g, ncomp, partial, dst, tile_mask, sub, sc,
+                                                                     fin ? 1 : 0);
+    };
+    switch (DIM == 3 ? ncomp : 0)
+      {
+#define SINT_NC(K)                                                                                                \
+  case K: go(std::integral_constant<int, K>{}); break;
+        SINT_NC(2) SINT_NC(3) SINT_NC(4) SINT_NC(5) SINT_NC(6) SINT_NC(7) SINT_NC(8) SINT_NC(9) SINT_NC(10)
+        SINT_NC(11) SINT_NC(12) SINT_NC(13) SINT_NC(14) SINT_NC(15) SINT_NC(16)
+#undef SINT_NC
+        default: go(std::integral_constant<int, 0>{}); break;
+      }
     count_launches(1);
     return cudaGetLastError();
   }

@@ -788,12 +788,16 @@ namespace sint
   // exists only when bit b of tile_mask[tile] is set; nullptr = all exist.
   // epi (the residual's epilogue hook, nullptr for none): the combined sums
   // are stored as (sum - sub) * scale.
-  template <int DIM, typename R>
+  // NC > 0 (3D): the component count at compile time, so a thread's partial
+  // loads of all components can be in flight together (same sums, same order).
+  template <int DIM, typename R, int NC = 0>
   __global__ void __launch_bounds__(256) combine_kernel(const Grid g, int ncomp, const R *__restrict__ partial,
                                                         R *__restrict__ dst, const uint16_t *__restrict__ tile_mask,
                                                         const double *__restrict__ epi_sub = nullptr,
                                                         double epi_scale = 1.0, int epi = 0)
   {
+    if constexpr (NC > 0)
+      ncomp = NC;
     using T              = Tile<DIM>;
     const long long idx  = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int       comp = blockIdx.y;
@@ -868,7 +872,8 @@ namespace sint
         any |= tm[k];
     // 2D: one component per thread (blockIdx.y); 3D: one thread loops over all components
     const int c_end = DIM == 2 ? comp + 1 : ncomp;
-    for (int cp = DIM == 2 ? comp : 0; cp < c_end; ++cp)
+#pragma unroll
+    for (int cp = DIM == 2 ? comp : 0; cp < (NC > 0 ? NC : c_end); ++cp)
       {
         R sum = R(0);
         if (cp < 2 || ((any >> (cp - 2)) & 1u) != 0u)
