@@ -42,17 +42,17 @@ namespace sint
   {
     const long long nb   = (g.N + 255) / 256;
     const bool      fin  = epi && epi->epilogue;
-    const dim3      grid((unsigned)nb, DIM == 2 ? (unsigned)ncomp : 1u);
     const double   *sub  = fin ? epi->subtract : nullptr;
     const double    sc   = fin ? epi->scale : 1.0;
-    // 3D: the instance for this component count (C = G + 2 <= 14, the
-    // preconditioner's G + 4 <= 16)
+    // the instance for this component count (C = G + 2 <= 14, the
+    // preconditioner's G + 4 <= 16): one thread per node; other counts in 2D
+    // one thread per (node, component)
     auto go = [&](auto nc) {
       constexpr int NC = decltype(nc)::value;
-      combine_kernel<DIM, R, DIM == 3 ? NC : 0><<<grid, 256, 0, s>>>(g, ncomp, partial, dst, tile_mask, sub, sc,
-                                                                     fin ? 1 : 0);
+      const dim3    grid((unsigned)nb, (DIM == 2 && NC == 0) ? (unsigned)ncomp : 1u);
+      combine_kernel<DIM, R, NC><<<grid, 256, 0, s>>>(g, ncomp, partial, dst, tile_mask, sub, sc, fin ? 1 : 0);
     };
-    switch (DIM == 3 ? ncomp : 0)
+    switch (ncomp)
       {
 #define SINT_NC(K)                                                                                                \
   case K: go(std::integral_constant<int, K>{}); break;

@@ -788,8 +788,9 @@ namespace sint
   // exists only when bit b of tile_mask[tile] is set; nullptr = all exist.
   // epi (the residual's epilogue hook, nullptr for none): the combined sums
   // are stored as (sum - sub) * scale.
-  // NC > 0 (3D): the component count at compile time, so a thread's partial
-  // loads of all components can be in flight together (same sums, same order).
+  // NC > 0: the component count at compile time, one thread per node, so a
+  // thread's partial loads of all components can be in flight together (same
+  // sums, same order).
   template <int DIM, typename R, int NC = 0>
   __global__ void __launch_bounds__(256) combine_kernel(const Grid g, int ncomp, const R *__restrict__ partial,
                                                         R *__restrict__ dst, const uint16_t *__restrict__ tile_mask,
@@ -870,10 +871,12 @@ namespace sint
     for (int k = 0; k < 8; ++k)
       if (has[k])
         any |= tm[k];
-    // 2D: one component per thread (blockIdx.y); 3D: one thread loops over all components
-    const int c_end = DIM == 2 ? comp + 1 : ncomp;
+    // NC > 0: one thread loops over all components (known at compile time);
+    // otherwise in 2D one component per thread (blockIdx.y), in 3D the loop
+    constexpr bool PER_COMP = DIM == 2 && NC == 0;
+    const int      c_end    = PER_COMP ? comp + 1 : ncomp;
 #pragma unroll
-    for (int cp = DIM == 2 ? comp : 0; cp < (NC > 0 ? NC : c_end); ++cp)
+    for (int cp = PER_COMP ? comp : 0; cp < (NC > 0 ? NC : c_end); ++cp)
       {
         R sum = R(0);
         if (cp < 2 || ((any >> (cp - 2)) & 1u) != 0u)
