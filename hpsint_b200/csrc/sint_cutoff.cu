@@ -171,33 +171,46 @@ namespace sint
     node_mask[n] = (uint16_t)u;
   }
 
-  // One warp per 32 chunks of LIVE_CHUNK elements of a block vector (C blocks
-  // of stride ld): the chunk is live when one of its elements is c or mu, or
-  // a grain relevant at its node.
-  __global__ void __launch_bounds__(256)
+  // One block of 32 warps per 32-bit word of the live bitmap, one warp per
+  // chunk of LIVE_CHUNK elements of a block vector (C blocks of stride ld):
+  // the chunk is live when one of its elements is c or mu, or a grain
+  // relevant at its node.
+  __global__ void __launch_bounds__(1024)
     live_chunk_kernel(const Grid g, int C, const uint16_t *__restrict__ node_mask, uint32_t *__restrict__ live,
                       long long n_words)
   {
-    const long long word = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int       lane = threadIdx.x & 31;
-    if (word >= n_words)
-      return;
+    __shared__ uint32_t s_bits;
+    const long long     word = blockIdx.x;
+    const int           k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0)
+      s_bits = 0u;
+    __syncthreads();
     const long long n_elem = (long long)C * g.ld;
-    uint32_t        bits   = 0;
-    for (int k = 0; k < 32; ++k)
+    const long long e0     = (word * 32 + k) * LIVE_CHUNK;
+    if (word < n_words && e0 < n_elem) // the same for the whole warp
       {
-        const long long e0 = (word * 32 + k) * LIVE_CHUNK;
-        bool            any = false;
-        for (long long e = e0 + lane; e < e0 + LIVE_CHUNK && e < n_elem; e += 32)
-          {
-            const long long b = e / g.ld, node = e - b * g.ld;
-            any = any || b < 2 || (node < g.N && ((node_mask[node] >> (b - 2)) & 1u) != 0u);
-          }
-        if (__any_sync(0xffffffffu, any))
-          bits |= 1u << k;
+        const long long e1 = (e0 + LIVE_CHUNK < n_elem ? e0 + LIVE_CHUNK : n_elem) - 1;
+        // one division per chunk for its first block (component); a chunk
+        // that starts in the c or mu block is live
+        const long long b0  = e0 / g.ld;
+        bool            any = b0 < 2;
+        if (!any)
+          for (long long e = e0 + lane; e <= e1; e += 32)
+            {
+              long long b = b0, node = e - b0 * g.ld;
+              while (node >= g.ld) // more than one block per chunk only when ld < LIVE_CHUNK
+                {
+                  node -= g.ld;
+                  ++b;
+                }
+              any = any || (node < g.N && ((node_mask[node] >> (b - 2)) & 1u) != 0u);
+            }
+        if (__any_sync(0xffffffffu, any) && lane == 0)
+          atomicOr(&s_bits, 1u << k);
       }
-    if (lane == 0)
-      live[word] = bits;
+    __syncthreads();
+    if (threadIdx.x == 0 && word < n_words)
+      live[word] = s_bits;
   }
 
   // u <- u_old on the grain DoFs no relevant cell reaches (node_mask bit clear).
@@ -297,9 +310,9 @@ int sint_set_component_mask(sint_ctx *c, const double *u, double tol, sint_strea
       class_scan_kernel<<<1, 32, 0, stream>>>(c->G, c->cut_count, c->cut_range);
       class_scatter_kernel<<<dim3((unsigned)nbt), 256, 0, stream>>>(c->grid.n_tiles, c->tile_union, c->cut_count,
                                                                     c->cut_tiles, c->cut_grains, c->cut_union);
-      const long long nbn = (c->grid.N + 255) / 256, nw = live_words(c), nbw = (nw * 32 + 255) / 256;
+      const long long nbn = (c->grid.N + 255) / 256, nw = live_words(c);
       node_mask_kernel<<<dim3((unsigned)nbn), 256, 0, stream>>>(c->grid, c->mask, c->node_mask);
-      live_chunk_kernel<<<dim3((unsigned)nbw), 256, 0, stream>>>(c->grid, c->C, c->node_mask, c->live, nw);
+      live_chunk_kernel<<<dim3((unsigned)nw), 1024, 0, stream>>>(c->grid, c->C, c->node_mask, c->live, nw);
       count_launches(6);
       e = cudaGetLastError();
     }
