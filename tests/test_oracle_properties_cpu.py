@@ -66,3 +66,21 @@ def test_relabelling_is_not_trivially_satisfied(tensorial):
     perm = np.array([1, 0, 2, 3])
     r = O.residual(mesh, prm, tm, u, [u_old], 2)
     assert block_rel_err(_permute(r, perm), r) > 1e-3
+
+
+@pytest.mark.parametrize("dim,cells,G,tensorial", CASES[::2])
+def test_residual_history_enters_linearly(dim, cells, G, tensorial):
+    """The history h enters the residual only through the time-derivative
+    mass term w_1 (phi_i, h) of the c and eta rows (BDF1 here): R(u, [h]) is
+    affine in h and its mu row does not depend on h."""
+    mesh, prm, tm, u, u_old = _case(dim, cells, G, tensorial)
+    rng = np.random.default_rng(17)
+    h1, h2 = u_old, u_old + 0.05 * rng.standard_normal(u.shape)
+    a, b = 0.4, 0.6
+    R = lambda h: O.residual(mesh, prm, tm, u, [h], 2)
+    r0 = R(np.zeros_like(u))
+    d1, d2 = R(h1) - r0, R(h2) - r0
+    d12 = R(a * h1 + b * h2) - r0
+    assert block_rel_err(d12[[0] + list(range(2, G + 2))], (a * d1 + b * d2)[[0] + list(range(2, G + 2))]) < 1e-10
+    assert np.max(np.abs(d1[1])) <= 1e-14 * max(1.0, np.max(np.abs(r0[1])))
+    assert np.max(np.abs(d1[0])) > 1e-3  # the history does act on the c row
